@@ -1,0 +1,338 @@
+"""ctypes binding of libanacapa_b200.so (include/anacapa_b200.h).
+
+The library is the only compute path: importing a renderer on a machine where
+the shared object is missing raises instead of falling back to anything else.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+from . import scenes as S
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libanacapa_b200.so")
+
+ANA_OK = 0
+ANA_ERR_INVALID_ARG = 1
+ANA_ERR_CUDA = 2
+ANA_ERR_OOM = 3
+ANA_ERR_TIMEOUT = 4
+ANA_ERR_UNSUPPORTED = 5
+ANA_ERR_STATE = 6
+ANA_ERR_DEVICE_CHECK = 7
+ANA_RENDER_CLEAR_FILM = 1
+
+F3 = C.c_float * 3
+
+
+class AnaMaterial(C.Structure):
+    _fields_ = [("type", C.c_uint32), ("albedo", F3), ("emission", F3), ("base_color", F3),
+                ("base", C.c_float), ("metalness", C.c_float), ("roughness", C.c_float),
+                ("specular", C.c_float), ("specular_color", F3), ("specular_ior", C.c_float),
+                ("coat", C.c_float), ("coat_roughness", C.c_float), ("transmission", C.c_float),
+                ("emission_weight", C.c_float), ("emission_color", F3), ("alpha_mask", C.c_uint32),
+                ("eta", C.c_float), ("sigma_a", F3), ("beta_m", C.c_float), ("beta_n", C.c_float),
+                ("alpha_deg", C.c_float), ("hair_mode", C.c_uint32)]
+
+
+class AnaLight(C.Structure):
+    _fields_ = [("type", C.c_uint32), ("center", F3), ("u", F3), ("v", F3), ("Le", F3)]
+
+
+class AnaCamera(C.Structure):
+    _fields_ = [("from_", F3), ("at", F3), ("up", F3), ("vfov_deg", C.c_float),
+                ("aperture_radius", C.c_float), ("focal_distance", C.c_float),
+                ("shutter_open", C.c_float), ("shutter_close", C.c_float)]
+
+
+_P = C.c_void_p
+
+
+class AnaSceneDesc(C.Structure):
+    _fields_ = [("num_meshes", C.c_uint32), ("mesh_vert_offset", _P), ("mesh_tri_offset", _P),
+                ("mesh_has_normals", _P), ("positions", _P), ("normals", _P), ("indices", _P),
+                ("num_strands", C.c_uint32), ("strand_cp_offset", _P), ("control_points", _P),
+                ("strand_width_offset", _P), ("widths", _P), ("strand_slot", _P),
+                ("strand_color", _P),
+                ("num_materials", C.c_uint32), ("materials", _P), ("num_slots", C.c_uint32),
+                ("slot_material", _P), ("num_lights", C.c_uint32), ("lights", _P),
+                ("env_rgb", _P), ("env_width", C.c_uint32), ("env_height", C.c_uint32),
+                ("env_intensity", C.c_float), ("env_radiance", F3), ("camera", AnaCamera),
+                ("max_leaf_tris", C.c_uint32), ("max_leaf_segments", C.c_uint32)]
+
+
+class AnaRenderDesc(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("sample_start", C.c_uint32),
+                ("sample_count", C.c_uint32), ("max_depth", C.c_uint32), ("min_depth", C.c_uint32),
+                ("seed", C.c_uint64), ("flags", C.c_uint32)]
+
+
+class AnaFilmPixel(C.Structure):
+    _fields_ = [("r", C.c_float), ("g", C.c_float), ("b", C.c_float), ("w", C.c_float),
+                ("sum_lum_sq", C.c_float)]
+
+
+class AnaHit(C.Structure):
+    _fields_ = [("hit", C.c_int32), ("mesh_id", C.c_int32), ("prim_id", C.c_int32),
+                ("strand_id", C.c_int32), ("t", C.c_float), ("u", C.c_float), ("v", C.c_float),
+                ("pad", C.c_float)]
+
+
+class AnaStats(C.Structure):
+    _fields_ = [("paths", C.c_uint64), ("extend_rays", C.c_uint64), ("shadow_rays", C.c_uint64),
+                ("mis_rays", C.c_uint64), ("render_ms", C.c_float), ("extend_ms", C.c_float),
+                ("shade_ms", C.c_float), ("shadow_ms", C.c_float), ("mis_ms", C.c_float),
+                ("film_ms", C.c_float), ("bounces", C.c_uint32), ("chunks", C.c_uint32)]
+
+
+class AnaDeviceOpts(C.Structure):
+    _fields_ = [("device", C.c_int), ("chunk_paths", C.c_uint32), ("block_size", C.c_uint32),
+                ("timing", C.c_uint32)]
+
+
+HIT_DTYPE = np.dtype([("hit", "<i4"), ("mesh_id", "<i4"), ("prim_id", "<i4"),
+                      ("strand_id", "<i4"), ("t", "<f4"), ("u", "<f4"), ("v", "<f4"),
+                      ("pad", "<f4")])
+
+# Every symbol include/anacapa_b200.h declares.
+EXPORTS = ["ana_create", "ana_destroy", "ana_upload_scene", "ana_prepare_scene",
+           "ana_upload_prepared", "ana_prepared_bytes", "ana_prepared_free", "ana_render",
+           "ana_film_clear", "ana_film_read", "ana_film_device_ptr", "ana_trace_batch",
+           "ana_get_stats", "ana_last_error", "ana_version"]
+
+_lib = None
+
+
+class AnaError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"anacapa_b200 error {code}: {msg}")
+        self.code = code
+
+
+def lib():
+    """Load the in-tree shared library (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: run `python -m anacapa_b200.build`")
+    L = C.CDLL(LIB_PATH)
+    L.ana_create.argtypes = [C.POINTER(_P), C.POINTER(AnaDeviceOpts)]
+    L.ana_destroy.argtypes = [_P]
+    L.ana_destroy.restype = None
+    L.ana_upload_scene.argtypes = [_P, C.POINTER(AnaSceneDesc)]
+    L.ana_prepare_scene.argtypes = [C.POINTER(AnaSceneDesc), C.POINTER(_P)]
+    L.ana_upload_prepared.argtypes = [_P, _P]
+    L.ana_prepared_bytes.argtypes = [_P]
+    L.ana_prepared_bytes.restype = C.c_uint64
+    L.ana_prepared_free.argtypes = [_P]
+    L.ana_prepared_free.restype = None
+    L.ana_render.argtypes = [_P, C.POINTER(AnaRenderDesc)]
+    L.ana_film_clear.argtypes = [_P, C.c_uint32, C.c_uint32]
+    L.ana_film_read.argtypes = [_P, _P, C.c_size_t]
+    L.ana_film_device_ptr.argtypes = [_P, C.POINTER(_P)]
+    L.ana_trace_batch.argtypes = [_P, _P, C.c_size_t, _P, C.c_int, C.c_int]
+    L.ana_get_stats.argtypes = [_P, C.POINTER(AnaStats)]
+    L.ana_last_error.argtypes = [_P, C.c_char_p, C.c_size_t]
+    L.ana_version.restype = C.c_int
+    _lib = L
+    return L
+
+
+def last_error(ctx=None) -> str:
+    buf = C.create_string_buffer(1024)
+    lib().ana_last_error(ctx, buf, len(buf))
+    return buf.value.decode(errors="replace")
+
+
+def check(rc, ctx=None):
+    if rc != ANA_OK:
+        raise AnaError(rc, last_error(ctx))
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data
+
+
+def material_struct(m: S.Material) -> AnaMaterial:
+    s = AnaMaterial()
+    s.type = m.type
+    s.albedo[:] = m.albedo
+    s.emission[:] = m.emission
+    s.base_color[:] = m.base_color
+    s.base = m.base
+    s.metalness = m.metalness
+    s.roughness = m.roughness
+    s.specular = m.specular
+    s.specular_color[:] = m.specular_color
+    s.specular_ior = m.specular_ior
+    s.coat = m.coat
+    s.coat_roughness = m.coat_roughness
+    s.transmission = m.transmission
+    s.emission_weight = m.emission_w
+    s.emission_color[:] = m.emission_color
+    s.alpha_mask = 0
+    s.eta = m.eta
+    s.sigma_a[:] = m.sigma_a
+    s.beta_m = m.beta_m
+    s.beta_n = m.beta_n
+    s.alpha_deg = m.alpha_deg
+    s.hair_mode = m.hair_mode
+    return s
+
+
+class SceneDesc:
+    """An AnaSceneDesc plus the numpy arrays it points into (kept alive)."""
+
+    def __init__(self, sc: S.Scene, max_leaf_tris=0, max_leaf_segments=0):
+        keep = []
+
+        def arr(x, dt):
+            a = np.ascontiguousarray(np.asarray(x, dtype=dt))
+            keep.append(a)
+            return a
+
+        d = AnaSceneDesc()
+        d.num_meshes = sc.num_meshes
+        d.mesh_vert_offset = _ptr(arr(sc.mesh_vert_offset, np.uint32))
+        d.mesh_tri_offset = _ptr(arr(sc.mesh_tri_offset, np.uint32))
+        d.mesh_has_normals = _ptr(arr(sc.mesh_has_normals, np.uint8))
+        d.positions = _ptr(arr(sc.positions, np.float32))
+        d.normals = _ptr(arr(sc.normals, np.float32)) if sc.normals is not None else None
+        d.indices = _ptr(arr(sc.indices, np.uint32))
+        d.num_strands = sc.num_strands
+        d.strand_cp_offset = _ptr(arr(sc.strand_cp_offset, np.uint32))
+        d.control_points = _ptr(arr(sc.control_points, np.float32))
+        d.strand_width_offset = _ptr(arr(sc.strand_width_offset, np.uint32))
+        d.widths = _ptr(arr(sc.widths, np.float32))
+        d.strand_slot = _ptr(arr(sc.strand_slot, np.uint32))
+        d.strand_color = _ptr(arr(sc.strand_color, np.float32))
+        mats = (AnaMaterial * max(1, len(sc.materials)))(*[material_struct(m) for m in sc.materials])
+        keep.append(mats)
+        d.num_materials = len(sc.materials)
+        d.materials = C.addressof(mats)
+        d.num_slots = len(sc.slots)
+        d.slot_material = _ptr(arr(sc.slots, np.int32))
+        lights = []
+        for a in sc.area_lights:
+            l = AnaLight()
+            l.type = S.LIGHT_AREA
+            l.center[:] = a.center
+            l.u[:] = a.u
+            l.v[:] = a.v
+            l.Le[:] = a.Le
+            lights.append(l)
+        if sc.dome_rgb is not None:
+            l = AnaLight()
+            l.type = S.LIGHT_DOME
+            lights.append(l)
+        la = (AnaLight * max(1, len(lights)))(*lights)
+        keep.append(la)
+        d.num_lights = len(lights)
+        d.lights = C.addressof(la)
+        if sc.dome_rgb is not None:
+            env = arr(sc.dome_rgb, np.float32)
+            d.env_rgb = _ptr(env)
+            d.env_width = env.shape[1]
+            d.env_height = env.shape[0]
+            d.env_intensity = sc.dome_intensity
+        d.env_radiance[:] = sc.env_radiance
+        cam = AnaCamera()
+        cam.from_[:] = sc.cam_from
+        cam.at[:] = sc.cam_at
+        cam.up[:] = sc.cam_up
+        cam.vfov_deg = sc.vfov
+        d.camera = cam
+        d.max_leaf_tris = max_leaf_tris
+        d.max_leaf_segments = max_leaf_segments
+        self.desc = d
+        self._keep = keep
+
+
+class Prepared:
+    """Host-prepared scene (BVHs built, device layout flattened into one blob)."""
+
+    def __init__(self, sc: S.Scene, **kw):
+        self.desc = SceneDesc(sc, **kw)
+        h = _P()
+        check(lib().ana_prepare_scene(C.byref(self.desc.desc), C.byref(h)))
+        self.h = h
+
+    @property
+    def nbytes(self) -> int:
+        return int(lib().ana_prepared_bytes(self.h))
+
+    def __del__(self):
+        try:
+            if self.h:
+                lib().ana_prepared_free(self.h)
+        except Exception:
+            pass
+
+
+class Renderer:
+    """One ana_ctx (one CUDA stream) on one device."""
+
+    def __init__(self, device=0, chunk_paths=0, block_size=0):
+        o = AnaDeviceOpts(device, chunk_paths, block_size, 0)
+        h = _P()
+        check(lib().ana_create(C.byref(h), C.byref(o)))
+        self.h = h
+        self.scene: Optional[S.Scene] = None
+
+    def close(self):
+        if self.h:
+            lib().ana_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        check(rc, self.h)
+
+    def upload(self, sc_or_prep, **kw):
+        if isinstance(sc_or_prep, Prepared):
+            self._check(lib().ana_upload_prepared(self.h, sc_or_prep.h))
+        else:
+            d = SceneDesc(sc_or_prep, **kw)
+            self._check(lib().ana_upload_scene(self.h, C.byref(d.desc)))
+            self.scene = sc_or_prep
+
+    def render(self, width, height, spp, max_depth, sample_start=0, min_depth=2, seed=0, clear=True):
+        r = AnaRenderDesc(width, height, sample_start, spp, max_depth, min_depth, seed,
+                          ANA_RENDER_CLEAR_FILM if clear else 0)
+        self._check(lib().ana_render(self.h, C.byref(r)))
+
+    def render_scene(self, sc: S.Scene, spp=None, clear=True, sample_start=0, seed=0):
+        self.render(sc.width, sc.height, sc.spp if spp is None else spp, sc.max_depth,
+                    sample_start=sample_start, seed=seed, clear=clear)
+
+    def film(self, width, height) -> np.ndarray:
+        """(H, W, 5) float32: pre-weighted r, g, b, weight, sum of lum^2."""
+        out = np.zeros((height, width, 5), np.float32)
+        self._check(lib().ana_film_read(self.h, out.ctypes.data, width * height))
+        return out
+
+    def image(self, width, height) -> np.ndarray:
+        f = self.film(width, height)
+        return f[..., :3] / np.maximum(f[..., 3:4], 1e-30)
+
+    def stats(self) -> AnaStats:
+        s = AnaStats()
+        self._check(lib().ana_get_stats(self.h, C.byref(s)))
+        return s
+
+    def trace(self, rays: np.ndarray, occlusion=False) -> np.ndarray:
+        rays = np.ascontiguousarray(np.asarray(rays, np.float32).reshape(-1, 8))
+        out = np.zeros(len(rays), HIT_DTYPE)
+        self._check(lib().ana_trace_batch(self.h, rays.ctypes.data, len(rays), out.ctypes.data,
+                                          1 if occlusion else 0, 0))
+        return out

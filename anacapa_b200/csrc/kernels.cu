@@ -1,0 +1,485 @@
+// Wavefront path tracing on sm_100a: one kernel per stage of
+// PathIntegrator::Li (src/integrator/PathIntegrator.cpp:71-265).
+//
+//   generate  camera rays for a chunk of paths      (renderTile, 33-38)
+//   extend    closest hit of every live path         (Li, 81)
+//   shade     emission, NEE light + BSDF samples, continuation, RR (Li 83-160,
+//             estimateDirect 166-265); emits shadow, MIS and extend queues
+//   shadow    any-hit of the NEE shadow rays         (shadowTransmittance)
+//   mis       closest hit of the BSDF-sampled MIS rays; adds emitter Le / env
+//   film      per-pixel reduction into the film      (renderTile 43-57)
+//
+// Queues are SoA float4 arrays. Each stage kernel appends to the next queue
+// with a block-level allocation: warp ballots give each lane its rank, one
+// shared-memory scan over the block's warps and a single atomicAdd per block
+// reserve a contiguous range, so every warp writes a contiguous, coalesced run.
+#include "kernels.h"
+#include "sampler.cuh"
+#include "shade.cuh"
+#include "traverse.cuh"
+
+namespace ana {
+
+constexpr uint32_t kMiss = 0xFFFFFFFFu;
+constexpr int kMaxBlock = 1024;
+
+// Reserve one slot per thread with want == true; returns the slot (valid only
+// for those threads). Must be reached by every thread of the block.
+__device__ __forceinline__ uint32_t block_push(bool want, uint32_t* counter) {
+    __shared__ uint32_t s_cnt[kMaxBlock / 32];
+    __shared__ uint32_t s_base;
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint32_t nwarps = (blockDim.x + 31u) >> 5;
+    uint32_t mask = __ballot_sync(0xFFFFFFFFu, want);
+    uint32_t rank = __popc(mask & ((1u << lane) - 1u));
+    if (lane == 0) s_cnt[warp] = __popc(mask);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t run = 0;
+        for (uint32_t w = 0; w < nwarps; ++w) {
+            uint32_t c = s_cnt[w];
+            s_cnt[w] = run;
+            run += c;
+        }
+        s_base = run ? atomicAdd(counter, run) : 0u;
+    }
+    __syncthreads();
+    uint32_t slot = s_base + s_cnt[warp] + rank;
+    __syncthreads();  // s_cnt / s_base are reused by the next call
+    return slot;
+}
+
+__device__ __forceinline__ float4 pack(float3 v, float w) { return make_float4(v.x, v.y, v.z, w); }
+__device__ __forceinline__ float4 pack_u(float3 v, uint32_t w) { return make_float4(v.x, v.y, v.z, __uint_as_float(w)); }
+
+__device__ __forceinline__ void path_coords(const Params& p, uint32_t pid, uint32_t& px, uint32_t& py,
+                                            uint32_t& sidx) {
+    uint32_t pixel = pid / p.spp;
+    sidx = p.sample_start + (pid - pixel * p.spp);
+    py = pixel / p.W;
+    px = pixel - py * p.W;
+}
+
+__device__ __forceinline__ void add_L(const Params& p, uint32_t pid, float3 v) {
+    size_t li = size_t(pid - p.chunk_first_pixel * p.spp) * 3;
+    p.q.L[li + 0] += v.x;
+    p.q.L[li + 1] += v.y;
+    p.q.L[li + 2] += v.z;
+}
+
+// ---------------------------------------------------------------------------
+// generate: Camera::generateRay (include/anacapa/integrator/IIntegrator.h:90-143)
+// with jitter = dims 0,1, lens = dims 2,3, time = dim 4. The pinhole ray is
+// computed with every operation rounded on its own (bit-identical origin and
+// direction to the reference built without contraction).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_generate(const __grid_constant__ Params p) {
+    const uint32_t n = p.chunk_pixels * p.spp;
+    const uint32_t first = p.chunk_first_pixel * p.spp;
+    if (blockIdx.x == 0 && threadIdx.x == 0) p.counters[0] = n;
+    const DevCamera& cam = p.S.cam;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint32_t pid = first + i, px, py, sidx;
+        path_coords(p, pid, px, py, sidx);
+        SampleStream ss{p.seed, px, py, sidx, 0};
+        float jx = ss.next(), jy = ss.next();
+        float lx = ss.next(), ly = ss.next();
+        float tu = ss.next();
+        (void)tu;  // shutter time: static scenes only
+        float s = xdiv(xadd(__uint2float_rn(px), jx), __uint2float_rn(cam.width));
+        float t = xdiv(xadd(__uint2float_rn(cam.height - 1u - py), jy), __uint2float_rn(cam.height));
+        float3 target = xadd3(xadd3(cam.lower_left, xmul3(cam.horizontal, s)), xmul3(cam.vertical, t));
+        float3 o = cam.origin, d;
+        if (cam.aperture <= 0.f) {
+            d = xnormalize(xsub3(target, o));
+        } else {
+            // thin lens, concentric disk mapping (IIntegrator.h:114-142)
+            float ax = 2.f * lx - 1.f, ay = 2.f * ly - 1.f, dx, dy;
+            if (ax == 0.f && ay == 0.f) {
+                dx = dy = 0.f;
+            } else if (fabsf(ax) >= fabsf(ay)) {
+                float ph = (kPi / 4.f) * (ay / ax);
+                dx = ax * cosf(ph);
+                dy = ax * sinf(ph);
+            } else {
+                float ph = (kPi / 2.f) - (kPi / 4.f) * (ax / ay);
+                dx = ay * cosf(ph);
+                dy = ay * sinf(ph);
+            }
+            float3 lens = o + cam.basis_u * (dx * cam.aperture) + cam.basis_v * (dy * cam.aperture);
+            float3 pd = normalize(target - o);
+            float3 fp = o + pd * cam.focal_distance;
+            o = lens;
+            d = normalize(fp - lens);
+        }
+        uint32_t meta = (ss.dim << 16);  // bounce 0, not specular
+        p.q.ext_o[0][i] = pack_u(o, pid);
+        p.q.ext_d[0][i] = pack_u(d, meta);
+        p.q.ext_b[0][i] = make_float4(1.f, 1.f, 1.f, 0.f);
+        size_t li = size_t(i) * 3;
+        p.q.L[li] = 0.f;
+        p.q.L[li + 1] = 0.f;
+        p.q.L[li + 2] = 0.f;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Closest hit over triangles then curves (CurveBrute::trace, CurveBrute.cpp:398-440).
+// ---------------------------------------------------------------------------
+struct SceneHit {
+    float t, u, v;
+    uint32_t prim;  // leaf-order triangle, 0x80000000 | segment, or kMiss
+    float3 tang;
+    float tseg;
+};
+
+__device__ __forceinline__ SceneHit closest_hit(const DevScene& S, const Ray& r, uint32_t* err) {
+    SceneHit h;
+    TriHit th = trace_tris<false>(S, r, err);
+    h.t = th.t;
+    h.u = th.u;
+    h.v = th.v;
+    h.prim = th.tri >= 0 ? uint32_t(th.tri) : kMiss;
+    h.tang = f3(0.f, 0.f, 0.f);
+    h.tseg = 0.f;
+    if (S.num_seg_nodes) {
+        CurveHit ch = trace_curves(S, r, th.tri >= 0 ? th.t : r.tmax, false, err);
+        if (ch.seg >= 0) {
+            h.t = ch.t;
+            h.prim = 0x80000000u | uint32_t(ch.seg);
+            h.tang = ch.tang;
+            h.tseg = ch.tSeg;
+            h.u = 0.f;
+            h.v = ch.tSeg;
+        }
+    }
+    return h;
+}
+
+__device__ __forceinline__ bool any_hit(const DevScene& S, const Ray& r, uint32_t* err) {
+    if (occluded_tris(S, r, err)) return true;
+    if (S.num_seg_nodes) return trace_curves(S, r, r.tmax, true, err).seg >= 0;
+    return false;
+}
+
+__global__ void __launch_bounds__(256) k_extend(const __grid_constant__ Params p) {
+    const uint32_t cur = p.bounce & 1u;
+    const uint32_t n = p.counters[p.bounce * kCountersPerBounce + 0];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float4 o = p.q.ext_o[cur][i], d = p.q.ext_d[cur][i];
+        Ray r{f3(o), f3(d), 1e-4f, INFINITY};
+        SceneHit h = closest_hit(p.S, r, p.err);
+        p.q.hit0[i] = make_float4(h.t, __uint_as_float(h.prim), h.u, h.v);
+        if (h.prim != kMiss && (h.prim & 0x80000000u)) p.q.hit1[i] = pack(h.tang, h.tseg);
+    }
+}
+
+// Surface interaction of a hit (BVHBackend::fillSurfaceInteraction,
+// BVHBackend.cpp:285-317; CurveBrute intersectOneSegment, CurveBrute.cpp:209-233).
+__device__ __forceinline__ SurfInt surf_int(const DevScene& S, float3 o, float3 d, float t, uint32_t prim, float u,
+                                            float v, float4 h1) {
+    SurfInt si;
+    if (!(prim & 0x80000000u)) {
+        const float4* tp = S.tri_isect + 3 * size_t(prim);
+        float4 a = ldg4(tp), e1 = ldg4(tp + 1), e2 = ldg4(tp + 2);
+        uint32_t orig = __float_as_uint(a.w);
+        const float4* sp = S.tri_shade + 4 * size_t(orig);
+        float4 s0 = ldg4(sp), s1 = ldg4(sp + 1), s2 = ldg4(sp + 2), s3 = ldg4(sp + 3);
+        float w = 1.f - u - v;
+        si.p = f3(a) + f3(e1) * u + f3(e2) * v;
+        si.ng = f3(s0);
+        float3 sn = safe_normalize(f3(s1) * w + f3(s2) * u + f3(s3) * v);
+        if (dot(sn, si.ng) < 0.f) sn = -sn;
+        si.n = sn;
+        si.dpdu = f3(e1);
+        si.slot = __float_as_uint(s0.w);
+        si.color = f3(1.f, 1.f, 1.f);
+        si.is_curve = false;
+    } else {
+        uint32_t j = prim & 0x7FFFFFFFu;
+        float4 rec = ldg4(S.segs + 5 * size_t(j) + 4);
+        uint32_t strand = __float_as_uint(rec.x);
+        float3 tang = f3(h1);
+        si.p = o + d * t;
+        float3 nd = -d;
+        float3 nrm = nd - tang * dot(nd, tang);
+        float3 fx, fy;
+        onb(d, fx, fy);
+        nrm = safe_normalize(nrm, fx);
+        si.n = nrm;
+        si.ng = nrm;
+        si.dpdu = tang;
+        si.slot = __float_as_uint(rec.z);
+        si.color = f3(__ldg(S.strand_color + 3 * strand), __ldg(S.strand_color + 3 * strand + 1),
+                      __ldg(S.strand_color + 3 * strand + 2));
+        si.is_curve = true;
+    }
+    return si;
+}
+
+__device__ __forceinline__ int slot_material(const DevScene& S, uint32_t slot) {
+    return slot < S.num_slots ? __ldg(S.slot_material + slot) : -1;
+}
+
+__global__ void __launch_bounds__(256) k_shade(const __grid_constant__ Params p) {
+    const uint32_t b = p.bounce;
+    const uint32_t cur = b & 1u, nxt = cur ^ 1u;
+    const uint32_t n = p.counters[b * kCountersPerBounce + 0];
+    const DevScene& S = p.S;
+    const uint32_t nL = S.num_lights;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += stride) {
+        const uint32_t i = base + threadIdx.x;
+        bool pushSh = false, pushMis = false, pushExt = false;
+        float4 shO, shD, shC, mO, mD, mC, eO, eD, eB;
+        if (i < n) {
+            float4 qo = p.q.ext_o[cur][i], qd = p.q.ext_d[cur][i], qb = p.q.ext_b[cur][i];
+            float4 h0 = p.q.hit0[i];
+            const uint32_t pid = __float_as_uint(qo.w), meta = __float_as_uint(qd.w);
+            const uint32_t bounce = meta & 0xFFu;
+            bool spec = (meta >> 8) & 1u;
+            float3 o = f3(qo), d = f3(qd), beta = f3(qb);
+            uint32_t prim = __float_as_uint(h0.y);
+            float3 Ladd = f3(0.f, 0.f, 0.f);
+            if (prim == kMiss) {
+                if (bounce == 0 || spec) Ladd = beta * env_le(S.env, d);
+            } else {
+                float4 h1 = (prim & 0x80000000u) ? p.q.hit1[i] : make_float4(0, 0, 0, 0);
+                SurfInt si = surf_int(S, o, d, h0.x, prim, h0.z, h0.w, h1);
+                int mi = slot_material(S, si.slot);
+                if (mi >= 0) {
+                    const DevMaterial m = S.materials[mi];
+                    uint32_t px, py, sidx;
+                    path_coords(p, pid, px, py, sidx);
+                    SampleStream ss{p.seed, px, py, sidx, meta >> 16};
+                    float3 wo = -d;
+                    ShadeCtx c = make_ctx(si, d);
+                    float3 Le = mat_le(m);
+                    if (!is_black(Le) && (bounce == 0 || spec)) Ladd = Ladd + beta * Le;
+                    if (!m.is_delta && nL > 0) {
+                        float ul = ss.next();
+                        uint32_t lidx = min(uint32_t(ul * float(nL)), nL - 1u);
+                        const DevLight L = S.lights[lidx];
+                        // light sampling
+                        float lu0 = ss.next(), lu1 = ss.next();
+                        LightSample ls = light_sample(S, L, si.p, lu0, lu1);
+                        if (ls.pdf > 0.f && !is_black(ls.Li)) {
+                            BsdfEval be = mat_eval(m, c, wo, ls.wi);
+                            if (!is_black(be.f)) {
+                                float3 target = si.p + ls.wi * ls.dist;
+                                float3 dir = target - si.p;
+                                float dist = length(dir);
+                                dir = dir * (1.f / dist);
+                                float3 org = spawn_origin(si.p, si.n, dir);
+                                float w = power_heuristic(ls.pdf, be.pdf);
+                                float cosI;
+                                if (si.is_curve) {
+                                    float dt = dot(ls.wi, c.t);
+                                    cosI = sqrtf(fmaxf(0.f, 1.f - dt * dt));
+                                } else {
+                                    cosI = absdot(ls.wi, si.n);
+                                }
+                                float3 contrib = beta * (be.f * ls.Li * cosI * w / ls.pdf) * float(nL);
+                                pushSh = true;
+                                shO = pack_u(org, pid);
+                                shD = pack(dir, dist * (1.f - 1e-4f));
+                                shC = pack(contrib, 0.f);
+                            }
+                        }
+                        // BSDF sampling toward the light (non-delta lights)
+                        float uc = ss.next();
+                        float bu0 = ss.next(), bu1 = ss.next();
+                        BsdfSample bs = mat_sample(m, c, wo, bu0, bu1, uc);
+                        if (bs.valid()) {
+                            float lp = light_pdf(S, L, si.p, bs.wi);
+                            if (lp > 0.f) {
+                                float w = bs.delta() ? 1.f : power_heuristic(bs.pdf, lp);
+                                float3 org = spawn_origin(si.p, si.ng, bs.wi);
+                                float cosI = absdot(bs.wi, si.n);
+                                float3 contrib = beta * (bs.f * cosI * w / bs.pdf) * float(nL);
+                                pushMis = true;
+                                mO = pack_u(org, pid);
+                                mD = pack(bs.wi, 0.f);
+                                mC = pack(contrib, 0.f);
+                            }
+                        }
+                    }
+                    // continuation
+                    float uc = ss.next();
+                    float u0 = ss.next(), u1 = ss.next();
+                    BsdfSample bs = mat_sample(m, c, wo, u0, u1, uc);
+                    if (bs.valid()) {
+                        spec = bs.delta();
+                        beta = beta * (bs.f / bs.pdf);
+                        float3 org = spawn_origin(si.p, si.n, bs.wi);
+                        bool alive = true;
+                        if (bounce >= p.min_depth) {
+                            float q = 1.f - fminf(max_comp(beta), 0.95f);
+                            if (ss.next() < q) alive = false;
+                            else beta = beta * (1.f / (1.f - q));
+                        }
+                        if (alive && bounce + 1u <= p.max_depth) {
+                            pushExt = true;
+                            uint32_t nm = (bounce + 1u) | (spec ? 0x100u : 0u) | (ss.dim << 16);
+                            eO = pack_u(org, pid);
+                            eD = pack_u(bs.wi, nm);
+                            eB = pack(beta, 0.f);
+                        }
+                    }
+                }
+            }
+            if (!is_black(Ladd)) add_L(p, pid, Ladd);
+        }
+        uint32_t* cb = p.counters + b * kCountersPerBounce;
+        uint32_t k = block_push(pushSh, cb + 1);
+        if (pushSh) {
+            p.q.sh_o[k] = shO;
+            p.q.sh_d[k] = shD;
+            p.q.sh_c[k] = shC;
+        }
+        k = block_push(pushMis, cb + 2);
+        if (pushMis) {
+            p.q.mis_o[k] = mO;
+            p.q.mis_d[k] = mD;
+            p.q.mis_c[k] = mC;
+        }
+        k = block_push(pushExt, cb + kCountersPerBounce + 0);
+        if (pushExt) {
+            p.q.ext_o[nxt][k] = eO;
+            p.q.ext_d[nxt][k] = eD;
+            p.q.ext_b[nxt][k] = eB;
+        }
+    }
+}
+
+// NEE shadow rays: shadowTransmittance (src/integrator/ShadowRay.h:26-61) for
+// opaque scenes — any blocker in [1e-4, tmax] makes the transmittance black.
+__global__ void __launch_bounds__(256) k_shadow(const __grid_constant__ Params p) {
+    const uint32_t n = p.counters[p.bounce * kCountersPerBounce + 1];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float4 o = p.q.sh_o[i], d = p.q.sh_d[i];
+        Ray r{f3(o), f3(d), 1e-4f, d.w};
+        if (!any_hit(p.S, r, p.err)) add_L(p, __float_as_uint(o.w), f3(p.q.sh_c[i]));
+    }
+}
+
+// BSDF-sampled MIS rays (PathIntegrator.cpp:214-259): the first surface hit
+// within 1e10 contributes its material's Le, a miss the environment.
+__global__ void __launch_bounds__(256) k_mis(const __grid_constant__ Params p) {
+    const uint32_t n = p.counters[p.bounce * kCountersPerBounce + 2];
+    const DevScene& S = p.S;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float4 o = p.q.mis_o[i], d = p.q.mis_d[i];
+        Ray r{f3(o), f3(d), 1e-4f, 1e10f};
+        SceneHit h = closest_hit(S, r, p.err);
+        float3 Li;
+        if (h.prim == kMiss) {
+            Li = env_le(S.env, r.d);
+        } else {
+            uint32_t slot;
+            if (h.prim & 0x80000000u)
+                slot = __float_as_uint(ldg4(S.segs + 5 * size_t(h.prim & 0x7FFFFFFFu) + 4).z);
+            else
+                slot = __float_as_uint(ldg4(S.tri_shade + 4 * size_t(__float_as_uint(
+                                                               ldg4(S.tri_isect + 3 * size_t(h.prim)).w))).w);
+            int mi = slot_material(S, slot);
+            Li = mi >= 0 ? mat_le(S.materials[mi]) : f3(0.f, 0.f, 0.f);
+        }
+        if (!is_black(Li)) add_L(p, __float_as_uint(o.w), f3(p.q.mis_c[i]) * Li);
+    }
+}
+
+// Film accumulation (PathIntegrator.cpp:43-57 + Film::mergeTile, Film.cpp:34-56):
+// finite samples summed in sample order, weight = sample count.
+__global__ void __launch_bounds__(256) k_film(const __grid_constant__ Params p) {
+    const float invSPP = 1.f / float(p.spp);
+    for (uint32_t pl = blockIdx.x * blockDim.x + threadIdx.x; pl < p.chunk_pixels; pl += gridDim.x * blockDim.x) {
+        float3 acc = f3(0.f, 0.f, 0.f);
+        float lsq = 0.f;
+        const float* Lp = p.q.L + size_t(pl) * p.spp * 3;
+        for (uint32_t s = 0; s < p.spp; ++s) {
+            float3 L = f3(Lp[3 * s], Lp[3 * s + 1], Lp[3 * s + 2]);
+            if (is_finite3(L)) {
+                acc = acc + L;
+                float lum = luminance(L);
+                lsq += lum * lum;
+            }
+        }
+        ana_film_pixel& f = p.film[p.chunk_first_pixel + pl];
+        float w = float(p.spp);
+        f.r += (acc.x * invSPP) * w;
+        f.g += (acc.y * invSPP) * w;
+        f.b += (acc.z * invSPP) * w;
+        f.w += w;
+        f.sum_lum_sq += lsq;
+    }
+}
+
+// IAccelerationStructure::traceBatch / occludedBatch over CurveBrute semantics.
+__global__ void __launch_bounds__(256) k_trace_batch(const __grid_constant__ DevScene S, const float* rays, size_t n,
+                                                     ana_hit* out, int occlusion, uint32_t* err) {
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
+        const float4* rp = reinterpret_cast<const float4*>(rays + 8 * i);
+        float4 a = rp[0], b = rp[1];
+        Ray r{f3(a), f3(b), a.w, b.w};
+        ana_hit h{0, -1, -1, -1, 0.f, 0.f, 0.f, 0.f};
+        if (occlusion) {
+            h.hit = any_hit(S, r, err) ? 1 : 0;
+        } else {
+            SceneHit sh = closest_hit(S, r, err);
+            if (sh.prim != kMiss) {
+                h.hit = 1;
+                h.t = sh.t;
+                h.u = sh.u;
+                h.v = sh.v;
+                if (sh.prim & 0x80000000u) {
+                    float4 rec = ldg4(S.segs + 5 * size_t(sh.prim & 0x7FFFFFFFu) + 4);
+                    h.mesh_id = int32_t(__float_as_uint(rec.z));
+                    h.prim_id = int32_t(__float_as_uint(rec.y));
+                    h.strand_id = int32_t(__float_as_uint(rec.x));
+                } else {
+                    uint32_t orig = __float_as_uint(ldg4(S.tri_isect + 3 * size_t(sh.prim)).w);
+                    const float4* sp = S.tri_shade + 4 * size_t(orig);
+                    h.mesh_id = int32_t(__float_as_uint(ldg4(sp).w));
+                    h.prim_id = int32_t(__float_as_uint(ldg4(sp + 1).w));
+                }
+            }
+        }
+        out[i] = h;
+    }
+}
+
+// ---------------------------------------------------------------------------
+static inline int blocks_for(uint32_t n, int block, int cap) {
+    long long b = ((long long)n + block - 1) / block;
+    if (b < 1) b = 1;
+    return int(b < cap ? b : cap);
+}
+
+void launch_generate(const Params& p, const LaunchCfg& c, cudaStream_t s) {
+    k_generate<<<blocks_for(p.chunk_pixels * p.spp, 256, c.grid_cap), 256, 0, s>>>(p);
+}
+void launch_extend(const Params& p, const LaunchCfg& c, cudaStream_t s) {
+    k_extend<<<c.grid_cap, c.block, 0, s>>>(p);
+}
+void launch_shade(const Params& p, const LaunchCfg& c, cudaStream_t s) {
+    k_shade<<<c.grid_cap, c.block, 0, s>>>(p);
+}
+void launch_shadow(const Params& p, const LaunchCfg& c, cudaStream_t s) {
+    k_shadow<<<c.grid_cap, c.block, 0, s>>>(p);
+}
+void launch_mis(const Params& p, const LaunchCfg& c, cudaStream_t s) {
+    k_mis<<<c.grid_cap, c.block, 0, s>>>(p);
+}
+void launch_film(const Params& p, const LaunchCfg& c, cudaStream_t s) {
+    k_film<<<blocks_for(p.chunk_pixels, 256, c.grid_cap), 256, 0, s>>>(p);
+}
+void launch_trace_batch(const DevScene& S, const float* rays, size_t n, ana_hit* out, int occlusion,
+                        uint32_t* err, cudaStream_t s) {
+    int blocks = int((n + 255) / 256);
+    if (blocks > 148 * 64) blocks = 148 * 64;
+    if (blocks < 1) blocks = 1;
+    k_trace_batch<<<blocks, 256, 0, s>>>(S, rays, n, out, occlusion, err);
+}
+
+}  // namespace ana

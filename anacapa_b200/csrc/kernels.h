@@ -1,0 +1,63 @@
+// Launch interface of the wavefront path-tracing kernels (kernels.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/anacapa_b200.h"
+#include "layout.h"
+
+namespace ana {
+
+// Queues are structure-of-arrays of float4, indexed by queue position.
+//   extend queue: o (xyz, global path id), d (xyz, meta), beta (xyz, -)
+//     meta bits: 0..7 bounce, 8 specular-bounce flag, 16..31 next sampler dimension
+//   hit record:   (t, prim, u, v) and, for curve hits, (tangent xyz, strand v)
+//     prim: leaf-order triangle index, 0x80000000 | segment index, or ~0 (miss)
+//   shadow queue: o (xyz, path id), d (xyz, tmax), contribution (xyz, -)
+//   MIS queue:    o (xyz, path id), d (xyz, -), contribution without Li (xyz, -)
+struct Queues {
+    float4* ext_o[2];
+    float4* ext_d[2];
+    float4* ext_b[2];
+    float4* hit0;
+    float4* hit1;
+    float4* sh_o;
+    float4* sh_d;
+    float4* sh_c;
+    float4* mis_o;
+    float4* mis_d;
+    float4* mis_c;
+    float* L;  // 3 floats per path of the chunk
+};
+
+// Per-bounce device counters: [bounce][0] extend queue length, [1] shadow
+// queue length, [2] MIS queue length. Zeroed per chunk.
+constexpr int kCountersPerBounce = 4;
+
+struct Params {
+    DevScene S;
+    Queues q;
+    ana_film_pixel* film;
+    uint32_t* counters;  // this chunk's counters
+    uint32_t* err;       // device error word (bit 0: traversal stack overflow)
+    uint64_t seed;
+    uint32_t W, H, spp, sample_start, max_depth, min_depth;
+    uint32_t chunk_first_pixel, chunk_pixels;
+    uint32_t bounce;
+};
+
+struct LaunchCfg {
+    int block;       // threads per block for the stage kernels
+    int grid_cap;    // blocks for grid-stride kernels over the chunk capacity
+};
+
+void launch_generate(const Params& p, const LaunchCfg& c, cudaStream_t s);
+void launch_extend(const Params& p, const LaunchCfg& c, cudaStream_t s);
+void launch_shade(const Params& p, const LaunchCfg& c, cudaStream_t s);
+void launch_shadow(const Params& p, const LaunchCfg& c, cudaStream_t s);
+void launch_mis(const Params& p, const LaunchCfg& c, cudaStream_t s);
+void launch_film(const Params& p, const LaunchCfg& c, cudaStream_t s);
+void launch_trace_batch(const DevScene& S, const float* rays, size_t n, ana_hit* out, int occlusion,
+                        uint32_t* err, cudaStream_t s);
+
+}  // namespace ana

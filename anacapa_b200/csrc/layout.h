@@ -1,0 +1,113 @@
+// Device-resident scene layout shared by the host preparation code and the
+// sm_100a kernels. Plain POD, no CUDA runtime calls.
+//
+// HBM layout (all arrays 16-byte aligned, read with 16-byte vector loads):
+//   tri_nodes   BVH2 interior nodes, 64 B each: both children's boxes live in
+//               the parent so one node fetch tests two boxes.
+//   tri_isect   48 B per triangle in leaf order: (v0, orig index) (e1) (e2),
+//               i.e. BVHTriangle::v0/e1/e2 (src/accel/BVHBackend.h:49-59).
+//   tri_shade   64 B per triangle in mesh order: (ng, meshID) (sn0, primID)
+//               (sn1) (sn2), read once per shaded hit.
+//   seg_nodes   BVH2 nodes over cubic Bezier segments (same 64 B format).
+//   segs        80 B per segment in leaf order: P0..P3 with the two half
+//               widths and the strand-parameter offset/scale, then ids.
+#pragma once
+#include <stdint.h>
+#include <vector_types.h>
+
+namespace ana {
+
+// BVH2 node with child boxes in the parent.
+//   n0 = (c0.lo.x, c0.hi.x, c0.lo.y, c0.hi.y)
+//   n1 = (c1.lo.x, c1.hi.x, c1.lo.y, c1.hi.y)
+//   n2 = (c0.lo.z, c0.hi.z, c1.lo.z, c1.hi.z)
+//   n3 = (c0 ref, c1 ref, c0 count, c1 count) as int bits
+// A child ref with count 0 is an interior node index; count > 0 means a leaf
+// whose primitives are [ref, ref + count) in the leaf-ordered primitive array.
+// An absent child has an empty box (lo = +inf, hi = -inf).
+struct BvhNode {
+    float4 n0, n1, n2, n3;
+};
+static_assert(sizeof(BvhNode) == 64, "BvhNode must be 64 bytes");
+
+constexpr uint32_t kMaxStack = 64;   // traversal stack depth (reference: 64)
+
+// Material, flattened with the derived constants each reference class
+// precomputes in its constructor.
+struct DevMaterial {
+    uint32_t type;       // ANA_MAT_*
+    uint32_t flags;      // BSDFFlags of IMaterial::flags()
+    uint32_t is_delta;   // IMaterial::isDelta()
+    uint32_t hair_mode;
+    float3 albedo;       // Lambert albedo / standard base_color
+    float3 emission;     // Le (Emissive) or emission_color * emission (standard)
+    // standard_surface
+    float base, metal, rough, spec;
+    float3 spec_color;
+    float coat;
+    float alpha2;        // max(1e-4, r^2)^2
+    float coat_alpha2;
+    float f0_dielectric; // F0_fromIOR(specular_IOR)
+    float coat_f0;       // F0_fromIOR(1.5)
+    // hair
+    float eta;
+    float3 sigma_a;
+    float v[3];          // longitudinal variances R, TT, TRT
+    float s;             // azimuthal logistic scale
+    float alpha_shift[3];// lobe shift angles (radians)
+    float beta_m;
+    float pad0, pad1;
+};
+
+struct DevLight {
+    uint32_t type;       // ANA_LIGHT_*
+    uint32_t pad[3];
+    float3 center, u, v, normal, Le;
+    float area;
+    float uLen2, vLen2;  // |u|^2, |v|^2 as AreaLight::pdf computes them
+    float pad2;
+};
+
+// Equirect dome with its 2-D piecewise-constant distribution
+// (Distribution1D per row + marginal, src/shading/lights/DomeLight.h:146-182, 355-386).
+struct DevEnv {
+    const float* rgb;        // W*H*3, row 0 = zenith
+    const float* cond_func;  // H rows of W
+    const float* cond_cdf;   // H rows of W+1
+    const float* cond_int;   // H
+    const float* marg_func;  // H
+    const float* marg_cdf;   // H+1
+    float marg_int;
+    float intensity;
+    uint32_t width, height;
+    float3 radiance;         // constant background when rgb == nullptr
+    uint32_t present;        // 1 if a dome exists
+};
+
+struct DevCamera {
+    float3 origin, lower_left, horizontal, vertical, basis_u, basis_v;
+    float aperture, focal_distance, shutter_open, shutter_close;
+    uint32_t width, height;
+};
+
+struct DevScene {
+    const BvhNode* tri_nodes;
+    const float4* tri_isect;
+    const float4* tri_shade;
+    uint32_t num_tri_nodes, num_tris;
+    uint32_t tri_root_is_empty;
+    const BvhNode* seg_nodes;
+    const float4* segs;
+    const float* strand_color;   // 3 per strand
+    uint32_t num_seg_nodes, num_segs;
+    const DevMaterial* materials;
+    const int32_t* slot_material;
+    uint32_t num_materials, num_slots;
+    const DevLight* lights;
+    uint32_t num_lights;
+    uint32_t pad;
+    DevEnv env;
+    DevCamera cam;
+};
+
+}  // namespace ana

@@ -1,0 +1,46 @@
+// Host-side scene preparation: validates an ana_scene_desc, builds the BVHs
+// and flattens everything into the device layout of layout.h.
+#pragma once
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/anacapa_b200.h"
+#include "layout.h"
+
+namespace ana {
+
+struct HostEnv {
+    std::vector<float> rgb, cond_func, cond_cdf, cond_int, marg_func, marg_cdf;
+    float marg_int = 0.f;
+    float intensity = 1.f;
+    uint32_t width = 0, height = 0;
+    float radiance[3] = {0.f, 0.f, 0.f};
+    bool present = false;
+};
+
+struct Prepared {
+    std::vector<BvhNode> tri_nodes;
+    std::vector<float4> tri_isect;   // 3 per triangle, leaf order
+    std::vector<float4> tri_shade;   // 4 per triangle, mesh order
+    bool tri_root_is_empty = true;
+    std::vector<BvhNode> seg_nodes;
+    std::vector<float4> segs;        // 5 per segment, leaf order
+    std::vector<float> strand_color;
+    std::vector<DevMaterial> materials;
+    std::vector<int32_t> slot_material;
+    std::vector<DevLight> lights;
+    HostEnv env;
+    ana_camera camera{};
+    uint32_t num_tris = 0, num_segs = 0;
+    uint64_t bytes() const;
+};
+
+// Returns ANA_OK or an error code with a message in err.
+int prepare_scene(const ana_scene_desc& d, Prepared& out, std::string& err);
+
+// Camera::makePinhole (include/anacapa/integrator/IIntegrator.h:49-74) for a film size.
+DevCamera make_camera(const ana_camera& c, uint32_t width, uint32_t height);
+
+}  // namespace ana

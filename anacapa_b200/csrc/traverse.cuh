@@ -1,0 +1,412 @@
+// Closest-hit and any-hit traversal of the triangle BVH2 and the curve BVH2.
+//
+// Hit-identity parity: the triangle test restates BVHBackend::intersectTriangle
+// (src/accel/BVHBackend.cpp:264-283) with every operation rounded on its own
+// (no FMA), so (t, u, v) equal the reference's float results compiled without
+// contraction; the box tests restate intersectAABB (BVHBackend.cpp:249-262):
+// ray tMin/tMax, the dirNeg slab selection and the `tMax <= tMin` rejection,
+// plus the caller's `tNear > closestT` cull; the curve path restates
+// CurveBrute::trace's aabbHit and the ray-ribbon subdivide
+// (src/accel/CurveBrute.cpp:85-234, 478-498).
+#pragma once
+#include "dmath.cuh"
+#include "layout.h"
+
+namespace ana {
+
+struct Ray {
+    float3 o, d;
+    float tmin, tmax;
+};
+
+// BVHBackend::makeRay4 (BVHBackend.cpp:233-247): invDir = 1/safe(d) where
+// safe(v) = |v| > 1e-9 ? v : 1e-9 (the sign of tiny components is dropped),
+// and the triangle test rebuilds dir = 1/invDir.
+struct TriRay {
+    float3 o, inv, dir;
+    float tmin, tmax;
+    bool nx, ny, nz;
+};
+
+__device__ __forceinline__ float safe_comp(float v) { return fabsf(v) > 1e-9f ? v : 1e-9f; }
+
+__device__ __forceinline__ TriRay make_tri_ray(const Ray& r) {
+    TriRay q;
+    q.o = r.o;
+    q.inv = f3(xdiv(1.f, safe_comp(r.d.x)), xdiv(1.f, safe_comp(r.d.y)), xdiv(1.f, safe_comp(r.d.z)));
+    q.dir = f3(xdiv(1.f, q.inv.x), xdiv(1.f, q.inv.y), xdiv(1.f, q.inv.z));
+    q.tmin = r.tmin;
+    q.tmax = r.tmax;
+    q.nx = r.d.x < 0.f;
+    q.ny = r.d.y < 0.f;
+    q.nz = r.d.z < 0.f;
+    return q;
+}
+
+// Slab test of one child box. Returns true and tNear when the box is entered
+// before `cull` (the current closest hit) and its interval is not empty.
+__device__ __forceinline__ bool box_hit(const TriRay& r, float lox, float hix, float loy, float hiy,
+                                        float loz, float hiz, float cull, float& tnear) {
+    float nx = r.nx ? hix : lox, fx = r.nx ? lox : hix;
+    float ny = r.ny ? hiy : loy, fy = r.ny ? loy : hiy;
+    float nz = r.nz ? hiz : loz, fz = r.nz ? loz : hiz;
+    float t0x = xmul(xsub(nx, r.o.x), r.inv.x), t1x = xmul(xsub(fx, r.o.x), r.inv.x);
+    float t0y = xmul(xsub(ny, r.o.y), r.inv.y), t1y = xmul(xsub(fy, r.o.y), r.inv.y);
+    float t0z = xmul(xsub(nz, r.o.z), r.inv.z), t1z = xmul(xsub(fz, r.o.z), r.inv.z);
+    float tmn = fmaxf(fmaxf(fmaxf(r.tmin, t0x), t0y), t0z);
+    float tmx = fminf(fminf(fminf(r.tmax, t1x), t1y), t1z);
+    tnear = tmn;
+    return tmx > tmn && tmn <= cull;
+}
+
+// Moller-Trumbore, BVHBackend::intersectTriangle.
+__device__ __forceinline__ bool tri_hit(const TriRay& r, float3 v0, float3 e1, float3 e2, float tmax,
+                                        float& t, float& u, float& v) {
+    float3 h = xcross(r.dir, e2);
+    float a = xdot(e1, h);
+    if (fabsf(a) < 1e-9f) return false;
+    float f = xdiv(1.f, a);
+    float3 s = xsub3(r.o, v0);
+    u = xmul(f, xdot(s, h));
+    if (u < 0.f || u > 1.f) return false;
+    float3 q = xcross(s, e1);
+    v = xmul(f, xdot(r.dir, q));
+    if (v < 0.f || xadd(u, v) > 1.f) return false;
+    t = xmul(f, xdot(e2, q));
+    return t >= r.tmin && t <= tmax;
+}
+
+// Stack entry: interior node index, or a leaf (bit 31) with count-1 in bits
+// 25..30 and the first primitive in bits 0..24.
+__device__ __forceinline__ uint32_t leaf_entry(uint32_t off, uint32_t cnt) {
+    return 0x80000000u | ((cnt - 1u) << 25) | off;
+}
+
+struct TriHit {
+    float t, u, v;
+    int32_t tri;  // leaf-order index, -1 on miss
+};
+
+struct Counters {
+    uint32_t nodes, prims;
+};
+
+// Closest hit over the triangle BVH. Returns the nearest accepted triangle;
+// ties (t == closest) go to the later-tested triangle, as `t <= r.tMax` does
+// in the reference.
+template <bool kCount>
+__device__ __forceinline__ TriHit trace_tris(const DevScene& S, const Ray& ray, uint32_t* err,
+                                             Counters* cnt = nullptr) {
+    TriHit h{ray.tmax, 0.f, 0.f, -1};
+    if (S.num_tri_nodes == 0) return h;
+    TriRay r = make_tri_ray(ray);
+    uint32_t stack[kMaxStack];
+    float stackT[kMaxStack];
+    int sp = 0;
+    uint32_t cur = 0;  // interior root
+    float closest = ray.tmax;
+    while (true) {
+        if (!(cur & 0x80000000u)) {
+            const float4* np = reinterpret_cast<const float4*>(S.tri_nodes + cur);
+            float4 n0 = ldg4(np), n1 = ldg4(np + 1), n2 = ldg4(np + 2), n3 = ldg4(np + 3);
+            if (kCount) cnt->nodes++;
+            float tn0, tn1;
+            bool h0 = box_hit(r, n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, closest, tn0);
+            bool h1 = box_hit(r, n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, closest, tn1);
+            uint32_t c0 = fbits_u(n3.z) ? leaf_entry(fbits_u(n3.x), fbits_u(n3.z)) : fbits_u(n3.x);
+            uint32_t c1 = fbits_u(n3.w) ? leaf_entry(fbits_u(n3.y), fbits_u(n3.w)) : fbits_u(n3.y);
+            if (h0 && h1) {
+                // nearer child next, farther one on the stack (BVHBackend.cpp:382-387)
+                bool swap = !(tn0 < tn1);
+                uint32_t nearC = swap ? c1 : c0, farC = swap ? c0 : c1;
+                float farT = swap ? tn0 : tn1;
+                if (sp >= int(kMaxStack)) { atomicOr(err, 1u); return h; }
+                stack[sp] = farC;
+                stackT[sp] = farT;
+                ++sp;
+                cur = nearC;
+                continue;
+            } else if (h0 || h1) {
+                cur = h0 ? c0 : c1;
+                continue;
+            }
+        } else {
+            uint32_t off = cur & 0x01FFFFFFu, c = ((cur >> 25) & 63u) + 1u;
+            for (uint32_t i = off; i < off + c; ++i) {
+                const float4* tp = S.tri_isect + 3 * size_t(i);
+                float4 a = ldg4(tp), b = ldg4(tp + 1), e = ldg4(tp + 2);
+                if (kCount) cnt->prims++;
+                float t, u, v;
+                if (tri_hit(r, f3(a), f3(b), f3(e), closest, t, u, v)) {
+                    closest = t;
+                    h.t = t;
+                    h.u = u;
+                    h.v = v;
+                    h.tri = int32_t(i);
+                }
+            }
+        }
+        // pop, skipping entries entered beyond the current closest hit
+        bool found = false;
+        while (sp > 0) {
+            --sp;
+            if (stackT[sp] > closest) continue;
+            cur = stack[sp];
+            found = true;
+            break;
+        }
+        if (!found) break;
+    }
+    return h;
+}
+
+// Any hit within [tmin, tmax] (BVHBackend::occluded, BVHBackend.cpp:409-444).
+__device__ __forceinline__ bool occluded_tris(const DevScene& S, const Ray& ray, uint32_t* err) {
+    if (S.num_tri_nodes == 0) return false;
+    TriRay r = make_tri_ray(ray);
+    uint32_t stack[kMaxStack];
+    int sp = 0;
+    uint32_t cur = 0;
+    while (true) {
+        if (!(cur & 0x80000000u)) {
+            const float4* np = reinterpret_cast<const float4*>(S.tri_nodes + cur);
+            float4 n0 = ldg4(np), n1 = ldg4(np + 1), n2 = ldg4(np + 2), n3 = ldg4(np + 3);
+            float tn0, tn1;
+            bool h0 = box_hit(r, n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, ray.tmax, tn0);
+            bool h1 = box_hit(r, n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, ray.tmax, tn1);
+            uint32_t c0 = fbits_u(n3.z) ? leaf_entry(fbits_u(n3.x), fbits_u(n3.z)) : fbits_u(n3.x);
+            uint32_t c1 = fbits_u(n3.w) ? leaf_entry(fbits_u(n3.y), fbits_u(n3.w)) : fbits_u(n3.y);
+            if (h0 && h1) {
+                bool swap = !(tn0 < tn1);
+                if (sp >= int(kMaxStack)) { atomicOr(err, 1u); return false; }
+                stack[sp++] = swap ? c0 : c1;
+                cur = swap ? c1 : c0;
+                continue;
+            } else if (h0 || h1) {
+                cur = h0 ? c0 : c1;
+                continue;
+            }
+        } else {
+            uint32_t off = cur & 0x01FFFFFFu, c = ((cur >> 25) & 63u) + 1u;
+            for (uint32_t i = off; i < off + c; ++i) {
+                const float4* tp = S.tri_isect + 3 * size_t(i);
+                float4 a = ldg4(tp), b = ldg4(tp + 1), e = ldg4(tp + 2);
+                float t, u, v;
+                if (tri_hit(r, f3(a), f3(b), f3(e), ray.tmax, t, u, v)) return true;
+            }
+        }
+        if (sp == 0) break;
+        cur = stack[--sp];
+    }
+    return false;
+}
+
+// ===========================================================================
+// Curves
+// ===========================================================================
+
+// CurveBrute::aabbHit (CurveBrute.cpp:478-498).
+__device__ __forceinline__ bool curve_box_hit(const Ray& r, float3 inv, float lox, float hix, float loy,
+                                              float hiy, float loz, float hiz, float maxT, float& tnear) {
+    float tmn = r.tmin, tmx = maxT;
+    float lo[3] = {lox, loy, loz}, hi[3] = {hix, hiy, hiz};
+    float o[3] = {r.o.x, r.o.y, r.o.z}, d[3] = {r.d.x, r.d.y, r.d.z}, iv[3] = {inv.x, inv.y, inv.z};
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        if (fabsf(d[i]) < 1e-9f) {
+            if (o[i] < lo[i] || o[i] > hi[i]) return false;
+            continue;
+        }
+        float t0 = xmul(xsub(lo[i], o[i]), iv[i]);
+        float t1 = xmul(xsub(hi[i], o[i]), iv[i]);
+        if (iv[i] < 0.f) {
+            float tt = t0;
+            t0 = t1;
+            t1 = tt;
+        }
+        tmn = fmaxf(tmn, t0);
+        tmx = fminf(tmx, t1);
+        if (tmx < tmn) return false;
+    }
+    tnear = tmn;
+    return true;
+}
+
+// Ray-space frame of makeRayFrame (CurveBrute.cpp:29-47): z = direction, x/y
+// from buildOrthonormalBasis (Types.h:108-114).
+struct RayFrame {
+    float3 o, x, y, z;
+};
+
+__device__ __forceinline__ void onb_exact(float3 n, float3& t, float3& b) {
+    float sign = copysignf(1.f, n.z);
+    float a = xdiv(-1.f, xadd(sign, n.z));
+    float bb = xmul(xmul(n.x, n.y), a);
+    t = f3(xadd(1.f, xmul(xmul(xmul(sign, n.x), n.x), a)), xmul(sign, bb), -xmul(sign, n.x));
+    b = f3(bb, xadd(sign, xmul(xmul(n.y, n.y), a)), -n.y);
+}
+
+__device__ __forceinline__ RayFrame make_frame(const Ray& r) {
+    RayFrame f;
+    f.o = r.o;
+    f.z = r.d;
+    onb_exact(r.d, f.x, f.y);
+    return f;
+}
+
+__device__ __forceinline__ float3 project(const RayFrame& f, float3 p) {
+    float3 q = xsub3(p, f.o);
+    return f3(xdot(q, f.x), xdot(q, f.y), xdot(q, f.z));
+}
+
+struct SubSeg {
+    float3 P0, P1, P2, P3;
+    float hw0, hw3, toff, tscale;
+    int depth;
+};
+
+__device__ __forceinline__ float3 xmid(float3 a, float3 b) { return xmul3(xadd3(a, b), 0.5f); }
+
+// bezierTangent (CurveBrute.cpp:59-64)
+__device__ __forceinline__ float3 bezier_tangent(float3 P0, float3 P1, float3 P2, float3 P3, float t) {
+    float mt = xsub(1.f, t);
+    float3 a = xmul3(xsub3(P1, P0), xmul(xmul(3.f, mt), mt));
+    float3 b = xmul3(xsub3(P2, P1), xmul(xmul(6.f, mt), t));
+    float3 c = xmul3(xsub3(P3, P2), xmul(xmul(3.f, t), t));
+    return xadd3(xadd3(a, b), c);
+}
+
+__device__ __forceinline__ float min4(float a, float b, float c, float d) {
+    return fminf(fminf(a, b), fminf(c, d));
+}
+__device__ __forceinline__ float max4(float a, float b, float c, float d) {
+    return fmaxf(fmaxf(a, b), fmaxf(c, d));
+}
+
+// subdivide (CurveBrute.cpp:85-176) as an explicit depth-first stack (left
+// half first, as the recursion visits it). Updates bestT on a closer hit.
+__device__ __forceinline__ bool ribbon_hit(const RayFrame& fr, float tmin, float3 P0, float3 P1, float3 P2,
+                                           float3 P3, float hw0, float hw3, float toff, float tscale,
+                                           float& bestT, float& tSeg, float3& tang) {
+    SubSeg st[8];
+    int sp = 0;
+    st[sp++] = SubSeg{P0, P1, P2, P3, hw0, hw3, toff, tscale, 6};
+    bool hit = false;
+    while (sp > 0) {
+        SubSeg s = st[--sp];
+        float3 c0 = project(fr, s.P0), c1 = project(fr, s.P1), c2 = project(fr, s.P2),
+               c3 = project(fr, s.P3);
+        float maxHalfW = fmaxf(s.hw0, s.hw3);
+        float zMin = min4(c0.z, c1.z, c2.z, c3.z), zMax = max4(c0.z, c1.z, c2.z, c3.z);
+        if (xsub(zMin, maxHalfW) > bestT) continue;
+        if (xadd(zMax, maxHalfW) < tmin) continue;
+        float xMin = min4(c0.x, c1.x, c2.x, c3.x), xMax = max4(c0.x, c1.x, c2.x, c3.x);
+        float yMin = min4(c0.y, c1.y, c2.y, c3.y), yMax = max4(c0.y, c1.y, c2.y, c3.y);
+        float cx = (0.f < xMin) ? xMin : (0.f > xMax ? xMax : 0.f);
+        float cy = (0.f < yMin) ? yMin : (0.f > yMax ? yMax : 0.f);
+        if (xadd(xmul(cx, cx), xmul(cy, cy)) > xmul(maxHalfW, maxHalfW)) continue;
+        if (s.depth == 0) {
+            float ax = c0.x, ay = c0.y, bx = c3.x, by = c3.y;
+            float dx = xsub(bx, ax), dy = xsub(by, ay);
+            float lenSq = xadd(xmul(dx, dx), xmul(dy, dy));
+            float tLine;
+            if (lenSq < 1e-12f) tLine = 0.f;
+            else
+                tLine = fmaxf(0.f, fminf(1.f, xdiv(xsub(xmul(-ax, dx), xmul(ay, dy)), lenSq)));
+            float px = xadd(ax, xmul(dx, tLine)), py = xadd(ay, xmul(dy, tLine));
+            float dist2 = xadd(xmul(px, px), xmul(py, py));
+            float halfW = xadd(xmul(s.hw0, xsub(1.f, tLine)), xmul(s.hw3, tLine));
+            if (dist2 > xmul(halfW, halfW)) continue;
+            float tRay = xadd(c0.z, xmul(xsub(c3.z, c0.z), tLine));
+            if (tRay < tmin || tRay >= bestT) continue;
+            float3 tg = bezier_tangent(s.P0, s.P1, s.P2, s.P3, tLine);
+            if (xdot(tg, tg) < 1e-12f) tg = xsub3(s.P3, s.P0);
+            float len = __fsqrt_rn(xdot(tg, tg));
+            tg = len > 1e-8f ? xmul3(tg, xdiv(1.f, len)) : f3(0.f, 0.f, 1.f);
+            bestT = tRay;
+            tSeg = xadd(s.toff, xmul(tLine, s.tscale));
+            tang = tg;
+            hit = true;
+            continue;
+        }
+        // bezierSplitMid (CurveBrute.cpp:66-80)
+        float3 Q01 = xmid(s.P0, s.P1), Q12 = xmid(s.P1, s.P2), Q23 = xmid(s.P2, s.P3);
+        float3 R01 = xmid(Q01, Q12), R12 = xmid(Q12, Q23), M = xmid(R01, R12);
+        float hwMid = xmul(xadd(s.hw0, s.hw3), 0.5f);
+        float tsh = xmul(s.tscale, 0.5f);
+        st[sp++] = SubSeg{M, R12, Q23, s.P3, hwMid, s.hw3, xadd(s.toff, tsh), tsh, s.depth - 1};
+        st[sp++] = SubSeg{s.P0, Q01, R01, M, s.hw0, hwMid, s.toff, tsh, s.depth - 1};
+    }
+    return hit;
+}
+
+struct CurveHit {
+    int32_t seg;   // leaf-order segment index, -1 if none
+    float t, tSeg;
+    float3 tang;
+};
+
+// Curve BVH pass of CurveBrute::trace (CurveBrute.cpp:398-440): starts from the
+// triangle hit distance and keeps only strictly closer ribbon hits.
+__device__ __forceinline__ CurveHit trace_curves(const DevScene& S, const Ray& ray, float bestT,
+                                                 bool anyHit, uint32_t* err) {
+    CurveHit ch{-1, bestT, 0.f, f3(0.f, 0.f, 0.f)};
+    if (S.num_seg_nodes == 0) return ch;
+    RayFrame fr = make_frame(ray);
+    float3 inv = f3(xdiv(1.f, ray.d.x), xdiv(1.f, ray.d.y), xdiv(1.f, ray.d.z));
+    uint32_t stack[kMaxStack];
+    float stackT[kMaxStack];
+    int sp = 0;
+    uint32_t cur = 0;
+    while (true) {
+        if (!(cur & 0x80000000u)) {
+            const float4* np = reinterpret_cast<const float4*>(S.seg_nodes + cur);
+            float4 n0 = ldg4(np), n1 = ldg4(np + 1), n2 = ldg4(np + 2), n3 = ldg4(np + 3);
+            float tn0 = 0.f, tn1 = 0.f;
+            bool h0 = curve_box_hit(ray, inv, n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, ch.t, tn0);
+            bool h1 = curve_box_hit(ray, inv, n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, ch.t, tn1);
+            uint32_t c0 = fbits_u(n3.z) ? leaf_entry(fbits_u(n3.x), fbits_u(n3.z)) : fbits_u(n3.x);
+            uint32_t c1 = fbits_u(n3.w) ? leaf_entry(fbits_u(n3.y), fbits_u(n3.w)) : fbits_u(n3.y);
+            if (h0 && h1) {
+                bool swap = !(tn0 < tn1);
+                if (sp >= int(kMaxStack)) { atomicOr(err, 1u); return ch; }
+                stack[sp] = swap ? c0 : c1;
+                stackT[sp] = swap ? tn0 : tn1;
+                ++sp;
+                cur = swap ? c1 : c0;
+                continue;
+            } else if (h0 || h1) {
+                cur = h0 ? c0 : c1;
+                continue;
+            }
+        } else {
+            uint32_t off = cur & 0x01FFFFFFu, c = ((cur >> 25) & 63u) + 1u;
+            for (uint32_t i = off; i < off + c; ++i) {
+                const float4* sp4 = S.segs + 5 * size_t(i);
+                float4 a = ldg4(sp4), b = ldg4(sp4 + 1), e = ldg4(sp4 + 2), g = ldg4(sp4 + 3);
+                float ts;
+                float3 tg;
+                float bt = ch.t;
+                if (ribbon_hit(fr, ray.tmin, f3(a), f3(b), f3(e), f3(g), a.w, b.w, e.w, g.w, bt, ts, tg)) {
+                    ch.seg = int32_t(i);
+                    ch.t = bt;
+                    ch.tSeg = ts;
+                    ch.tang = tg;
+                    if (anyHit) return ch;
+                }
+            }
+        }
+        bool found = false;
+        while (sp > 0) {
+            --sp;
+            if (stackT[sp] > ch.t) continue;
+            cur = stack[sp];
+            found = true;
+            break;
+        }
+        if (!found) break;
+    }
+    return ch;
+}
+
+}  // namespace ana

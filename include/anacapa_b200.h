@@ -1,0 +1,269 @@
+/*
+ * anacapa_b200 — C ABI of the B200 path-tracing hot path.
+ *
+ * This is the boundary a host renderer binds. Every entry point returns an
+ * int status (ANA_OK = 0); no C++ exception crosses it. All pointers are plain
+ * host pointers unless a parameter says otherwise; the library copies what it
+ * needs and the caller keeps ownership of every array it passes in.
+ *
+ * Each declaration names the reference interface it replaces (paths relative
+ * to the nhaflinger/anacapa source tree).
+ *
+ * Threading: one ana_ctx per host thread, one CUDA stream per context; calls
+ * on one context are serialised by the caller (the reference calls
+ * IIntegrator::renderFrame from its main thread only,
+ * src/render/RenderSession.cpp:541).
+ */
+#ifndef ANACAPA_B200_H
+#define ANACAPA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+enum {
+    ANA_OK = 0,
+    ANA_ERR_INVALID_ARG = 1,   /* bad pointer, size, index or enum            */
+    ANA_ERR_CUDA = 2,          /* a CUDA runtime call failed                   */
+    ANA_ERR_OOM = 3,           /* device allocation failed                     */
+    ANA_ERR_TIMEOUT = 4,       /* a device-side bounded wait gave up           */
+    ANA_ERR_UNSUPPORTED = 5,   /* feature outside the implemented path         */
+    ANA_ERR_STATE = 6,         /* call out of order (e.g. render before scene) */
+    ANA_ERR_DEVICE_CHECK = 7   /* a device bounds check tripped (stack, index) */
+};
+
+/* ---- materials (src/shading/*.h) ----------------------------------------- */
+enum {
+    ANA_MAT_LAMBERT = 0,   /* LambertianMaterial  src/shading/Lambertian.h:29-82        */
+    ANA_MAT_EMISSIVE = 1,  /* EmissiveMaterial    src/shading/Lambertian.h:88-99        */
+    ANA_MAT_STANDARD = 2,  /* StandardSurfaceMaterial src/shading/StandardSurface.h:115 */
+    ANA_MAT_HAIR = 3       /* MarschnerHairMaterial src/shading/MarschnerHair.h:190     */
+};
+
+/* Hair evaluation mode. The reference's MarschnerHairMaterial::evaluate/sample
+ * return the Kajiya-Kay lobe before reaching the Marschner code
+ * (src/shading/MarschnerHair.h:240, 267-282); KAJIYA_KAY reproduces what the
+ * reference executes, MARSCHNER evaluates the R/TT/TRT lobes it defines. */
+enum { ANA_HAIR_KAJIYA_KAY = 0, ANA_HAIR_MARSCHNER = 1 };
+
+typedef struct ana_material {
+    uint32_t type;
+    /* Lambert / Emissive */
+    float albedo[3];
+    float emission[3];
+    /* standard_surface, StandardSurfaceMaterial::Params (StandardSurface.h:117-148);
+     * constant values only (evalTOV's non-texture branch, Texture.cpp:126-136) */
+    float base_color[3];
+    float base;
+    float metalness;
+    float roughness;
+    float specular;
+    float specular_color[3];
+    float specular_ior;
+    float coat;
+    float coat_roughness;
+    float transmission;    /* must be <= 0.001: glass is outside the implemented path */
+    float emission_weight; /* Params::emission */
+    float emission_color[3];
+    uint32_t alpha_mask;   /* must be 0 */
+    /* hair, MarschnerHairMaterial::Params (MarschnerHair.h:192-198) */
+    float eta;
+    float sigma_a[3];
+    float beta_m;
+    float beta_n;
+    float alpha_deg;
+    uint32_t hair_mode;    /* ANA_HAIR_* */
+} ana_material;
+
+/* ---- lights (include/anacapa/shading/ILight.h) ----------------------------- */
+enum {
+    ANA_LIGHT_AREA = 0,  /* AreaLight src/shading/lights/AreaLight.h:17-125: quad centre,
+                            half-extent axes u and v, radiance Le                     */
+    ANA_LIGHT_DOME = 1   /* DomeLight src/shading/lights/DomeLight.h:205: the scene's
+                            equirect environment (ana_scene_desc.env_*)               */
+};
+
+typedef struct ana_light {
+    uint32_t type;
+    float center[3];
+    float u[3];
+    float v[3];
+    float Le[3];
+} ana_light;
+
+/* ---- camera (Camera, include/anacapa/integrator/IIntegrator.h:27-144) ------ */
+typedef struct ana_camera {
+    float from[3];
+    float at[3];
+    float up[3];
+    float vfov_deg;
+    float aperture_radius;  /* 0 = pinhole (Camera::makePinhole)                  */
+    float focal_distance;   /* thin lens (Camera::makeThinLens) when aperture > 0 */
+    float shutter_open;
+    float shutter_close;
+} ana_camera;
+
+/* ---- scene (GeometryPool + CurvePool + SceneView) ------------------------- */
+typedef struct ana_scene_desc {
+    /* Triangle meshes (MeshDesc, include/anacapa/accel/GeometryPool.h:28-77),
+     * concatenated. Mesh i owns vertices [mesh_vert_offset[i], mesh_vert_offset[i+1])
+     * and triangles [mesh_tri_offset[i], mesh_tri_offset[i+1]); indices are local to
+     * the mesh's vertex range. meshID = i, primID = triangle index within the mesh. */
+    uint32_t num_meshes;
+    const uint32_t* mesh_vert_offset;  /* num_meshes + 1 */
+    const uint32_t* mesh_tri_offset;   /* num_meshes + 1 */
+    const uint8_t* mesh_has_normals;   /* num_meshes; 0 = geometric normal everywhere */
+    const float* positions;            /* 3 per vertex, world space (static meshes)   */
+    const float* normals;              /* 3 per vertex (read where has_normals)       */
+    const uint32_t* indices;           /* 3 per triangle                               */
+
+    /* Hair strands (StrandDesc, include/anacapa/accel/CurvePool.h:27-55). */
+    uint32_t num_strands;
+    const uint32_t* strand_cp_offset;    /* num_strands + 1 */
+    const float* control_points;         /* 3 per CV; segment k uses CVs 3k..3k+3 */
+    const uint32_t* strand_width_offset; /* num_strands + 1 */
+    const float* widths;                 /* diameters, StrandDesc::widthAt rules */
+    const uint32_t* strand_slot;         /* StrandDesc::materialIndex            */
+    const float* strand_color;           /* 3 per strand                          */
+
+    /* SceneView::materials: slot -> material (index into materials, -1 = none).
+     * Indexed by meshID and by StrandDesc::materialIndex. */
+    uint32_t num_materials;
+    const ana_material* materials;
+    uint32_t num_slots;
+    const int32_t* slot_material;
+
+    /* SceneView::lights in order (the integrator picks one uniformly). */
+    uint32_t num_lights;
+    const ana_light* lights;
+
+    /* SceneView::envLight: equirect RGB float, row 0 = zenith (DomeLight.h:190-201).
+     * env_rgb == NULL: constant SceneView::envRadiance. */
+    const float* env_rgb;
+    uint32_t env_width;
+    uint32_t env_height;
+    float env_intensity;
+    float env_radiance[3];
+
+    ana_camera camera;
+
+    /* BVH build: maximum triangles / curve segments per leaf (reference: 4,
+     * BVHBackend.h:67, CurveBrute.cpp:455). 0 = default. */
+    uint32_t max_leaf_tris;
+    uint32_t max_leaf_segments;
+} ana_scene_desc;
+
+/* ---- render ---------------------------------------------------------------- */
+typedef struct ana_render_desc {
+    uint32_t width;        /* film size (filmWidth, filmHeight)                     */
+    uint32_t height;
+    uint32_t sample_start; /* first sample index (TileRequest::sampleStart)         */
+    uint32_t sample_count; /* samples per pixel this call (TileRequest::sampleCount)*/
+    uint32_t max_depth;    /* PathIntegrator(maxDepth), PathIntegrator.h:24          */
+    uint32_t min_depth;    /* Russian roulette from this bounce (reference: 2)      */
+    uint64_t seed;         /* HaltonSampler seed (RenderSession uses 0)             */
+    uint32_t flags;        /* ANA_RENDER_* */
+} ana_render_desc;
+
+enum {
+    ANA_RENDER_CLEAR_FILM = 1u << 0  /* zero the film before accumulating */
+};
+
+/* One device-resident film pixel: the reference's PixelAccumulator
+ * (include/anacapa/film/Film.h:24-56): pre-weighted r, g, b, weight, and
+ * sum of luminance(sample)^2. */
+typedef struct ana_film_pixel {
+    float r, g, b, w, sum_lum_sq;
+} ana_film_pixel;
+
+/* Closest-hit record of ana_trace_batch (SurfaceInteraction ids,
+ * include/anacapa/accel/IAccelerationStructure.h:12-30). */
+typedef struct ana_hit {
+    int32_t hit;        /* 1 hit, 0 miss (occlusion queries: 1 = occluded)   */
+    int32_t mesh_id;    /* meshID, or the strand's material slot for curves   */
+    int32_t prim_id;    /* triangle index in its mesh, or curve segment index */
+    int32_t strand_id;  /* -1 for triangles                                    */
+    float t;
+    float u, v;         /* barycentrics (triangles) / strand parameter (curves)*/
+    float pad;
+} ana_hit;
+
+typedef struct ana_stats {
+    uint64_t paths;             /* camera paths traced by the last render     */
+    uint64_t extend_rays;       /* closest-hit continuation rays              */
+    uint64_t shadow_rays;       /* NEE shadow rays                            */
+    uint64_t mis_rays;          /* BSDF-sampled MIS rays toward lights         */
+    float render_ms;            /* device time of the last render (CUDA events)*/
+    float extend_ms, shade_ms, shadow_ms, mis_ms, film_ms; /* per-stage totals  */
+    uint32_t bounces;           /* wavefront iterations of the last render      */
+    uint32_t chunks;            /* path chunks of the last render               */
+} ana_stats;
+
+typedef struct ana_ctx ana_ctx;
+
+typedef struct ana_device_opts {
+    int device;              /* CUDA ordinal                                   */
+    uint32_t chunk_paths;    /* wavefront capacity in paths (0 = default)      */
+    uint32_t block_size;     /* threads per block of the stage kernels (0 = default) */
+    uint32_t timing;         /* 1: record per-stage CUDA-event times           */
+} ana_device_opts;
+
+/* Create a context on a device. Replaces CudaPathIntegrator's constructor /
+ * CudaContext (src/gpu/cuda/CudaContext.cu:37-58). */
+int ana_create(ana_ctx** out, const ana_device_opts* opts);
+void ana_destroy(ana_ctx* ctx);
+
+/* Copy a scene to the device and build its BVHs on the host with the
+ * reference's algorithms (triangle SAH BVH, BVHBackend::commit,
+ * src/accel/BVHBackend.cpp:17-228; curve median-split BVH,
+ * src/accel/CurveBrute.cpp:247-396). Replaces IIntegrator::prepare
+ * (include/anacapa/integrator/IIntegrator.h:177) + IAccelerationStructure::commit. */
+int ana_upload_scene(ana_ctx* ctx, const ana_scene_desc* scene);
+
+/* Host-side scene preparation split from the device copy, so a caller can
+ * build once and re-upload: ana_prepare_scene builds the device layout on the
+ * host; ana_upload_prepared copies it (host -> device) into the context. */
+typedef struct ana_prepared ana_prepared;
+int ana_prepare_scene(const ana_scene_desc* scene, ana_prepared** out);
+int ana_upload_prepared(ana_ctx* ctx, const ana_prepared* prep);
+uint64_t ana_prepared_bytes(const ana_prepared* prep);
+void ana_prepared_free(ana_prepared* prep);
+
+/* Render sample_count samples per pixel of the whole frame into the
+ * device-resident film (adds, as Film::mergeTile does). Replaces
+ * IIntegrator::renderFrame (IIntegrator.h:192-197) for PathIntegrator
+ * (src/integrator/PathIntegrator.cpp:8-265). */
+int ana_render(ana_ctx* ctx, const ana_render_desc* desc);
+
+/* Zero / read back the device film (width*height ana_film_pixel, row 0 = top). */
+int ana_film_clear(ana_ctx* ctx, uint32_t width, uint32_t height);
+int ana_film_read(ana_ctx* ctx, ana_film_pixel* host_out, size_t count);
+/* Device pointer of the film, for callers that keep the result on the GPU. */
+int ana_film_device_ptr(ana_ctx* ctx, void** dptr);
+
+/* Batched closest-hit / occlusion queries. rays: n x 8 floats
+ * (ox, oy, oz, tmin, dx, dy, dz, tmax). Replaces
+ * IAccelerationStructure::traceBatch / occludedBatch
+ * (include/anacapa/accel/IAccelerationStructure.h:75-87) over CurveBrute
+ * (src/accel/CurveBrute.cpp:398-476). rays_on_device != 0: rays and out are
+ * device pointers. */
+int ana_trace_batch(ana_ctx* ctx, const float* rays, size_t n, ana_hit* out, int occlusion_only,
+                    int rays_on_device);
+
+int ana_get_stats(ana_ctx* ctx, ana_stats* out);
+
+/* Copy the last error message of this context (or of the last failed
+ * context-less call when ctx is NULL) into buf. */
+int ana_last_error(ana_ctx* ctx, char* buf, size_t len);
+
+/* Library/ABI version: major * 10000 + minor * 100 + patch. */
+int ana_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ANACAPA_B200_H */

@@ -1,0 +1,497 @@
+// ============================================================================
+// TEST INFRASTRUCTURE — NOT PART OF THE PRODUCT.
+//
+// A C harness over the reference renderer's own hot-path classes. It is linked
+// with the reference's unmodified sources (src/accel/BVHBackend.cpp,
+// src/accel/CurveBrute.cpp, src/integrator/PathIntegrator.cpp and the
+// header-only materials, lights, sampler and thread pool) by oracle/Makefile
+// into oracle/_ref/. Only tests/, __graft_entry__.smoke() and bench.py's CPU
+// baseline leg load it, as the checker and as the timed CPU baseline.
+//
+// What this file supplies on its own:
+//   * evalTOV (src/shading/Texture.cpp:126-136): the constant-value branch
+//     only; image textures need OpenImageIO, which is absent, and no workload
+//     uses them.
+//   * DomeLight::loadImage (src/shading/lights/DomeLight.cpp:15-107): instead
+//     of reading a file it copies an in-memory RGB float equirect that the
+//     caller registered; DomeLight::buildDistribution then runs unchanged.
+//   * the frame driver: RenderSession::render's non-adaptive CPU branch
+//     (src/render/RenderSession.cpp:465-547) — HaltonSampler(spp, seed 0),
+//     ThreadPool, 64x64 tiles, PathIntegrator::renderTile, and a merge of each
+//     TileBuffer into plain arrays with Film::mergeTile's arithmetic
+//     (src/film/Film.cpp:34-73; Film.cpp itself needs OpenImageIO).
+// ============================================================================
+#include <anacapa/core/Types.h>
+#include <anacapa/accel/GeometryPool.h>
+#include <anacapa/accel/CurvePool.h>
+#include <anacapa/integrator/IIntegrator.h>
+#include <anacapa/shading/ShadingContext.h>
+
+#include "accel/BVHBackend.h"
+#include "accel/CurveBrute.h"
+#include "integrator/PathIntegrator.h"
+#include "render/ThreadPool.h"
+#include "sampling/HaltonSampler.h"
+#include "sampling/PCGRng.h"
+#include "shading/Lambertian.h"
+#include "shading/MarschnerHair.h"
+#include "shading/StandardSurface.h"
+#include "shading/Texture.h"
+#include "shading/lights/AreaLight.h"
+#include "shading/lights/DomeLight.h"
+
+#include <chrono>
+#include <cstdint>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <vector>
+
+namespace anacapa {
+
+Spectrum evalTOV(const SpectrumTOV& t, Vec2f) { return t.value; }
+float evalTOV(const FloatTOV& t, Vec2f) { return t.value; }
+
+namespace {
+const float* g_pendingEnv = nullptr;
+uint32_t g_pendingW = 0, g_pendingH = 0;
+}  // namespace
+
+void DomeLight::loadImage(const std::string&) {
+    if (!g_pendingEnv || g_pendingW == 0 || g_pendingH == 0) return;
+    m_width = g_pendingW;
+    m_height = g_pendingH;
+    m_pixels.assign(g_pendingEnv, g_pendingEnv + size_t(m_width) * m_height * 3);
+}
+
+}  // namespace anacapa
+
+using namespace anacapa;
+
+namespace {
+
+struct RefScene {
+    GeometryPool geom;
+    CurvePool curves;
+    std::vector<std::unique_ptr<IMaterial>> mats;
+    std::vector<std::unique_ptr<ILight>> lights;
+    std::unique_ptr<CurveBrute> accel;
+    SceneView view;
+    bool committed = false;
+};
+
+Vec3f v3(const float* p) { return {p[0], p[1], p[2]}; }
+void put3(float* o, Vec3f v) { o[0] = v.x; o[1] = v.y; o[2] = v.z; }
+
+// Records the order in which the integrator draws sampler dimensions.
+class LoggingSampler : public ISampler {
+public:
+    explicit LoggingSampler(uint32_t spp) : m_inner(spp, 0) {}
+    std::unique_ptr<ISampler> clone() const override {
+        return std::make_unique<LoggingSampler>(*this);
+    }
+    void startPixelSample(uint32_t x, uint32_t y, uint32_t s) override {
+        m_inner.startPixelSample(x, y, s);
+        m_dim = 0;
+    }
+    float get1D() override {
+        log.push_back(int32_t(m_dim++));
+        return m_inner.get1D();
+    }
+    Vec2f get2D() override {
+        // Dimensions of one 2-D draw are logged as negative pairs so the
+        // caller can tell 1-D draws from 2-D draws.
+        log.push_back(-1 - int32_t(m_dim));
+        m_dim += 2;
+        return m_inner.get2D();
+    }
+    SamplerState getState() const override { return m_inner.getState(); }
+    std::vector<int32_t> log;
+
+private:
+    HaltonSampler m_inner;
+    uint32_t m_dim = 0;
+};
+
+StandardSurfaceMaterial::Params ssParams(const float* p) {
+    // Packed layout (18 floats): base_color[3], base, metalness, roughness,
+    // specular, specular_color[3], specular_IOR, coat, coat_roughness,
+    // transmission, emission, emission_color[3]
+    StandardSurfaceMaterial::Params q;
+    q.base_color = SpectrumTOV(Vec3f{p[0], p[1], p[2]});
+    q.base = p[3];
+    q.metalness = FloatTOV(p[4]);
+    q.roughness = FloatTOV(p[5]);
+    q.specular = FloatTOV(p[6]);
+    q.specular_color = {p[7], p[8], p[9]};
+    q.specular_IOR = p[10];
+    q.coat = p[11];
+    q.coat_roughness = p[12];
+    q.transmission = p[13];
+    q.emission = p[14];
+    q.emission_color = SpectrumTOV(Vec3f{p[15], p[16], p[17]});
+    return q;
+}
+
+SurfaceInteraction makeSI(const float* s) {
+    // s: p[3], n[3], ng[3], dpdu[3], color[3], isCurve
+    SurfaceInteraction si;
+    si.p = v3(s + 0);
+    si.n = v3(s + 3);
+    si.ng = v3(s + 6);
+    si.dpdu = v3(s + 9);
+    si.color = v3(s + 12);
+    si.isCurve = s[15] != 0.f;
+    return si;
+}
+
+}  // namespace
+
+extern "C" {
+
+void* ref_scene_new() { return new RefScene(); }
+void ref_scene_free(void* s) { delete static_cast<RefScene*>(s); }
+
+int ref_add_mesh(void* sp, const float* pos, const float* nrm, const float* uv,
+                 uint32_t nv, const uint32_t* idx, uint32_t ntri) {
+    auto* s = static_cast<RefScene*>(sp);
+    MeshDesc m;
+    m.positions.resize(nv);
+    for (uint32_t i = 0; i < nv; ++i) m.positions[i] = v3(pos + 3 * i);
+    if (nrm) {
+        m.normals.resize(nv);
+        for (uint32_t i = 0; i < nv; ++i) m.normals[i] = v3(nrm + 3 * i);
+    }
+    if (uv) {
+        m.uvs.resize(nv);
+        for (uint32_t i = 0; i < nv; ++i) m.uvs[i] = {uv[2 * i], uv[2 * i + 1]};
+    }
+    m.indices.assign(idx, idx + size_t(ntri) * 3);
+    return int(s->geom.addMesh(std::move(m)));
+}
+
+int ref_add_strand(void* sp, const float* cps, uint32_t ncp, const float* widths,
+                   uint32_t nw, uint32_t matSlot, const float* color) {
+    auto* s = static_cast<RefScene*>(sp);
+    StrandDesc d;
+    d.controlPoints.resize(ncp);
+    for (uint32_t i = 0; i < ncp; ++i) d.controlPoints[i] = v3(cps + 3 * i);
+    d.widths.assign(widths, widths + nw);
+    d.materialIndex = matSlot;
+    if (color) d.color = v3(color);
+    return int(s->curves.addStrand(std::move(d)));
+}
+
+int ref_mat_lambert(void* sp, const float* albedo) {
+    auto* s = static_cast<RefScene*>(sp);
+    s->mats.push_back(std::make_unique<LambertianMaterial>(v3(albedo)));
+    return int(s->mats.size() - 1);
+}
+
+int ref_mat_emissive(void* sp, const float* albedo, const float* emission) {
+    auto* s = static_cast<RefScene*>(sp);
+    s->mats.push_back(std::make_unique<EmissiveMaterial>(v3(albedo), v3(emission)));
+    return int(s->mats.size() - 1);
+}
+
+int ref_mat_standard(void* sp, const float* packed18) {
+    auto* s = static_cast<RefScene*>(sp);
+    s->mats.push_back(std::make_unique<StandardSurfaceMaterial>(ssParams(packed18)));
+    return int(s->mats.size() - 1);
+}
+
+int ref_mat_marschner(void* sp, float eta, const float* sigma_a, float beta_m,
+                      float beta_n, float alpha_deg) {
+    auto* s = static_cast<RefScene*>(sp);
+    MarschnerHairMaterial::Params p;
+    p.eta = eta;
+    p.sigma_a = v3(sigma_a);
+    p.beta_m = beta_m;
+    p.beta_n = beta_n;
+    p.alpha = alpha_deg;
+    s->mats.push_back(std::make_unique<MarschnerHairMaterial>(p));
+    return int(s->mats.size() - 1);
+}
+
+// SceneView::materials is indexed by meshID (and by StrandDesc::materialIndex).
+void ref_set_slot(void* sp, uint32_t slot, int matHandle) {
+    auto* s = static_cast<RefScene*>(sp);
+    if (s->view.materials.size() <= slot) s->view.materials.resize(slot + 1, nullptr);
+    s->view.materials[slot] = matHandle >= 0 ? s->mats[size_t(matHandle)].get() : nullptr;
+}
+
+int ref_light_area(void* sp, const float* c, const float* u, const float* v, const float* Le) {
+    auto* s = static_cast<RefScene*>(sp);
+    s->lights.push_back(std::make_unique<AreaLight>(v3(c), v3(u), v3(v), v3(Le)));
+    s->view.lights.push_back(s->lights.back().get());
+    return int(s->lights.size() - 1);
+}
+
+// Dome light: registered as SceneView::envLight and appended to the light list,
+// as RenderSession::render does (src/render/RenderSession.cpp:407-422).
+int ref_light_dome(void* sp, const float* rgb, uint32_t w, uint32_t h, float intensity,
+                   int inLightList) {
+    auto* s = static_cast<RefScene*>(sp);
+    g_pendingEnv = rgb;
+    g_pendingW = w;
+    g_pendingH = h;
+    auto dome = std::make_unique<DomeLight>(rgb ? std::string("mem") : std::string(),
+                                            intensity, 10.f, Vec3f{});
+    g_pendingEnv = nullptr;
+    s->view.envLight = dome.get();
+    if (inLightList) s->view.lights.push_back(dome.get());
+    s->lights.push_back(std::move(dome));
+    return int(s->lights.size() - 1);
+}
+
+void ref_set_env_radiance(void* sp, const float* rgb) {
+    static_cast<RefScene*>(sp)->view.envRadiance = v3(rgb);
+}
+
+void ref_set_camera(void* sp, const float* from, const float* at, const float* up,
+                    float vfov, uint32_t w, uint32_t h) {
+    auto* s = static_cast<RefScene*>(sp);
+    s->view.camera = Camera::makePinhole(v3(from), v3(at), v3(up), vfov, w, h);
+}
+
+int ref_commit(void* sp) {
+    auto* s = static_cast<RefScene*>(sp);
+    s->accel = std::make_unique<CurveBrute>(s->geom, s->curves);
+    s->accel->commit();
+    s->view.accel = s->accel.get();
+    s->committed = true;
+    return 0;
+}
+
+// rays: n x 8 floats (ox, oy, oz, tmin, dx, dy, dz, tmax)
+// out_ids: n x 4 int32 (hit, meshID, primID, strandID); out_t: n floats
+void ref_trace(void* sp, const float* rays, uint64_t n, int32_t* out_ids, float* out_t,
+               int nthreads) {
+    auto* s = static_cast<RefScene*>(sp);
+    ThreadPool pool(uint32_t(nthreads > 0 ? nthreads : 0));
+    const uint64_t chunk = 4096;
+    uint32_t nChunks = uint32_t((n + chunk - 1) / chunk);
+    pool.parallelFor(nChunks, [&](uint32_t c) {
+        uint64_t b = uint64_t(c) * chunk, e = std::min<uint64_t>(n, b + chunk);
+        for (uint64_t i = b; i < e; ++i) {
+            const float* r = rays + 8 * i;
+            Ray ray{v3(r), v3(r + 4), r[3], r[7]};
+            TraceResult tr = s->accel->trace(ray);
+            out_ids[4 * i + 0] = tr.hit ? 1 : 0;
+            out_ids[4 * i + 1] = tr.hit ? int32_t(tr.si.meshID) : -1;
+            out_ids[4 * i + 2] = tr.hit ? int32_t(tr.si.primID) : -1;
+            out_ids[4 * i + 3] = tr.hit && tr.si.isCurve ? int32_t(tr.si.strandID) : -1;
+            out_t[i] = tr.hit ? tr.si.t : 0.f;
+        }
+    });
+}
+
+void ref_occluded(void* sp, const float* rays, uint64_t n, uint8_t* out, int nthreads) {
+    auto* s = static_cast<RefScene*>(sp);
+    ThreadPool pool(uint32_t(nthreads > 0 ? nthreads : 0));
+    const uint64_t chunk = 4096;
+    uint32_t nChunks = uint32_t((n + chunk - 1) / chunk);
+    pool.parallelFor(nChunks, [&](uint32_t c) {
+        uint64_t b = uint64_t(c) * chunk, e = std::min<uint64_t>(n, b + chunk);
+        for (uint64_t i = b; i < e; ++i) {
+            const float* r = rays + 8 * i;
+            Ray ray{v3(r), v3(r + 4), r[3], r[7]};
+            out[i] = s->accel->occluded(ray) ? 1 : 0;
+        }
+    });
+}
+
+// Non-adaptive frame render of the pixel rectangle [x0,x1) x [y0,y1) through the
+// reference's ThreadPool and PathIntegrator::renderTile, 64x64 tiles.
+// out_rgbw: W*H*4 (pre-weighted r,g,b and weight, as Film's accumulators hold),
+// out_lumsq: W*H. Only pixels inside the rectangle are written (added to).
+// Returns the render wall time in seconds (scene build excluded).
+double ref_render(void* sp, uint32_t W, uint32_t H, uint32_t spp, uint32_t sampleStart,
+                  uint32_t maxDepth, int nthreads, uint32_t x0, uint32_t y0, uint32_t x1,
+                  uint32_t y1, float* out_rgbw, float* out_lumsq) {
+    auto* s = static_cast<RefScene*>(sp);
+    PathIntegrator integ(maxDepth);
+    integ.prepare(s->view);
+    HaltonSampler base(spp);
+    ThreadPool pool(uint32_t(nthreads > 0 ? nthreads : 0));
+    std::vector<TileRequest> tiles;
+    const uint32_t ts = 64;
+    for (uint32_t y = y0; y < y1; y += ts)
+        for (uint32_t x = x0; x < x1; x += ts)
+            tiles.push_back({x, y, std::min(ts, x1 - x), std::min(ts, y1 - y), sampleStart, spp});
+    std::mutex mu;
+    auto t0 = std::chrono::steady_clock::now();
+    pool.parallelFor(uint32_t(tiles.size()), [&](uint32_t ti) {
+        const TileRequest& t = tiles[ti];
+        auto sampler = base.clone();
+        TileBuffer tb(t.x0, t.y0, t.width, t.height);
+        integ.renderTile(s->view, t, W, H, *sampler, tb);
+        std::lock_guard<std::mutex> lk(mu);
+        for (uint32_t ty = 0; ty < t.height; ++ty)
+            for (uint32_t tx = 0; tx < t.width; ++tx) {
+                size_t fi = size_t(t.y0 + ty) * W + (t.x0 + tx);
+                size_t li = size_t(ty) * t.width + tx;
+                const auto& px = tb.pixels[li];
+                if (px.weight > 0.f) {
+                    out_rgbw[4 * fi + 0] += px.r;
+                    out_rgbw[4 * fi + 1] += px.g;
+                    out_rgbw[4 * fi + 2] += px.b;
+                    out_rgbw[4 * fi + 3] += px.weight;
+                    out_lumsq[fi] += tb.sumLumSq[li];
+                }
+            }
+    });
+    auto t1 = std::chrono::steady_clock::now();
+    return std::chrono::duration<double>(t1 - t0).count();
+}
+
+// Radiance of single camera samples (pixel px,py, sample index s), through a
+// 1x1 tile with sampleCount 1: the tile holds exactly the sample (0 if it was
+// not finite). out: n x 3.
+void ref_li(void* sp, uint32_t W, uint32_t H, uint32_t maxDepth, const uint32_t* pxy_s,
+            uint64_t n, float* out, int nthreads) {
+    auto* s = static_cast<RefScene*>(sp);
+    PathIntegrator integ(maxDepth);
+    integ.prepare(s->view);
+    HaltonSampler base(1);
+    ThreadPool pool(uint32_t(nthreads > 0 ? nthreads : 0));
+    pool.parallelFor(uint32_t(n), [&](uint32_t i) {
+        auto sampler = base.clone();
+        TileRequest t{pxy_s[3 * i], pxy_s[3 * i + 1], 1, 1, pxy_s[3 * i + 2], 1};
+        TileBuffer tb(t.x0, t.y0, 1, 1);
+        integ.renderTile(s->view, t, W, H, *sampler, tb);
+        out[3 * i + 0] = tb.pixels[0].r;
+        out[3 * i + 1] = tb.pixels[0].g;
+        out[3 * i + 2] = tb.pixels[0].b;
+    });
+}
+
+// Order of sampler draws for one camera sample. Entries >= 0 are 1-D draws of
+// that dimension; entries < 0 encode a 2-D draw starting at dimension -1-e.
+int ref_dim_log(void* sp, uint32_t W, uint32_t H, uint32_t maxDepth, uint32_t px, uint32_t py,
+                uint32_t sIdx, int32_t* out, int cap) {
+    auto* s = static_cast<RefScene*>(sp);
+    PathIntegrator integ(maxDepth);
+    integ.prepare(s->view);
+    LoggingSampler ls(1);
+    TileRequest t{px, py, 1, 1, sIdx, 1};
+    TileBuffer tb(px, py, 1, 1);
+    integ.renderTile(s->view, t, W, H, ls, tb);
+    int n = int(std::min<size_t>(ls.log.size(), size_t(cap)));
+    for (int i = 0; i < n; ++i) out[i] = ls.log[size_t(i)];
+    return int(ls.log.size());
+}
+
+// Camera rays exactly as PathIntegrator::renderTile builds them.
+void ref_camera_rays(void* sp, uint32_t W, uint32_t H, const uint32_t* pxy_s, uint64_t n,
+                     float* out /* n x 6 */) {
+    auto* s = static_cast<RefScene*>(sp);
+    Camera cam = s->view.camera.value_or(
+        Camera::makePinhole({0.f, 0.f, -2.5f}, {0.f, 0.f, 1.f}, {0.f, 1.f, 0.f}, 50.f, W, H));
+    HaltonSampler smp(1);
+    for (uint64_t i = 0; i < n; ++i) {
+        smp.startPixelSample(pxy_s[3 * i], pxy_s[3 * i + 1], pxy_s[3 * i + 2]);
+        Vec2f j = smp.get2D();
+        Vec2f l = smp.get2D();
+        float tu = smp.get1D();
+        Ray r = cam.generateRay(pxy_s[3 * i], pxy_s[3 * i + 1], j.x, j.y, l.x, l.y, tu);
+        put3(out + 6 * i, r.origin);
+        put3(out + 6 * i + 3, r.direction);
+    }
+}
+
+// ---- sampler -------------------------------------------------------------
+void ref_halton(uint32_t px, uint32_t py, uint32_t sampleIndex, uint64_t seed, uint32_t ndims,
+                float* out) {
+    HaltonSampler s(1, seed);
+    s.startPixelSample(px, py, sampleIndex);
+    for (uint32_t d = 0; d < ndims; ++d) out[d] = s.get1D();
+}
+
+void ref_pcg(uint64_t seed, uint32_t n, uint32_t* out) {
+    PCGRng r{seed};
+    for (uint32_t i = 0; i < n; ++i) out[i] = r.nextUint32();
+}
+
+// ---- materials (single evaluations) ----------------------------------------
+// si: see makeSI. out: f[3], pdf, pdfRev
+void ref_mat_evaluate(void* sp, int h, const float* si, const float* rayDir, const float* wo,
+                      const float* wi, float* out) {
+    auto* s = static_cast<RefScene*>(sp);
+    ShadingContext ctx(makeSI(si), v3(rayDir));
+    BSDFEval e = s->mats[size_t(h)]->evaluate(ctx, v3(wo), v3(wi));
+    put3(out, e.f);
+    out[3] = e.pdf;
+    out[4] = e.pdfRev;
+}
+
+// out: f[3], wi[3], pdf, flags
+void ref_mat_sample(void* sp, int h, const float* si, const float* rayDir, const float* wo,
+                    const float* u2, float uc, float* out) {
+    auto* s = static_cast<RefScene*>(sp);
+    ShadingContext ctx(makeSI(si), v3(rayDir));
+    BSDFSample b = s->mats[size_t(h)]->sample(ctx, v3(wo), Vec2f{u2[0], u2[1]}, uc);
+    put3(out, b.f);
+    put3(out + 3, b.wi);
+    out[6] = b.pdf;
+    out[7] = float(b.flags);
+}
+
+void ref_mat_le(void* sp, int h, const float* si, const float* rayDir, const float* wo,
+                float* out) {
+    auto* s = static_cast<RefScene*>(sp);
+    ShadingContext ctx(makeSI(si), v3(rayDir));
+    put3(out, s->mats[size_t(h)]->Le(ctx, v3(wo)));
+}
+
+float ref_ggx_D(float cosH, float alpha2) { return D_GGX(cosH, alpha2); }
+
+// ---- lights ----------------------------------------------------------------
+// out: Li[3], wi[3], pdf, dist
+void ref_light_sample(void* sp, int h, const float* p, const float* n, const float* u2,
+                      float* out) {
+    auto* s = static_cast<RefScene*>(sp);
+    LightSample ls = s->lights[size_t(h)]->sample(v3(p), v3(n), Vec2f{u2[0], u2[1]});
+    put3(out, ls.Li);
+    put3(out + 3, ls.wi);
+    out[6] = ls.pdf;
+    out[7] = ls.dist;
+}
+
+float ref_light_pdf(void* sp, int h, const float* p, const float* wi) {
+    auto* s = static_cast<RefScene*>(sp);
+    return s->lights[size_t(h)]->pdf(v3(p), v3(wi));
+}
+
+void ref_light_le(void* sp, int h, const float* wo, float* out) {
+    auto* s = static_cast<RefScene*>(sp);
+    put3(out, s->lights[size_t(h)]->Le({}, {}, v3(wo)));
+}
+
+// out: pdfPos, pdfDir, dot(dir, normal), Le[3]
+void ref_light_sample_le(void* sp, int h, const float* uPos, const float* uDir, float* out) {
+    auto* s = static_cast<RefScene*>(sp);
+    LightLeSample ls = s->lights[size_t(h)]->sampleLe({uPos[0], uPos[1]}, {uDir[0], uDir[1]});
+    out[0] = ls.pdfPos;
+    out[1] = ls.pdfDir;
+    out[2] = dot(ls.dir, ls.normal);
+    put3(out + 3, ls.Le);
+}
+
+// ---- Distribution1D ---------------------------------------------------------
+// out per u: idx, pdf, uRemapped
+void ref_dist1d(const float* vals, uint32_t n, const float* us, uint32_t nu, float* out,
+                float* integral) {
+    Distribution1D d;
+    d.build(vals, n);
+    *integral = d.integral;
+    for (uint32_t i = 0; i < nu; ++i) {
+        float pdf, ur;
+        uint32_t idx = d.sample(us[i], pdf, ur);
+        out[3 * i] = float(idx);
+        out[3 * i + 1] = pdf;
+        out[3 * i + 2] = ur;
+    }
+}
+
+}  // extern "C"
