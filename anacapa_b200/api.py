@@ -25,6 +25,7 @@ ANA_ERR_UNSUPPORTED = 5
 ANA_ERR_STATE = 6
 ANA_ERR_DEVICE_CHECK = 7
 ANA_RENDER_CLEAR_FILM = 1
+ANA_RENDER_COUNT_WORK = 2
 
 F3 = C.c_float * 3
 
@@ -86,7 +87,9 @@ class AnaStats(C.Structure):
     _fields_ = [("paths", C.c_uint64), ("extend_rays", C.c_uint64), ("shadow_rays", C.c_uint64),
                 ("mis_rays", C.c_uint64), ("render_ms", C.c_float), ("extend_ms", C.c_float),
                 ("shade_ms", C.c_float), ("shadow_ms", C.c_float), ("mis_ms", C.c_float),
-                ("film_ms", C.c_float), ("bounces", C.c_uint32), ("chunks", C.c_uint32)]
+                ("film_ms", C.c_float), ("bounces", C.c_uint32), ("chunks", C.c_uint32),
+                ("kernel_launches", C.c_uint64), ("extend_launches", C.c_uint64),
+                ("node_fetches", C.c_uint64), ("tri_tests", C.c_uint64), ("seg_tests", C.c_uint64)]
 
 
 class AnaDeviceOpts(C.Structure):
@@ -277,8 +280,8 @@ class Prepared:
 class Renderer:
     """One ana_ctx (one CUDA stream) on one device."""
 
-    def __init__(self, device=0, chunk_paths=0, block_size=0):
-        o = AnaDeviceOpts(device, chunk_paths, block_size, 0)
+    def __init__(self, device=0, chunk_paths=0, block_size=0, timing=False):
+        o = AnaDeviceOpts(device, chunk_paths, block_size, 1 if timing else 0)
         h = _P()
         check(lib().ana_create(C.byref(h), C.byref(o)))
         self.h = h
@@ -306,14 +309,15 @@ class Renderer:
             self._check(lib().ana_upload_scene(self.h, C.byref(d.desc)))
             self.scene = sc_or_prep
 
-    def render(self, width, height, spp, max_depth, sample_start=0, min_depth=2, seed=0, clear=True):
-        r = AnaRenderDesc(width, height, sample_start, spp, max_depth, min_depth, seed,
-                          ANA_RENDER_CLEAR_FILM if clear else 0)
+    def render(self, width, height, spp, max_depth, sample_start=0, min_depth=2, seed=0, clear=True,
+               count_work=False):
+        flags = (ANA_RENDER_CLEAR_FILM if clear else 0) | (ANA_RENDER_COUNT_WORK if count_work else 0)
+        r = AnaRenderDesc(width, height, sample_start, spp, max_depth, min_depth, seed, flags)
         self._check(lib().ana_render(self.h, C.byref(r)))
 
-    def render_scene(self, sc: S.Scene, spp=None, clear=True, sample_start=0, seed=0):
+    def render_scene(self, sc: S.Scene, spp=None, clear=True, sample_start=0, seed=0, count_work=False):
         self.render(sc.width, sc.height, sc.spp if spp is None else spp, sc.max_depth,
-                    sample_start=sample_start, seed=seed, clear=clear)
+                    sample_start=sample_start, seed=seed, clear=clear, count_work=count_work)
 
     def film(self, width, height) -> np.ndarray:
         """(H, W, 5) float32: pre-weighted r, g, b, weight, sum of lum^2."""

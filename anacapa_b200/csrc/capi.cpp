@@ -72,7 +72,9 @@ struct ana_ctx {
     uint32_t* d_counters = nullptr;
     size_t counters_cap = 0;
     uint32_t* d_err = nullptr;
+    unsigned long long* d_work = nullptr;  // 3 work counters (in the error-word allocation)
     std::vector<uint32_t> h_counters;
+    std::vector<cudaEvent_t> stage_ev;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     ana_stats stats{};
     int num_sms = 148;
@@ -262,6 +264,7 @@ int ana_create(ana_ctx** out, const ana_device_opts* opts) {
     void* ep = nullptr;
     if ((e = cudaMalloc(&ep, 256)) != cudaSuccess) return bail(e, "cudaMalloc(error word)");
     c->d_err = static_cast<uint32_t*>(ep);
+    c->d_work = reinterpret_cast<unsigned long long*>(static_cast<unsigned char*>(ep) + 64);
     cudaMemset(c->d_err, 0, 256);
     cudaEventCreate(&c->ev0);
     cudaEventCreate(&c->ev1);
@@ -279,6 +282,7 @@ void ana_destroy(ana_ctx* c) {
     cudaFree(c->d_queues);
     cudaFree(c->d_counters);
     cudaFree(c->d_err);
+    for (cudaEvent_t e : c->stage_ev) cudaEventDestroy(e);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -454,24 +458,50 @@ int ana_render(ana_ctx* c, const ana_render_desc* r) {
     cfg.block = c->opts.block_size ? int(c->opts.block_size) : 256;
     long long gcap = ((long long)cap + cfg.block - 1) / cfg.block;
     cfg.grid_cap = int(std::max<long long>(1, std::min<long long>(gcap, 1 << 20)));
+    const bool count_work = (r->flags & ANA_RENDER_COUNT_WORK) != 0;
+    p.work = c->d_work;
+    if (count_work) CK(cudaMemsetAsync(c->d_work, 0, 3 * sizeof(unsigned long long), c->stream), "memset work");
+    // Per-stage CUDA events (timing mode): one pair per launch, on this stream.
+    const bool timing = c->opts.timing != 0;
+    const size_t launches = size_t(nchunks) * (2 + 4 * (r->max_depth + 1));
+    if (timing && c->stage_ev.size() < 2 * launches) {
+        size_t old = c->stage_ev.size();
+        c->stage_ev.resize(2 * launches);
+        for (size_t i = old; i < c->stage_ev.size(); ++i) CK(cudaEventCreate(&c->stage_ev[i]), "event create");
+    }
+    std::vector<int> stage_of;
+    if (timing) stage_of.reserve(launches);
+    size_t ev_i = 0;
+    auto timed = [&](int stage, auto&& launch) {
+        if (timing) cudaEventRecord(c->stage_ev[2 * ev_i], c->stream);
+        launch();
+        if (timing) {
+            cudaEventRecord(c->stage_ev[2 * ev_i + 1], c->stream);
+            stage_of.push_back(stage);
+            ++ev_i;
+        }
+    };
     CK(cudaEventRecord(c->ev0, c->stream), "event");
     for (uint32_t k = 0; k < nchunks; ++k) {
         p.chunk_first_pixel = k * chunk_px;
         p.chunk_pixels = uint32_t(std::min<uint64_t>(chunk_px, npix - uint64_t(k) * chunk_px));
         p.counters = c->d_counters + size_t(k) * rows * ana::kCountersPerBounce;
         p.bounce = 0;
-        ana::launch_generate(p, cfg, c->stream);
+        timed(4, [&] { ana::launch_generate(p, cfg, c->stream); });
         for (uint32_t b = 0; b <= r->max_depth; ++b) {
             p.bounce = b;
-            ana::launch_extend(p, cfg, c->stream);
-            ana::launch_shade(p, cfg, c->stream);
-            ana::launch_shadow(p, cfg, c->stream);
-            ana::launch_mis(p, cfg, c->stream);
+            timed(0, [&] { ana::launch_extend(p, cfg, c->stream, count_work); });
+            timed(1, [&] { ana::launch_shade(p, cfg, c->stream); });
+            timed(2, [&] { ana::launch_shadow(p, cfg, c->stream); });
+            timed(3, [&] { ana::launch_mis(p, cfg, c->stream); });
         }
-        ana::launch_film(p, cfg, c->stream);
+        timed(4, [&] { ana::launch_film(p, cfg, c->stream); });
     }
     CK(cudaGetLastError(), "kernel launch");
     CK(cudaEventRecord(c->ev1, c->stream), "event");
+    unsigned long long hwork[3] = {0, 0, 0};
+    if (count_work)
+        CK(cudaMemcpyAsync(hwork, c->d_work, sizeof(hwork), cudaMemcpyDeviceToHost, c->stream), "work D2H");
     c->h_counters.resize(ncount);
     CK(cudaMemcpyAsync(c->h_counters.data(), c->d_counters, ncount * 4, cudaMemcpyDeviceToHost, c->stream),
        "counters D2H");
@@ -493,6 +523,24 @@ int ana_render(ana_ctx* c, const ana_render_desc* r) {
         }
     st.render_ms = ms;
     st.chunks = nchunks;
+    st.kernel_launches = launches;
+    st.extend_launches = size_t(nchunks) * (r->max_depth + 1);
+    st.node_fetches = hwork[0];
+    st.tri_tests = hwork[1];
+    st.seg_tests = hwork[2];
+    if (timing) {
+        float acc[5] = {0, 0, 0, 0, 0};
+        for (size_t i = 0; i < ev_i; ++i) {
+            float e = 0.f;
+            cudaEventElapsedTime(&e, c->stage_ev[2 * i], c->stage_ev[2 * i + 1]);
+            acc[stage_of[i]] += e;
+        }
+        st.extend_ms = acc[0];
+        st.shade_ms = acc[1];
+        st.shadow_ms = acc[2];
+        st.mis_ms = acc[3];
+        st.film_ms = acc[4];
+    }
     if (herr) return fail(c, ANA_ERR_DEVICE_CHECK, "ana_render: traversal stack overflow on the device");
     return ANA_OK;
 }

@@ -133,9 +133,11 @@ struct SceneHit {
     float tseg;
 };
 
-__device__ __forceinline__ SceneHit closest_hit(const DevScene& S, const Ray& r, uint32_t* err) {
+template <bool kCount = false>
+__device__ __forceinline__ SceneHit closest_hit(const DevScene& S, const Ray& r, uint32_t* err,
+                                                Counters* cnt = nullptr) {
     SceneHit h;
-    TriHit th = trace_tris<false>(S, r, err);
+    TriHit th = trace_tris<kCount>(S, r, err, cnt);
     h.t = th.t;
     h.u = th.u;
     h.v = th.v;
@@ -143,7 +145,7 @@ __device__ __forceinline__ SceneHit closest_hit(const DevScene& S, const Ray& r,
     h.tang = f3(0.f, 0.f, 0.f);
     h.tseg = 0.f;
     if (S.num_seg_nodes) {
-        CurveHit ch = trace_curves(S, r, th.tri >= 0 ? th.t : r.tmax, false, err);
+        CurveHit ch = trace_curves<kCount>(S, r, th.tri >= 0 ? th.t : r.tmax, false, err, cnt);
         if (ch.seg >= 0) {
             h.t = ch.t;
             h.prim = 0x80000000u | uint32_t(ch.seg);
@@ -162,15 +164,32 @@ __device__ __forceinline__ bool any_hit(const DevScene& S, const Ray& r, uint32_
     return false;
 }
 
+// kCount: the same traversal, counting node fetches and primitive tests
+// (warp-aggregated into p.work) to derive the stage's algorithmic bytes.
+template <bool kCount>
 __global__ void __launch_bounds__(256) k_extend(const __grid_constant__ Params p) {
     const uint32_t cur = p.bounce & 1u;
     const uint32_t n = p.counters[p.bounce * kCountersPerBounce + 0];
+    Counters cnt{0, 0, 0};
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         float4 o = p.q.ext_o[cur][i], d = p.q.ext_d[cur][i];
         Ray r{f3(o), f3(d), 1e-4f, INFINITY};
-        SceneHit h = closest_hit(p.S, r, p.err);
+        SceneHit h = closest_hit<kCount>(p.S, r, p.err, &cnt);
         p.q.hit0[i] = make_float4(h.t, __uint_as_float(h.prim), h.u, h.v);
         if (h.prim != kMiss && (h.prim & 0x80000000u)) p.q.hit1[i] = pack(h.tang, h.tseg);
+    }
+    if (kCount) {
+        unsigned long long a = cnt.nodes, b = cnt.prims, c = cnt.segs;
+        for (int off = 16; off > 0; off >>= 1) {
+            a += __shfl_down_sync(0xFFFFFFFFu, a, off);
+            b += __shfl_down_sync(0xFFFFFFFFu, b, off);
+            c += __shfl_down_sync(0xFFFFFFFFu, c, off);
+        }
+        if ((threadIdx.x & 31u) == 0) {
+            atomicAdd(p.work + 0, a);
+            atomicAdd(p.work + 1, b);
+            atomicAdd(p.work + 2, c);
+        }
     }
 }
 
@@ -459,8 +478,9 @@ static inline int blocks_for(uint32_t n, int block, int cap) {
 void launch_generate(const Params& p, const LaunchCfg& c, cudaStream_t s) {
     k_generate<<<blocks_for(p.chunk_pixels * p.spp, 256, c.grid_cap), 256, 0, s>>>(p);
 }
-void launch_extend(const Params& p, const LaunchCfg& c, cudaStream_t s) {
-    k_extend<<<c.grid_cap, c.block, 0, s>>>(p);
+void launch_extend(const Params& p, const LaunchCfg& c, cudaStream_t s, bool count_work) {
+    if (count_work) k_extend<true><<<c.grid_cap, c.block, 0, s>>>(p);
+    else k_extend<false><<<c.grid_cap, c.block, 0, s>>>(p);
 }
 void launch_shade(const Params& p, const LaunchCfg& c, cudaStream_t s) {
     k_shade<<<c.grid_cap, c.block, 0, s>>>(p);

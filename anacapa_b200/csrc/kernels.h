@@ -40,6 +40,7 @@ struct Params {
     ana_film_pixel* film;
     uint32_t* counters;  // this chunk's counters
     uint32_t* err;       // device error word (bit 0: traversal stack overflow)
+    unsigned long long* work;  // [node fetches, triangle tests, segment tests] (count mode)
     uint64_t seed;
     uint32_t W, H, spp, sample_start, max_depth, min_depth;
     uint32_t chunk_first_pixel, chunk_pixels;
@@ -52,7 +53,7 @@ struct LaunchCfg {
 };
 
 void launch_generate(const Params& p, const LaunchCfg& c, cudaStream_t s);
-void launch_extend(const Params& p, const LaunchCfg& c, cudaStream_t s);
+void launch_extend(const Params& p, const LaunchCfg& c, cudaStream_t s, bool count_work);
 void launch_shade(const Params& p, const LaunchCfg& c, cudaStream_t s);
 void launch_shadow(const Params& p, const LaunchCfg& c, cudaStream_t s);
 void launch_mis(const Params& p, const LaunchCfg& c, cudaStream_t s);

@@ -88,7 +88,7 @@ struct TriHit {
 };
 
 struct Counters {
-    uint32_t nodes, prims;
+    uint32_t nodes, prims, segs;
 };
 
 // Closest hit over the triangle BVH. Returns the nearest accepted triangle;
@@ -348,8 +348,9 @@ struct CurveHit {
 
 // Curve BVH pass of CurveBrute::trace (CurveBrute.cpp:398-440): starts from the
 // triangle hit distance and keeps only strictly closer ribbon hits.
+template <bool kCount = false>
 __device__ __forceinline__ CurveHit trace_curves(const DevScene& S, const Ray& ray, float bestT,
-                                                 bool anyHit, uint32_t* err) {
+                                                 bool anyHit, uint32_t* err, Counters* cnt = nullptr) {
     CurveHit ch{-1, bestT, 0.f, f3(0.f, 0.f, 0.f)};
     if (S.num_seg_nodes == 0) return ch;
     RayFrame fr = make_frame(ray);
@@ -362,6 +363,7 @@ __device__ __forceinline__ CurveHit trace_curves(const DevScene& S, const Ray& r
         if (!(cur & 0x80000000u)) {
             const float4* np = reinterpret_cast<const float4*>(S.seg_nodes + cur);
             float4 n0 = ldg4(np), n1 = ldg4(np + 1), n2 = ldg4(np + 2), n3 = ldg4(np + 3);
+            if (kCount) cnt->nodes++;
             float tn0 = 0.f, tn1 = 0.f;
             bool h0 = curve_box_hit(ray, inv, n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, ch.t, tn0);
             bool h1 = curve_box_hit(ray, inv, n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, ch.t, tn1);
@@ -384,6 +386,7 @@ __device__ __forceinline__ CurveHit trace_curves(const DevScene& S, const Ray& r
             for (uint32_t i = off; i < off + c; ++i) {
                 const float4* sp4 = S.segs + 5 * size_t(i);
                 float4 a = ldg4(sp4), b = ldg4(sp4 + 1), e = ldg4(sp4 + 2), g = ldg4(sp4 + 3);
+                if (kCount) cnt->segs++;
                 float ts;
                 float3 tg;
                 float bt = ch.t;

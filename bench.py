@@ -1,0 +1,339 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 path-tracing hot path.
+
+Workload (one step = one frame): the throughput scene — 4096 subdivision-3
+icospheres (5,242,880 triangles) plus a ground quad, GGX standard_surface
+materials, a 1024x512 importance-sampled HDR dome with a 0.5 deg sun — rendered
+at 1920x1080, 64 samples per pixel, max depth 12: 132,710,400 camera paths.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Prints one JSON line. `value` is path samples/s with the scene resident in HBM
+(device time from CUDA events on the library's stream, max over ranks); `e2e`
+is the same metric through the C ABI with host buffers: every step uploads
+the prepared scene from pinned host memory, renders and reads the film back.
+`--impl reference` times the reference's own CPU PathIntegrator (compiled from
+its sources into oracle/_ref) on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "path samples/s"
+UNIT = "samples/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n-spheres", type=int, default=4096)
+    ap.add_argument("--width", type=int, default=1920)
+    ap.add_argument("--height", type=int, default=1080)
+    ap.add_argument("--spp", type=int, default=64)
+    ap.add_argument("--depth", type=int, default=12)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0,
+                    help="target CPU work of the reference sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def workload_config(a, scene):
+    return {
+        "workload": (f"throughput scene: {a.n_spheres} icospheres (subdiv 3) + ground, "
+                     f"{scene.num_triangles} triangles, GGX standard_surface, 1024x512 HDR dome; "
+                     f"{a.width}x{a.height}, {a.spp} spp, max depth {a.depth}"),
+        "paths_per_step": scene.num_paths,
+        "triangles": scene.num_triangles,
+        "l2": "inputs larger than L2 (scene arrays + wavefront queues ~1.7 GB vs 126 MB L2)",
+        "sampler": "scrambled Halton seed 0",
+    }
+
+
+# ---------------------------------------------------------------------------
+def dist_setup(a):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if ws > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return ws, rank, local, pg
+
+
+def barrier(pg, local):
+    import torch
+    if torch.cuda.is_available():
+        torch.cuda.synchronize(local)
+    if pg is not None:
+        pg.barrier()
+    if torch.cuda.is_available():
+        torch.cuda.synchronize(local)
+
+
+def allreduce_max(pg, x, local):
+    if pg is None:
+        return x
+    import torch
+    dev = f"cuda:{local}" if torch.cuda.is_available() else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+class Clocks:
+    """nvidia-smi samples (every 200 ms) during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.f = None
+
+    def start(self):
+        try:
+            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+                for n, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(n)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def extend_traffic_per_ray():
+    """DRAM bytes per closest-hit ray of the extend kernel, from the committed
+    ncu summary (profiles/extend_throughput.md), or None."""
+    p = os.path.join(ROOT, "profiles", "extend_throughput.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("dram_bytes_per_ray:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+# ---------------------------------------------------------------------------
+def cpu_reference_sample(scene, target_s, steps=1, warmup=0):
+    """Time the reference's CPU PathIntegrator (oracle/_ref, flags of record)
+    through its own ThreadPool on a band of image rows at the full spp. Returns
+    (samples/s per step list, description, cores)."""
+    from oracle import refbind as R
+    if not R.available("record"):
+        R.build()
+    rs = R.RefScene(scene, variant="record")
+    W, H = scene.width, scene.height
+    cores = os.cpu_count() or 1
+    # calibrate on 2 rows in the middle of the frame
+    y0 = H // 2
+    _, _, secs = rs.render(rect=(0, y0, W, y0 + 2))
+    per_row = max(secs / 2.0, 1e-6)
+    rows = int(max(1, min(H - y0, target_s / per_row)))
+    for _ in range(warmup):
+        rs.render(rect=(0, y0, W, y0 + rows))
+    vals = []
+    for _ in range(steps):
+        _, _, secs = rs.render(rect=(0, y0, W, y0 + rows))
+        vals.append(W * rows * scene.spp / secs)
+    desc = (f"rows {y0}..{y0 + rows - 1} of the {W}x{H} frame at {scene.spp} spp "
+            f"({W * rows * scene.spp} paths), reference PathIntegrator via its ThreadPool, "
+            f"64x64 tiles, non-adaptive")
+    return vals, desc, cores
+
+
+def run_reference(a):
+    ws, rank, local, pg = dist_setup(a)
+    if rank != 0:
+        return 0
+    from anacapa_b200 import scenes as S
+    scene = S.throughput(a.width, a.height, a.spp, a.depth, n_spheres=a.n_spheres)
+    vals, desc, cores = cpu_reference_sample(scene, a.cpu_seconds, steps=a.steps, warmup=a.warmup)
+    v = statistics.mean(vals)
+    paths = scene.num_paths
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": paths / v * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded numpy scene generator)",
+        "config": workload_config(a, scene),
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "reference",
+                         "sample": desc},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(a):
+    ws, rank, local, pg = dist_setup(a)
+    import torch
+    from anacapa_b200 import api
+    from anacapa_b200 import scenes as S
+    if torch.cuda.is_available():
+        torch.cuda.set_device(local)
+    scene = S.throughput(a.width, a.height, a.spp, a.depth, n_spheres=a.n_spheres)
+    prep = api.Prepared(scene)
+    r = api.Renderer(device=local, timing=True)
+    r.upload(prep)
+    W, H, spp = scene.width, scene.height, scene.spp
+    start = rank * spp  # each rank renders its own disjoint sample range of the frame
+
+    def step():
+        r.render(W, H, spp, scene.max_depth, sample_start=start, clear=True)
+        return r.stats()
+
+    for _ in range(a.warmup):
+        step()
+    # instrumented pass (untimed): algorithmic work of the closest-hit stage
+    r.render(W, H, spp, scene.max_depth, sample_start=start, clear=True, count_work=True)
+    work = r.stats()
+    # timed region
+    clocks = Clocks(local)
+    barrier(pg, local)
+    clocks.start()
+    stats = [step() for _ in range(a.steps)]
+    barrier(pg, local)
+    ck = clocks.stop()
+    dev_ms = sum(s.render_ms for s in stats)
+    dev_ms = allreduce_max(pg, dev_ms, local)
+    ms_step = dev_ms / a.steps
+    paths_step = scene.num_paths
+    value = ws * paths_step / (ms_step / 1e3)
+    rays = sum(s.extend_rays + s.shadow_rays + s.mis_rays for s in stats) / a.steps
+    ext_ms = sum(s.extend_ms for s in stats) / a.steps
+    shade_ms = sum(s.shade_ms for s in stats) / a.steps
+    shadow_ms = sum(s.shadow_ms for s in stats) / a.steps
+    mis_ms = sum(s.mis_ms for s in stats) / a.steps
+    launches = int(sum(s.kernel_launches for s in stats))
+    # roofline of the dominant kernel (closest-hit traversal)
+    ext_launches = stats[0].extend_launches
+    alg_bytes = (64 * work.node_fetches + 48 * work.tri_tests + 80 * work.seg_tests
+                 + (32 + 16) * work.extend_rays)
+    peak, peak_kind = measured_peaks()
+    achieved = (alg_bytes / ext_launches) / ((ext_ms / ext_launches) / 1e3) / 1e9 if ext_ms > 0 else None
+    tpr = extend_traffic_per_ray()
+    traffic = (tpr * work.extend_rays / ext_launches) if tpr else None
+    # end to end through the C ABI with host buffers
+    e2e = None
+    if not a.no_e2e:
+        film = np.zeros((H, W, 5), np.float32)
+        barrier(pg, local)
+        t0 = time.perf_counter()
+        for _ in range(a.steps):
+            r.upload(prep)
+            r.render(W, H, spp, scene.max_depth, sample_start=start, clear=True)
+            api.check(api.lib().ana_film_read(r.h, film.ctypes.data, W * H), r.h)
+        t1 = time.perf_counter()
+        e2e_s = allreduce_max(pg, (t1 - t0) / a.steps, local)
+        e2e = {"value": ws * paths_step / e2e_s, "unit": UNIT,
+               "h2d_bytes_per_step": int(prep.nbytes), "d2h_bytes_per_step": int(W * H * 20)}
+    cpu = None
+    if rank == 0 and ws == 1 and not a.no_cpu_baseline:
+        try:
+            vals, desc, cores = cpu_reference_sample(scene, a.cpu_seconds)
+            cpu = {"value": vals[0], "unit": UNIT, "cores": cores, "kind": "reference", "sample": desc}
+        except Exception as e:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                   "sample": f"failed: {e}"}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded numpy scene generator)",
+            "config": workload_config(a, scene),
+            "rays_per_s": ws * rays / (ms_step / 1e3),
+            "stage_ms": {"extend": ext_ms, "shade": shade_ms, "shadow": shadow_ms, "mis": mis_ms},
+            "roofline": {"bound": "hbm", "kernel": "k_extend (closest-hit BVH traversal)",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": (achieved / peak) if achieved else None,
+                         "peak_kind": peak_kind, "traffic": traffic,
+                         "alg_bytes_per_launch": alg_bytes / ext_launches,
+                         "launches_per_step": ext_launches},
+            "gpu_launches": launches,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+            "clocks": ck,
+        }
+        print(json.dumps(line), flush=True)
+    r.close()
+    if pg is not None:
+        pg.destroy_process_group()
+    return 0
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        return run_reference(a)
+    return run_ours(a)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

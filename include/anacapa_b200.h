@@ -170,7 +170,9 @@ typedef struct ana_render_desc {
 } ana_render_desc;
 
 enum {
-    ANA_RENDER_CLEAR_FILM = 1u << 0  /* zero the film before accumulating */
+    ANA_RENDER_CLEAR_FILM = 1u << 0, /* zero the film before accumulating              */
+    ANA_RENDER_COUNT_WORK = 1u << 1  /* count BVH node fetches and primitive tests of the
+                                        closest-hit stage (instrumented, slower)        */
 };
 
 /* One device-resident film pixel: the reference's PixelAccumulator
@@ -198,9 +200,16 @@ typedef struct ana_stats {
     uint64_t shadow_rays;       /* NEE shadow rays                            */
     uint64_t mis_rays;          /* BSDF-sampled MIS rays toward lights         */
     float render_ms;            /* device time of the last render (CUDA events)*/
-    float extend_ms, shade_ms, shadow_ms, mis_ms, film_ms; /* per-stage totals  */
+    float extend_ms, shade_ms, shadow_ms, mis_ms, film_ms; /* per-stage totals
+                                   (device_opts.timing = 1), CUDA events on the
+                                   context's stream around every launch           */
     uint32_t bounces;           /* wavefront iterations of the last render      */
     uint32_t chunks;            /* path chunks of the last render               */
+    uint64_t kernel_launches;   /* kernels this library launched in the render  */
+    uint64_t extend_launches;   /* of which closest-hit (extend) launches       */
+    uint64_t node_fetches;      /* ANA_RENDER_COUNT_WORK: 64-byte BVH node loads */
+    uint64_t tri_tests;         /*   triangle tests (48 bytes each)              */
+    uint64_t seg_tests;         /*   curve segment tests (80 bytes each)         */
 } ana_stats;
 
 typedef struct ana_ctx ana_ctx;

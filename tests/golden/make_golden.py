@@ -1,0 +1,89 @@
+"""Generates the committed golden fixtures from the reference's own code.
+
+    python tests/golden/make_golden.py
+
+Runs here (where the reference tree was compiled into oracle/_ref by
+oracle/Makefile); the resulting .npz files travel with the repository, so the
+tests that read them need neither the reference tree nor a rebuild. Every
+array is produced by the reference build without FMA contraction
+(-ffp-contract=off), except where a name says `record` (the reference's
+Release flags of record).
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from anacapa_b200 import scenes as S  # noqa: E402
+from oracle import refbind as R  # noqa: E402
+
+
+def seeded_rays(seed, n, lo, hi):
+    rng = np.random.default_rng(seed)
+    o = rng.uniform(lo, hi, (n, 3))
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    r = np.zeros((n, 8), np.float32)
+    r[:, :3] = o
+    r[:, 3] = 1e-4
+    r[:, 4:7] = d
+    r[:, 7] = np.inf
+    return r
+
+
+def main():
+    R.build()
+    out = {}
+    # --- sampler: HaltonSampler (src/sampling/HaltonSampler.h) and PCG32 ---
+    pts = [(0, 0, 0), (1, 0, 0), (0, 1, 0), (17, 33, 5), (255, 255, 15), (1919, 1079, 63),
+           (640, 360, 1000), (3, 7, 123456)]
+    out["halton_pts"] = np.array(pts, np.uint32)
+    out["halton_vals"] = np.stack([R.halton(x, y, s, 140, variant="nocontract") for x, y, s in pts])
+    out["pcg_seeds"] = np.array([0, 42, 12345, 2 ** 40 + 7], np.uint64)
+    out["pcg_vals"] = np.stack([R.pcg(int(s), 16, variant="nocontract") for s in out["pcg_seeds"]])
+    # --- Distribution1D (DomeLight.h:146-182), the reference unit test's input ---
+    us = np.linspace(0.0, 0.999, 64).astype(np.float32)
+    d, integ = R.dist1d([1.0, 3.0, 2.0, 4.0], us, variant="nocontract")
+    out["dist_u"] = us
+    out["dist_out"] = d
+    out["dist_integral"] = np.float32(integ)
+    # --- closest-hit ids on the Cornell scene (1024 seeded rays) ---
+    sc = S.cornell()
+    rays = seeded_rays(7, 1024, 0.0, 1.0)
+    rs = R.RefScene(sc, variant="nocontract")
+    ids, t = rs.trace(rays, nthreads=1)
+    out["cornell_rays"] = rays
+    out["cornell_ids"] = ids
+    out["cornell_t"] = t
+    occ_rays = rays.copy()
+    occ_rays[:, 7] = 0.5
+    out["cornell_occ"] = rs.occluded(occ_rays, nthreads=1)
+    # --- camera rays and per-sample radiance on Cornell (PathIntegrator::Li) ---
+    q = np.array([[x, y, s] for x, y in [(128, 128), (40, 200), (200, 60), (90, 30), (150, 230)]
+                  for s in range(8)], np.uint32)
+    out["cornell_li_q"] = q
+    out["cornell_li"] = rs.li(q, nthreads=1)
+    out["cornell_cam"] = rs.camera_rays(q)
+    # --- hair scene: closest-hit ids (small strand count) ---
+    hs = S.hair(width=64, height=36, spp=1, n_strands=2000)
+    hrays = seeded_rays(11, 1024, -1.6, 1.6)
+    hr = R.RefScene(hs, variant="nocontract")
+    hid, ht = hr.trace(hrays, nthreads=1)
+    out["hair_rays"] = hrays
+    out["hair_ids"] = hid
+    out["hair_t"] = ht
+    # --- a small Cornell film at 4 spp (renderTile + merge) ---
+    small = S.cornell(width=32, height=32, spp=4)
+    sr = R.RefScene(small, variant="nocontract")
+    rgbw, lsq, _ = sr.render(nthreads=1)
+    out["cornell32_rgbw"] = rgbw
+    out["cornell32_lumsq"] = lsq
+    np.savez_compressed(os.path.join(HERE, "reference_vectors.npz"), **out)
+    print("wrote", os.path.join(HERE, "reference_vectors.npz"))
+
+
+if __name__ == "__main__":
+    main()
