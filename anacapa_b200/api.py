@@ -26,6 +26,9 @@ ANA_ERR_STATE = 6
 ANA_ERR_DEVICE_CHECK = 7
 ANA_RENDER_CLEAR_FILM = 1
 ANA_RENDER_COUNT_WORK = 2
+ANA_TRAVERSAL_DEFAULT = 0
+ANA_TRAVERSAL_PERSISTENT = 1
+ANA_TRAVERSAL_PER_RAY = 2
 
 F3 = C.c_float * 3
 
@@ -94,7 +97,7 @@ class AnaStats(C.Structure):
 
 class AnaDeviceOpts(C.Structure):
     _fields_ = [("device", C.c_int), ("chunk_paths", C.c_uint32), ("block_size", C.c_uint32),
-                ("timing", C.c_uint32)]
+                ("timing", C.c_uint32), ("traversal", C.c_uint32)]
 
 
 HIT_DTYPE = np.dtype([("hit", "<i4"), ("mesh_id", "<i4"), ("prim_id", "<i4"),
@@ -280,8 +283,8 @@ class Prepared:
 class Renderer:
     """One ana_ctx (one CUDA stream) on one device."""
 
-    def __init__(self, device=0, chunk_paths=0, block_size=0, timing=False):
-        o = AnaDeviceOpts(device, chunk_paths, block_size, 1 if timing else 0)
+    def __init__(self, device=0, chunk_paths=0, block_size=0, timing=False, traversal=0):
+        o = AnaDeviceOpts(device, chunk_paths, block_size, 1 if timing else 0, traversal)
         h = _P()
         check(lib().ana_create(C.byref(h), C.byref(o)))
         self.h = h

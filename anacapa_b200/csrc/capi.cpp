@@ -42,6 +42,7 @@ struct ana_prepared {
            o_mc = 0;
     uint32_t n_tri_nodes = 0, n_tris = 0, n_seg_nodes = 0, n_segs = 0, n_mats = 0, n_slots = 0, n_lights = 0;
     bool tri_root_empty = true;
+    bool has_emitters = false;
     ana::HostEnv env_meta;  // sizes and scalars only (arrays live in the blob)
     ana_camera camera{};
     ~ana_prepared() {
@@ -162,6 +163,7 @@ int build_prepared(const ana::Prepared& P, ana_prepared& out) {
     out.n_slots = uint32_t(P.slot_material.size());
     out.n_lights = uint32_t(P.lights.size());
     out.tri_root_empty = P.tri_root_is_empty;
+    out.has_emitters = P.has_emitters;
     out.env_meta.present = P.env.present;
     out.env_meta.width = P.env.width;
     out.env_meta.height = P.env.height;
@@ -349,6 +351,7 @@ int ana_upload_prepared(ana_ctx* c, const ana_prepared* p) {
     S.num_slots = p->n_slots;
     S.lights = reinterpret_cast<const ana::DevLight*>(b + p->o_lights);
     S.num_lights = p->n_lights;
+    S.has_emitters = p->has_emitters ? 1 : 0;
     ana::DevEnv& E = S.env;
     E.present = p->env_meta.present ? 1 : 0;
     E.rgb = E.present ? reinterpret_cast<const float*>(b + p->o_env_rgb) : nullptr;
@@ -456,6 +459,7 @@ int ana_render(ana_ctx* c, const ana_render_desc* r) {
     p.min_depth = r->min_depth;
     ana::LaunchCfg cfg;
     cfg.block = c->opts.block_size ? int(c->opts.block_size) : 256;
+    cfg.persistent = c->opts.traversal == ANA_TRAVERSAL_PER_RAY ? 0 : 1;
     long long gcap = ((long long)cap + cfg.block - 1) / cfg.block;
     cfg.grid_cap = int(std::max<long long>(1, std::min<long long>(gcap, 1 << 20)));
     const bool count_work = (r->flags & ANA_RENDER_COUNT_WORK) != 0;
@@ -563,8 +567,12 @@ int ana_trace_batch(ana_ctx* c, const float* rays, size_t n, ana_hit* out, int o
             return cuda_fail(c, e, "rays H2D");
         }
     }
+    if (n >= (size_t(1) << 32) - 64) return fail(c, ANA_ERR_INVALID_ARG, "ana_trace_batch: n >= 2^32");
+    uint32_t* d_fetch = c->d_err + 32;  // fetch counter of the persistent kernel
     CK(cudaMemsetAsync(c->d_err, 0, 4, c->stream), "memset err");
-    ana::launch_trace_batch(c->ds, d_rays, n, d_out, occlusion, c->d_err, c->stream);
+    CK(cudaMemsetAsync(d_fetch, 0, 4, c->stream), "memset fetch");
+    ana::launch_trace_batch(c->ds, d_rays, n, d_out, occlusion, d_fetch, c->d_err,
+                            c->opts.traversal == ANA_TRAVERSAL_PER_RAY ? 0 : 1, c->stream);
     cudaError_t e = cudaGetLastError();
     uint32_t herr = 0;
     if (e == cudaSuccess && !on_device)

@@ -22,6 +22,8 @@ namespace ana {
 
 constexpr uint32_t kMiss = 0xFFFFFFFFu;
 constexpr int kMaxBlock = 1024;
+constexpr int kPersistBlock = 256;     // persistent traversal kernels: 8 warps per block
+constexpr int kPersistMinBlocks = 4;   // 4 resident blocks per SM: at most 64 registers
 
 // Reserve one slot per thread with want == true; returns the slot (valid only
 // for those threads). Must be reached by every thread of the block.
@@ -133,19 +135,21 @@ struct SceneHit {
     float tseg;
 };
 
-template <bool kCount = false>
-__device__ __forceinline__ SceneHit closest_hit(const DevScene& S, const Ray& r, uint32_t* err,
-                                                Counters* cnt = nullptr) {
+// Completes a triangle traversal with the curve pass (strictly closer ribbon
+// hits win) and packs the result. kCurves = false compiles the curve code out
+// of kernels for triangle-only scenes.
+template <bool kCurves>
+__device__ __forceinline__ SceneHit finish_closest(const DevScene& S, const Ray& r, const Traversal& T,
+                                                   uint32_t* err) {
     SceneHit h;
-    TriHit th = trace_tris<kCount>(S, r, err, cnt);
-    h.t = th.t;
-    h.u = th.u;
-    h.v = th.v;
-    h.prim = th.tri >= 0 ? uint32_t(th.tri) : kMiss;
+    h.t = T.tri >= 0 ? T.closest : r.tmax;
+    h.u = T.u;
+    h.v = T.v;
+    h.prim = T.tri >= 0 ? uint32_t(T.tri) : kMiss;
     h.tang = f3(0.f, 0.f, 0.f);
     h.tseg = 0.f;
-    if (S.num_seg_nodes) {
-        CurveHit ch = trace_curves<kCount>(S, r, th.tri >= 0 ? th.t : r.tmax, false, err, cnt);
+    if (kCurves) {
+        CurveHit ch = trace_curves(S, r, T.tri >= 0 ? T.closest : r.tmax, false, err);
         if (ch.seg >= 0) {
             h.t = ch.t;
             h.prim = 0x80000000u | uint32_t(ch.seg);
@@ -158,39 +162,77 @@ __device__ __forceinline__ SceneHit closest_hit(const DevScene& S, const Ray& r,
     return h;
 }
 
-__device__ __forceinline__ bool any_hit(const DevScene& S, const Ray& r, uint32_t* err) {
-    if (occluded_tris(S, r, err)) return true;
-    if (S.num_seg_nodes) return trace_curves(S, r, r.tmax, true, err).seg >= 0;
+template <bool kCurves>
+__device__ __forceinline__ bool finish_any(const DevScene& S, const Ray& r, const Traversal& T, uint32_t* err) {
+    if (T.tri >= 0) return true;
+    if (kCurves) return trace_curves(S, r, r.tmax, true, err).seg >= 0;
     return false;
 }
 
+__device__ __forceinline__ void warp_add_work(unsigned long long* work, const Counters& cnt) {
+    unsigned long long a = cnt.nodes, b = cnt.prims, c = cnt.segs;
+    for (int off = 16; off > 0; off >>= 1) {
+        a += __shfl_down_sync(0xFFFFFFFFu, a, off);
+        b += __shfl_down_sync(0xFFFFFFFFu, b, off);
+        c += __shfl_down_sync(0xFFFFFFFFu, c, off);
+    }
+    if ((threadIdx.x & 31u) == 0) {
+        atomicAdd(work + 0, a);
+        atomicAdd(work + 1, b);
+        atomicAdd(work + 2, c);
+    }
+}
+
+// Runs the traversal of queue entries [0, n) in one of two schedules:
+//   kPersist: persistent warps with per-lane refill (persistent_traverse);
+//   otherwise one thread per ray over a grid-stride loop.
+// Both use the same interior/leaf steps, so results are identical.
+template <bool kAny, bool kCount, bool kPersist, class Load, class Done>
+__device__ __forceinline__ void run_traversal(const DevScene& S, uint32_t n, uint32_t* fetch, uint32_t* err,
+                                              Counters* cnt, Load load, Done done) {
+    if (kPersist) {
+        persistent_traverse<kAny, kCount>(S, n, fetch, err, cnt, load, done);
+        return;
+    }
+    uint32_t stack[kMaxStack];
+    float stackT[kMaxStack];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        Ray ray;
+        load(i, ray);
+        Traversal T;
+        trav_init<kAny>(T, S, ray);
+        while (!T.exhausted) {
+            if (!(T.cur & 0x80000000u)) trav_interior<kAny, kCount>(T, S, stack, stackT, err, cnt);
+            else trav_leaf<kAny, kCount>(T, S, stack, stackT, cnt);
+        }
+        done(i, T);
+    }
+}
+
+#define ANA_TRAVERSAL_BOUNDS __launch_bounds__(kPersistBlock, kPersist ? kPersistMinBlocks : 1)
+
+// extend: closest hit of every live path (PathIntegrator::Li, line 81).
 // kCount: the same traversal, counting node fetches and primitive tests
 // (warp-aggregated into p.work) to derive the stage's algorithmic bytes.
-template <bool kCount>
-__global__ void __launch_bounds__(256) k_extend(const __grid_constant__ Params p) {
+template <bool kCount, bool kCurves, bool kPersist>
+__global__ void ANA_TRAVERSAL_BOUNDS k_extend(const __grid_constant__ Params p) {
     const uint32_t cur = p.bounce & 1u;
-    const uint32_t n = p.counters[p.bounce * kCountersPerBounce + 0];
+    uint32_t* cb = p.counters + p.bounce * kCountersPerBounce;
     Counters cnt{0, 0, 0};
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        float4 o = p.q.ext_o[cur][i], d = p.q.ext_d[cur][i];
-        Ray r{f3(o), f3(d), 1e-4f, INFINITY};
-        SceneHit h = closest_hit<kCount>(p.S, r, p.err, &cnt);
-        p.q.hit0[i] = make_float4(h.t, __uint_as_float(h.prim), h.u, h.v);
-        if (h.prim != kMiss && (h.prim & 0x80000000u)) p.q.hit1[i] = pack(h.tang, h.tseg);
-    }
-    if (kCount) {
-        unsigned long long a = cnt.nodes, b = cnt.prims, c = cnt.segs;
-        for (int off = 16; off > 0; off >>= 1) {
-            a += __shfl_down_sync(0xFFFFFFFFu, a, off);
-            b += __shfl_down_sync(0xFFFFFFFFu, b, off);
-            c += __shfl_down_sync(0xFFFFFFFFu, c, off);
-        }
-        if ((threadIdx.x & 31u) == 0) {
-            atomicAdd(p.work + 0, a);
-            atomicAdd(p.work + 1, b);
-            atomicAdd(p.work + 2, c);
-        }
-    }
+    run_traversal<false, kCount, kPersist>(
+        p.S, cb[0], cb + 3, p.err, &cnt,
+        [&](uint32_t i, Ray& r) {
+            float4 o = p.q.ext_o[cur][i], d = p.q.ext_d[cur][i];
+            r = Ray{f3(o), f3(d), 1e-4f, INFINITY};
+        },
+        [&](uint32_t i, const Traversal& T) {
+            float4 o = p.q.ext_o[cur][i], d = p.q.ext_d[cur][i];
+            Ray r{f3(o), f3(d), 1e-4f, INFINITY};
+            SceneHit h = finish_closest<kCurves>(p.S, r, T, p.err);
+            p.q.hit0[i] = make_float4(h.t, __uint_as_float(h.prim), h.u, h.v);
+            if (kCurves && h.prim != kMiss && (h.prim & 0x80000000u)) p.q.hit1[i] = pack(h.tang, h.tseg);
+        });
+    if (kCount) warp_add_work(p.work, cnt);
 }
 
 // Surface interaction of a hit (BVHBackend::fillSurfaceInteraction,
@@ -373,39 +415,60 @@ __global__ void __launch_bounds__(256) k_shade(const __grid_constant__ Params p)
 
 // NEE shadow rays: shadowTransmittance (src/integrator/ShadowRay.h:26-61) for
 // opaque scenes — any blocker in [1e-4, tmax] makes the transmittance black.
-__global__ void __launch_bounds__(256) k_shadow(const __grid_constant__ Params p) {
-    const uint32_t n = p.counters[p.bounce * kCountersPerBounce + 1];
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        float4 o = p.q.sh_o[i], d = p.q.sh_d[i];
-        Ray r{f3(o), f3(d), 1e-4f, d.w};
-        if (!any_hit(p.S, r, p.err)) add_L(p, __float_as_uint(o.w), f3(p.q.sh_c[i]));
-    }
+template <bool kCurves, bool kPersist>
+__global__ void ANA_TRAVERSAL_BOUNDS k_shadow(const __grid_constant__ Params p) {
+    uint32_t* cb = p.counters + p.bounce * kCountersPerBounce;
+    run_traversal<true, false, kPersist>(
+        p.S, cb[1], cb + 4, p.err, nullptr,
+        [&](uint32_t i, Ray& r) {
+            float4 o = p.q.sh_o[i], d = p.q.sh_d[i];
+            r = Ray{f3(o), f3(d), 1e-4f, d.w};
+        },
+        [&](uint32_t i, const Traversal& T) {
+            float4 o = p.q.sh_o[i], d = p.q.sh_d[i];
+            Ray r{f3(o), f3(d), 1e-4f, d.w};
+            if (!finish_any<kCurves>(p.S, r, T, p.err)) add_L(p, __float_as_uint(o.w), f3(p.q.sh_c[i]));
+        });
 }
 
 // BSDF-sampled MIS rays (PathIntegrator.cpp:214-259): the first surface hit
-// within 1e10 contributes its material's Le, a miss the environment.
-__global__ void __launch_bounds__(256) k_mis(const __grid_constant__ Params p) {
-    const uint32_t n = p.counters[p.bounce * kCountersPerBounce + 2];
+// within 1e10 contributes its material's Le, a miss the environment. In a
+// scene without emissive surfaces every hit contributes zero, so the ray only
+// needs to know whether anything is hit (kAny): identical result, cheaper
+// query.
+template <bool kAny, bool kCurves, bool kPersist>
+__global__ void ANA_TRAVERSAL_BOUNDS k_mis(const __grid_constant__ Params p) {
+    uint32_t* cb = p.counters + p.bounce * kCountersPerBounce;
     const DevScene& S = p.S;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        float4 o = p.q.mis_o[i], d = p.q.mis_d[i];
-        Ray r{f3(o), f3(d), 1e-4f, 1e10f};
-        SceneHit h = closest_hit(S, r, p.err);
-        float3 Li;
-        if (h.prim == kMiss) {
-            Li = env_le(S.env, r.d);
-        } else {
-            uint32_t slot;
-            if (h.prim & 0x80000000u)
-                slot = __float_as_uint(ldg4(S.segs + 5 * size_t(h.prim & 0x7FFFFFFFu) + 4).z);
-            else
-                slot = __float_as_uint(ldg4(S.tri_shade + 4 * size_t(__float_as_uint(
-                                                               ldg4(S.tri_isect + 3 * size_t(h.prim)).w))).w);
-            int mi = slot_material(S, slot);
-            Li = mi >= 0 ? mat_le(S.materials[mi]) : f3(0.f, 0.f, 0.f);
-        }
-        if (!is_black(Li)) add_L(p, __float_as_uint(o.w), f3(p.q.mis_c[i]) * Li);
-    }
+    run_traversal<kAny, false, kPersist>(
+        S, cb[2], cb + 5, p.err, nullptr,
+        [&](uint32_t i, Ray& r) {
+            float4 o = p.q.mis_o[i], d = p.q.mis_d[i];
+            r = Ray{f3(o), f3(d), 1e-4f, 1e10f};
+        },
+        [&](uint32_t i, const Traversal& T) {
+            float4 o = p.q.mis_o[i], d = p.q.mis_d[i];
+            Ray r{f3(o), f3(d), 1e-4f, 1e10f};
+            float3 Li;
+            if (kAny) {
+                Li = finish_any<kCurves>(S, r, T, p.err) ? f3(0.f, 0.f, 0.f) : env_le(S.env, r.d);
+            } else {
+                SceneHit h = finish_closest<kCurves>(S, r, T, p.err);
+                if (h.prim == kMiss) {
+                    Li = env_le(S.env, r.d);
+                } else {
+                    uint32_t slot;
+                    if (h.prim & 0x80000000u)
+                        slot = __float_as_uint(ldg4(S.segs + 5 * size_t(h.prim & 0x7FFFFFFFu) + 4).z);
+                    else
+                        slot = __float_as_uint(ldg4(S.tri_shade + 4 * size_t(__float_as_uint(
+                                                                       ldg4(S.tri_isect + 3 * size_t(h.prim)).w))).w);
+                    int mi = slot_material(S, slot);
+                    Li = mi >= 0 ? mat_le(S.materials[mi]) : f3(0.f, 0.f, 0.f);
+                }
+            }
+            if (!is_black(Li)) add_L(p, __float_as_uint(o.w), f3(p.q.mis_c[i]) * Li);
+        });
 }
 
 // Film accumulation (PathIntegrator.cpp:43-57 + Film::mergeTile, Film.cpp:34-56):
@@ -435,17 +498,23 @@ __global__ void __launch_bounds__(256) k_film(const __grid_constant__ Params p) 
 }
 
 // IAccelerationStructure::traceBatch / occludedBatch over CurveBrute semantics.
-__global__ void __launch_bounds__(256) k_trace_batch(const __grid_constant__ DevScene S, const float* rays, size_t n,
-                                                     ana_hit* out, int occlusion, uint32_t* err) {
-    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
-        const float4* rp = reinterpret_cast<const float4*>(rays + 8 * i);
+template <bool kAny, bool kCurves, bool kPersist>
+__global__ void ANA_TRAVERSAL_BOUNDS
+    k_trace_batch(const __grid_constant__ DevScene S, const float* rays, uint32_t n, ana_hit* out, uint32_t* fetch,
+                  uint32_t* err) {
+    auto load = [&](uint32_t i, Ray& r) {
+        const float4* rp = reinterpret_cast<const float4*>(rays + 8 * size_t(i));
         float4 a = rp[0], b = rp[1];
-        Ray r{f3(a), f3(b), a.w, b.w};
+        r = Ray{f3(a), f3(b), a.w, b.w};
+    };
+    run_traversal<kAny, false, kPersist>(S, n, fetch, err, nullptr, load, [&](uint32_t i, const Traversal& T) {
+        Ray r;
+        load(i, r);
         ana_hit h{0, -1, -1, -1, 0.f, 0.f, 0.f, 0.f};
-        if (occlusion) {
-            h.hit = any_hit(S, r, err) ? 1 : 0;
+        if (kAny) {
+            h.hit = finish_any<kCurves>(S, r, T, err) ? 1 : 0;
         } else {
-            SceneHit sh = closest_hit(S, r, err);
+            SceneHit sh = finish_closest<kCurves>(S, r, T, err);
             if (sh.prim != kMiss) {
                 h.hit = 1;
                 h.t = sh.t;
@@ -465,7 +534,7 @@ __global__ void __launch_bounds__(256) k_trace_batch(const __grid_constant__ Dev
             }
         }
         out[i] = h;
-    }
+    });
 }
 
 // ---------------------------------------------------------------------------
@@ -475,31 +544,100 @@ static inline int blocks_for(uint32_t n, int block, int cap) {
     return int(b < cap ? b : cap);
 }
 
+// Resident blocks of a kernel on this device (one wave of the persistent schedule).
+template <class K>
+static int resident_grid(K kernel) {
+    int dev = 0, sms = 148, per = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kPersistBlock, 0);
+    return sms * (per > 0 ? per : 1);
+}
+
+// Grid for a traversal kernel: one resident wave when persistent, otherwise
+// enough blocks to cover the chunk capacity (grid-stride beyond it).
+template <bool kPersist, class K>
+static int traversal_grid(K kernel, const LaunchCfg& c) {
+    if (kPersist) {
+        static int g = resident_grid(kernel);
+        return g;
+    }
+    return c.grid_cap;
+}
+
 void launch_generate(const Params& p, const LaunchCfg& c, cudaStream_t s) {
     k_generate<<<blocks_for(p.chunk_pixels * p.spp, 256, c.grid_cap), 256, 0, s>>>(p);
 }
+
+template <bool kCount, bool kCurves, bool kPersist>
+static void ext_launch(const Params& p, const LaunchCfg& c, cudaStream_t s) {
+    auto k = k_extend<kCount, kCurves, kPersist>;
+    k<<<traversal_grid<kPersist>(k, c), kPersistBlock, 0, s>>>(p);
+}
 void launch_extend(const Params& p, const LaunchCfg& c, cudaStream_t s, bool count_work) {
-    if (count_work) k_extend<true><<<c.grid_cap, c.block, 0, s>>>(p);
-    else k_extend<false><<<c.grid_cap, c.block, 0, s>>>(p);
+    const bool cv = p.S.num_seg_nodes != 0, ps = c.persistent != 0;
+    if (count_work) {
+        if (cv) ps ? ext_launch<true, true, true>(p, c, s) : ext_launch<true, true, false>(p, c, s);
+        else ps ? ext_launch<true, false, true>(p, c, s) : ext_launch<true, false, false>(p, c, s);
+    } else {
+        if (cv) ps ? ext_launch<false, true, true>(p, c, s) : ext_launch<false, true, false>(p, c, s);
+        else ps ? ext_launch<false, false, true>(p, c, s) : ext_launch<false, false, false>(p, c, s);
+    }
 }
 void launch_shade(const Params& p, const LaunchCfg& c, cudaStream_t s) {
     k_shade<<<c.grid_cap, c.block, 0, s>>>(p);
 }
+template <bool kCurves, bool kPersist>
+static void sh_launch(const Params& p, const LaunchCfg& c, cudaStream_t s) {
+    auto k = k_shadow<kCurves, kPersist>;
+    k<<<traversal_grid<kPersist>(k, c), kPersistBlock, 0, s>>>(p);
+}
 void launch_shadow(const Params& p, const LaunchCfg& c, cudaStream_t s) {
-    k_shadow<<<c.grid_cap, c.block, 0, s>>>(p);
+    const bool cv = p.S.num_seg_nodes != 0, ps = c.persistent != 0;
+    if (cv) ps ? sh_launch<true, true>(p, c, s) : sh_launch<true, false>(p, c, s);
+    else ps ? sh_launch<false, true>(p, c, s) : sh_launch<false, false>(p, c, s);
+}
+template <bool kAny, bool kCurves, bool kPersist>
+static void mis_launch(const Params& p, const LaunchCfg& c, cudaStream_t s) {
+    auto k = k_mis<kAny, kCurves, kPersist>;
+    k<<<traversal_grid<kPersist>(k, c), kPersistBlock, 0, s>>>(p);
 }
 void launch_mis(const Params& p, const LaunchCfg& c, cudaStream_t s) {
-    k_mis<<<c.grid_cap, c.block, 0, s>>>(p);
+    const bool cv = p.S.num_seg_nodes != 0, ps = c.persistent != 0, any = !p.S.has_emitters;
+    if (any) {
+        if (cv) ps ? mis_launch<true, true, true>(p, c, s) : mis_launch<true, true, false>(p, c, s);
+        else ps ? mis_launch<true, false, true>(p, c, s) : mis_launch<true, false, false>(p, c, s);
+    } else {
+        if (cv) ps ? mis_launch<false, true, true>(p, c, s) : mis_launch<false, true, false>(p, c, s);
+        else ps ? mis_launch<false, false, true>(p, c, s) : mis_launch<false, false, false>(p, c, s);
+    }
 }
 void launch_film(const Params& p, const LaunchCfg& c, cudaStream_t s) {
     k_film<<<blocks_for(p.chunk_pixels, 256, c.grid_cap), 256, 0, s>>>(p);
 }
+template <bool kAny, bool kCurves, bool kPersist>
+static void tb_launch(const DevScene& S, const float* rays, uint32_t n, ana_hit* out, uint32_t* fetch,
+                      uint32_t* err, int grid, cudaStream_t s) {
+    auto k = k_trace_batch<kAny, kCurves, kPersist>;
+    int g = kPersist ? resident_grid(k) : grid;
+    k<<<g, kPersistBlock, 0, s>>>(S, rays, n, out, fetch, err);
+}
 void launch_trace_batch(const DevScene& S, const float* rays, size_t n, ana_hit* out, int occlusion,
-                        uint32_t* err, cudaStream_t s) {
-    int blocks = int((n + 255) / 256);
-    if (blocks > 148 * 64) blocks = 148 * 64;
-    if (blocks < 1) blocks = 1;
-    k_trace_batch<<<blocks, 256, 0, s>>>(S, rays, n, out, occlusion, err);
+                        uint32_t* fetch, uint32_t* err, int persistent, cudaStream_t s) {
+    const bool cv = S.num_seg_nodes != 0;
+    int grid = blocks_for(uint32_t(n), kPersistBlock, 1 << 20);
+    uint32_t nn = uint32_t(n);
+    if (occlusion) {
+        if (cv) persistent ? tb_launch<true, true, true>(S, rays, nn, out, fetch, err, grid, s)
+                           : tb_launch<true, true, false>(S, rays, nn, out, fetch, err, grid, s);
+        else persistent ? tb_launch<true, false, true>(S, rays, nn, out, fetch, err, grid, s)
+                        : tb_launch<true, false, false>(S, rays, nn, out, fetch, err, grid, s);
+    } else {
+        if (cv) persistent ? tb_launch<false, true, true>(S, rays, nn, out, fetch, err, grid, s)
+                           : tb_launch<false, true, false>(S, rays, nn, out, fetch, err, grid, s);
+        else persistent ? tb_launch<false, false, true>(S, rays, nn, out, fetch, err, grid, s)
+                        : tb_launch<false, false, false>(S, rays, nn, out, fetch, err, grid, s);
+    }
 }
 
 }  // namespace ana

@@ -31,8 +31,9 @@ struct Queues {
 };
 
 // Per-bounce device counters: [bounce][0] extend queue length, [1] shadow
-// queue length, [2] MIS queue length. Zeroed per chunk.
-constexpr int kCountersPerBounce = 4;
+// queue length, [2] MIS queue length, [3..5] the persistent kernels' fetch
+// counters of extend, shadow and MIS. Zeroed per chunk.
+constexpr int kCountersPerBounce = 8;
 
 struct Params {
     DevScene S;
@@ -50,6 +51,7 @@ struct Params {
 struct LaunchCfg {
     int block;       // threads per block for the stage kernels
     int grid_cap;    // blocks for grid-stride kernels over the chunk capacity
+    int persistent;  // traversal schedule: 1 persistent warps with refill, 0 thread per ray
 };
 
 void launch_generate(const Params& p, const LaunchCfg& c, cudaStream_t s);
@@ -58,7 +60,7 @@ void launch_shade(const Params& p, const LaunchCfg& c, cudaStream_t s);
 void launch_shadow(const Params& p, const LaunchCfg& c, cudaStream_t s);
 void launch_mis(const Params& p, const LaunchCfg& c, cudaStream_t s);
 void launch_film(const Params& p, const LaunchCfg& c, cudaStream_t s);
-void launch_trace_batch(const DevScene& S, const float* rays, size_t n, ana_hit* out, int occlusion,
-                        uint32_t* err, cudaStream_t s);
+void launch_trace_batch(const DevScene& S, const float* rays, size_t n, ana_hit* out, int occlusion, uint32_t* fetch,
+                        uint32_t* err, int persistent, cudaStream_t s);
 
 }  // namespace ana

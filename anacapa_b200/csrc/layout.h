@@ -105,7 +105,7 @@ struct DevScene {
     uint32_t num_materials, num_slots;
     const DevLight* lights;
     uint32_t num_lights;
-    uint32_t pad;
+    uint32_t has_emitters;  // any material reachable from a slot emits (Le != 0)
     DevEnv env;
     DevCamera cam;
 };

@@ -612,8 +612,14 @@ int prepare_scene(const ana_scene_desc& d, Prepared& P, std::string& err) {
         }
     }
     P.slot_material.assign(d.slot_material, d.slot_material + d.num_slots);
-    for (int32_t s : P.slot_material)
+    P.has_emitters = false;
+    for (int32_t s : P.slot_material) {
         if (s >= int32_t(d.num_materials)) return bad("slot refers to a missing material");
+        if (s >= 0) {
+            const float3 e = P.materials[size_t(s)].emission;
+            if (e.x != 0.f || e.y != 0.f || e.z != 0.f) P.has_emitters = true;
+        }
+    }
 
     // ---- lights --------------------------------------------------------------
     P.lights.clear();

@@ -34,6 +34,7 @@ struct Prepared {
     HostEnv env;
     ana_camera camera{};
     uint32_t num_tris = 0, num_segs = 0;
+    bool has_emitters = false;
     uint64_t bytes() const;
 };
 

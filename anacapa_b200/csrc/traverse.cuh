@@ -160,6 +160,153 @@ __device__ __forceinline__ TriHit trace_tris(const DevScene& S, const Ray& ray, 
     return h;
 }
 
+// ---------------------------------------------------------------------------
+// Persistent-warp triangle traversal. Each lane owns one ray at a time; a
+// warp loops over
+//   1. refill: lanes without a ray take the next queue entries (one
+//      warp-aggregated atomicAdd on the stage's fetch counter);
+//   2. interior phase: every lane descends interior nodes until it reaches a
+//      leaf or runs out of nodes; the phase ends when no lane needs another
+//      interior step, so lanes stay converged on the node-test code;
+//   3. leaf phase: one leaf's triangles per lane.
+// A lane whose stack is exhausted (or, for occlusion, that found a blocker)
+// reports its ray and picks up a new one at the next refill, so finished rays
+// do not idle the warp until its slowest ray completes. Box and triangle
+// tests are the same functions as above, so results are identical.
+// ---------------------------------------------------------------------------
+struct Traversal {
+    TriRay r;
+    float closest, u, v;
+    int32_t tri;
+    uint32_t cur;
+    int sp;
+    bool exhausted;
+};
+
+template <bool kAny>
+__device__ __forceinline__ void trav_init(Traversal& T, const DevScene& S, const Ray& ray) {
+    T.r = make_tri_ray(ray);
+    T.closest = ray.tmax;
+    T.u = T.v = 0.f;
+    T.tri = -1;
+    T.cur = 0;
+    T.sp = 0;
+    T.exhausted = S.num_tri_nodes == 0;
+}
+
+__device__ __forceinline__ bool trav_pop(Traversal& T, const uint32_t* stack, const float* stackT) {
+    while (T.sp > 0) {
+        --T.sp;
+        if (stackT[T.sp] > T.closest) continue;
+        T.cur = stack[T.sp];
+        return true;
+    }
+    return false;
+}
+
+// Interior step: one node fetch and two child-box tests.
+template <bool kAny, bool kCount>
+__device__ __forceinline__ void trav_interior(Traversal& T, const DevScene& S, uint32_t* stack, float* stackT,
+                                              uint32_t* err, Counters* cnt) {
+    const float4* np = reinterpret_cast<const float4*>(S.tri_nodes + T.cur);
+    float4 n0 = ldg4(np), n1 = ldg4(np + 1), n2 = ldg4(np + 2), n3 = ldg4(np + 3);
+    if (kCount) cnt->nodes++;
+    float tn0, tn1;
+    const float cull = kAny ? T.r.tmax : T.closest;
+    bool h0 = box_hit(T.r, n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, cull, tn0);
+    bool h1 = box_hit(T.r, n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, cull, tn1);
+    uint32_t c0 = fbits_u(n3.z) ? leaf_entry(fbits_u(n3.x), fbits_u(n3.z)) : fbits_u(n3.x);
+    uint32_t c1 = fbits_u(n3.w) ? leaf_entry(fbits_u(n3.y), fbits_u(n3.w)) : fbits_u(n3.y);
+    if (h0 && h1) {
+        bool swap = !(tn0 < tn1);
+        if (T.sp >= int(kMaxStack)) {
+            atomicOr(err, 1u);
+            T.exhausted = true;
+            return;
+        }
+        stack[T.sp] = swap ? c0 : c1;
+        stackT[T.sp] = swap ? tn0 : tn1;
+        ++T.sp;
+        T.cur = swap ? c1 : c0;
+    } else if (h0 || h1) {
+        T.cur = h0 ? c0 : c1;
+    } else if (!trav_pop(T, stack, stackT)) {
+        T.exhausted = true;
+    }
+}
+
+// Leaf step: test the leaf's triangles, then pop.
+template <bool kAny, bool kCount>
+__device__ __forceinline__ void trav_leaf(Traversal& T, const DevScene& S, const uint32_t* stack,
+                                          const float* stackT, Counters* cnt) {
+    uint32_t off = T.cur & 0x01FFFFFFu, c = ((T.cur >> 25) & 63u) + 1u;
+    for (uint32_t i = off; i < off + c; ++i) {
+        const float4* tp = S.tri_isect + 3 * size_t(i);
+        float4 a = ldg4(tp), b = ldg4(tp + 1), e = ldg4(tp + 2);
+        if (kCount) cnt->prims++;
+        float t, u, v;
+        if (tri_hit(T.r, f3(a), f3(b), f3(e), kAny ? T.r.tmax : T.closest, t, u, v)) {
+            T.closest = t;
+            T.u = u;
+            T.v = v;
+            T.tri = int32_t(i);
+            if (kAny) {
+                T.exhausted = true;
+                return;
+            }
+        }
+    }
+    if (!trav_pop(T, stack, stackT)) T.exhausted = true;
+}
+
+// Runs the persistent loop. Load(i, ray) reads queue entry i; Done(i, T)
+// consumes the finished traversal of entry i (a lane-local call).
+template <bool kAny, bool kCount, class Load, class Done>
+__device__ __forceinline__ void persistent_traverse(const DevScene& S, uint32_t n, uint32_t* fetch, uint32_t* err,
+                                                    Counters* cnt, Load load, Done done) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t ltmask = (1u << lane) - 1u;
+    uint32_t stack[kMaxStack];
+    float stackT[kMaxStack];
+    Traversal T;
+    bool active = false, drained = false;
+    uint32_t idx = 0;
+    while (true) {
+        // 1. refill idle lanes
+        if (!drained) {
+            uint32_t need = __ballot_sync(0xFFFFFFFFu, !active);
+            if (need) {
+                uint32_t leader = __ffs(need) - 1u, base = 0;
+                if (lane == leader) base = atomicAdd(fetch, __popc(need));
+                base = __shfl_sync(0xFFFFFFFFu, base, leader);
+                if (base >= n) drained = true;
+                if (!active) {
+                    idx = base + __popc(need & ltmask);
+                    if (idx < n) {
+                        Ray ray;
+                        load(idx, ray);
+                        trav_init<kAny>(T, S, ray);
+                        active = true;
+                    }
+                }
+            }
+        }
+        if (!__any_sync(0xFFFFFFFFu, active)) break;
+        // 2. interior phase
+        while (true) {
+            bool want = active && !T.exhausted && !(T.cur & 0x80000000u);
+            if (!__any_sync(0xFFFFFFFFu, want)) break;
+            if (want) trav_interior<kAny, kCount>(T, S, stack, stackT, err, cnt);
+        }
+        // 3. leaf phase
+        if (active && !T.exhausted) trav_leaf<kAny, kCount>(T, S, stack, stackT, cnt);
+        if (active && T.exhausted) {
+            done(idx, T);
+            active = false;
+        }
+    }
+}
+
 // Any hit within [tmin, tmax] (BVHBackend::occluded, BVHBackend.cpp:409-444).
 __device__ __forceinline__ bool occluded_tris(const DevScene& S, const Ray& ray, uint32_t* err) {
     if (S.num_tri_nodes == 0) return false;

@@ -50,6 +50,8 @@ def parse():
                     help="target CPU work of the reference sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--traversal", type=int, default=0,
+                    help="0 library default, 1 persistent warps, 2 one thread per ray")
     return ap.parse_args()
 
 
@@ -239,7 +241,7 @@ def run_ours(a):
         torch.cuda.set_device(local)
     scene = S.throughput(a.width, a.height, a.spp, a.depth, n_spheres=a.n_spheres)
     prep = api.Prepared(scene)
-    r = api.Renderer(device=local, timing=True)
+    r = api.Renderer(device=local, timing=True, traversal=a.traversal)
     r.upload(prep)
     W, H, spp = scene.width, scene.height, scene.spp
     start = rank * spp  # each rank renders its own disjoint sample range of the frame

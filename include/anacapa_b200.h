@@ -219,7 +219,14 @@ typedef struct ana_device_opts {
     uint32_t chunk_paths;    /* wavefront capacity in paths (0 = default)      */
     uint32_t block_size;     /* threads per block of the stage kernels (0 = default) */
     uint32_t timing;         /* 1: record per-stage CUDA-event times           */
+    uint32_t traversal;      /* ANA_TRAVERSAL_*: schedule of the BVH traversal kernels */
 } ana_device_opts;
+
+enum {
+    ANA_TRAVERSAL_DEFAULT = 0,     /* the library's choice (persistent)              */
+    ANA_TRAVERSAL_PERSISTENT = 1,  /* persistent warps refilling finished lanes      */
+    ANA_TRAVERSAL_PER_RAY = 2      /* one thread per ray, grid-stride               */
+};
 
 /* Create a context on a device. Replaces CudaPathIntegrator's constructor /
  * CudaContext (src/gpu/cuda/CudaContext.cu:37-58). */
