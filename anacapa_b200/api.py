@@ -108,7 +108,10 @@ HIT_DTYPE = np.dtype([("hit", "<i4"), ("mesh_id", "<i4"), ("prim_id", "<i4"),
 EXPORTS = ["ana_create", "ana_destroy", "ana_upload_scene", "ana_prepare_scene",
            "ana_upload_prepared", "ana_prepared_bytes", "ana_prepared_free", "ana_render",
            "ana_film_clear", "ana_film_read", "ana_film_device_ptr", "ana_trace_batch",
-           "ana_get_stats", "ana_last_error", "ana_version"]
+           "ana_get_stats", "ana_last_error", "ana_version", "ana_batch_create", "ana_batch_free",
+           "ana_batch_bytes", "ana_upload_batch", "ana_render_batch", "ana_batch_film_read",
+           "ana_prepared_digest"]
+ANA_RENDER_GRAPH = 4
 
 _lib = None
 
@@ -145,6 +148,16 @@ def lib():
     L.ana_get_stats.argtypes = [_P, C.POINTER(AnaStats)]
     L.ana_last_error.argtypes = [_P, C.c_char_p, C.c_size_t]
     L.ana_version.restype = C.c_int
+    L.ana_batch_create.argtypes = [C.POINTER(_P), C.c_uint32, C.POINTER(_P)]
+    L.ana_batch_free.argtypes = [_P]
+    L.ana_batch_free.restype = None
+    L.ana_batch_bytes.argtypes = [_P]
+    L.ana_batch_bytes.restype = C.c_uint64
+    L.ana_upload_batch.argtypes = [_P, _P]
+    L.ana_render_batch.argtypes = [_P, C.POINTER(AnaRenderDesc), C.c_uint32, C.c_uint32]
+    L.ana_batch_film_read.argtypes = [_P, C.c_uint32, _P, C.c_size_t]
+    L.ana_prepared_digest.argtypes = [_P]
+    L.ana_prepared_digest.restype = C.c_uint64
     _lib = L
     return L
 
@@ -343,3 +356,50 @@ class Renderer:
         self._check(lib().ana_trace_batch(self.h, rays.ctypes.data, len(rays), out.ctypes.data,
                                           1 if occlusion else 0, 0))
         return out
+
+    # ---- batches -------------------------------------------------------------
+    def upload_batch(self, batch: "Batch"):
+        self._check(lib().ana_upload_batch(self.h, batch.h))
+
+    def render_batch(self, descs, clear=True, graph=False):
+        """descs: list of (width, height, spp, max_depth[, sample_start, min_depth, seed])."""
+        flags = (ANA_RENDER_CLEAR_FILM if clear else 0) | (ANA_RENDER_GRAPH if graph else 0)
+        arr = (AnaRenderDesc * len(descs))()
+        for k, d in enumerate(descs):
+            w, h, spp, depth = d[:4]
+            start = d[4] if len(d) > 4 else 0
+            mind = d[5] if len(d) > 5 else 2
+            seed = d[6] if len(d) > 6 else 0
+            arr[k] = AnaRenderDesc(w, h, start, spp, depth, mind, seed, 0)
+        self._check(lib().ana_render_batch(self.h, arr, len(descs), flags))
+
+    def batch_film(self, item, width, height) -> np.ndarray:
+        out = np.zeros((height, width, 5), np.float32)
+        self._check(lib().ana_batch_film_read(self.h, item, out.ctypes.data, width * height))
+        return out
+
+
+class Batch:
+    """Several prepared scenes concatenated into one device arena."""
+
+    def __init__(self, prepared):
+        self.items = list(prepared)
+        arr = (_P * len(self.items))(*[p.h for p in self.items])
+        h = _P()
+        check(lib().ana_batch_create(arr, len(self.items), C.byref(h)))
+        self.h = h
+
+    @property
+    def nbytes(self) -> int:
+        return int(lib().ana_batch_bytes(self.h))
+
+    def __del__(self):
+        try:
+            if self.h:
+                lib().ana_batch_free(self.h)
+        except Exception:
+            pass
+
+
+def scene_desc_tuple(sc: S.Scene, sample_start=0, seed=0):
+    return (sc.width, sc.height, sc.spp, sc.max_depth, sample_start, 2, seed)

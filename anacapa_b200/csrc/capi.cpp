@@ -5,6 +5,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <new>
 #include <string>
@@ -27,29 +28,204 @@ void set_global_err(const std::string& m) {
 constexpr size_t kAlign = 256;
 inline size_t align_up(size_t x) { return (x + kAlign - 1) & ~(kAlign - 1); }
 
-}  // namespace
+inline float fbits(uint32_t u) {
+    float f;
+    std::memcpy(&f, &u, 4);
+    return f;
+}
+inline uint32_t ubits(float f) {
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    return u;
+}
 
-// A prepared scene: one contiguous host blob (pinned when CUDA is present)
-// holding every device array at 256-byte aligned offsets, so uploading is a
-// single host-to-device copy.
-struct ana_prepared {
-    unsigned char* blob = nullptr;
+// Per-scene facts of a blob that the per-render scene records need.
+struct SceneStatic {
+    uint32_t tri_root = ana::kNoRoot, seg_root = ana::kNoRoot;
+    uint32_t slot_base = 0, num_slots = 0, light_base = 0, num_lights = 0;
+    bool has_dome = false;
+    float env_radiance[3] = {0.f, 0.f, 0.f};
+    ana_camera camera{};
+};
+
+// One or more prepared scenes laid out as a single device arena in pinned
+// host memory (256-byte aligned sections), so an upload is one copy.
+struct Blob {
+    unsigned char* mem = nullptr;
     size_t size = 0;
     bool pinned = false;
-    // offsets into blob
-    size_t o_tri_nodes = 0, o_tri_isect = 0, o_tri_shade = 0, o_seg_nodes = 0, o_segs = 0, o_scol = 0,
-           o_mats = 0, o_slots = 0, o_lights = 0, o_env_rgb = 0, o_cf = 0, o_cc = 0, o_ci = 0, o_mf = 0,
-           o_mc = 0;
-    uint32_t n_tri_nodes = 0, n_tris = 0, n_seg_nodes = 0, n_segs = 0, n_mats = 0, n_slots = 0, n_lights = 0;
-    bool tri_root_empty = true;
-    bool has_emitters = false;
-    ana::HostEnv env_meta;  // sizes and scalars only (arrays live in the blob)
-    ana_camera camera{};
-    ~ana_prepared() {
-        if (!blob) return;
-        if (pinned) cudaFreeHost(blob);
-        else std::free(blob);
+    size_t o_tri_nodes = 0, o_tri_isect = 0, o_tri_shade = 0, o_seg_nodes = 0, o_segs = 0, o_scol = 0, o_mats = 0,
+           o_slots = 0, o_lights = 0, o_env_rgb = 0, o_cf = 0, o_cc = 0, o_ci = 0, o_mf = 0, o_mc = 0;
+    std::vector<SceneStatic> scenes;
+    bool has_curves = false, has_emitters = false;
+    ana::HostEnv env_meta;  // scalars only
+    Blob() = default;
+    Blob(const Blob&) = delete;
+    Blob& operator=(const Blob&) = delete;
+    ~Blob() {
+        if (!mem) return;
+        if (pinned) cudaFreeHost(mem);
+        else std::free(mem);
     }
+};
+
+int build_blob(const ana::Prepared* const* list, uint32_t n, Blob& B, std::string& err) {
+    size_t nNodes = 0, nTris = 0, nSegNodes = 0, nSegs = 0, nStr = 0, nMats = 0, nSlots = 0, nLights = 0;
+    const ana::Prepared* dome = nullptr;
+    for (uint32_t k = 0; k < n; ++k) {
+        const ana::Prepared& P = *list[k];
+        nNodes += P.tri_nodes.size();
+        nTris += P.num_tris;
+        nSegNodes += P.seg_nodes.size();
+        nSegs += P.num_segs;
+        nStr += P.strand_color.size() / 3;
+        nMats += P.materials.size();
+        nSlots += P.slot_material.size();
+        nLights += P.lights.size();
+        if (P.env.present) {
+            if (dome) {
+                err = "a batch may hold at most one dome light";
+                return ANA_ERR_UNSUPPORTED;
+            }
+            dome = &P;
+        }
+    }
+    if (nTris >= (1u << 25) || nSegs >= (1u << 25)) {
+        err = "more than 2^25 triangles or curve segments in the batch";
+        return ANA_ERR_INVALID_ARG;
+    }
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        size_t o = off;
+        off = align_up(off + bytes);
+        return o;
+    };
+    B.o_tri_nodes = take(nNodes * sizeof(ana::BvhNode));
+    B.o_tri_isect = take(nTris * 48);
+    B.o_tri_shade = take(nTris * 64);
+    B.o_seg_nodes = take(nSegNodes * sizeof(ana::BvhNode));
+    B.o_segs = take(nSegs * 80);
+    B.o_scol = take(nStr * 12);
+    B.o_mats = take(nMats * sizeof(ana::DevMaterial));
+    B.o_slots = take(nSlots * 4);
+    B.o_lights = take(nLights * sizeof(ana::DevLight));
+    B.o_env_rgb = take(dome ? dome->env.rgb.size() * 4 : 0);
+    B.o_cf = take(dome ? dome->env.cond_func.size() * 4 : 0);
+    B.o_cc = take(dome ? dome->env.cond_cdf.size() * 4 : 0);
+    B.o_ci = take(dome ? dome->env.cond_int.size() * 4 : 0);
+    B.o_mf = take(dome ? dome->env.marg_func.size() * 4 : 0);
+    B.o_mc = take(dome ? dome->env.marg_cdf.size() * 4 : 0);
+    B.size = std::max<size_t>(off, kAlign);
+    void* mem = nullptr;
+    if (cudaHostAlloc(&mem, B.size, cudaHostAllocPortable) == cudaSuccess) {
+        B.pinned = true;
+    } else {
+        cudaGetLastError();
+        mem = std::aligned_alloc(kAlign, B.size);
+        B.pinned = false;
+        if (!mem) {
+            err = "host allocation failed";
+            return ANA_ERR_OOM;
+        }
+    }
+    B.mem = static_cast<unsigned char*>(mem);
+    std::memset(B.mem, 0, B.size);
+    auto* nodes = reinterpret_cast<ana::BvhNode*>(B.mem + B.o_tri_nodes);
+    auto* isect = reinterpret_cast<float4*>(B.mem + B.o_tri_isect);
+    auto* shade = reinterpret_cast<float4*>(B.mem + B.o_tri_shade);
+    auto* snodes = reinterpret_cast<ana::BvhNode*>(B.mem + B.o_seg_nodes);
+    auto* segs = reinterpret_cast<float4*>(B.mem + B.o_segs);
+    auto* scol = reinterpret_cast<float*>(B.mem + B.o_scol);
+    auto* mats = reinterpret_cast<ana::DevMaterial*>(B.mem + B.o_mats);
+    auto* slots = reinterpret_cast<int32_t*>(B.mem + B.o_slots);
+    auto* lights = reinterpret_cast<ana::DevLight*>(B.mem + B.o_lights);
+    // child refs: interior nodes shift by the scene's node base, leaves by its primitive base
+    auto fix_node = [](ana::BvhNode nd, uint32_t nodeBase, uint32_t primBase) {
+        float* n3 = &nd.n3.x;
+        for (int ch = 0; ch < 2; ++ch) {
+            uint32_t ref = ubits(n3[ch]), cnt = ubits(n3[2 + ch]);
+            n3[ch] = fbits(ref + (cnt ? primBase : nodeBase));
+        }
+        return nd;
+    };
+    size_t iN = 0, iT = 0, iSN = 0, iS = 0, iStr = 0, iM = 0, iSl = 0, iL = 0;
+    B.scenes.assign(n, SceneStatic{});
+    B.has_curves = false;
+    B.has_emitters = false;
+    for (uint32_t k = 0; k < n; ++k) {
+        const ana::Prepared& P = *list[k];
+        SceneStatic& st = B.scenes[k];
+        const uint32_t nodeBase = uint32_t(iN), triBase = uint32_t(iT), sNodeBase = uint32_t(iSN),
+                       segBase = uint32_t(iS), strBase = uint32_t(iStr), matBase = uint32_t(iM);
+        st.tri_root = (P.num_tris && !P.tri_nodes.empty()) ? nodeBase : ana::kNoRoot;
+        for (const ana::BvhNode& nd : P.tri_nodes) nodes[iN++] = fix_node(nd, nodeBase, triBase);
+        for (uint32_t t = 0; t < P.num_tris; ++t) {
+            float4 a = P.tri_isect[3 * size_t(t)];
+            a.w = fbits(ubits(a.w) + triBase);  // index into the batch's shading array
+            isect[3 * (size_t(triBase) + t)] = a;
+            isect[3 * (size_t(triBase) + t) + 1] = P.tri_isect[3 * size_t(t) + 1];
+            isect[3 * (size_t(triBase) + t) + 2] = P.tri_isect[3 * size_t(t) + 2];
+            for (int j = 0; j < 4; ++j) shade[4 * (size_t(triBase) + t) + j] = P.tri_shade[4 * size_t(t) + j];
+        }
+        iT += P.num_tris;
+        st.seg_root = (P.num_segs && !P.seg_nodes.empty()) ? sNodeBase : ana::kNoRoot;
+        if (P.num_segs) B.has_curves = true;
+        for (const ana::BvhNode& nd : P.seg_nodes) snodes[iSN++] = fix_node(nd, sNodeBase, segBase);
+        for (uint32_t s = 0; s < P.num_segs; ++s) {
+            for (int j = 0; j < 4; ++j) segs[5 * (size_t(segBase) + s) + j] = P.segs[5 * size_t(s) + j];
+            float4 r = P.segs[5 * size_t(s) + 4];
+            r.x = fbits(ubits(r.x) + strBase);  // batch strand index
+            r.w = fbits(strBase);               // strand - w is the scene-local strand index
+            segs[5 * (size_t(segBase) + s) + 4] = r;
+        }
+        iS += P.num_segs;
+        for (size_t i = 0; i < P.strand_color.size(); ++i) scol[3 * size_t(strBase) + i] = P.strand_color[i];
+        iStr += P.strand_color.size() / 3;
+        for (const ana::DevMaterial& m : P.materials) mats[iM++] = m;
+        st.slot_base = uint32_t(iSl);
+        st.num_slots = uint32_t(P.slot_material.size());
+        for (int32_t s : P.slot_material) slots[iSl++] = s >= 0 ? s + int32_t(matBase) : -1;
+        st.light_base = uint32_t(iL);
+        st.num_lights = uint32_t(P.lights.size());
+        for (const ana::DevLight& l : P.lights) lights[iL++] = l;
+        st.has_dome = P.env.present;
+        std::memcpy(st.env_radiance, P.env.radiance, sizeof(st.env_radiance));
+        st.camera = P.camera;
+        if (P.has_emitters) B.has_emitters = true;
+    }
+    if (dome) {
+        std::memcpy(B.mem + B.o_env_rgb, dome->env.rgb.data(), dome->env.rgb.size() * 4);
+        std::memcpy(B.mem + B.o_cf, dome->env.cond_func.data(), dome->env.cond_func.size() * 4);
+        std::memcpy(B.mem + B.o_cc, dome->env.cond_cdf.data(), dome->env.cond_cdf.size() * 4);
+        std::memcpy(B.mem + B.o_ci, dome->env.cond_int.data(), dome->env.cond_int.size() * 4);
+        std::memcpy(B.mem + B.o_mf, dome->env.marg_func.data(), dome->env.marg_func.size() * 4);
+        std::memcpy(B.mem + B.o_mc, dome->env.marg_cdf.data(), dome->env.marg_cdf.size() * 4);
+        B.env_meta.present = true;
+        B.env_meta.width = dome->env.width;
+        B.env_meta.height = dome->env.height;
+        B.env_meta.intensity = dome->env.intensity;
+        B.env_meta.marg_int = dome->env.marg_int;
+    }
+    return ANA_OK;
+}
+
+}  // namespace
+
+// A prepared scene: the host-built device layout (BVHs, flattened materials,
+// dome distribution) and its single-scene pinned blob.
+struct ana_prepared {
+    ana::Prepared P;
+    Blob blob;
+};
+
+struct ana_batch {
+    std::vector<const ana_prepared*> items;
+    Blob blob;
+};
+
+struct GraphCache {
+    cudaGraphExec_t exec = nullptr;
+    std::vector<unsigned char> key;
 };
 
 struct ana_ctx {
@@ -57,28 +233,36 @@ struct ana_ctx {
     cudaStream_t stream = nullptr;
     std::string err;
     ana_device_opts opts{};
-    // scene
+    // scenes
     unsigned char* d_scene = nullptr;
     size_t d_scene_size = 0;
     ana::DevScene ds{};
-    ana_camera camera{};
+    std::vector<SceneStatic> scenes;
     bool has_scene = false;
-    // film
-    ana_film_pixel* film = nullptr;
-    uint32_t fw = 0, fh = 0;
+    uint64_t upload_serial = 0;
+    // per-render tables: scene records, path offsets, chunk pixel runs
+    unsigned char* d_tables = nullptr;
+    size_t d_tables_size = 0;
+    std::vector<unsigned char> h_tables;
+    // film (all items of the last render, back to back)
+    unsigned char* film = nullptr;
+    size_t film_bytes = 0, film_pixels = 0;
+    std::vector<size_t> item_film_offset, item_film_pixels;
     // wavefront buffers
     ana::Queues q{};
     unsigned char* d_queues = nullptr;
     uint32_t cap = 0;
-    uint32_t* d_counters = nullptr;
-    size_t counters_cap = 0;
+    unsigned char* d_counters = nullptr;
+    size_t counters_bytes = 0;
     uint32_t* d_err = nullptr;
-    unsigned long long* d_work = nullptr;  // 3 work counters (in the error-word allocation)
+    unsigned long long* d_work = nullptr;
     std::vector<uint32_t> h_counters;
     std::vector<cudaEvent_t> stage_ev;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    GraphCache graph;
     ana_stats stats{};
     int num_sms = 148;
+    ana_film_pixel* film_px() const { return reinterpret_cast<ana_film_pixel*>(film); }
 };
 
 namespace {
@@ -95,98 +279,51 @@ int cuda_fail(ana_ctx* c, cudaError_t e, const char* what) {
     return fail(c, e == cudaErrorMemoryAllocation ? ANA_ERR_OOM : ANA_ERR_CUDA, m);
 }
 
-#define CK(call, what)                                   \
-    do {                                                 \
-        cudaError_t e_ = (call);                         \
+#define CK(call, what)                                        \
+    do {                                                      \
+        cudaError_t e_ = (call);                              \
         if (e_ != cudaSuccess) return cuda_fail(c, e_, what); \
     } while (0)
 
-template <class T>
-void put(unsigned char* blob, size_t off, const std::vector<T>& v) {
-    if (!v.empty()) std::memcpy(blob + off, v.data(), v.size() * sizeof(T));
+void drop_graph(ana_ctx* c) {
+    if (c->graph.exec) cudaGraphExecDestroy(c->graph.exec);
+    c->graph.exec = nullptr;
+    c->graph.key.clear();
 }
 
-int build_prepared(const ana::Prepared& P, ana_prepared& out) {
-    size_t off = 0;
-    auto take = [&](size_t bytes) {
-        size_t o = off;
-        off = align_up(off + bytes);
-        return o;
-    };
-    out.o_tri_nodes = take(P.tri_nodes.size() * sizeof(ana::BvhNode));
-    out.o_tri_isect = take(P.tri_isect.size() * 16);
-    out.o_tri_shade = take(P.tri_shade.size() * 16);
-    out.o_seg_nodes = take(P.seg_nodes.size() * sizeof(ana::BvhNode));
-    out.o_segs = take(P.segs.size() * 16);
-    out.o_scol = take(P.strand_color.size() * 4);
-    out.o_mats = take(P.materials.size() * sizeof(ana::DevMaterial));
-    out.o_slots = take(P.slot_material.size() * 4);
-    out.o_lights = take(P.lights.size() * sizeof(ana::DevLight));
-    out.o_env_rgb = take(P.env.rgb.size() * 4);
-    out.o_cf = take(P.env.cond_func.size() * 4);
-    out.o_cc = take(P.env.cond_cdf.size() * 4);
-    out.o_ci = take(P.env.cond_int.size() * 4);
-    out.o_mf = take(P.env.marg_func.size() * 4);
-    out.o_mc = take(P.env.marg_cdf.size() * 4);
-    out.size = std::max<size_t>(off, kAlign);
-    void* mem = nullptr;
-    if (cudaHostAlloc(&mem, out.size, cudaHostAllocPortable) == cudaSuccess) {
-        out.pinned = true;
-    } else {
-        cudaGetLastError();
-        mem = std::aligned_alloc(kAlign, out.size);
-        out.pinned = false;
-        if (!mem) return ANA_ERR_OOM;
+// Grows a device buffer (contents are not kept). Any cached graph refers to
+// the old address, so it is dropped.
+int ensure_buffer(ana_ctx* c, unsigned char** p, size_t* have, size_t need, const char* what) {
+    if (*have >= need && *p) return ANA_OK;
+    if (*p) {
+        CK(cudaStreamSynchronize(c->stream), "sync");
+        cudaFree(*p);
+        *p = nullptr;
+        *have = 0;
     }
-    out.blob = static_cast<unsigned char*>(mem);
-    std::memset(out.blob, 0, out.size);
-    put(out.blob, out.o_tri_nodes, P.tri_nodes);
-    put(out.blob, out.o_tri_isect, P.tri_isect);
-    put(out.blob, out.o_tri_shade, P.tri_shade);
-    put(out.blob, out.o_seg_nodes, P.seg_nodes);
-    put(out.blob, out.o_segs, P.segs);
-    put(out.blob, out.o_scol, P.strand_color);
-    put(out.blob, out.o_mats, P.materials);
-    put(out.blob, out.o_slots, P.slot_material);
-    put(out.blob, out.o_lights, P.lights);
-    put(out.blob, out.o_env_rgb, P.env.rgb);
-    put(out.blob, out.o_cf, P.env.cond_func);
-    put(out.blob, out.o_cc, P.env.cond_cdf);
-    put(out.blob, out.o_ci, P.env.cond_int);
-    put(out.blob, out.o_mf, P.env.marg_func);
-    put(out.blob, out.o_mc, P.env.marg_cdf);
-    out.n_tri_nodes = uint32_t(P.tri_nodes.size());
-    out.n_tris = P.num_tris;
-    out.n_seg_nodes = uint32_t(P.seg_nodes.size());
-    out.n_segs = P.num_segs;
-    out.n_mats = uint32_t(P.materials.size());
-    out.n_slots = uint32_t(P.slot_material.size());
-    out.n_lights = uint32_t(P.lights.size());
-    out.tri_root_empty = P.tri_root_is_empty;
-    out.has_emitters = P.has_emitters;
-    out.env_meta.present = P.env.present;
-    out.env_meta.width = P.env.width;
-    out.env_meta.height = P.env.height;
-    out.env_meta.intensity = P.env.intensity;
-    out.env_meta.marg_int = P.env.marg_int;
-    std::memcpy(out.env_meta.radiance, P.env.radiance, sizeof(P.env.radiance));
-    out.camera = P.camera;
+    drop_graph(c);
+    void* mem = nullptr;
+    CK(cudaMalloc(&mem, need), what);
+    *p = static_cast<unsigned char*>(mem);
+    *have = need;
     return ANA_OK;
 }
 
 // Wavefront buffers for `cap` paths.
 int ensure_queues(ana_ctx* c, uint32_t cap) {
     if (c->cap >= cap && c->d_queues) return ANA_OK;
-    if (c->d_queues) {
-        cudaFree(c->d_queues);
-        c->d_queues = nullptr;
-        c->cap = 0;
-    }
     size_t f4 = size_t(cap) * 16;
     size_t total = 14 * align_up(f4) + align_up(size_t(cap) * 12);
-    void* mem = nullptr;
-    CK(cudaMalloc(&mem, total), "cudaMalloc(wavefront queues)");
-    unsigned char* b = static_cast<unsigned char*>(mem);
+    size_t have = c->d_queues ? size_t(1) : 0;  // force reallocation
+    if (c->d_queues) {
+        CK(cudaStreamSynchronize(c->stream), "sync");
+        cudaFree(c->d_queues);
+        c->d_queues = nullptr;
+        have = 0;
+    }
+    int rc = ensure_buffer(c, &c->d_queues, &have, total, "cudaMalloc(wavefront queues)");
+    if (rc) return rc;
+    unsigned char* b = c->d_queues;
     size_t off = 0;
     auto take = [&](size_t bytes) {
         unsigned char* p = b + off;
@@ -205,27 +342,327 @@ int ensure_queues(ana_ctx* c, uint32_t cap) {
     c->q.sh_c = reinterpret_cast<float4*>(take(f4));
     c->q.mis_o = reinterpret_cast<float4*>(take(f4));
     c->q.mis_d = reinterpret_cast<float4*>(take(f4));
-    c->q.L = reinterpret_cast<float*>(take(size_t(cap) * 12));
     c->q.mis_c = reinterpret_cast<float4*>(take(f4));
-    c->d_queues = b;
+    c->q.L = reinterpret_cast<float*>(take(size_t(cap) * 12));
     c->cap = cap;
     return ANA_OK;
 }
 
-int ensure_film(ana_ctx* c, uint32_t w, uint32_t h, bool clear) {
-    if (c->film && (c->fw != w || c->fh != h)) {
-        cudaFree(c->film);
-        c->film = nullptr;
+int upload_blob(ana_ctx* c, const Blob& B) {
+    CK(cudaSetDevice(c->device), "cudaSetDevice");
+    int rc = ensure_buffer(c, &c->d_scene, &c->d_scene_size, B.size, "cudaMalloc(scene)");
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(c->d_scene, B.mem, B.size, cudaMemcpyHostToDevice, c->stream), "scene upload");
+    unsigned char* b = c->d_scene;
+    ana::DevScene& S = c->ds;
+    S = ana::DevScene{};
+    S.tri_nodes = reinterpret_cast<const ana::BvhNode*>(b + B.o_tri_nodes);
+    S.tri_isect = reinterpret_cast<const float4*>(b + B.o_tri_isect);
+    S.tri_shade = reinterpret_cast<const float4*>(b + B.o_tri_shade);
+    S.seg_nodes = reinterpret_cast<const ana::BvhNode*>(b + B.o_seg_nodes);
+    S.segs = reinterpret_cast<const float4*>(b + B.o_segs);
+    S.strand_color = reinterpret_cast<const float*>(b + B.o_scol);
+    S.materials = reinterpret_cast<const ana::DevMaterial*>(b + B.o_mats);
+    S.slot_material = reinterpret_cast<const int32_t*>(b + B.o_slots);
+    S.lights = reinterpret_cast<const ana::DevLight*>(b + B.o_lights);
+    S.has_curves = B.has_curves ? 1 : 0;
+    S.has_emitters = B.has_emitters ? 1 : 0;
+    ana::DevEnv& E = S.env;
+    E.present = B.env_meta.present ? 1 : 0;
+    E.rgb = E.present ? reinterpret_cast<const float*>(b + B.o_env_rgb) : nullptr;
+    E.cond_func = reinterpret_cast<const float*>(b + B.o_cf);
+    E.cond_cdf = reinterpret_cast<const float*>(b + B.o_cc);
+    E.cond_int = reinterpret_cast<const float*>(b + B.o_ci);
+    E.marg_func = reinterpret_cast<const float*>(b + B.o_mf);
+    E.marg_cdf = reinterpret_cast<const float*>(b + B.o_mc);
+    E.marg_int = B.env_meta.marg_int;
+    E.intensity = B.env_meta.intensity;
+    E.width = B.env_meta.width;
+    E.height = B.env_meta.height;
+    c->scenes = B.scenes;
+    c->has_scene = true;
+    c->upload_serial++;
+    drop_graph(c);
+    return ANA_OK;
+}
+
+struct ChunkPlan {
+    uint32_t first_path, paths, pixels, seg_begin, seg_count;
+};
+
+// The batch render: descs[k] renders uploaded scene k into its film.
+int render_items(ana_ctx* c, const ana_render_desc* descs, uint32_t n, uint32_t flags) {
+    if (!c || !descs || n == 0) return fail(c, ANA_ERR_INVALID_ARG, "ana_render: NULL argument or no items");
+    if (!c->has_scene) return fail(c, ANA_ERR_STATE, "ana_render: no scene uploaded");
+    if (n != c->scenes.size())
+        return fail(c, ANA_ERR_INVALID_ARG, "ana_render_batch: one desc per uploaded scene is required");
+    uint64_t totalPaths = 0, totalPixels = 0;
+    uint32_t maxSpp = 0, maxDepth = 0;
+    for (uint32_t k = 0; k < n; ++k) {
+        const ana_render_desc& r = descs[k];
+        if (r.width == 0 || r.height == 0 || r.sample_count == 0)
+            return fail(c, ANA_ERR_INVALID_ARG, "ana_render: empty frame or zero samples");
+        if (r.max_depth > 255) return fail(c, ANA_ERR_INVALID_ARG, "ana_render: max_depth > 255");
+        totalPixels += uint64_t(r.width) * r.height;
+        totalPaths += uint64_t(r.width) * r.height * r.sample_count;
+        maxSpp = std::max(maxSpp, r.sample_count);
+        maxDepth = std::max(maxDepth, r.max_depth);
     }
-    if (!c->film) {
-        void* mem = nullptr;
-        CK(cudaMalloc(&mem, size_t(w) * h * sizeof(ana_film_pixel)), "cudaMalloc(film)");
-        c->film = static_cast<ana_film_pixel*>(mem);
-        c->fw = w;
-        c->fh = h;
-        clear = true;
+    if (totalPaths >= (1ull << 32))
+        return fail(c, ANA_ERR_INVALID_ARG, "ana_render: total width*height*sample_count must be < 2^32");
+    CK(cudaSetDevice(c->device), "cudaSetDevice");
+    const bool count_work = (flags & ANA_RENDER_COUNT_WORK) != 0;
+    const bool use_graph = (flags & ANA_RENDER_GRAPH) != 0 && !count_work;
+    const bool timing = c->opts.timing != 0 && !use_graph;
+    uint32_t cap = c->opts.chunk_paths ? c->opts.chunk_paths : (1u << 22);
+    cap = std::max(cap, maxSpp);
+    if (uint64_t(cap) > totalPaths) cap = uint32_t(totalPaths);
+    int rc = ensure_queues(c, cap);
+    if (rc) return rc;
+    // film: all items back to back
+    rc = ensure_buffer(c, &c->film, &c->film_bytes, totalPixels * sizeof(ana_film_pixel), "cudaMalloc(film)");
+    if (rc) return rc;
+    if (c->film_pixels != totalPixels) flags |= ANA_RENDER_CLEAR_FILM;
+    c->film_pixels = totalPixels;
+    c->item_film_offset.assign(n, 0);
+    c->item_film_pixels.assign(n, 0);
+    // scene records, path offsets, chunk plan
+    std::vector<ana::DevSceneRec> recs(n);
+    std::vector<uint32_t> pathOff(n + 1, 0);
+    uint64_t pix = 0, path = 0;
+    for (uint32_t k = 0; k < n; ++k) {
+        const ana_render_desc& r = descs[k];
+        const SceneStatic& st = c->scenes[k];
+        ana::DevSceneRec& R = recs[k];
+        std::memset(&R, 0, sizeof(R));
+        R.tri_root = st.tri_root;
+        R.seg_root = st.seg_root;
+        R.slot_base = st.slot_base;
+        R.num_slots = st.num_slots;
+        R.light_base = st.light_base;
+        R.num_lights = st.num_lights;
+        R.spp = r.sample_count;
+        R.sample_start = r.sample_start;
+        R.max_depth = r.max_depth;
+        R.min_depth = r.min_depth;
+        R.film_offset = uint32_t(pix);
+        R.path_offset = uint32_t(path);
+        R.seed = r.seed;
+        R.env_radiance = make_float3(st.env_radiance[0], st.env_radiance[1], st.env_radiance[2]);
+        R.has_dome = st.has_dome ? 1 : 0;
+        R.cam = ana::make_camera(st.camera, r.width, r.height);
+        c->item_film_offset[k] = pix;
+        c->item_film_pixels[k] = size_t(r.width) * r.height;
+        pathOff[k] = uint32_t(path);
+        pix += uint64_t(r.width) * r.height;
+        path += uint64_t(r.width) * r.height * r.sample_count;
     }
-    if (clear) CK(cudaMemsetAsync(c->film, 0, size_t(w) * h * sizeof(ana_film_pixel), c->stream), "memset film");
+    pathOff[n] = uint32_t(path);
+    // chunks: cut the global path space at pixel boundaries, `cap` paths each
+    std::vector<ana::ChunkSeg> segs;
+    std::vector<ChunkPlan> chunks;
+    {
+        ChunkPlan cp{0, 0, 0, 0, 0};
+        uint32_t gpath = 0;
+        for (uint32_t k = 0; k < n; ++k) {
+            const uint32_t spp = descs[k].sample_count;
+            const uint32_t npx = descs[k].width * descs[k].height;
+            uint32_t px = 0;
+            while (px < npx) {
+                uint32_t fit = std::min(npx - px, (cap - cp.paths) / spp);
+                if (fit == 0) {  // chunk full
+                    chunks.push_back(cp);
+                    cp = ChunkPlan{gpath, 0, 0, uint32_t(segs.size()), 0};
+                    continue;
+                }
+                ana::ChunkSeg sg{};
+                sg.scene = k;
+                sg.first_pixel = px;
+                sg.num_pixels = fit;
+                sg.local_pixel = cp.pixels;
+                sg.local_path = cp.paths;
+                segs.push_back(sg);
+                cp.seg_count++;
+                cp.paths += fit * spp;
+                cp.pixels += fit;
+                px += fit;
+                gpath += fit * spp;
+            }
+        }
+        if (cp.paths) chunks.push_back(cp);
+    }
+    const uint32_t nchunks = uint32_t(chunks.size());
+    // tables: records | path offsets | chunk pixel runs
+    const size_t oRec = 0, oOff = align_up(n * sizeof(ana::DevSceneRec)), oSeg = oOff + align_up((n + 1) * 4);
+    const size_t tbytes = oSeg + segs.size() * sizeof(ana::ChunkSeg);
+    std::vector<unsigned char> tables(tbytes, 0);
+    std::memcpy(tables.data() + oRec, recs.data(), n * sizeof(ana::DevSceneRec));
+    std::memcpy(tables.data() + oOff, pathOff.data(), (n + 1) * 4);
+    std::memcpy(tables.data() + oSeg, segs.data(), segs.size() * sizeof(ana::ChunkSeg));
+    rc = ensure_buffer(c, &c->d_tables, &c->d_tables_size, tbytes, "cudaMalloc(tables)");
+    if (rc) return rc;
+    if (tables != c->h_tables) {
+        c->h_tables = tables;
+        CK(cudaMemcpyAsync(c->d_tables, c->h_tables.data(), tbytes, cudaMemcpyHostToDevice, c->stream),
+           "tables H2D");
+    }
+    const uint32_t rows = maxDepth + 2;
+    const size_t ncount = size_t(nchunks) * rows * ana::kCountersPerBounce;
+    rc = ensure_buffer(c, &c->d_counters, &c->counters_bytes, ncount * 4, "cudaMalloc(counters)");
+    if (rc) return rc;
+    uint32_t* counters = reinterpret_cast<uint32_t*>(c->d_counters);
+    ana::Params p{};
+    p.S = c->ds;
+    p.S.scenes = reinterpret_cast<const ana::DevSceneRec*>(c->d_tables + oRec);
+    p.S.scene_path_offset = reinterpret_cast<const uint32_t*>(c->d_tables + oOff);
+    p.S.num_scenes = n;
+    p.q = c->q;
+    p.film = c->film_px();
+    p.err = c->d_err;
+    p.work = c->d_work;
+    ana::LaunchCfg cfg;
+    cfg.block = c->opts.block_size ? int(c->opts.block_size) : 256;
+    cfg.persistent = c->opts.traversal == ANA_TRAVERSAL_PER_RAY ? 0 : 1;
+    const long long gcap = ((long long)cap + cfg.block - 1) / cfg.block;
+    cfg.grid_cap = int(std::max<long long>(1, std::min<long long>(gcap, 1 << 20)));
+    const size_t launches = size_t(nchunks) * (2 + 4 * size_t(maxDepth + 1));
+    if (timing && c->stage_ev.size() < 2 * launches) {
+        size_t old = c->stage_ev.size();
+        c->stage_ev.resize(2 * launches);
+        for (size_t i = old; i < c->stage_ev.size(); ++i) CK(cudaEventCreate(&c->stage_ev[i]), "event create");
+    }
+    std::vector<int> stage_of;
+    size_t ev_i = 0;
+    cudaError_t first_launch_err = cudaSuccess;
+    const char* first_launch_stage = "";
+    static const char* kStageNames[5] = {"extend", "shade", "shadow", "mis", "generate/film"};
+    auto timed = [&](int stage, auto&& launch) {
+        if (timing) cudaEventRecord(c->stage_ev[2 * ev_i], c->stream);
+        launch();
+        cudaError_t le = cudaGetLastError();
+        if (le != cudaSuccess && first_launch_err == cudaSuccess) {
+            first_launch_err = le;
+            first_launch_stage = kStageNames[stage];
+        }
+        if (timing) {
+            cudaEventRecord(c->stage_ev[2 * ev_i + 1], c->stream);
+            stage_of.push_back(stage);
+            ++ev_i;
+        }
+    };
+    // the launch sequence (captured into a graph when requested)
+    const bool clear = (flags & ANA_RENDER_CLEAR_FILM) != 0;
+    auto enqueue = [&]() {
+        if (clear) cudaMemsetAsync(c->film, 0, totalPixels * sizeof(ana_film_pixel), c->stream);
+        cudaMemsetAsync(c->d_counters, 0, ncount * 4, c->stream);
+        cudaMemsetAsync(c->d_err, 0, 4, c->stream);
+        if (count_work) cudaMemsetAsync(c->d_work, 0, 3 * sizeof(unsigned long long), c->stream);
+        for (uint32_t k = 0; k < nchunks; ++k) {
+            const ChunkPlan& cp = chunks[k];
+            p.chunk_first_path = cp.first_path;
+            p.chunk_paths = cp.paths;
+            p.chunk_pixels = cp.pixels;
+            p.segs = reinterpret_cast<const ana::ChunkSeg*>(c->d_tables + oSeg) + cp.seg_begin;
+            p.num_segs = cp.seg_count;
+            p.counters = counters + size_t(k) * rows * ana::kCountersPerBounce;
+            p.bounce = 0;
+            timed(4, [&] { ana::launch_generate(p, cfg, c->stream); });
+            for (uint32_t b = 0; b <= maxDepth; ++b) {
+                p.bounce = b;
+                timed(0, [&] { ana::launch_extend(p, cfg, c->stream, count_work); });
+                timed(1, [&] { ana::launch_shade(p, cfg, c->stream); });
+                timed(2, [&] { ana::launch_shadow(p, cfg, c->stream); });
+                timed(3, [&] { ana::launch_mis(p, cfg, c->stream); });
+            }
+            timed(4, [&] { ana::launch_film(p, cfg, c->stream); });
+        }
+    };
+    CK(cudaEventRecord(c->ev0, c->stream), "event");
+    if (use_graph) {
+        // the graph is reused while the tables, flags, launch configuration,
+        // buffers and uploaded scene are unchanged
+        std::vector<unsigned char> key = c->h_tables;
+        auto put = [&](const void* x, size_t nb) {
+            const unsigned char* bb = static_cast<const unsigned char*>(x);
+            key.insert(key.end(), bb, bb + nb);
+        };
+        put(&clear, sizeof(clear));
+        put(&cfg, sizeof(cfg));
+        put(&cap, sizeof(cap));
+        put(&c->upload_serial, sizeof(c->upload_serial));
+        if (!c->graph.exec || c->graph.key != key) {
+            drop_graph(c);
+            cudaGraph_t g = nullptr;
+            CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+            enqueue();
+            cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+            if (first_launch_err != cudaSuccess) {
+                if (g) cudaGraphDestroy(g);
+                std::string what = std::string("graph capture: ") + first_launch_stage + " launch";
+                return cuda_fail(c, first_launch_err, what.c_str());
+            }
+            if (e != cudaSuccess) return cuda_fail(c, e, "end capture");
+            e = cudaGraphInstantiate(&c->graph.exec, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) {
+                c->graph.exec = nullptr;
+                return cuda_fail(c, e, "graph instantiate");
+            }
+            c->graph.key = key;
+        }
+        CK(cudaGraphLaunch(c->graph.exec, c->stream), "graph launch");
+    } else {
+        enqueue();
+        if (first_launch_err != cudaSuccess) {
+            std::string what = std::string(first_launch_stage) + " launch";
+            return cuda_fail(c, first_launch_err, what.c_str());
+        }
+    }
+    CK(cudaGetLastError(), "kernel launch");
+    CK(cudaEventRecord(c->ev1, c->stream), "event");
+    unsigned long long hwork[3] = {0, 0, 0};
+    if (count_work)
+        CK(cudaMemcpyAsync(hwork, c->d_work, sizeof(hwork), cudaMemcpyDeviceToHost, c->stream), "work D2H");
+    c->h_counters.resize(ncount);
+    CK(cudaMemcpyAsync(c->h_counters.data(), counters, ncount * 4, cudaMemcpyDeviceToHost, c->stream),
+       "counters D2H");
+    uint32_t herr = 0;
+    CK(cudaMemcpyAsync(&herr, c->d_err, 4, cudaMemcpyDeviceToHost, c->stream), "err D2H");
+    CK(cudaStreamSynchronize(c->stream), "render sync");
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    ana_stats& st = c->stats;
+    st = ana_stats{};
+    st.paths = totalPaths;
+    for (uint32_t k = 0; k < nchunks; ++k)
+        for (uint32_t b = 0; b < rows; ++b) {
+            const uint32_t* cc = c->h_counters.data() + (size_t(k) * rows + b) * ana::kCountersPerBounce;
+            if (b <= maxDepth) st.extend_rays += cc[0];
+            st.shadow_rays += cc[1];
+            st.mis_rays += cc[2];
+            if (cc[0]) st.bounces = std::max(st.bounces, b + 1);
+        }
+    st.render_ms = ms;
+    st.chunks = nchunks;
+    st.kernel_launches = launches;
+    st.extend_launches = size_t(nchunks) * (maxDepth + 1);
+    st.node_fetches = hwork[0];
+    st.tri_tests = hwork[1];
+    st.seg_tests = hwork[2];
+    if (timing) {
+        float acc[5] = {0, 0, 0, 0, 0};
+        for (size_t i = 0; i < ev_i; ++i) {
+            float e = 0.f;
+            cudaEventElapsedTime(&e, c->stage_ev[2 * i], c->stage_ev[2 * i + 1]);
+            acc[stage_of[i]] += e;
+        }
+        st.extend_ms = acc[0];
+        st.shade_ms = acc[1];
+        st.shadow_ms = acc[2];
+        st.mis_ms = acc[3];
+        st.film_ms = acc[4];
+    }
+    if (herr) return fail(c, ANA_ERR_DEVICE_CHECK, "ana_render: traversal stack overflow on the device");
     return ANA_OK;
 }
 
@@ -254,6 +691,14 @@ int ana_create(ana_ctx** out, const ana_device_opts* opts) {
         delete c;
         return fail(nullptr, ANA_ERR_INVALID_ARG, "ana_create: device ordinal out of range");
     }
+    if (c->opts.block_size && (c->opts.block_size % 32 || c->opts.block_size > 512)) {
+        delete c;
+        return fail(nullptr, ANA_ERR_INVALID_ARG, "ana_create: block_size must be a multiple of 32, <= 512");
+    }
+    if (c->opts.traversal > ANA_TRAVERSAL_PER_RAY) {
+        delete c;
+        return fail(nullptr, ANA_ERR_INVALID_ARG, "ana_create: unknown traversal schedule");
+    }
     auto bail = [&](cudaError_t err, const char* what) {
         std::string m = std::string(what) + ": " + cudaGetErrorString(err);
         cudaGetLastError();
@@ -271,6 +716,8 @@ int ana_create(ana_ctx** out, const ana_device_opts* opts) {
     cudaEventCreate(&c->ev0);
     cudaEventCreate(&c->ev1);
     cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device);
+    ana::prime_kernels();
+    if ((e = cudaGetLastError()) != cudaSuccess) return bail(e, "kernel load");
     *out = c;
     return ANA_OK;
 }
@@ -279,7 +726,9 @@ void ana_destroy(ana_ctx* c) {
     if (!c) return;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    drop_graph(c);
     cudaFree(c->d_scene);
+    cudaFree(c->d_tables);
     cudaFree(c->film);
     cudaFree(c->d_queues);
     cudaFree(c->d_counters);
@@ -294,80 +743,44 @@ void ana_destroy(ana_ctx* c) {
 int ana_prepare_scene(const ana_scene_desc* d, ana_prepared** out) {
     if (!d || !out) return fail(nullptr, ANA_ERR_INVALID_ARG, "ana_prepare_scene: NULL argument");
     *out = nullptr;
-    ana::Prepared P;
+    ana_prepared* pp = new (std::nothrow) ana_prepared();
+    if (!pp) return fail(nullptr, ANA_ERR_OOM, "ana_prepare_scene: host allocation failed");
     std::string err;
     int rc;
     try {
-        rc = ana::prepare_scene(*d, P, err);
+        rc = ana::prepare_scene(*d, pp->P, err);
+        if (rc == ANA_OK) {
+            const ana::Prepared* one = &pp->P;
+            rc = build_blob(&one, 1, pp->blob, err);
+        }
     } catch (const std::bad_alloc&) {
+        delete pp;
         return fail(nullptr, ANA_ERR_OOM, "ana_prepare_scene: host allocation failed");
     }
-    if (rc != ANA_OK) return fail(nullptr, rc, "ana_prepare_scene: " + err);
-    ana_prepared* pp = new (std::nothrow) ana_prepared();
-    if (!pp) return fail(nullptr, ANA_ERR_OOM, "ana_prepare_scene: host allocation failed");
-    rc = build_prepared(P, *pp);
     if (rc != ANA_OK) {
         delete pp;
-        return fail(nullptr, rc, "ana_prepare_scene: blob allocation failed");
+        return fail(nullptr, rc, "ana_prepare_scene: " + err);
     }
     *out = pp;
     return ANA_OK;
 }
 
-uint64_t ana_prepared_bytes(const ana_prepared* p) { return p ? p->size : 0; }
+uint64_t ana_prepared_bytes(const ana_prepared* p) { return p ? p->blob.size : 0; }
+
+uint64_t ana_prepared_digest(const ana_prepared* p) {
+    if (!p || !p->blob.mem) return 0;
+    uint64_t h = 1469598103934665603ULL;
+    for (size_t i = 0; i < p->blob.size; ++i) {
+        h ^= p->blob.mem[i];
+        h *= 1099511628211ULL;
+    }
+    return h;
+}
 void ana_prepared_free(ana_prepared* p) { delete p; }
 
 int ana_upload_prepared(ana_ctx* c, const ana_prepared* p) {
     if (!c || !p) return fail(c, ANA_ERR_INVALID_ARG, "ana_upload_prepared: NULL argument");
-    CK(cudaSetDevice(c->device), "cudaSetDevice");
-    if (c->d_scene_size < p->size) {
-        CK(cudaStreamSynchronize(c->stream), "sync");
-        cudaFree(c->d_scene);
-        c->d_scene = nullptr;
-        c->d_scene_size = 0;
-        void* mem = nullptr;
-        CK(cudaMalloc(&mem, p->size), "cudaMalloc(scene)");
-        c->d_scene = static_cast<unsigned char*>(mem);
-        c->d_scene_size = p->size;
-    }
-    CK(cudaMemcpyAsync(c->d_scene, p->blob, p->size, cudaMemcpyHostToDevice, c->stream), "scene upload");
-    unsigned char* b = c->d_scene;
-    ana::DevScene& S = c->ds;
-    S = ana::DevScene{};
-    S.tri_nodes = reinterpret_cast<const ana::BvhNode*>(b + p->o_tri_nodes);
-    S.tri_isect = reinterpret_cast<const float4*>(b + p->o_tri_isect);
-    S.tri_shade = reinterpret_cast<const float4*>(b + p->o_tri_shade);
-    S.num_tri_nodes = p->n_tri_nodes;
-    S.num_tris = p->n_tris;
-    S.tri_root_is_empty = p->tri_root_empty ? 1 : 0;
-    S.seg_nodes = reinterpret_cast<const ana::BvhNode*>(b + p->o_seg_nodes);
-    S.segs = reinterpret_cast<const float4*>(b + p->o_segs);
-    S.strand_color = reinterpret_cast<const float*>(b + p->o_scol);
-    S.num_seg_nodes = p->n_seg_nodes;
-    S.num_segs = p->n_segs;
-    S.materials = reinterpret_cast<const ana::DevMaterial*>(b + p->o_mats);
-    S.slot_material = reinterpret_cast<const int32_t*>(b + p->o_slots);
-    S.num_materials = p->n_mats;
-    S.num_slots = p->n_slots;
-    S.lights = reinterpret_cast<const ana::DevLight*>(b + p->o_lights);
-    S.num_lights = p->n_lights;
-    S.has_emitters = p->has_emitters ? 1 : 0;
-    ana::DevEnv& E = S.env;
-    E.present = p->env_meta.present ? 1 : 0;
-    E.rgb = E.present ? reinterpret_cast<const float*>(b + p->o_env_rgb) : nullptr;
-    E.cond_func = reinterpret_cast<const float*>(b + p->o_cf);
-    E.cond_cdf = reinterpret_cast<const float*>(b + p->o_cc);
-    E.cond_int = reinterpret_cast<const float*>(b + p->o_ci);
-    E.marg_func = reinterpret_cast<const float*>(b + p->o_mf);
-    E.marg_cdf = reinterpret_cast<const float*>(b + p->o_mc);
-    E.marg_int = p->env_meta.marg_int;
-    E.intensity = p->env_meta.intensity;
-    E.width = p->env_meta.width;
-    E.height = p->env_meta.height;
-    E.radiance = make_float3(p->env_meta.radiance[0], p->env_meta.radiance[1], p->env_meta.radiance[2]);
-    c->camera = p->camera;
-    c->has_scene = true;
-    return ANA_OK;
+    return upload_blob(c, p->blob);
 }
 
 int ana_upload_scene(ana_ctx* c, const ana_scene_desc* d) {
@@ -388,18 +801,77 @@ int ana_upload_scene(ana_ctx* c, const ana_scene_desc* d) {
     return rc;
 }
 
+int ana_batch_create(const ana_prepared* const* scenes, uint32_t count, ana_batch** out) {
+    if (!scenes || !out || count == 0) return fail(nullptr, ANA_ERR_INVALID_ARG, "ana_batch_create: bad arguments");
+    *out = nullptr;
+    std::vector<const ana::Prepared*> list(count);
+    for (uint32_t k = 0; k < count; ++k) {
+        if (!scenes[k]) return fail(nullptr, ANA_ERR_INVALID_ARG, "ana_batch_create: NULL scene");
+        list[k] = &scenes[k]->P;
+    }
+    ana_batch* b = new (std::nothrow) ana_batch();
+    if (!b) return fail(nullptr, ANA_ERR_OOM, "ana_batch_create: host allocation failed");
+    std::string err;
+    int rc = build_blob(list.data(), count, b->blob, err);
+    if (rc != ANA_OK) {
+        delete b;
+        return fail(nullptr, rc, "ana_batch_create: " + err);
+    }
+    b->items.assign(scenes, scenes + count);
+    *out = b;
+    return ANA_OK;
+}
+
+void ana_batch_free(ana_batch* b) { delete b; }
+uint64_t ana_batch_bytes(const ana_batch* b) { return b ? b->blob.size : 0; }
+
+int ana_upload_batch(ana_ctx* c, const ana_batch* b) {
+    if (!c || !b) return fail(c, ANA_ERR_INVALID_ARG, "ana_upload_batch: NULL argument");
+    return upload_blob(c, b->blob);
+}
+
+int ana_render(ana_ctx* c, const ana_render_desc* r) {
+    if (!c || !r) return fail(c, ANA_ERR_INVALID_ARG, "ana_render: NULL argument");
+    if (c->has_scene && c->scenes.size() != 1)
+        return fail(c, ANA_ERR_STATE, "ana_render: a batch is uploaded; use ana_render_batch");
+    return render_items(c, r, 1, r->flags);
+}
+
+int ana_render_batch(ana_ctx* c, const ana_render_desc* descs, uint32_t count, uint32_t flags) {
+    return render_items(c, descs, count, flags);
+}
+
 int ana_film_clear(ana_ctx* c, uint32_t w, uint32_t h) {
     if (!c || w == 0 || h == 0) return fail(c, ANA_ERR_INVALID_ARG, "ana_film_clear: bad size");
     CK(cudaSetDevice(c->device), "cudaSetDevice");
-    return ensure_film(c, w, h, true);
+    size_t n = size_t(w) * h;
+    int rc = ensure_buffer(c, &c->film, &c->film_bytes, n * sizeof(ana_film_pixel), "cudaMalloc(film)");
+    if (rc) return rc;
+    c->film_pixels = n;
+    CK(cudaMemsetAsync(c->film, 0, n * sizeof(ana_film_pixel), c->stream), "memset film");
+    return ANA_OK;
 }
 
 int ana_film_read(ana_ctx* c, ana_film_pixel* out, size_t count) {
     if (!c || !out) return fail(c, ANA_ERR_INVALID_ARG, "ana_film_read: NULL argument");
-    if (!c->film) return fail(c, ANA_ERR_STATE, "ana_film_read: no film");
-    if (count != size_t(c->fw) * c->fh) return fail(c, ANA_ERR_INVALID_ARG, "ana_film_read: count != width*height");
+    if (!c->film || c->film_pixels == 0) return fail(c, ANA_ERR_STATE, "ana_film_read: no film");
+    if (count != c->film_pixels)
+        return fail(c, ANA_ERR_INVALID_ARG, "ana_film_read: count != pixels of the last render");
     CK(cudaSetDevice(c->device), "cudaSetDevice");
     CK(cudaMemcpyAsync(out, c->film, count * sizeof(ana_film_pixel), cudaMemcpyDeviceToHost, c->stream), "film D2H");
+    CK(cudaStreamSynchronize(c->stream), "film sync");
+    return ANA_OK;
+}
+
+int ana_batch_film_read(ana_ctx* c, uint32_t item, ana_film_pixel* out, size_t count) {
+    if (!c || !out) return fail(c, ANA_ERR_INVALID_ARG, "ana_batch_film_read: NULL argument");
+    if (item >= c->item_film_offset.size()) return fail(c, ANA_ERR_INVALID_ARG, "ana_batch_film_read: bad item");
+    if (count != c->item_film_pixels[item])
+        return fail(c, ANA_ERR_INVALID_ARG, "ana_batch_film_read: count != the item's pixels");
+    CK(cudaSetDevice(c->device), "cudaSetDevice");
+    CK(cudaMemcpyAsync(out, c->film_px() + c->item_film_offset[item], count * sizeof(ana_film_pixel),
+                       cudaMemcpyDeviceToHost, c->stream),
+       "film D2H");
     CK(cudaStreamSynchronize(c->stream), "film sync");
     return ANA_OK;
 }
@@ -411,175 +883,48 @@ int ana_film_device_ptr(ana_ctx* c, void** dptr) {
     return ANA_OK;
 }
 
-int ana_render(ana_ctx* c, const ana_render_desc* r) {
-    if (!c || !r) return fail(c, ANA_ERR_INVALID_ARG, "ana_render: NULL argument");
-    if (!c->has_scene) return fail(c, ANA_ERR_STATE, "ana_render: no scene uploaded");
-    if (r->width == 0 || r->height == 0 || r->sample_count == 0)
-        return fail(c, ANA_ERR_INVALID_ARG, "ana_render: empty frame or zero samples");
-    if (r->max_depth > 255) return fail(c, ANA_ERR_INVALID_ARG, "ana_render: max_depth > 255");
-    uint64_t npix = uint64_t(r->width) * r->height;
-    if (npix * r->sample_count >= (1ull << 32))
-        return fail(c, ANA_ERR_INVALID_ARG, "ana_render: width*height*sample_count must be < 2^32");
-    CK(cudaSetDevice(c->device), "cudaSetDevice");
-    int rc = ensure_film(c, r->width, r->height, (r->flags & ANA_RENDER_CLEAR_FILM) != 0);
-    if (rc) return rc;
-    uint32_t want = c->opts.chunk_paths ? c->opts.chunk_paths : (1u << 22);
-    if (want < r->sample_count) want = r->sample_count;
-    uint32_t chunk_px = want / r->sample_count;
-    if (uint64_t(chunk_px) > npix) chunk_px = uint32_t(npix);
-    uint32_t cap = chunk_px * r->sample_count;
-    rc = ensure_queues(c, cap);
-    if (rc) return rc;
-    uint32_t nchunks = uint32_t((npix + chunk_px - 1) / chunk_px);
-    uint32_t rows = r->max_depth + 2;
-    size_t ncount = size_t(nchunks) * rows * ana::kCountersPerBounce;
-    if (c->counters_cap < ncount) {
-        cudaFree(c->d_counters);
-        c->d_counters = nullptr;
-        void* mem = nullptr;
-        CK(cudaMalloc(&mem, ncount * 4), "cudaMalloc(counters)");
-        c->d_counters = static_cast<uint32_t*>(mem);
-        c->counters_cap = ncount;
-    }
-    CK(cudaMemsetAsync(c->d_counters, 0, ncount * 4, c->stream), "memset counters");
-    CK(cudaMemsetAsync(c->d_err, 0, 4, c->stream), "memset err");
-
-    ana::Params p{};
-    p.S = c->ds;
-    p.S.cam = ana::make_camera(c->camera, r->width, r->height);
-    p.q = c->q;
-    p.film = c->film;
-    p.err = c->d_err;
-    p.seed = r->seed;
-    p.W = r->width;
-    p.H = r->height;
-    p.spp = r->sample_count;
-    p.sample_start = r->sample_start;
-    p.max_depth = r->max_depth;
-    p.min_depth = r->min_depth;
-    ana::LaunchCfg cfg;
-    cfg.block = c->opts.block_size ? int(c->opts.block_size) : 256;
-    cfg.persistent = c->opts.traversal == ANA_TRAVERSAL_PER_RAY ? 0 : 1;
-    long long gcap = ((long long)cap + cfg.block - 1) / cfg.block;
-    cfg.grid_cap = int(std::max<long long>(1, std::min<long long>(gcap, 1 << 20)));
-    const bool count_work = (r->flags & ANA_RENDER_COUNT_WORK) != 0;
-    p.work = c->d_work;
-    if (count_work) CK(cudaMemsetAsync(c->d_work, 0, 3 * sizeof(unsigned long long), c->stream), "memset work");
-    // Per-stage CUDA events (timing mode): one pair per launch, on this stream.
-    const bool timing = c->opts.timing != 0;
-    const size_t launches = size_t(nchunks) * (2 + 4 * (r->max_depth + 1));
-    if (timing && c->stage_ev.size() < 2 * launches) {
-        size_t old = c->stage_ev.size();
-        c->stage_ev.resize(2 * launches);
-        for (size_t i = old; i < c->stage_ev.size(); ++i) CK(cudaEventCreate(&c->stage_ev[i]), "event create");
-    }
-    std::vector<int> stage_of;
-    if (timing) stage_of.reserve(launches);
-    size_t ev_i = 0;
-    auto timed = [&](int stage, auto&& launch) {
-        if (timing) cudaEventRecord(c->stage_ev[2 * ev_i], c->stream);
-        launch();
-        if (timing) {
-            cudaEventRecord(c->stage_ev[2 * ev_i + 1], c->stream);
-            stage_of.push_back(stage);
-            ++ev_i;
-        }
-    };
-    CK(cudaEventRecord(c->ev0, c->stream), "event");
-    for (uint32_t k = 0; k < nchunks; ++k) {
-        p.chunk_first_pixel = k * chunk_px;
-        p.chunk_pixels = uint32_t(std::min<uint64_t>(chunk_px, npix - uint64_t(k) * chunk_px));
-        p.counters = c->d_counters + size_t(k) * rows * ana::kCountersPerBounce;
-        p.bounce = 0;
-        timed(4, [&] { ana::launch_generate(p, cfg, c->stream); });
-        for (uint32_t b = 0; b <= r->max_depth; ++b) {
-            p.bounce = b;
-            timed(0, [&] { ana::launch_extend(p, cfg, c->stream, count_work); });
-            timed(1, [&] { ana::launch_shade(p, cfg, c->stream); });
-            timed(2, [&] { ana::launch_shadow(p, cfg, c->stream); });
-            timed(3, [&] { ana::launch_mis(p, cfg, c->stream); });
-        }
-        timed(4, [&] { ana::launch_film(p, cfg, c->stream); });
-    }
-    CK(cudaGetLastError(), "kernel launch");
-    CK(cudaEventRecord(c->ev1, c->stream), "event");
-    unsigned long long hwork[3] = {0, 0, 0};
-    if (count_work)
-        CK(cudaMemcpyAsync(hwork, c->d_work, sizeof(hwork), cudaMemcpyDeviceToHost, c->stream), "work D2H");
-    c->h_counters.resize(ncount);
-    CK(cudaMemcpyAsync(c->h_counters.data(), c->d_counters, ncount * 4, cudaMemcpyDeviceToHost, c->stream),
-       "counters D2H");
-    uint32_t herr = 0;
-    CK(cudaMemcpyAsync(&herr, c->d_err, 4, cudaMemcpyDeviceToHost, c->stream), "err D2H");
-    CK(cudaStreamSynchronize(c->stream), "render sync");
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
-    ana_stats& st = c->stats;
-    st = ana_stats{};
-    st.paths = npix * r->sample_count;
-    for (uint32_t k = 0; k < nchunks; ++k)
-        for (uint32_t b = 0; b < rows; ++b) {
-            const uint32_t* cc = c->h_counters.data() + (size_t(k) * rows + b) * ana::kCountersPerBounce;
-            if (b <= r->max_depth) st.extend_rays += cc[0];
-            st.shadow_rays += cc[1];
-            st.mis_rays += cc[2];
-            if (cc[0]) st.bounces = std::max(st.bounces, b + 1);
-        }
-    st.render_ms = ms;
-    st.chunks = nchunks;
-    st.kernel_launches = launches;
-    st.extend_launches = size_t(nchunks) * (r->max_depth + 1);
-    st.node_fetches = hwork[0];
-    st.tri_tests = hwork[1];
-    st.seg_tests = hwork[2];
-    if (timing) {
-        float acc[5] = {0, 0, 0, 0, 0};
-        for (size_t i = 0; i < ev_i; ++i) {
-            float e = 0.f;
-            cudaEventElapsedTime(&e, c->stage_ev[2 * i], c->stage_ev[2 * i + 1]);
-            acc[stage_of[i]] += e;
-        }
-        st.extend_ms = acc[0];
-        st.shade_ms = acc[1];
-        st.shadow_ms = acc[2];
-        st.mis_ms = acc[3];
-        st.film_ms = acc[4];
-    }
-    if (herr) return fail(c, ANA_ERR_DEVICE_CHECK, "ana_render: traversal stack overflow on the device");
-    return ANA_OK;
-}
-
 int ana_trace_batch(ana_ctx* c, const float* rays, size_t n, ana_hit* out, int occlusion, int on_device) {
     if (!c || (!rays && n) || (!out && n)) return fail(c, ANA_ERR_INVALID_ARG, "ana_trace_batch: NULL argument");
     if (!c->has_scene) return fail(c, ANA_ERR_STATE, "ana_trace_batch: no scene uploaded");
     if (n == 0) return ANA_OK;
+    if (n >= (size_t(1) << 32) - 64) return fail(c, ANA_ERR_INVALID_ARG, "ana_trace_batch: n >= 2^32");
     CK(cudaSetDevice(c->device), "cudaSetDevice");
+    // one scene record (scene 0: its roots) ahead of the rays
+    ana::DevSceneRec R{};
+    R.tri_root = c->scenes[0].tri_root;
+    R.seg_root = c->scenes[0].seg_root;
+    const size_t recBytes = align_up(sizeof(R));
+    const size_t tmpBytes = recBytes + (on_device ? 0 : n * 32 + n * sizeof(ana_hit));
+    void* tmp = nullptr;
+    CK(cudaMalloc(&tmp, tmpBytes), "cudaMalloc(trace batch)");
+    unsigned char* tb = static_cast<unsigned char*>(tmp);
     const float* d_rays = rays;
     ana_hit* d_out = out;
-    void* tmp = nullptr;
+    cudaError_t e = cudaMemcpyAsync(tb, &R, sizeof(R), cudaMemcpyHostToDevice, c->stream);
     if (!on_device) {
-        CK(cudaMalloc(&tmp, n * 32 + n * sizeof(ana_hit)), "cudaMalloc(trace batch)");
-        d_rays = static_cast<const float*>(tmp);
-        d_out = reinterpret_cast<ana_hit*>(static_cast<unsigned char*>(tmp) + n * 32);
-        cudaError_t e = cudaMemcpyAsync(tmp, rays, n * 32, cudaMemcpyHostToDevice, c->stream);
-        if (e != cudaSuccess) {
-            cudaFree(tmp);
-            return cuda_fail(c, e, "rays H2D");
-        }
+        d_rays = reinterpret_cast<const float*>(tb + recBytes);
+        d_out = reinterpret_cast<ana_hit*>(tb + recBytes + n * 32);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(tb + recBytes, rays, n * 32, cudaMemcpyHostToDevice, c->stream);
     }
-    if (n >= (size_t(1) << 32) - 64) return fail(c, ANA_ERR_INVALID_ARG, "ana_trace_batch: n >= 2^32");
     uint32_t* d_fetch = c->d_err + 32;  // fetch counter of the persistent kernel
-    CK(cudaMemsetAsync(c->d_err, 0, 4, c->stream), "memset err");
-    CK(cudaMemsetAsync(d_fetch, 0, 4, c->stream), "memset fetch");
-    ana::launch_trace_batch(c->ds, d_rays, n, d_out, occlusion, d_fetch, c->d_err,
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->d_err, 0, 4, c->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_fetch, 0, 4, c->stream);
+    if (e != cudaSuccess) {
+        cudaFree(tmp);
+        return cuda_fail(c, e, "trace batch setup");
+    }
+    ana::DevScene S = c->ds;
+    S.scenes = reinterpret_cast<const ana::DevSceneRec*>(tb);
+    S.num_scenes = 1;
+    ana::launch_trace_batch(S, 0, d_rays, n, d_out, occlusion, d_fetch, c->d_err,
                             c->opts.traversal == ANA_TRAVERSAL_PER_RAY ? 0 : 1, c->stream);
-    cudaError_t e = cudaGetLastError();
+    e = cudaGetLastError();
     uint32_t herr = 0;
     if (e == cudaSuccess && !on_device)
         e = cudaMemcpyAsync(out, d_out, n * sizeof(ana_hit), cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, c->d_err, 4, cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-    if (tmp) cudaFree(tmp);
+    cudaFree(tmp);
     if (e != cudaSuccess) return cuda_fail(c, e, "trace batch");
     if (herr) return fail(c, ANA_ERR_DEVICE_CHECK, "ana_trace_batch: traversal stack overflow on the device");
     return ANA_OK;

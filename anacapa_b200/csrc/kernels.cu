@@ -9,10 +9,20 @@
 //   mis       closest hit of the BSDF-sampled MIS rays; adds emitter Le / env
 //   film      per-pixel reduction into the film      (renderTile 43-57)
 //
+// A render is a batch of scenes (a plain render is a batch of one): every
+// path carries its scene index, and the scene record gives its BVH roots,
+// slot and light ranges, camera, spp and depth. Chunks are cut in the global
+// path space at pixel boundaries, so one chunk can hold paths of several
+// scenes and the queues stay full across scene boundaries.
+//
 // Queues are SoA float4 arrays. Each stage kernel appends to the next queue
 // with a block-level allocation: warp ballots give each lane its rank, one
 // shared-memory scan over the block's warps and a single atomicAdd per block
 // reserve a contiguous range, so every warp writes a contiguous, coalesced run.
+#include <map>
+#include <mutex>
+#include <utility>
+
 #include "kernels.h"
 #include "sampler.cuh"
 #include "shade.cuh"
@@ -22,8 +32,9 @@ namespace ana {
 
 constexpr uint32_t kMiss = 0xFFFFFFFFu;
 constexpr int kMaxBlock = 1024;
-constexpr int kPersistBlock = 256;     // persistent traversal kernels: 8 warps per block
-constexpr int kPersistMinBlocks = 4;   // 4 resident blocks per SM: at most 64 registers
+constexpr int kPersistBlock = 256;    // traversal kernels: 8 warps per block
+constexpr int kPersistMinBlocks = 4;  // persistent schedule: 4 resident blocks/SM (<= 64 registers)
+constexpr int kMaxStageBlock = 512;   // largest block of k_shade (the tunable stage kernel)
 
 // Reserve one slot per thread with want == true; returns the slot (valid only
 // for those threads). Must be reached by every thread of the block.
@@ -52,18 +63,32 @@ __device__ __forceinline__ uint32_t block_push(bool want, uint32_t* counter) {
 }
 
 __device__ __forceinline__ float4 pack(float3 v, float w) { return make_float4(v.x, v.y, v.z, w); }
-__device__ __forceinline__ float4 pack_u(float3 v, uint32_t w) { return make_float4(v.x, v.y, v.z, __uint_as_float(w)); }
-
-__device__ __forceinline__ void path_coords(const Params& p, uint32_t pid, uint32_t& px, uint32_t& py,
-                                            uint32_t& sidx) {
-    uint32_t pixel = pid / p.spp;
-    sidx = p.sample_start + (pid - pixel * p.spp);
-    py = pixel / p.W;
-    px = pixel - py * p.W;
+__device__ __forceinline__ float4 pack_u(float3 v, uint32_t w) {
+    return make_float4(v.x, v.y, v.z, __uint_as_float(w));
 }
 
-__device__ __forceinline__ void add_L(const Params& p, uint32_t pid, float3 v) {
-    size_t li = size_t(pid - p.chunk_first_pixel * p.spp) * 3;
+// Scene of a global path id: the last scene whose first path is <= gid.
+__device__ __forceinline__ uint32_t scene_of(const DevScene& S, uint32_t gid) {
+    uint32_t lo = 0, hi = S.num_scenes;  // invariant: offset[lo] <= gid < offset[hi]
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(S.scene_path_offset + mid) <= gid) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ void path_coords(const DevSceneRec& R, uint32_t gid, uint32_t& px, uint32_t& py,
+                                            uint32_t& sidx) {
+    uint32_t local = gid - R.path_offset;
+    uint32_t pixel = local / R.spp;
+    sidx = R.sample_start + (local - pixel * R.spp);
+    py = pixel / R.cam.width;
+    px = pixel - py * R.cam.width;
+}
+
+__device__ __forceinline__ void add_L(const Params& p, uint32_t gid, float3 v) {
+    size_t li = size_t(gid - p.chunk_first_path) * 3;
     p.q.L[li + 0] += v.x;
     p.q.L[li + 1] += v.y;
     p.q.L[li + 2] += v.z;
@@ -76,14 +101,16 @@ __device__ __forceinline__ void add_L(const Params& p, uint32_t pid, float3 v) {
 // direction to the reference built without contraction).
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_generate(const __grid_constant__ Params p) {
-    const uint32_t n = p.chunk_pixels * p.spp;
-    const uint32_t first = p.chunk_first_pixel * p.spp;
+    const uint32_t n = p.chunk_paths;
     if (blockIdx.x == 0 && threadIdx.x == 0) p.counters[0] = n;
-    const DevCamera& cam = p.S.cam;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        uint32_t pid = first + i, px, py, sidx;
-        path_coords(p, pid, px, py, sidx);
-        SampleStream ss{p.seed, px, py, sidx, 0};
+        const uint32_t gid = p.chunk_first_path + i;
+        const uint32_t sc = scene_of(p.S, gid);
+        const DevSceneRec& R = p.S.scenes[sc];
+        const DevCamera& cam = R.cam;
+        uint32_t px, py, sidx;
+        path_coords(R, gid, px, py, sidx);
+        SampleStream ss{R.seed, px, py, sidx, 0};
         float jx = ss.next(), jy = ss.next();
         float lx = ss.next(), ly = ss.next();
         float tu = ss.next();
@@ -115,9 +142,9 @@ __global__ void __launch_bounds__(256) k_generate(const __grid_constant__ Params
             d = normalize(fp - lens);
         }
         uint32_t meta = (ss.dim << 16);  // bounce 0, not specular
-        p.q.ext_o[0][i] = pack_u(o, pid);
+        p.q.ext_o[0][i] = pack_u(o, gid);
         p.q.ext_d[0][i] = pack_u(d, meta);
-        p.q.ext_b[0][i] = make_float4(1.f, 1.f, 1.f, 0.f);
+        p.q.ext_b[0][i] = make_float4(1.f, 1.f, 1.f, __uint_as_float(sc));
         size_t li = size_t(i) * 3;
         p.q.L[li] = 0.f;
         p.q.L[li + 1] = 0.f;
@@ -137,10 +164,10 @@ struct SceneHit {
 
 // Completes a triangle traversal with the curve pass (strictly closer ribbon
 // hits win) and packs the result. kCurves = false compiles the curve code out
-// of kernels for triangle-only scenes.
+// of kernels for triangle-only batches.
 template <bool kCurves>
-__device__ __forceinline__ SceneHit finish_closest(const DevScene& S, const Ray& r, const Traversal& T,
-                                                   uint32_t* err) {
+__device__ __forceinline__ SceneHit finish_closest(const DevScene& S, uint32_t segRoot, const Ray& r,
+                                                   const Traversal& T, uint32_t* err) {
     SceneHit h;
     h.t = T.tri >= 0 ? T.closest : r.tmax;
     h.u = T.u;
@@ -149,7 +176,7 @@ __device__ __forceinline__ SceneHit finish_closest(const DevScene& S, const Ray&
     h.tang = f3(0.f, 0.f, 0.f);
     h.tseg = 0.f;
     if (kCurves) {
-        CurveHit ch = trace_curves(S, r, T.tri >= 0 ? T.closest : r.tmax, false, err);
+        CurveHit ch = trace_curves(S, segRoot, r, T.tri >= 0 ? T.closest : r.tmax, false, err);
         if (ch.seg >= 0) {
             h.t = ch.t;
             h.prim = 0x80000000u | uint32_t(ch.seg);
@@ -163,9 +190,10 @@ __device__ __forceinline__ SceneHit finish_closest(const DevScene& S, const Ray&
 }
 
 template <bool kCurves>
-__device__ __forceinline__ bool finish_any(const DevScene& S, const Ray& r, const Traversal& T, uint32_t* err) {
+__device__ __forceinline__ bool finish_any(const DevScene& S, uint32_t segRoot, const Ray& r, const Traversal& T,
+                                           uint32_t* err) {
     if (T.tri >= 0) return true;
-    if (kCurves) return trace_curves(S, r, r.tmax, true, err).seg >= 0;
+    if (kCurves) return trace_curves(S, segRoot, r, r.tmax, true, err).seg >= 0;
     return false;
 }
 
@@ -190,26 +218,29 @@ __device__ __forceinline__ void warp_add_work(unsigned long long* work, const Co
 template <bool kAny, bool kCount, bool kPersist, class Load, class Done>
 __device__ __forceinline__ void run_traversal(const DevScene& S, uint32_t n, uint32_t* fetch, uint32_t* err,
                                               Counters* cnt, Load load, Done done) {
-    if (kPersist) {
+    if constexpr (kPersist) {
         persistent_traverse<kAny, kCount>(S, n, fetch, err, cnt, load, done);
-        return;
-    }
-    uint32_t stack[kMaxStack];
-    float stackT[kMaxStack];
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        Ray ray;
-        load(i, ray);
-        Traversal T;
-        trav_init<kAny>(T, S, ray);
-        while (!T.exhausted) {
-            if (!(T.cur & 0x80000000u)) trav_interior<kAny, kCount>(T, S, stack, stackT, err, cnt);
-            else trav_leaf<kAny, kCount>(T, S, stack, stackT, cnt);
+    } else {
+        uint32_t stack[kMaxStack];
+        float stackT[kMaxStack];
+        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+            Ray ray;
+            uint32_t root;
+            load(i, ray, root);
+            Traversal T;
+            trav_init(T, ray, root);
+            while (!T.exhausted) {
+                if (!(T.cur & 0x80000000u)) trav_interior<kAny, kCount>(T, S, stack, stackT, err, cnt);
+                else trav_leaf<kAny, kCount>(T, S, stack, stackT, cnt);
+            }
+            done(i, T);
         }
-        done(i, T);
     }
 }
 
 #define ANA_TRAVERSAL_BOUNDS __launch_bounds__(kPersistBlock, kPersist ? kPersistMinBlocks : 1)
+
+__device__ __forceinline__ uint32_t scene_bits(float w) { return __float_as_uint(w); }
 
 // extend: closest hit of every live path (PathIntegrator::Li, line 81).
 // kCount: the same traversal, counting node fetches and primitive tests
@@ -221,14 +252,16 @@ __global__ void ANA_TRAVERSAL_BOUNDS k_extend(const __grid_constant__ Params p) 
     Counters cnt{0, 0, 0};
     run_traversal<false, kCount, kPersist>(
         p.S, cb[0], cb + 3, p.err, &cnt,
-        [&](uint32_t i, Ray& r) {
+        [&](uint32_t i, Ray& r, uint32_t& root) {
             float4 o = p.q.ext_o[cur][i], d = p.q.ext_d[cur][i];
             r = Ray{f3(o), f3(d), 1e-4f, INFINITY};
+            root = p.S.scenes[scene_bits(p.q.ext_b[cur][i].w)].tri_root;
         },
         [&](uint32_t i, const Traversal& T) {
             float4 o = p.q.ext_o[cur][i], d = p.q.ext_d[cur][i];
             Ray r{f3(o), f3(d), 1e-4f, INFINITY};
-            SceneHit h = finish_closest<kCurves>(p.S, r, T, p.err);
+            uint32_t segRoot = kCurves ? p.S.scenes[scene_bits(p.q.ext_b[cur][i].w)].seg_root : kNoRoot;
+            SceneHit h = finish_closest<kCurves>(p.S, segRoot, r, T, p.err);
             p.q.hit0[i] = make_float4(h.t, __uint_as_float(h.prim), h.u, h.v);
             if (kCurves && h.prim != kMiss && (h.prim & 0x80000000u)) p.q.hit1[i] = pack(h.tang, h.tseg);
         });
@@ -278,16 +311,21 @@ __device__ __forceinline__ SurfInt surf_int(const DevScene& S, float3 o, float3 
     return si;
 }
 
-__device__ __forceinline__ int slot_material(const DevScene& S, uint32_t slot) {
-    return slot < S.num_slots ? __ldg(S.slot_material + slot) : -1;
+// SceneView::materials[meshID] of a scene (-1: no material).
+__device__ __forceinline__ int slot_material(const DevScene& S, const DevSceneRec& R, uint32_t slot) {
+    return slot < R.num_slots ? __ldg(S.slot_material + R.slot_base + slot) : -1;
 }
 
-__global__ void __launch_bounds__(256) k_shade(const __grid_constant__ Params p) {
+// Environment radiance seen along a direction that leaves the scene.
+__device__ __forceinline__ float3 scene_env(const DevScene& S, const DevSceneRec& R, float3 d) {
+    return R.has_dome ? env_eval(S.env, d) : R.env_radiance;
+}
+
+__global__ void __launch_bounds__(kMaxStageBlock) k_shade(const __grid_constant__ Params p) {
     const uint32_t b = p.bounce;
     const uint32_t cur = b & 1u, nxt = cur ^ 1u;
     const uint32_t n = p.counters[b * kCountersPerBounce + 0];
     const DevScene& S = p.S;
-    const uint32_t nL = S.num_lights;
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += stride) {
         const uint32_t i = base + threadIdx.x;
@@ -297,22 +335,25 @@ __global__ void __launch_bounds__(256) k_shade(const __grid_constant__ Params p)
             float4 qo = p.q.ext_o[cur][i], qd = p.q.ext_d[cur][i], qb = p.q.ext_b[cur][i];
             float4 h0 = p.q.hit0[i];
             const uint32_t pid = __float_as_uint(qo.w), meta = __float_as_uint(qd.w);
+            const uint32_t sc = scene_bits(qb.w);
+            const DevSceneRec& R = S.scenes[sc];
+            const uint32_t nL = R.num_lights;
             const uint32_t bounce = meta & 0xFFu;
             bool spec = (meta >> 8) & 1u;
             float3 o = f3(qo), d = f3(qd), beta = f3(qb);
             uint32_t prim = __float_as_uint(h0.y);
             float3 Ladd = f3(0.f, 0.f, 0.f);
             if (prim == kMiss) {
-                if (bounce == 0 || spec) Ladd = beta * env_le(S.env, d);
+                if (bounce == 0 || spec) Ladd = beta * scene_env(S, R, d);
             } else {
                 float4 h1 = (prim & 0x80000000u) ? p.q.hit1[i] : make_float4(0, 0, 0, 0);
                 SurfInt si = surf_int(S, o, d, h0.x, prim, h0.z, h0.w, h1);
-                int mi = slot_material(S, si.slot);
+                int mi = slot_material(S, R, si.slot);
                 if (mi >= 0) {
                     const DevMaterial m = S.materials[mi];
                     uint32_t px, py, sidx;
-                    path_coords(p, pid, px, py, sidx);
-                    SampleStream ss{p.seed, px, py, sidx, meta >> 16};
+                    path_coords(R, pid, px, py, sidx);
+                    SampleStream ss{R.seed, px, py, sidx, meta >> 16};
                     float3 wo = -d;
                     ShadeCtx c = make_ctx(si, d);
                     float3 Le = mat_le(m);
@@ -320,7 +361,7 @@ __global__ void __launch_bounds__(256) k_shade(const __grid_constant__ Params p)
                     if (!m.is_delta && nL > 0) {
                         float ul = ss.next();
                         uint32_t lidx = min(uint32_t(ul * float(nL)), nL - 1u);
-                        const DevLight L = S.lights[lidx];
+                        const DevLight L = S.lights[R.light_base + lidx];
                         // light sampling
                         float lu0 = ss.next(), lu1 = ss.next();
                         LightSample ls = light_sample(S, L, si.p, lu0, lu1);
@@ -344,7 +385,7 @@ __global__ void __launch_bounds__(256) k_shade(const __grid_constant__ Params p)
                                 pushSh = true;
                                 shO = pack_u(org, pid);
                                 shD = pack(dir, dist * (1.f - 1e-4f));
-                                shC = pack(contrib, 0.f);
+                                shC = pack_u(contrib, sc);
                             }
                         }
                         // BSDF sampling toward the light (non-delta lights)
@@ -361,7 +402,7 @@ __global__ void __launch_bounds__(256) k_shade(const __grid_constant__ Params p)
                                 pushMis = true;
                                 mO = pack_u(org, pid);
                                 mD = pack(bs.wi, 0.f);
-                                mC = pack(contrib, 0.f);
+                                mC = pack_u(contrib, sc);
                             }
                         }
                     }
@@ -374,17 +415,17 @@ __global__ void __launch_bounds__(256) k_shade(const __grid_constant__ Params p)
                         beta = beta * (bs.f / bs.pdf);
                         float3 org = spawn_origin(si.p, si.n, bs.wi);
                         bool alive = true;
-                        if (bounce >= p.min_depth) {
+                        if (bounce >= R.min_depth) {
                             float q = 1.f - fminf(max_comp(beta), 0.95f);
                             if (ss.next() < q) alive = false;
                             else beta = beta * (1.f / (1.f - q));
                         }
-                        if (alive && bounce + 1u <= p.max_depth) {
+                        if (alive && bounce + 1u <= R.max_depth) {
                             pushExt = true;
                             uint32_t nm = (bounce + 1u) | (spec ? 0x100u : 0u) | (ss.dim << 16);
                             eO = pack_u(org, pid);
                             eD = pack_u(bs.wi, nm);
-                            eB = pack(beta, 0.f);
+                            eB = pack_u(beta, sc);
                         }
                     }
                 }
@@ -420,20 +461,22 @@ __global__ void ANA_TRAVERSAL_BOUNDS k_shadow(const __grid_constant__ Params p) 
     uint32_t* cb = p.counters + p.bounce * kCountersPerBounce;
     run_traversal<true, false, kPersist>(
         p.S, cb[1], cb + 4, p.err, nullptr,
-        [&](uint32_t i, Ray& r) {
+        [&](uint32_t i, Ray& r, uint32_t& root) {
             float4 o = p.q.sh_o[i], d = p.q.sh_d[i];
             r = Ray{f3(o), f3(d), 1e-4f, d.w};
+            root = p.S.scenes[scene_bits(p.q.sh_c[i].w)].tri_root;
         },
         [&](uint32_t i, const Traversal& T) {
-            float4 o = p.q.sh_o[i], d = p.q.sh_d[i];
+            float4 o = p.q.sh_o[i], d = p.q.sh_d[i], c = p.q.sh_c[i];
             Ray r{f3(o), f3(d), 1e-4f, d.w};
-            if (!finish_any<kCurves>(p.S, r, T, p.err)) add_L(p, __float_as_uint(o.w), f3(p.q.sh_c[i]));
+            uint32_t segRoot = kCurves ? p.S.scenes[scene_bits(c.w)].seg_root : kNoRoot;
+            if (!finish_any<kCurves>(p.S, segRoot, r, T, p.err)) add_L(p, __float_as_uint(o.w), f3(c));
         });
 }
 
 // BSDF-sampled MIS rays (PathIntegrator.cpp:214-259): the first surface hit
 // within 1e10 contributes its material's Le, a miss the environment. In a
-// scene without emissive surfaces every hit contributes zero, so the ray only
+// batch without emissive surfaces every hit contributes zero, so the ray only
 // needs to know whether anything is hit (kAny): identical result, cheaper
 // query.
 template <bool kAny, bool kCurves, bool kPersist>
@@ -442,20 +485,23 @@ __global__ void ANA_TRAVERSAL_BOUNDS k_mis(const __grid_constant__ Params p) {
     const DevScene& S = p.S;
     run_traversal<kAny, false, kPersist>(
         S, cb[2], cb + 5, p.err, nullptr,
-        [&](uint32_t i, Ray& r) {
+        [&](uint32_t i, Ray& r, uint32_t& root) {
             float4 o = p.q.mis_o[i], d = p.q.mis_d[i];
             r = Ray{f3(o), f3(d), 1e-4f, 1e10f};
+            root = S.scenes[scene_bits(p.q.mis_c[i].w)].tri_root;
         },
         [&](uint32_t i, const Traversal& T) {
-            float4 o = p.q.mis_o[i], d = p.q.mis_d[i];
+            float4 o = p.q.mis_o[i], d = p.q.mis_d[i], c = p.q.mis_c[i];
             Ray r{f3(o), f3(d), 1e-4f, 1e10f};
+            const DevSceneRec& R = S.scenes[scene_bits(c.w)];
+            uint32_t segRoot = kCurves ? R.seg_root : kNoRoot;
             float3 Li;
             if (kAny) {
-                Li = finish_any<kCurves>(S, r, T, p.err) ? f3(0.f, 0.f, 0.f) : env_le(S.env, r.d);
+                Li = finish_any<kCurves>(S, segRoot, r, T, p.err) ? f3(0.f, 0.f, 0.f) : scene_env(S, R, r.d);
             } else {
-                SceneHit h = finish_closest<kCurves>(S, r, T, p.err);
+                SceneHit h = finish_closest<kCurves>(S, segRoot, r, T, p.err);
                 if (h.prim == kMiss) {
-                    Li = env_le(S.env, r.d);
+                    Li = scene_env(S, R, r.d);
                 } else {
                     uint32_t slot;
                     if (h.prim & 0x80000000u)
@@ -463,23 +509,33 @@ __global__ void ANA_TRAVERSAL_BOUNDS k_mis(const __grid_constant__ Params p) {
                     else
                         slot = __float_as_uint(ldg4(S.tri_shade + 4 * size_t(__float_as_uint(
                                                                        ldg4(S.tri_isect + 3 * size_t(h.prim)).w))).w);
-                    int mi = slot_material(S, slot);
+                    int mi = slot_material(S, R, slot);
                     Li = mi >= 0 ? mat_le(S.materials[mi]) : f3(0.f, 0.f, 0.f);
                 }
             }
-            if (!is_black(Li)) add_L(p, __float_as_uint(o.w), f3(p.q.mis_c[i]) * Li);
+            if (!is_black(Li)) add_L(p, __float_as_uint(o.w), f3(c) * Li);
         });
 }
 
 // Film accumulation (PathIntegrator.cpp:43-57 + Film::mergeTile, Film.cpp:34-56):
 // finite samples summed in sample order, weight = sample count.
 __global__ void __launch_bounds__(256) k_film(const __grid_constant__ Params p) {
-    const float invSPP = 1.f / float(p.spp);
-    for (uint32_t pl = blockIdx.x * blockDim.x + threadIdx.x; pl < p.chunk_pixels; pl += gridDim.x * blockDim.x) {
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < p.chunk_pixels; q += gridDim.x * blockDim.x) {
+        // the chunk's pixel run holding local pixel q
+        uint32_t lo = 0, hi = p.num_segs;
+        while (hi - lo > 1) {
+            uint32_t mid = (lo + hi) >> 1;
+            if (p.segs[mid].local_pixel <= q) lo = mid;
+            else hi = mid;
+        }
+        const ChunkSeg sg = p.segs[lo];
+        const DevSceneRec& R = p.S.scenes[sg.scene];
+        const uint32_t spp = R.spp;
+        const uint32_t k = q - sg.local_pixel;
         float3 acc = f3(0.f, 0.f, 0.f);
         float lsq = 0.f;
-        const float* Lp = p.q.L + size_t(pl) * p.spp * 3;
-        for (uint32_t s = 0; s < p.spp; ++s) {
+        const float* Lp = p.q.L + (size_t(sg.local_path) + size_t(k) * spp) * 3;
+        for (uint32_t s = 0; s < spp; ++s) {
             float3 L = f3(Lp[3 * s], Lp[3 * s + 1], Lp[3 * s + 2]);
             if (is_finite3(L)) {
                 acc = acc + L;
@@ -487,8 +543,9 @@ __global__ void __launch_bounds__(256) k_film(const __grid_constant__ Params p) 
                 lsq += lum * lum;
             }
         }
-        ana_film_pixel& f = p.film[p.chunk_first_pixel + pl];
-        float w = float(p.spp);
+        const float invSPP = 1.f / float(spp);
+        ana_film_pixel& f = p.film[R.film_offset + sg.first_pixel + k];
+        float w = float(spp);
         f.r += (acc.x * invSPP) * w;
         f.g += (acc.y * invSPP) * w;
         f.b += (acc.z * invSPP) * w;
@@ -497,24 +554,28 @@ __global__ void __launch_bounds__(256) k_film(const __grid_constant__ Params p) 
     }
 }
 
-// IAccelerationStructure::traceBatch / occludedBatch over CurveBrute semantics.
+// IAccelerationStructure::traceBatch / occludedBatch over CurveBrute semantics,
+// against one scene of the batch.
 template <bool kAny, bool kCurves, bool kPersist>
-__global__ void ANA_TRAVERSAL_BOUNDS
-    k_trace_batch(const __grid_constant__ DevScene S, const float* rays, uint32_t n, ana_hit* out, uint32_t* fetch,
-                  uint32_t* err) {
-    auto load = [&](uint32_t i, Ray& r) {
+__global__ void ANA_TRAVERSAL_BOUNDS k_trace_batch(const __grid_constant__ DevScene S, uint32_t scene,
+                                                   const float* rays, uint32_t n, ana_hit* out, uint32_t* fetch,
+                                                   uint32_t* err) {
+    const uint32_t triRoot = S.scenes[scene].tri_root, segRoot = S.scenes[scene].seg_root;
+    auto load = [&](uint32_t i, Ray& r, uint32_t& root) {
         const float4* rp = reinterpret_cast<const float4*>(rays + 8 * size_t(i));
         float4 a = rp[0], b = rp[1];
         r = Ray{f3(a), f3(b), a.w, b.w};
+        root = triRoot;
     };
     run_traversal<kAny, false, kPersist>(S, n, fetch, err, nullptr, load, [&](uint32_t i, const Traversal& T) {
         Ray r;
-        load(i, r);
+        uint32_t root;
+        load(i, r, root);
         ana_hit h{0, -1, -1, -1, 0.f, 0.f, 0.f, 0.f};
         if (kAny) {
-            h.hit = finish_any<kCurves>(S, r, T, err) ? 1 : 0;
+            h.hit = finish_any<kCurves>(S, segRoot, r, T, err) ? 1 : 0;
         } else {
-            SceneHit sh = finish_closest<kCurves>(S, r, T, err);
+            SceneHit sh = finish_closest<kCurves>(S, segRoot, r, T, err);
             if (sh.prim != kMiss) {
                 h.hit = 1;
                 h.t = sh.t;
@@ -524,7 +585,7 @@ __global__ void ANA_TRAVERSAL_BOUNDS
                     float4 rec = ldg4(S.segs + 5 * size_t(sh.prim & 0x7FFFFFFFu) + 4);
                     h.mesh_id = int32_t(__float_as_uint(rec.z));
                     h.prim_id = int32_t(__float_as_uint(rec.y));
-                    h.strand_id = int32_t(__float_as_uint(rec.x));
+                    h.strand_id = int32_t(__float_as_uint(rec.x) - __float_as_uint(rec.w));
                 } else {
                     uint32_t orig = __float_as_uint(ldg4(S.tri_isect + 3 * size_t(sh.prim)).w);
                     const float4* sp = S.tri_shade + 4 * size_t(orig);
@@ -544,29 +605,82 @@ static inline int blocks_for(uint32_t n, int block, int cap) {
     return int(b < cap ? b : cap);
 }
 
-// Resident blocks of a kernel on this device (one wave of the persistent schedule).
+// Resident blocks per kernel on each device (one wave of the persistent
+// schedule), filled by prime_kernels() before any launch so that no
+// occupancy query or lazy module load happens while a stream is captured.
+static std::mutex g_grid_mu;
+static std::map<std::pair<int, const void*>, int> g_grid;
+
 template <class K>
 static int resident_grid(K kernel) {
-    int dev = 0, sms = 148, per = 1;
+    int dev = 0;
     cudaGetDevice(&dev);
+    const void* key = reinterpret_cast<const void*>(kernel);
+    {
+        std::lock_guard<std::mutex> lk(g_grid_mu);
+        auto it = g_grid.find({dev, key});
+        if (it != g_grid.end()) return it->second;
+    }
+    int sms = 148, per = 1;
+    cudaFuncAttributes attr;
+    cudaFuncGetAttributes(&attr, kernel);  // loads the function
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kPersistBlock, 0);
-    return sms * (per > 0 ? per : 1);
+    int g = sms * (per > 0 ? per : 1);
+    std::lock_guard<std::mutex> lk(g_grid_mu);
+    g_grid[{dev, key}] = g;
+    return g;
 }
 
 // Grid for a traversal kernel: one resident wave when persistent, otherwise
 // enough blocks to cover the chunk capacity (grid-stride beyond it).
 template <bool kPersist, class K>
 static int traversal_grid(K kernel, const LaunchCfg& c) {
-    if (kPersist) {
-        static int g = resident_grid(kernel);
-        return g;
-    }
+    if (kPersist) return resident_grid(kernel);
     return c.grid_cap;
 }
 
+template <class K>
+static void prime(K kernel) {
+    resident_grid(kernel);
+}
+
+void prime_kernels() {
+    prime(k_generate);
+    prime(k_shade);
+    prime(k_film);
+    prime(k_extend<false, false, false>);
+    prime(k_extend<false, false, true>);
+    prime(k_extend<false, true, false>);
+    prime(k_extend<false, true, true>);
+    prime(k_extend<true, false, false>);
+    prime(k_extend<true, false, true>);
+    prime(k_extend<true, true, false>);
+    prime(k_extend<true, true, true>);
+    prime(k_shadow<false, false>);
+    prime(k_shadow<false, true>);
+    prime(k_shadow<true, false>);
+    prime(k_shadow<true, true>);
+    prime(k_mis<false, false, false>);
+    prime(k_mis<false, false, true>);
+    prime(k_mis<false, true, false>);
+    prime(k_mis<false, true, true>);
+    prime(k_mis<true, false, false>);
+    prime(k_mis<true, false, true>);
+    prime(k_mis<true, true, false>);
+    prime(k_mis<true, true, true>);
+    prime(k_trace_batch<false, false, false>);
+    prime(k_trace_batch<false, false, true>);
+    prime(k_trace_batch<false, true, false>);
+    prime(k_trace_batch<false, true, true>);
+    prime(k_trace_batch<true, false, false>);
+    prime(k_trace_batch<true, false, true>);
+    prime(k_trace_batch<true, true, false>);
+    prime(k_trace_batch<true, true, true>);
+}
+
 void launch_generate(const Params& p, const LaunchCfg& c, cudaStream_t s) {
-    k_generate<<<blocks_for(p.chunk_pixels * p.spp, 256, c.grid_cap), 256, 0, s>>>(p);
+    k_generate<<<blocks_for(p.chunk_paths, 256, c.grid_cap), 256, 0, s>>>(p);
 }
 
 template <bool kCount, bool kCurves, bool kPersist>
@@ -575,7 +689,7 @@ static void ext_launch(const Params& p, const LaunchCfg& c, cudaStream_t s) {
     k<<<traversal_grid<kPersist>(k, c), kPersistBlock, 0, s>>>(p);
 }
 void launch_extend(const Params& p, const LaunchCfg& c, cudaStream_t s, bool count_work) {
-    const bool cv = p.S.num_seg_nodes != 0, ps = c.persistent != 0;
+    const bool cv = p.S.has_curves != 0, ps = c.persistent != 0;
     if (count_work) {
         if (cv) ps ? ext_launch<true, true, true>(p, c, s) : ext_launch<true, true, false>(p, c, s);
         else ps ? ext_launch<true, false, true>(p, c, s) : ext_launch<true, false, false>(p, c, s);
@@ -593,7 +707,7 @@ static void sh_launch(const Params& p, const LaunchCfg& c, cudaStream_t s) {
     k<<<traversal_grid<kPersist>(k, c), kPersistBlock, 0, s>>>(p);
 }
 void launch_shadow(const Params& p, const LaunchCfg& c, cudaStream_t s) {
-    const bool cv = p.S.num_seg_nodes != 0, ps = c.persistent != 0;
+    const bool cv = p.S.has_curves != 0, ps = c.persistent != 0;
     if (cv) ps ? sh_launch<true, true>(p, c, s) : sh_launch<true, false>(p, c, s);
     else ps ? sh_launch<false, true>(p, c, s) : sh_launch<false, false>(p, c, s);
 }
@@ -603,7 +717,7 @@ static void mis_launch(const Params& p, const LaunchCfg& c, cudaStream_t s) {
     k<<<traversal_grid<kPersist>(k, c), kPersistBlock, 0, s>>>(p);
 }
 void launch_mis(const Params& p, const LaunchCfg& c, cudaStream_t s) {
-    const bool cv = p.S.num_seg_nodes != 0, ps = c.persistent != 0, any = !p.S.has_emitters;
+    const bool cv = p.S.has_curves != 0, ps = c.persistent != 0, any = !p.S.has_emitters;
     if (any) {
         if (cv) ps ? mis_launch<true, true, true>(p, c, s) : mis_launch<true, true, false>(p, c, s);
         else ps ? mis_launch<true, false, true>(p, c, s) : mis_launch<true, false, false>(p, c, s);
@@ -616,27 +730,27 @@ void launch_film(const Params& p, const LaunchCfg& c, cudaStream_t s) {
     k_film<<<blocks_for(p.chunk_pixels, 256, c.grid_cap), 256, 0, s>>>(p);
 }
 template <bool kAny, bool kCurves, bool kPersist>
-static void tb_launch(const DevScene& S, const float* rays, uint32_t n, ana_hit* out, uint32_t* fetch,
-                      uint32_t* err, int grid, cudaStream_t s) {
+static void tb_launch(const DevScene& S, uint32_t scene, const float* rays, uint32_t n, ana_hit* out,
+                      uint32_t* fetch, uint32_t* err, int grid, cudaStream_t s) {
     auto k = k_trace_batch<kAny, kCurves, kPersist>;
     int g = kPersist ? resident_grid(k) : grid;
-    k<<<g, kPersistBlock, 0, s>>>(S, rays, n, out, fetch, err);
+    k<<<g, kPersistBlock, 0, s>>>(S, scene, rays, n, out, fetch, err);
 }
-void launch_trace_batch(const DevScene& S, const float* rays, size_t n, ana_hit* out, int occlusion,
+void launch_trace_batch(const DevScene& S, uint32_t scene, const float* rays, size_t n, ana_hit* out, int occlusion,
                         uint32_t* fetch, uint32_t* err, int persistent, cudaStream_t s) {
-    const bool cv = S.num_seg_nodes != 0;
+    const bool cv = S.has_curves != 0;
     int grid = blocks_for(uint32_t(n), kPersistBlock, 1 << 20);
     uint32_t nn = uint32_t(n);
     if (occlusion) {
-        if (cv) persistent ? tb_launch<true, true, true>(S, rays, nn, out, fetch, err, grid, s)
-                           : tb_launch<true, true, false>(S, rays, nn, out, fetch, err, grid, s);
-        else persistent ? tb_launch<true, false, true>(S, rays, nn, out, fetch, err, grid, s)
-                        : tb_launch<true, false, false>(S, rays, nn, out, fetch, err, grid, s);
+        if (cv) persistent ? tb_launch<true, true, true>(S, scene, rays, nn, out, fetch, err, grid, s)
+                           : tb_launch<true, true, false>(S, scene, rays, nn, out, fetch, err, grid, s);
+        else persistent ? tb_launch<true, false, true>(S, scene, rays, nn, out, fetch, err, grid, s)
+                        : tb_launch<true, false, false>(S, scene, rays, nn, out, fetch, err, grid, s);
     } else {
-        if (cv) persistent ? tb_launch<false, true, true>(S, rays, nn, out, fetch, err, grid, s)
-                           : tb_launch<false, true, false>(S, rays, nn, out, fetch, err, grid, s);
-        else persistent ? tb_launch<false, false, true>(S, rays, nn, out, fetch, err, grid, s)
-                        : tb_launch<false, false, false>(S, rays, nn, out, fetch, err, grid, s);
+        if (cv) persistent ? tb_launch<false, true, true>(S, scene, rays, nn, out, fetch, err, grid, s)
+                           : tb_launch<false, true, false>(S, scene, rays, nn, out, fetch, err, grid, s);
+        else persistent ? tb_launch<false, false, true>(S, scene, rays, nn, out, fetch, err, grid, s)
+                        : tb_launch<false, false, false>(S, scene, rays, nn, out, fetch, err, grid, s);
     }
 }
 

@@ -9,12 +9,12 @@
 namespace ana {
 
 // Queues are structure-of-arrays of float4, indexed by queue position.
-//   extend queue: o (xyz, global path id), d (xyz, meta), beta (xyz, -)
+//   extend queue: o (xyz, global path id), d (xyz, meta), beta (xyz, scene)
 //     meta bits: 0..7 bounce, 8 specular-bounce flag, 16..31 next sampler dimension
 //   hit record:   (t, prim, u, v) and, for curve hits, (tangent xyz, strand v)
 //     prim: leaf-order triangle index, 0x80000000 | segment index, or ~0 (miss)
-//   shadow queue: o (xyz, path id), d (xyz, tmax), contribution (xyz, -)
-//   MIS queue:    o (xyz, path id), d (xyz, -), contribution without Li (xyz, -)
+//   shadow queue: o (xyz, path id), d (xyz, tmax), contribution (xyz, scene)
+//   MIS queue:    o (xyz, path id), d (xyz, -), contribution without Li (xyz, scene)
 struct Queues {
     float4* ext_o[2];
     float4* ext_d[2];
@@ -35,16 +35,28 @@ struct Queues {
 // counters of extend, shadow and MIS. Zeroed per chunk.
 constexpr int kCountersPerBounce = 8;
 
+// A run of whole pixels of one scene inside a chunk. Chunks are cut in the
+// global path space at pixel boundaries, so a chunk may span several scenes.
+struct ChunkSeg {
+    uint32_t scene;        // scene index
+    uint32_t first_pixel;  // first pixel (within the scene's film)
+    uint32_t num_pixels;
+    uint32_t local_pixel;  // chunk-local index of the first pixel
+    uint32_t local_path;   // chunk-local index of the first path
+    uint32_t pad[3];
+};
+
 struct Params {
     DevScene S;
     Queues q;
-    ana_film_pixel* film;
-    uint32_t* counters;  // this chunk's counters
-    uint32_t* err;       // device error word (bit 0: traversal stack overflow)
+    ana_film_pixel* film;      // batch film (all scenes)
+    uint32_t* counters;        // this chunk's counters
+    uint32_t* err;             // device error word (bit 0: traversal stack overflow)
     unsigned long long* work;  // [node fetches, triangle tests, segment tests] (count mode)
-    uint64_t seed;
-    uint32_t W, H, spp, sample_start, max_depth, min_depth;
-    uint32_t chunk_first_pixel, chunk_pixels;
+    const ChunkSeg* segs;      // this chunk's pixel runs
+    uint32_t num_segs;
+    uint32_t chunk_first_path; // global path id of the chunk's first path
+    uint32_t chunk_paths, chunk_pixels;
     uint32_t bounce;
 };
 
@@ -54,13 +66,17 @@ struct LaunchCfg {
     int persistent;  // traversal schedule: 1 persistent warps with refill, 0 thread per ray
 };
 
+// Loads every kernel and caches its resident grid on the current device.
+// Called when a context is created, so a later stream capture launches only.
+void prime_kernels();
+
 void launch_generate(const Params& p, const LaunchCfg& c, cudaStream_t s);
 void launch_extend(const Params& p, const LaunchCfg& c, cudaStream_t s, bool count_work);
 void launch_shade(const Params& p, const LaunchCfg& c, cudaStream_t s);
 void launch_shadow(const Params& p, const LaunchCfg& c, cudaStream_t s);
 void launch_mis(const Params& p, const LaunchCfg& c, cudaStream_t s);
 void launch_film(const Params& p, const LaunchCfg& c, cudaStream_t s);
-void launch_trace_batch(const DevScene& S, const float* rays, size_t n, ana_hit* out, int occlusion, uint32_t* fetch,
-                        uint32_t* err, int persistent, cudaStream_t s);
+void launch_trace_batch(const DevScene& S, uint32_t scene, const float* rays, size_t n, ana_hit* out, int occlusion,
+                        uint32_t* fetch, uint32_t* err, int persistent, cudaStream_t s);
 
 }  // namespace ana

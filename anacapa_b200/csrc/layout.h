@@ -90,24 +90,42 @@ struct DevCamera {
     uint32_t width, height;
 };
 
+// Per-scene record of a batch (a plain render is a batch of one). Global
+// arrays hold every scene's data; a scene's BVH roots and its slot / light
+// ranges index into them.
+constexpr uint32_t kNoRoot = 0xFFFFFFFFu;
+
+struct DevSceneRec {
+    uint32_t tri_root, seg_root;     // interior root node, or kNoRoot
+    uint32_t slot_base, num_slots;   // SceneView::materials of this scene
+    uint32_t light_base, num_lights; // SceneView::lights of this scene
+    uint32_t spp, sample_start;
+    uint32_t max_depth, min_depth;
+    uint32_t film_offset;            // first pixel of this scene's film in the batch film
+    uint32_t path_offset;            // first global path id of this scene
+    uint64_t seed;                   // HaltonSampler seed
+    float3 env_radiance;             // SceneView::envRadiance (no dome)
+    uint32_t has_dome;
+    DevCamera cam;                   // includes the film size
+};
+
 struct DevScene {
     const BvhNode* tri_nodes;
     const float4* tri_isect;
     const float4* tri_shade;
-    uint32_t num_tri_nodes, num_tris;
-    uint32_t tri_root_is_empty;
     const BvhNode* seg_nodes;
     const float4* segs;
     const float* strand_color;   // 3 per strand
-    uint32_t num_seg_nodes, num_segs;
     const DevMaterial* materials;
     const int32_t* slot_material;
-    uint32_t num_materials, num_slots;
     const DevLight* lights;
-    uint32_t num_lights;
+    const DevSceneRec* scenes;
+    const uint32_t* scene_path_offset;  // num_scenes + 1 (global path id ranges)
+    uint32_t num_scenes;
+    uint32_t has_curves;    // any scene has curve segments
     uint32_t has_emitters;  // any material reachable from a slot emits (Le != 0)
-    DevEnv env;
-    DevCamera cam;
+    uint32_t pad;
+    DevEnv env;             // the (single) dome of the batch
 };
 
 }  // namespace ana

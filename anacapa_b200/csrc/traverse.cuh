@@ -91,75 +91,6 @@ struct Counters {
     uint32_t nodes, prims, segs;
 };
 
-// Closest hit over the triangle BVH. Returns the nearest accepted triangle;
-// ties (t == closest) go to the later-tested triangle, as `t <= r.tMax` does
-// in the reference.
-template <bool kCount>
-__device__ __forceinline__ TriHit trace_tris(const DevScene& S, const Ray& ray, uint32_t* err,
-                                             Counters* cnt = nullptr) {
-    TriHit h{ray.tmax, 0.f, 0.f, -1};
-    if (S.num_tri_nodes == 0) return h;
-    TriRay r = make_tri_ray(ray);
-    uint32_t stack[kMaxStack];
-    float stackT[kMaxStack];
-    int sp = 0;
-    uint32_t cur = 0;  // interior root
-    float closest = ray.tmax;
-    while (true) {
-        if (!(cur & 0x80000000u)) {
-            const float4* np = reinterpret_cast<const float4*>(S.tri_nodes + cur);
-            float4 n0 = ldg4(np), n1 = ldg4(np + 1), n2 = ldg4(np + 2), n3 = ldg4(np + 3);
-            if (kCount) cnt->nodes++;
-            float tn0, tn1;
-            bool h0 = box_hit(r, n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, closest, tn0);
-            bool h1 = box_hit(r, n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, closest, tn1);
-            uint32_t c0 = fbits_u(n3.z) ? leaf_entry(fbits_u(n3.x), fbits_u(n3.z)) : fbits_u(n3.x);
-            uint32_t c1 = fbits_u(n3.w) ? leaf_entry(fbits_u(n3.y), fbits_u(n3.w)) : fbits_u(n3.y);
-            if (h0 && h1) {
-                // nearer child next, farther one on the stack (BVHBackend.cpp:382-387)
-                bool swap = !(tn0 < tn1);
-                uint32_t nearC = swap ? c1 : c0, farC = swap ? c0 : c1;
-                float farT = swap ? tn0 : tn1;
-                if (sp >= int(kMaxStack)) { atomicOr(err, 1u); return h; }
-                stack[sp] = farC;
-                stackT[sp] = farT;
-                ++sp;
-                cur = nearC;
-                continue;
-            } else if (h0 || h1) {
-                cur = h0 ? c0 : c1;
-                continue;
-            }
-        } else {
-            uint32_t off = cur & 0x01FFFFFFu, c = ((cur >> 25) & 63u) + 1u;
-            for (uint32_t i = off; i < off + c; ++i) {
-                const float4* tp = S.tri_isect + 3 * size_t(i);
-                float4 a = ldg4(tp), b = ldg4(tp + 1), e = ldg4(tp + 2);
-                if (kCount) cnt->prims++;
-                float t, u, v;
-                if (tri_hit(r, f3(a), f3(b), f3(e), closest, t, u, v)) {
-                    closest = t;
-                    h.t = t;
-                    h.u = u;
-                    h.v = v;
-                    h.tri = int32_t(i);
-                }
-            }
-        }
-        // pop, skipping entries entered beyond the current closest hit
-        bool found = false;
-        while (sp > 0) {
-            --sp;
-            if (stackT[sp] > closest) continue;
-            cur = stack[sp];
-            found = true;
-            break;
-        }
-        if (!found) break;
-    }
-    return h;
-}
-
 // ---------------------------------------------------------------------------
 // Persistent-warp triangle traversal. Each lane owns one ray at a time; a
 // warp loops over
@@ -183,15 +114,19 @@ struct Traversal {
     bool exhausted;
 };
 
-template <bool kAny>
-__device__ __forceinline__ void trav_init(Traversal& T, const DevScene& S, const Ray& ray) {
+// Starts a traversal at a scene's root (kNoRoot: the scene has no triangles).
+// Closest hit keeps the nearest accepted triangle; ties (t == closest) go to
+// the later-tested triangle, as `t <= r.tMax` does in the reference; any hit
+// (kAny) stops at the first accepted triangle (BVHBackend::occluded,
+// BVHBackend.cpp:409-444).
+__device__ __forceinline__ void trav_init(Traversal& T, const Ray& ray, uint32_t root) {
     T.r = make_tri_ray(ray);
     T.closest = ray.tmax;
     T.u = T.v = 0.f;
     T.tri = -1;
-    T.cur = 0;
+    T.cur = root;
     T.sp = 0;
-    T.exhausted = S.num_tri_nodes == 0;
+    T.exhausted = root == kNoRoot;
 }
 
 __device__ __forceinline__ bool trav_pop(Traversal& T, const uint32_t* stack, const float* stackT) {
@@ -259,8 +194,9 @@ __device__ __forceinline__ void trav_leaf(Traversal& T, const DevScene& S, const
     if (!trav_pop(T, stack, stackT)) T.exhausted = true;
 }
 
-// Runs the persistent loop. Load(i, ray) reads queue entry i; Done(i, T)
-// consumes the finished traversal of entry i (a lane-local call).
+// Runs the persistent loop. Load(i, ray, root) reads queue entry i and its
+// scene's BVH root; Done(i, T) consumes the finished traversal of entry i (a
+// lane-local call).
 template <bool kAny, bool kCount, class Load, class Done>
 __device__ __forceinline__ void persistent_traverse(const DevScene& S, uint32_t n, uint32_t* fetch, uint32_t* err,
                                                     Counters* cnt, Load load, Done done) {
@@ -284,8 +220,9 @@ __device__ __forceinline__ void persistent_traverse(const DevScene& S, uint32_t 
                     idx = base + __popc(need & ltmask);
                     if (idx < n) {
                         Ray ray;
-                        load(idx, ray);
-                        trav_init<kAny>(T, S, ray);
+                        uint32_t root;
+                        load(idx, ray, root);
+                        trav_init(T, ray, root);
                         active = true;
                     }
                 }
@@ -305,47 +242,6 @@ __device__ __forceinline__ void persistent_traverse(const DevScene& S, uint32_t 
             active = false;
         }
     }
-}
-
-// Any hit within [tmin, tmax] (BVHBackend::occluded, BVHBackend.cpp:409-444).
-__device__ __forceinline__ bool occluded_tris(const DevScene& S, const Ray& ray, uint32_t* err) {
-    if (S.num_tri_nodes == 0) return false;
-    TriRay r = make_tri_ray(ray);
-    uint32_t stack[kMaxStack];
-    int sp = 0;
-    uint32_t cur = 0;
-    while (true) {
-        if (!(cur & 0x80000000u)) {
-            const float4* np = reinterpret_cast<const float4*>(S.tri_nodes + cur);
-            float4 n0 = ldg4(np), n1 = ldg4(np + 1), n2 = ldg4(np + 2), n3 = ldg4(np + 3);
-            float tn0, tn1;
-            bool h0 = box_hit(r, n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, ray.tmax, tn0);
-            bool h1 = box_hit(r, n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, ray.tmax, tn1);
-            uint32_t c0 = fbits_u(n3.z) ? leaf_entry(fbits_u(n3.x), fbits_u(n3.z)) : fbits_u(n3.x);
-            uint32_t c1 = fbits_u(n3.w) ? leaf_entry(fbits_u(n3.y), fbits_u(n3.w)) : fbits_u(n3.y);
-            if (h0 && h1) {
-                bool swap = !(tn0 < tn1);
-                if (sp >= int(kMaxStack)) { atomicOr(err, 1u); return false; }
-                stack[sp++] = swap ? c0 : c1;
-                cur = swap ? c1 : c0;
-                continue;
-            } else if (h0 || h1) {
-                cur = h0 ? c0 : c1;
-                continue;
-            }
-        } else {
-            uint32_t off = cur & 0x01FFFFFFu, c = ((cur >> 25) & 63u) + 1u;
-            for (uint32_t i = off; i < off + c; ++i) {
-                const float4* tp = S.tri_isect + 3 * size_t(i);
-                float4 a = ldg4(tp), b = ldg4(tp + 1), e = ldg4(tp + 2);
-                float t, u, v;
-                if (tri_hit(r, f3(a), f3(b), f3(e), ray.tmax, t, u, v)) return true;
-            }
-        }
-        if (sp == 0) break;
-        cur = stack[--sp];
-    }
-    return false;
 }
 
 // ===========================================================================
@@ -496,16 +392,16 @@ struct CurveHit {
 // Curve BVH pass of CurveBrute::trace (CurveBrute.cpp:398-440): starts from the
 // triangle hit distance and keeps only strictly closer ribbon hits.
 template <bool kCount = false>
-__device__ __forceinline__ CurveHit trace_curves(const DevScene& S, const Ray& ray, float bestT,
+__device__ __forceinline__ CurveHit trace_curves(const DevScene& S, uint32_t root, const Ray& ray, float bestT,
                                                  bool anyHit, uint32_t* err, Counters* cnt = nullptr) {
     CurveHit ch{-1, bestT, 0.f, f3(0.f, 0.f, 0.f)};
-    if (S.num_seg_nodes == 0) return ch;
+    if (root == kNoRoot) return ch;
     RayFrame fr = make_frame(ray);
     float3 inv = f3(xdiv(1.f, ray.d.x), xdiv(1.f, ray.d.y), xdiv(1.f, ray.d.z));
     uint32_t stack[kMaxStack];
     float stackT[kMaxStack];
     int sp = 0;
-    uint32_t cur = 0;
+    uint32_t cur = root;
     while (true) {
         if (!(cur & 0x80000000u)) {
             const float4* np = reinterpret_cast<const float4*>(S.seg_nodes + cur);

@@ -171,8 +171,12 @@ typedef struct ana_render_desc {
 
 enum {
     ANA_RENDER_CLEAR_FILM = 1u << 0, /* zero the film before accumulating              */
-    ANA_RENDER_COUNT_WORK = 1u << 1  /* count BVH node fetches and primitive tests of the
+    ANA_RENDER_COUNT_WORK = 1u << 1, /* count BVH node fetches and primitive tests of the
                                         closest-hit stage (instrumented, slower)        */
+    ANA_RENDER_GRAPH = 1u << 2       /* capture the whole chunk x bounce launch sequence
+                                        in a CUDA graph on first use and replay it while
+                                        the scenes and descs are unchanged (no per-stage
+                                        timing, no work counting)                         */
 };
 
 /* One device-resident film pixel: the reference's PixelAccumulator
@@ -247,6 +251,9 @@ typedef struct ana_prepared ana_prepared;
 int ana_prepare_scene(const ana_scene_desc* scene, ana_prepared** out);
 int ana_upload_prepared(ana_ctx* ctx, const ana_prepared* prep);
 uint64_t ana_prepared_bytes(const ana_prepared* prep);
+/* 64-bit FNV-1a digest of the prepared device layout (a cache key; equal
+ * scenes and build options give equal digests). */
+uint64_t ana_prepared_digest(const ana_prepared* prep);
 void ana_prepared_free(ana_prepared* prep);
 
 /* Render sample_count samples per pixel of the whole frame into the
@@ -255,7 +262,25 @@ void ana_prepared_free(ana_prepared* prep);
  * (src/integrator/PathIntegrator.cpp:8-265). */
 int ana_render(ana_ctx* ctx, const ana_render_desc* desc);
 
-/* Zero / read back the device film (width*height ana_film_pixel, row 0 = top). */
+/* ---- batches: many scenes, resolutions, spp budgets and depths in one launch
+ * sequence. A batch concatenates prepared scenes into one device arena (each
+ * scene keeps its own BVHs, materials and lights); ana_render_batch renders
+ * item k with descs[k] into its own film. Paths of all items share the
+ * wavefront queues, so small items do not leave the GPU idle. There is no
+ * reference counterpart: the reference renders one scene per RenderSession
+ * (src/render/RenderSession.cpp:402-547); this is the batched form north of
+ * it. A batch may hold at most one dome light. */
+typedef struct ana_batch ana_batch;
+int ana_batch_create(const ana_prepared* const* scenes, uint32_t count, ana_batch** out);
+void ana_batch_free(ana_batch* batch);
+uint64_t ana_batch_bytes(const ana_batch* batch);
+int ana_upload_batch(ana_ctx* ctx, const ana_batch* batch);
+int ana_render_batch(ana_ctx* ctx, const ana_render_desc* descs, uint32_t count, uint32_t flags);
+/* Film of one item of the last batch render (width*height pixels of that item). */
+int ana_batch_film_read(ana_ctx* ctx, uint32_t item, ana_film_pixel* host_out, size_t count);
+
+/* Zero / read back the device film (width*height ana_film_pixel, row 0 = top).
+ * After a batch render, ana_film_read returns all items' films back to back. */
 int ana_film_clear(ana_ctx* ctx, uint32_t width, uint32_t height);
 int ana_film_read(ana_ctx* ctx, ana_film_pixel* host_out, size_t count);
 /* Device pointer of the film, for callers that keep the result on the GPU. */

@@ -100,12 +100,11 @@ def test_prepare_is_deterministic(lib_built):
     a = api.Prepared(sc)
     b = api.Prepared(sc)
     assert a.nbytes == b.nbytes
+    # identical layouts: the parallel subtree build does not change the result
     L = api.lib()
-    # identical blobs: the parallel subtree build does not change the result
-    ba = C.string_at(C.cast(a.h, C.POINTER(C.c_void_p))[0], a.nbytes)
-    bb = C.string_at(C.cast(b.h, C.POINTER(C.c_void_p))[0], b.nbytes)
-    assert ba == bb
-    del L
+    assert L.ana_prepared_digest(a.h) == L.ana_prepared_digest(b.h) != 0
+    c = api.Prepared(sc, max_leaf_tris=8)
+    assert L.ana_prepared_digest(c.h) != L.ana_prepared_digest(a.h)
 
 
 def test_calls_on_null_context_are_rejected(lib_built):
