@@ -50,7 +50,9 @@ class AnaLight(C.Structure):
 class AnaCamera(C.Structure):
     _fields_ = [("from_", F3), ("at", F3), ("up", F3), ("vfov_deg", C.c_float),
                 ("aperture_radius", C.c_float), ("focal_distance", C.c_float),
-                ("shutter_open", C.c_float), ("shutter_close", C.c_float)]
+                ("shutter_open", C.c_float), ("shutter_close", C.c_float),
+                ("explicit_basis", C.c_uint32), ("origin", F3), ("lower_left", F3),
+                ("horizontal", F3), ("vertical", F3), ("basis_u", F3), ("basis_v", F3)]
 
 
 _P = C.c_void_p
@@ -265,6 +267,12 @@ class SceneDesc:
         cam.at[:] = sc.cam_at
         cam.up[:] = sc.cam_up
         cam.vfov_deg = sc.vfov
+        if sc.cam_basis is not None:
+            b = [float(x) for x in sc.cam_basis]
+            cam.explicit_basis = 1
+            cam.origin[:], cam.lower_left[:], cam.horizontal[:] = b[0:3], b[3:6], b[6:9]
+            cam.vertical[:], cam.basis_u[:], cam.basis_v[:] = b[9:12], b[12:15], b[15:18]
+            cam.aperture_radius, cam.focal_distance, cam.shutter_open, cam.shutter_close = b[18:22]
         d.camera = cam
         d.max_leaf_tris = max_leaf_tris
         d.max_leaf_segments = max_leaf_segments
@@ -284,6 +292,11 @@ class Prepared:
     @property
     def nbytes(self) -> int:
         return int(lib().ana_prepared_bytes(self.h))
+
+    @property
+    def digest(self) -> int:
+        """FNV-1a of the device layout (BVHs, primitives, materials, lights, dome)."""
+        return int(lib().ana_prepared_digest(self.h))
 
     def __del__(self):
         try:

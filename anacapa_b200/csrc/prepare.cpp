@@ -358,6 +358,23 @@ uint64_t Prepared::bytes() const {
 }
 
 DevCamera make_camera(const ana_camera& c, uint32_t width, uint32_t height) {
+    if (c.explicit_basis) {
+        DevCamera d{};
+        auto f3 = [](const float* p) { return make_float3(p[0], p[1], p[2]); };
+        d.origin = f3(c.origin);
+        d.lower_left = f3(c.lower_left);
+        d.horizontal = f3(c.horizontal);
+        d.vertical = f3(c.vertical);
+        d.basis_u = f3(c.basis_u);
+        d.basis_v = f3(c.basis_v);
+        d.aperture = c.aperture_radius;
+        d.focal_distance = c.focal_distance;
+        d.shutter_open = c.shutter_open;
+        d.shutter_close = c.shutter_close;
+        d.width = width;
+        d.height = height;
+        return d;
+    }
     float theta = c.vfov_deg * 3.14159265f / 180.f;
     float h = std::tan(theta * 0.5f);
     float aspect = static_cast<float>(width) / static_cast<float>(height);

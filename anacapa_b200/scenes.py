@@ -109,6 +109,11 @@ class Scene:
     height: int = 256
     spp: int = 16
     max_depth: int = 8
+    # An already built Camera for width x height (ana_camera.explicit_basis):
+    # origin, lowerLeftCorner, horizontal, vertical, basisU, basisV (3 floats
+    # each), apertureRadius, focalDistance, shutterOpen, shutterClose. None:
+    # built from cam_from/cam_at/cam_up/vfov.
+    cam_basis: Optional[tuple] = None
 
     @property
     def num_meshes(self) -> int:

@@ -105,6 +105,16 @@ typedef struct ana_camera {
     float focal_distance;   /* thin lens (Camera::makeThinLens) when aperture > 0 */
     float shutter_open;
     float shutter_close;
+    /* explicit_basis != 0: use an already built Camera (its origin,
+     * lowerLeftCorner, horizontal, vertical, basisU, basisV) instead of
+     * from/at/up/vfov; the film size must be the one it was built for. */
+    uint32_t explicit_basis;
+    float origin[3];
+    float lower_left[3];
+    float horizontal[3];
+    float vertical[3];
+    float basis_u[3];
+    float basis_v[3];
 } ana_camera;
 
 /* ---- scene (GeometryPool + CurvePool + SceneView) ------------------------- */

@@ -400,6 +400,25 @@ void ref_camera_rays(void* sp, uint32_t W, uint32_t H, const uint32_t* pxy_s, ui
     }
 }
 
+// The scene's Camera as this build of the reference computed it: origin,
+// lowerLeftCorner, horizontal, vertical, basisU, basisV, apertureRadius,
+// focalDistance, shutterOpen, shutterClose (22 floats).
+void ref_camera_basis(void* sp, uint32_t W, uint32_t H, float* out) {
+    auto* s = static_cast<RefScene*>(sp);
+    Camera cam = s->view.camera.value_or(
+        Camera::makePinhole({0.f, 0.f, -2.5f}, {0.f, 0.f, 1.f}, {0.f, 1.f, 0.f}, 50.f, W, H));
+    put3(out, cam.origin);
+    put3(out + 3, cam.lowerLeftCorner);
+    put3(out + 6, cam.horizontal);
+    put3(out + 9, cam.vertical);
+    put3(out + 12, cam.basisU);
+    put3(out + 15, cam.basisV);
+    out[18] = cam.apertureRadius;
+    out[19] = cam.focalDistance;
+    out[20] = cam.shutterOpen;
+    out[21] = cam.shutterClose;
+}
+
 // ---- sampler -------------------------------------------------------------
 void ref_halton(uint32_t px, uint32_t py, uint32_t sampleIndex, uint64_t seed, uint32_t ndims,
                 float* out) {
@@ -495,3 +514,99 @@ void ref_dist1d(const float* vals, uint32_t n, const float* us, uint32_t nu, flo
 }
 
 }  // extern "C"
+
+// ============================================================================
+// Drop-in check (built only into oracle/_ref/libanacapa_ref_dropin.so, which
+// also links this repository's B200PathIntegrator and CUDA library): the
+// reference's SceneView and Film driven through IIntegrator::prepare /
+// renderFrame exactly as RenderSession::render's non-adaptive branch does
+// (src/render/RenderSession.cpp:468, 541-547).
+// ============================================================================
+#ifdef ANA_DROPIN
+#include "B200PathIntegrator.h"
+
+namespace anacapa {
+// Film.cpp needs OpenImageIO; the check supplies Film's accumulation members
+// with the arithmetic of src/film/Film.cpp:18-90 (I/O and denoising report
+// failure).
+Film::Film(uint32_t width, uint32_t height)
+    : m_width(width), m_height(height), m_pixels(width * height), m_albedo(width * height),
+      m_normals(width * height) {}
+void Film::splatPixel(float x, float y, Spectrum value) {
+    if (!value.isFinite()) return;
+    int px = int(x), py = int(y);
+    if (!inBounds(px, py)) return;
+    m_pixels[py * m_width + px].add(value.x, value.y, value.z, 1.f);
+}
+void Film::mergeTile(const TileBuffer& tile) {
+    m_dirty.store(true, std::memory_order_relaxed);
+    for (uint32_t ty = 0; ty < tile.height; ++ty)
+        for (uint32_t tx = 0; tx < tile.width; ++tx) {
+            uint32_t fx = tile.x0 + tx, fy = tile.y0 + ty;
+            if (!inBounds(int(fx), int(fy))) continue;
+            uint32_t fi = fy * m_width + fx, ti = ty * tile.width + tx;
+            const auto& s = tile.pixels[ti];
+            if (s.weight > 0.f) {
+                m_pixels[fi].r.fetch_add(s.r, std::memory_order_relaxed);
+                m_pixels[fi].g.fetch_add(s.g, std::memory_order_relaxed);
+                m_pixels[fi].b.fetch_add(s.b, std::memory_order_relaxed);
+                m_pixels[fi].weight.fetch_add(s.weight, std::memory_order_relaxed);
+                m_pixels[fi].sumLumSq.fetch_add(tile.sumLumSq[ti], std::memory_order_relaxed);
+            }
+        }
+}
+Spectrum Film::getPixel(uint32_t x, uint32_t y) const { return m_pixels[y * m_width + x].resolve(); }
+float Film::varianceAt(uint32_t x, uint32_t y) const {
+    const auto& p = m_pixels[y * m_width + x];
+    float w = p.weight.load(std::memory_order_relaxed);
+    if (w <= 0.f) return 0.f;
+    float invW = 1.f / w;
+    float meanL = (p.r.load() * 0.2126f + p.g.load() * 0.7152f + p.b.load() * 0.0722f) * invW;
+    float eLsq = p.sumLumSq.load() * invW;
+    return std::max(0.f, eLsq - meanL * meanL);
+}
+bool Film::denoise() { return false; }
+bool Film::writeEXR(const std::string&, const DenoiseOptions&) const { return false; }
+bool Film::writePNG(const std::string&, float) const { return false; }
+}  // namespace anacapa
+
+extern "C" int ref_dropin_render(void* sp, uint32_t W, uint32_t H, uint32_t spp, uint32_t maxDepth,
+                                 int passes, float* out_rgb, float* out_var, char* err, int errlen) {
+    auto* s = static_cast<RefScene*>(sp);
+    anacapa_b200::B200PathIntegrator integ(maxDepth);
+    if (!integ.isValid()) {
+        std::snprintf(err, size_t(errlen), "%s", integ.lastError().c_str());
+        return 1;
+    }
+    integ.prepare(s->view);
+    Film film(W, H);
+    // `passes` renderFrame calls of spp samples each continue the sample
+    // indices (progressive accumulation into the same Film)
+    for (int k = 0; k < passes; ++k)
+        if (!integ.renderFrame(s->view, W, H, uint32_t(k) * spp, spp, film)) {
+            std::snprintf(err, size_t(errlen), "%s", integ.lastError().c_str());
+            return 2;
+        }
+    for (uint32_t y = 0; y < H; ++y)
+        for (uint32_t x = 0; x < W; ++x) {
+            Spectrum c = film.getPixel(x, y);
+            size_t i = size_t(y) * W + x;
+            out_rgb[3 * i] = c.x;
+            out_rgb[3 * i + 1] = c.y;
+            out_rgb[3 * i + 2] = c.z;
+            out_var[i] = film.varianceAt(x, y);
+        }
+    return 0;
+}
+// The host half of the drop-in's prepare (no device needed): the prepared
+// layout built from the reference's SceneView, for comparison with the layout
+// the C ABI builds from the same scene description. Free with
+// ana_prepared_free.
+extern "C" void* ref_dropin_prepare(void* sp, uint32_t W, uint32_t H, char* err, int errlen) {
+    auto* s = static_cast<RefScene*>(sp);
+    std::string e;
+    ana_prepared* p = anacapa_b200::B200PathIntegrator::prepareHost(s->view, W, H, e);
+    if (!p) std::snprintf(err, size_t(errlen), "%s", e.c_str());
+    return p;
+}
+#endif  // ANA_DROPIN

@@ -28,15 +28,17 @@ def _fp(a):
 
 
 def build(reference="/root/reference", quiet=True):
-    """Compile the reference variants (needs the reference tree; a no-op when
-    the libraries already exist)."""
+    """Compile the reference variants and, when the CUDA library exists, the
+    drop-in check (needs the reference tree; a no-op when the libraries are
+    already built)."""
     libs = [os.path.join(REF_DIR, n) for n in ("libanacapa_ref.so", "libanacapa_ref_nocontract.so")]
-    if all(os.path.exists(p) for p in libs):
-        return True
     if not os.path.isdir(reference):
-        return False
+        return all(os.path.exists(p) for p in libs)
     subprocess.run(["make", "-C", HERE, "ref", f"REF={reference}"], check=True,
                    stdout=subprocess.DEVNULL if quiet else None)
+    if os.path.exists(os.path.join(os.path.dirname(HERE), "anacapa_b200", "libanacapa_b200.so")):
+        subprocess.run(["make", "-C", HERE, "dropin", f"REF={reference}"], check=True,
+                       stdout=subprocess.DEVNULL if quiet else None)
     return True
 
 
@@ -45,8 +47,9 @@ def available(variant="record"):
 
 
 def _libpath(variant):
-    return os.path.join(REF_DIR, "libanacapa_ref.so" if variant == "record"
-                        else "libanacapa_ref_nocontract.so")
+    return os.path.join(REF_DIR, {"record": "libanacapa_ref.so",
+                                  "nocontract": "libanacapa_ref_nocontract.so",
+                                  "dropin": "libanacapa_ref_dropin.so"}[variant])
 
 
 _LIBS = {}
@@ -79,6 +82,7 @@ def lib(variant="record"):
     L.ref_dim_log.argtypes = [_P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
                               C.c_uint32, _I32, C.c_int]
     L.ref_camera_rays.argtypes = [_P, C.c_uint32, C.c_uint32, _U32, C.c_uint64, _F]
+    L.ref_camera_basis.argtypes = [_P, C.c_uint32, C.c_uint32, _F]
     L.ref_halton.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32, _F]
     L.ref_pcg.argtypes = [C.c_uint64, C.c_uint32, _U32]
     L.ref_mat_evaluate.argtypes = [_P, C.c_int, _F, _F, _F, _F, _F]
@@ -92,6 +96,11 @@ def lib(variant="record"):
     L.ref_light_le.argtypes = [_P, C.c_int, _F, _F]
     L.ref_light_sample_le.argtypes = [_P, C.c_int, _F, _F, _F]
     L.ref_dist1d.argtypes = [_F, C.c_uint32, _F, C.c_uint32, _F, _F]
+    if variant == "dropin":
+        L.ref_dropin_render.argtypes = [_P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int,
+                                        _F, _F, C.c_char_p, C.c_int]
+        L.ref_dropin_prepare.argtypes = [_P, C.c_uint32, C.c_uint32, C.c_char_p, C.c_int]
+        L.ref_dropin_prepare.restype = _P
     _LIBS[variant] = L
     return L
 
@@ -186,6 +195,39 @@ class RefScene:
         secs = self.L.ref_render(self.h, W, H, spp, sample_start, md, nthreads, x0, y0, x1, y1,
                                  _fp(rgbw), _fp(lsq))
         return rgbw, lsq, secs
+
+    def dropin_render(self, spp=None, passes=1, max_depth=None):
+        """Render through this repository's B200PathIntegrator driven by the
+        reference's SceneView and Film (variant "dropin" only). Returns the
+        resolved RGB image and Film::varianceAt."""
+        s = self.scene
+        rgb = np.zeros((s.height, s.width, 3), np.float32)
+        var = np.zeros((s.height, s.width), np.float32)
+        err = C.create_string_buffer(512)
+        rc = self.L.ref_dropin_render(self.h, s.width, s.height, s.spp if spp is None else spp,
+                                      s.max_depth if max_depth is None else max_depth, passes,
+                                      _fp(rgb), _fp(var), err, len(err))
+        if rc:
+            raise RuntimeError(f"drop-in render failed ({rc}): {err.value.decode()}")
+        return rgb, var
+
+    def dropin_prepare(self):
+        """The drop-in's host-side prepare of this scene (variant "dropin"
+        only): a raw ana_prepared handle, freed by the caller."""
+        s = self.scene
+        err = C.create_string_buffer(512)
+        p = self.L.ref_dropin_prepare(self.h, s.width, s.height, err, len(err))
+        if not p:
+            raise RuntimeError(f"drop-in prepare failed: {err.value.decode()}")
+        return p
+
+    def camera_basis(self):
+        """The scene's Camera as this build computed it (22 floats, the layout
+        of Scene.cam_basis)."""
+        s = self.scene
+        out = np.zeros(22, np.float32)
+        self.L.ref_camera_basis(self.h, s.width, s.height, _fp(out))
+        return tuple(out.tolist())
 
     def li(self, pxy_s, max_depth=None, nthreads=0):
         s = self.scene
