@@ -29,6 +29,7 @@ ANA_RENDER_COUNT_WORK = 2
 ANA_TRAVERSAL_DEFAULT = 0
 ANA_TRAVERSAL_PERSISTENT = 1
 ANA_TRAVERSAL_PER_RAY = 2
+TRACE_NOALLOC_MAX_RAYS = 65536  # ANA_TRACE_NOALLOC_MAX_RAYS
 
 F3 = C.c_float * 3
 
@@ -112,7 +113,7 @@ EXPORTS = ["ana_create", "ana_destroy", "ana_upload_scene", "ana_prepare_scene",
            "ana_film_clear", "ana_film_read", "ana_film_device_ptr", "ana_trace_batch",
            "ana_get_stats", "ana_last_error", "ana_version", "ana_batch_create", "ana_batch_free",
            "ana_batch_bytes", "ana_upload_batch", "ana_render_batch", "ana_batch_film_read",
-           "ana_prepared_digest"]
+           "ana_prepared_digest", "ana_trace_batch_noalloc"]
 ANA_RENDER_GRAPH = 4
 
 _lib = None
@@ -147,6 +148,7 @@ def lib():
     L.ana_film_read.argtypes = [_P, _P, C.c_size_t]
     L.ana_film_device_ptr.argtypes = [_P, C.POINTER(_P)]
     L.ana_trace_batch.argtypes = [_P, _P, C.c_size_t, _P, C.c_int, C.c_int]
+    L.ana_trace_batch_noalloc.argtypes = [_P, _P, C.c_size_t, _P, C.c_int]
     L.ana_get_stats.argtypes = [_P, C.POINTER(AnaStats)]
     L.ana_last_error.argtypes = [_P, C.c_char_p, C.c_size_t]
     L.ana_version.restype = C.c_int
@@ -368,6 +370,16 @@ class Renderer:
         out = np.zeros(len(rays), HIT_DTYPE)
         self._check(lib().ana_trace_batch(self.h, rays.ctypes.data, len(rays), out.ctypes.data,
                                           1 if occlusion else 0, 0))
+        return out
+
+    def trace_noalloc(self, rays: np.ndarray, occlusion=False) -> np.ndarray:
+        """ana_trace_batch_noalloc: the same query staged in the library's fixed
+        device scratch (at most TRACE_NOALLOC_MAX_RAYS rays, no device
+        allocation), for callers that must not allocate while tracing."""
+        rays = np.ascontiguousarray(np.asarray(rays, np.float32).reshape(-1, 8))
+        out = np.zeros(len(rays), HIT_DTYPE)
+        self._check(lib().ana_trace_batch_noalloc(self.h, rays.ctypes.data, len(rays), out.ctypes.data,
+                                                  1 if occlusion else 0))
         return out
 
     # ---- batches -------------------------------------------------------------

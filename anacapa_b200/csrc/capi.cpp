@@ -930,6 +930,52 @@ int ana_trace_batch(ana_ctx* c, const float* rays, size_t n, ana_hit* out, int o
     return ANA_OK;
 }
 
+// The same query as ana_trace_batch with host buffers, staged in the fixed
+// module scratch (kernels.cu) instead of a per-call cudaMalloc: callers that
+// must not allocate (a pick query beside an in-flight frame, where cudaFree
+// would wait for the frame; a device already full) use this one. Nothing on
+// the success path allocates, on the device or on the host.
+int ana_trace_batch_noalloc(ana_ctx* c, const float* rays, size_t n, ana_hit* out, int occlusion) {
+    if (!c || (!rays && n) || (!out && n))
+        return fail(c, ANA_ERR_INVALID_ARG, "ana_trace_batch_noalloc: NULL argument");
+    if (n > ANA_TRACE_NOALLOC_MAX_RAYS)
+        return fail(c, ANA_ERR_INVALID_ARG,
+                    "ana_trace_batch_noalloc: " + std::to_string(n) + " rays exceed the fixed scratch of " +
+                        std::to_string(ANA_TRACE_NOALLOC_MAX_RAYS) +
+                        " rays; split the batch or use ana_trace_batch");
+    if (!c->has_scene) return fail(c, ANA_ERR_STATE, "ana_trace_batch_noalloc: no scene uploaded");
+    if (n == 0) return ANA_OK;
+    CK(cudaSetDevice(c->device), "cudaSetDevice");
+    unsigned char* base = nullptr;
+    cudaError_t e = ana::noalloc_trace_scratch(c->device, &base);
+    if (e != cudaSuccess) return cuda_fail(c, e, "ana_trace_batch_noalloc: scratch address (cudaGetSymbolAddress)");
+    ana::DevSceneRec R{};
+    R.tri_root = c->scenes[0].tri_root;
+    R.seg_root = c->scenes[0].seg_root;
+    float* d_rays = reinterpret_cast<float*>(base + ana::kNoAllocRays);
+    ana_hit* d_out = reinterpret_cast<ana_hit*>(base + ana::kNoAllocHits);
+    uint32_t* d_err = reinterpret_cast<uint32_t*>(base + ana::kNoAllocErrOffset);
+    uint32_t* d_fetch = d_err + 1;
+    e = cudaMemcpyAsync(base, &R, sizeof(R), cudaMemcpyHostToDevice, c->stream);
+    // the error word and the persistent schedule's work counter start at zero
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_err, 0, 8, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_rays, rays, n * 32, cudaMemcpyHostToDevice, c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "ana_trace_batch_noalloc: setup");
+    ana::DevScene S = c->ds;
+    S.scenes = reinterpret_cast<const ana::DevSceneRec*>(base);
+    S.num_scenes = 1;
+    ana::launch_trace_batch(S, 0, d_rays, n, d_out, occlusion, d_fetch, d_err,
+                            c->opts.traversal == ANA_TRAVERSAL_PER_RAY ? 0 : 1, c->stream);
+    e = cudaGetLastError();
+    uint32_t herr = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, d_out, n * sizeof(ana_hit), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, d_err, 4, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "ana_trace_batch_noalloc");
+    if (herr) return fail(c, ANA_ERR_DEVICE_CHECK, "ana_trace_batch_noalloc: traversal stack overflow on the device");
+    return ANA_OK;
+}
+
 int ana_get_stats(ana_ctx* c, ana_stats* out) {
     if (!c || !out) return fail(c, ANA_ERR_INVALID_ARG, "ana_get_stats: NULL argument");
     *out = c->stats;

@@ -754,4 +754,28 @@ void launch_trace_batch(const DevScene& S, uint32_t scene, const float* rays, si
     }
 }
 
+// ---------------------------------------------------------------------------
+// Scratch of the allocation-free trace entry point: module global memory,
+// created with the module on each device (about 4 MiB), so the entry point
+// never asks the allocator for memory. One copy per device, shared by every
+// context on that device.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) unsigned char g_noalloc_trace[kNoAllocBytes];
+
+cudaError_t noalloc_trace_scratch(int device, unsigned char** base) {
+    constexpr int kMaxDevices = 64;
+    static std::mutex mu;
+    static void* addr[kMaxDevices] = {};
+    if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lk(mu);
+    if (!addr[device]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_trace);
+        if (e != cudaSuccess) return e;
+        addr[device] = p;
+    }
+    *base = static_cast<unsigned char*>(addr[device]);
+    return cudaSuccess;
+}
+
 }  // namespace ana

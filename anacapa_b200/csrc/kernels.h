@@ -79,4 +79,21 @@ void launch_film(const Params& p, const LaunchCfg& c, cudaStream_t s);
 void launch_trace_batch(const DevScene& S, uint32_t scene, const float* rays, size_t n, ana_hit* out, int occlusion,
                         uint32_t* fetch, uint32_t* err, int persistent, cudaStream_t s);
 
+// Fixed device scratch of the allocation-free trace entry point: a 256-byte
+// header (the scene record at 0, the error word at kNoAllocErrOffset and the
+// persistent schedule's work counter 4 bytes after it), then room for
+// ANA_TRACE_NOALLOC_MAX_RAYS rays of 32 bytes, then as many 32-byte hits.
+constexpr size_t kNoAllocHeader = 256;
+constexpr size_t kNoAllocErrOffset = 192;
+constexpr size_t kNoAllocRays = kNoAllocHeader;
+constexpr size_t kNoAllocHits = kNoAllocRays + size_t(ANA_TRACE_NOALLOC_MAX_RAYS) * 32;
+constexpr size_t kNoAllocBytes = kNoAllocHits + size_t(ANA_TRACE_NOALLOC_MAX_RAYS) * sizeof(ana_hit);
+static_assert(sizeof(DevSceneRec) <= kNoAllocErrOffset, "scene record overlaps the error word");
+static_assert(sizeof(ana_hit) == 32, "hit record size");
+
+// Device address of that scratch on `device`, which must be the current
+// device. The first call per device looks it up (cudaGetSymbolAddress) and
+// caches it; later calls only read the cache.
+cudaError_t noalloc_trace_scratch(int device, unsigned char** base);
+
 }  // namespace ana

@@ -305,6 +305,29 @@ int ana_film_device_ptr(ana_ctx* ctx, void** dptr);
 int ana_trace_batch(ana_ctx* ctx, const float* rays, size_t n, ana_hit* out, int occlusion_only,
                     int rays_on_device);
 
+/* ana_trace_batch without any device allocation (no counterpart in the
+ * reference). ana_trace_batch takes a temporary device buffer per call
+ * (cudaMalloc / cudaFree); this variant stages the rays, the hits and its
+ * counters in a fixed scratch array that lives in the library's module
+ * memory, one per device. It is for callers that cannot allocate device
+ * memory at the moment they trace: a viewer answering a pick or hover query
+ * while a frame renders on another stream (cudaFree waits for all work on
+ * the device, so the query would stall until the frame ends), and a process
+ * whose device memory is already held by the scene, the films and a caching
+ * allocator (an allocation there can fail mid-session).
+ *   rays: host array of n x 8 floats as for ana_trace_batch; out: host array
+ *   of n hits. n <= ANA_TRACE_NOALLOC_MAX_RAYS, else ANA_ERR_INVALID_ARG and
+ *   nothing runs. The call returns after the hits are in `out`.
+ * The first call on a device looks up the scratch address
+ * (cudaGetSymbolAddress, with the context's device current) and caches it;
+ * make that first call before any stream capture begins on the device. Each
+ * call zeroes the error word and work counter of the scratch itself; rays
+ * and hits need no clearing. The scratch is shared by every context on the
+ * device: calls that overlap in time (two threads, two contexts on one
+ * device) race on it and must be serialised by the caller. */
+#define ANA_TRACE_NOALLOC_MAX_RAYS 65536
+int ana_trace_batch_noalloc(ana_ctx* ctx, const float* rays, size_t n, ana_hit* out, int occlusion_only);
+
 int ana_get_stats(ana_ctx* ctx, ana_stats* out);
 
 /* Copy the last error message of this context (or of the last failed
