@@ -98,6 +98,10 @@ class AnaStats(C.Structure):
                 ("node_fetches", C.c_uint64), ("tri_tests", C.c_uint64), ("seg_tests", C.c_uint64)]
 
 
+class AnaDiffParams(C.Structure):
+    _fields_ = [("albedo", _P), ("roughness", _P), ("emission", _P), ("light_le", _P)]
+
+
 class AnaDeviceOpts(C.Structure):
     _fields_ = [("device", C.c_int), ("chunk_paths", C.c_uint32), ("block_size", C.c_uint32),
                 ("timing", C.c_uint32), ("traversal", C.c_uint32)]
@@ -113,7 +117,8 @@ EXPORTS = ["ana_create", "ana_destroy", "ana_upload_scene", "ana_prepare_scene",
            "ana_film_clear", "ana_film_read", "ana_film_device_ptr", "ana_trace_batch",
            "ana_get_stats", "ana_last_error", "ana_version", "ana_batch_create", "ana_batch_free",
            "ana_batch_bytes", "ana_upload_batch", "ana_render_batch", "ana_batch_film_read",
-           "ana_prepared_digest", "ana_trace_batch_noalloc"]
+           "ana_prepared_digest", "ana_trace_batch_noalloc", "ana_diff_counts", "ana_diff_get_params",
+           "ana_forward", "ana_backward"]
 ANA_RENDER_GRAPH = 4
 
 _lib = None
@@ -162,6 +167,10 @@ def lib():
     L.ana_batch_film_read.argtypes = [_P, C.c_uint32, _P, C.c_size_t]
     L.ana_prepared_digest.argtypes = [_P]
     L.ana_prepared_digest.restype = C.c_uint64
+    L.ana_diff_counts.argtypes = [_P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
+    L.ana_diff_get_params.argtypes = [_P, C.POINTER(AnaDiffParams)]
+    L.ana_forward.argtypes = [_P, C.POINTER(AnaRenderDesc), C.POINTER(AnaDiffParams), _P]
+    L.ana_backward.argtypes = [_P, _P, C.POINTER(AnaDiffParams)]
     _lib = L
     return L
 
@@ -359,6 +368,57 @@ class Renderer:
     def image(self, width, height) -> np.ndarray:
         f = self.film(width, height)
         return f[..., :3] / np.maximum(f[..., 3:4], 1e-30)
+
+    # ---- differentiable rendering (ana_forward / ana_backward) ----
+    def diff_counts(self):
+        nm, nl = C.c_uint32(), C.c_uint32()
+        self._check(lib().ana_diff_counts(self.h, C.byref(nm), C.byref(nl)))
+        return nm.value, nl.value
+
+    def _diff_arrays(self):
+        nm, nl = self.diff_counts()
+        return {"albedo": np.zeros((nm, 3), np.float32), "roughness": np.zeros(nm, np.float32),
+                "emission": np.zeros((nm, 3), np.float32), "light_le": np.zeros((nl, 3), np.float32)}
+
+    @staticmethod
+    def _diff_struct(d):
+        st = AnaDiffParams()
+        for k in ("albedo", "roughness", "emission", "light_le"):
+            a = d.get(k)
+            setattr(st, k, None if a is None else a.ctypes.data)
+        return st
+
+    def diff_params(self):
+        """Current differentiable parameters: albedo (M,3), roughness (M,),
+        emission (M,3), light_le (L,3), by uploaded material / light index."""
+        d = self._diff_arrays()
+        st = self._diff_struct(d)
+        self._check(lib().ana_diff_get_params(self.h, C.byref(st)))
+        return d
+
+    def forward(self, width, height, spp, max_depth, params=None, sample_start=0, min_depth=2, seed=0):
+        """ana_forward: set `params` (dict of arrays, missing keys unchanged),
+        render, return the (H, W, 3) image."""
+        keep = None
+        st = None
+        if params is not None:
+            keep = {k: np.ascontiguousarray(np.asarray(v, np.float32)) for k, v in params.items()
+                    if v is not None}
+            st = self._diff_struct(keep)
+        r = AnaRenderDesc(width, height, sample_start, spp, max_depth, min_depth, seed, ANA_RENDER_CLEAR_FILM)
+        img = np.zeros((height, width, 3), np.float32)
+        self._check(lib().ana_forward(self.h, C.byref(r), C.byref(st) if st is not None else None,
+                                      img.ctypes.data))
+        del keep
+        return img
+
+    def backward(self, d_image):
+        """ana_backward: dLoss/d image (H, W, 3) -> dict of dLoss/d parameters."""
+        g = np.ascontiguousarray(np.asarray(d_image, np.float32))
+        d = self._diff_arrays()
+        st = self._diff_struct(d)
+        self._check(lib().ana_backward(self.h, g.ctypes.data, C.byref(st)))
+        return d
 
     def stats(self) -> AnaStats:
         s = AnaStats()

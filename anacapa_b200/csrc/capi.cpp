@@ -58,6 +58,7 @@ struct Blob {
            o_slots = 0, o_lights = 0, o_env_rgb = 0, o_cf = 0, o_cc = 0, o_ci = 0, o_mf = 0, o_mc = 0;
     std::vector<SceneStatic> scenes;
     bool has_curves = false, has_emitters = false;
+    size_t n_mats = 0, n_lights = 0;
     ana::HostEnv env_meta;  // scalars only
     Blob() = default;
     Blob(const Blob&) = delete;
@@ -109,6 +110,8 @@ int build_blob(const ana::Prepared* const* list, uint32_t n, Blob& B, std::strin
     B.o_mats = take(nMats * sizeof(ana::DevMaterial));
     B.o_slots = take(nSlots * 4);
     B.o_lights = take(nLights * sizeof(ana::DevLight));
+    B.n_mats = nMats;
+    B.n_lights = nLights;
     B.o_env_rgb = take(dome ? dome->env.rgb.size() * 4 : 0);
     B.o_cf = take(dome ? dome->env.cond_func.size() * 4 : 0);
     B.o_cc = take(dome ? dome->env.cond_cdf.size() * 4 : 0);
@@ -262,6 +265,22 @@ struct ana_ctx {
     GraphCache graph;
     ana_stats stats{};
     int num_sms = 148;
+    // differentiable rendering: host copies of the uploaded material and
+    // light tables (parameters are written into them and copied back), the
+    // last ana_forward's frame (its seeds determine every path), and the
+    // adjoint replay's buffers
+    std::vector<ana::DevMaterial> h_mats;
+    std::vector<ana::DevLight> h_lights;
+    size_t o_mats = 0, o_lights = 0;
+    bool fwd_valid = false;
+    ana_render_desc fwd_desc{};
+    ana::AdjQueues aq{};
+    unsigned char* d_adj = nullptr;
+    size_t adj_size = 0;
+    uint32_t adj_cap = 0;
+    float* adj_L = nullptr;
+    unsigned char* d_adj_io = nullptr;  // adjoint image + gradient accumulators
+    size_t adj_io_size = 0;
     ana_film_pixel* film_px() const { return reinterpret_cast<ana_film_pixel*>(film); }
 };
 
@@ -382,6 +401,13 @@ int upload_blob(ana_ctx* c, const Blob& B) {
     c->scenes = B.scenes;
     c->has_scene = true;
     c->upload_serial++;
+    const auto* hm = reinterpret_cast<const ana::DevMaterial*>(B.mem + B.o_mats);
+    const auto* hl = reinterpret_cast<const ana::DevLight*>(B.mem + B.o_lights);
+    c->h_mats.assign(hm, hm + B.n_mats);
+    c->h_lights.assign(hl, hl + B.n_lights);
+    c->o_mats = B.o_mats;
+    c->o_lights = B.o_lights;
+    c->fwd_valid = false;
     drop_graph(c);
     return ANA_OK;
 }
@@ -390,8 +416,47 @@ struct ChunkPlan {
     uint32_t first_path, paths, pixels, seg_begin, seg_count;
 };
 
+// Adjoint replay buffers for `cap` paths, next to the forward queues.
+int ensure_adjoint(ana_ctx* c, uint32_t cap) {
+    if (c->adj_cap >= cap && c->d_adj) return ANA_OK;
+    const size_t f4 = size_t(cap) * 16;
+    const size_t total = 9 * align_up(f4) + align_up(size_t(cap) * 4) + 2 * align_up(size_t(cap) * 12);
+    int rc = ensure_buffer(c, &c->d_adj, &c->adj_size, total, "cudaMalloc(adjoint queues)");
+    if (rc) return rc;
+    unsigned char* b = c->d_adj;
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        unsigned char* q = b + off;
+        off += align_up(bytes);
+        return q;
+    };
+    ana::AdjQueues& a = c->aq;
+    for (int k = 0; k < 2; ++k) {
+        a.ext_g0[k] = reinterpret_cast<float4*>(take(f4));
+        a.ext_g1[k] = reinterpret_cast<float4*>(take(f4));
+    }
+    a.sh_g0 = reinterpret_cast<float4*>(take(f4));
+    a.sh_g1 = reinterpret_cast<float4*>(take(f4));
+    a.mis_g0 = reinterpret_cast<float4*>(take(f4));
+    a.mis_g1 = reinterpret_cast<float4*>(take(f4));
+    a.mis_res = reinterpret_cast<float4*>(take(f4));
+    a.sh_vis = reinterpret_cast<uint32_t*>(take(size_t(cap) * 4));
+    a.dL = reinterpret_cast<float*>(take(size_t(cap) * 12));
+    // the adjoint replay's running radiance (the primal's lives in the queues' L)
+    c->adj_L = reinterpret_cast<float*>(take(size_t(cap) * 12));
+    c->adj_cap = cap;
+    return ANA_OK;
+}
+
 // The batch render: descs[k] renders uploaded scene k into its film.
-int render_items(ana_ctx* c, const ana_render_desc* descs, uint32_t n, uint32_t flags) {
+// With adj_image (host, 3 floats per film pixel: dLoss / d pixel) it runs the
+// path-replay adjoint instead: per chunk a primal replay of the same paths
+// (their radiance L) and an adjoint replay that accumulates dLoss / d theta
+// into adj_grad (host, 8 floats per material then 4 per light).
+int render_items(ana_ctx* c, const ana_render_desc* descs, uint32_t n, uint32_t flags,
+                 const float* adj_image = nullptr, float* adj_grad = nullptr) {
+    const bool backward = adj_image != nullptr;
+    if (backward) flags &= ~uint32_t(ANA_RENDER_GRAPH | ANA_RENDER_COUNT_WORK);
     if (!c || !descs || n == 0) return fail(c, ANA_ERR_INVALID_ARG, "ana_render: NULL argument or no items");
     if (!c->has_scene) return fail(c, ANA_ERR_STATE, "ana_render: no scene uploaded");
     if (n != c->scenes.size())
@@ -419,6 +484,17 @@ int render_items(ana_ctx* c, const ana_render_desc* descs, uint32_t n, uint32_t 
     if (uint64_t(cap) > totalPaths) cap = uint32_t(totalPaths);
     int rc = ensure_queues(c, cap);
     if (rc) return rc;
+    const size_t nparams = 8 * c->h_mats.size() + 4 * c->h_lights.size();
+    const size_t oGrad = align_up(size_t(totalPixels) * 12);
+    if (backward) {
+        rc = ensure_adjoint(c, cap);
+        if (rc) return rc;
+        rc = ensure_buffer(c, &c->d_adj_io, &c->adj_io_size, oGrad + std::max<size_t>(nparams, 1) * 4,
+                           "cudaMalloc(adjoint image)");
+        if (rc) return rc;
+        CK(cudaMemcpyAsync(c->d_adj_io, adj_image, size_t(totalPixels) * 12, cudaMemcpyHostToDevice, c->stream),
+           "adjoint image H2D");
+    }
     // film: all items back to back
     rc = ensure_buffer(c, &c->film, &c->film_bytes, totalPixels * sizeof(ana_film_pixel), "cudaMalloc(film)");
     if (rc) return rc;
@@ -508,7 +584,9 @@ int render_items(ana_ctx* c, const ana_render_desc* descs, uint32_t n, uint32_t 
     }
     const uint32_t rows = maxDepth + 2;
     const size_t ncount = size_t(nchunks) * rows * ana::kCountersPerBounce;
-    rc = ensure_buffer(c, &c->d_counters, &c->counters_bytes, ncount * 4, "cudaMalloc(counters)");
+    // the backward pass keeps the adjoint replay's counters after the primal's
+    const size_t ncountAll = (backward ? 2 : 1) * ncount;
+    rc = ensure_buffer(c, &c->d_counters, &c->counters_bytes, ncountAll * 4, "cudaMalloc(counters)");
     if (rc) return rc;
     uint32_t* counters = reinterpret_cast<uint32_t*>(c->d_counters);
     ana::Params p{};
@@ -525,7 +603,8 @@ int render_items(ana_ctx* c, const ana_render_desc* descs, uint32_t n, uint32_t 
     cfg.persistent = c->opts.traversal == ANA_TRAVERSAL_PER_RAY ? 0 : 1;
     const long long gcap = ((long long)cap + cfg.block - 1) / cfg.block;
     cfg.grid_cap = int(std::max<long long>(1, std::min<long long>(gcap, 1 << 20)));
-    const size_t launches = size_t(nchunks) * (2 + 4 * size_t(maxDepth + 1));
+    const size_t launches = backward ? size_t(nchunks) * (3 + 9 * size_t(maxDepth + 1))
+                                     : size_t(nchunks) * (2 + 4 * size_t(maxDepth + 1));
     if (timing && c->stage_ev.size() < 2 * launches) {
         size_t old = c->stage_ev.size();
         c->stage_ev.resize(2 * launches);
@@ -552,6 +631,56 @@ int render_items(ana_ctx* c, const ana_render_desc* descs, uint32_t n, uint32_t 
     };
     // the launch sequence (captured into a graph when requested)
     const bool clear = (flags & ANA_RENDER_CLEAR_FILM) != 0;
+    auto enqueue_backward = [&]() {
+        cudaMemsetAsync(c->d_counters, 0, ncountAll * 4, c->stream);
+        cudaMemsetAsync(c->d_err, 0, 4, c->stream);
+        cudaMemsetAsync(c->d_adj_io + oGrad, 0, nparams * 4, c->stream);
+        ana::Params pa = p;
+        // the emission gradient of MIS hits needs the emissive material hit,
+        // which the any-hit MIS query of emitter-free scenes does not find
+        for (const ana::DevMaterial& m : c->h_mats)
+            if (m.type == ANA_MAT_EMISSIVE) pa.S.has_emitters = 1;
+        pa.a = c->aq;
+        pa.a.Lp = c->q.L;
+        pa.a.d_image = reinterpret_cast<const float*>(c->d_adj_io);
+        pa.a.grad = reinterpret_cast<float*>(c->d_adj_io + oGrad);
+        pa.a.num_materials = uint32_t(c->h_mats.size());
+        for (uint32_t k = 0; k < nchunks; ++k) {
+            const ChunkPlan& cp = chunks[k];
+            pa.chunk_first_path = cp.first_path;
+            pa.chunk_paths = cp.paths;
+            pa.chunk_pixels = cp.pixels;
+            pa.segs = reinterpret_cast<const ana::ChunkSeg*>(c->d_tables + oSeg) + cp.seg_begin;
+            pa.num_segs = cp.seg_count;
+            // primal replay: the forward pass's paths, their radiance into q.L
+            pa.q.L = c->q.L;
+            pa.counters = counters + size_t(k) * rows * ana::kCountersPerBounce;
+            pa.bounce = 0;
+            timed(4, [&] { ana::launch_generate(pa, cfg, c->stream); });
+            for (uint32_t b = 0; b <= maxDepth; ++b) {
+                pa.bounce = b;
+                timed(0, [&] { ana::launch_extend(pa, cfg, c->stream, false); });
+                timed(1, [&] { ana::launch_shade(pa, cfg, c->stream); });
+                timed(2, [&] { ana::launch_shadow(pa, cfg, c->stream); });
+                timed(3, [&] { ana::launch_mis(pa, cfg, c->stream); });
+            }
+            // adjoint replay: the same paths again, gathering radiance into
+            // adj_L so that L - adj_L is the radiance still to come
+            pa.q.L = c->adj_L;
+            pa.counters = counters + ncount + size_t(k) * rows * ana::kCountersPerBounce;
+            pa.bounce = 0;
+            timed(4, [&] { ana::launch_generate(pa, cfg, c->stream); });
+            timed(4, [&] { ana::launch_adj_init(pa, cfg, c->stream); });
+            for (uint32_t b = 0; b <= maxDepth; ++b) {
+                pa.bounce = b;
+                timed(0, [&] { ana::launch_extend(pa, cfg, c->stream, false); });
+                timed(1, [&] { ana::launch_shade_adj(pa, cfg, c->stream); });
+                timed(2, [&] { ana::launch_shadow_adj(pa, cfg, c->stream); });
+                timed(3, [&] { ana::launch_mis_adj(pa, cfg, c->stream); });
+                timed(4, [&] { ana::launch_adj_direct(pa, cfg, c->stream); });
+            }
+        }
+    };
     auto enqueue = [&]() {
         if (clear) cudaMemsetAsync(c->film, 0, totalPixels * sizeof(ana_film_pixel), c->stream);
         cudaMemsetAsync(c->d_counters, 0, ncount * 4, c->stream);
@@ -612,7 +741,8 @@ int render_items(ana_ctx* c, const ana_render_desc* descs, uint32_t n, uint32_t 
         }
         CK(cudaGraphLaunch(c->graph.exec, c->stream), "graph launch");
     } else {
-        enqueue();
+        if (backward) enqueue_backward();
+        else enqueue();
         if (first_launch_err != cudaSuccess) {
             std::string what = std::string(first_launch_stage) + " launch";
             return cuda_fail(c, first_launch_err, what.c_str());
@@ -623,9 +753,12 @@ int render_items(ana_ctx* c, const ana_render_desc* descs, uint32_t n, uint32_t 
     unsigned long long hwork[3] = {0, 0, 0};
     if (count_work)
         CK(cudaMemcpyAsync(hwork, c->d_work, sizeof(hwork), cudaMemcpyDeviceToHost, c->stream), "work D2H");
-    c->h_counters.resize(ncount);
-    CK(cudaMemcpyAsync(c->h_counters.data(), counters, ncount * 4, cudaMemcpyDeviceToHost, c->stream),
+    c->h_counters.resize(ncountAll);
+    CK(cudaMemcpyAsync(c->h_counters.data(), counters, ncountAll * 4, cudaMemcpyDeviceToHost, c->stream),
        "counters D2H");
+    if (backward && nparams)
+        CK(cudaMemcpyAsync(adj_grad, c->d_adj_io + oGrad, nparams * 4, cudaMemcpyDeviceToHost, c->stream),
+           "gradient D2H");
     uint32_t herr = 0;
     CK(cudaMemcpyAsync(&herr, c->d_err, 4, cudaMemcpyDeviceToHost, c->stream), "err D2H");
     CK(cudaStreamSynchronize(c->stream), "render sync");
@@ -634,7 +767,7 @@ int render_items(ana_ctx* c, const ana_render_desc* descs, uint32_t n, uint32_t 
     ana_stats& st = c->stats;
     st = ana_stats{};
     st.paths = totalPaths;
-    for (uint32_t k = 0; k < nchunks; ++k)
+    for (uint32_t k = 0; k < nchunks * (backward ? 2u : 1u); ++k)
         for (uint32_t b = 0; b < rows; ++b) {
             const uint32_t* cc = c->h_counters.data() + (size_t(k) * rows + b) * ana::kCountersPerBounce;
             if (b <= maxDepth) st.extend_rays += cc[0];
@@ -663,6 +796,49 @@ int render_items(ana_ctx* c, const ana_render_desc* descs, uint32_t n, uint32_t 
         st.film_ms = acc[4];
     }
     if (herr) return fail(c, ANA_ERR_DEVICE_CHECK, "ana_render: traversal stack overflow on the device");
+    return ANA_OK;
+}
+
+// Writes differentiable parameters into the host material / light tables and
+// copies both tables to the device. Derived fields follow prepare_scene:
+// standard_surface alpha2 = max(1e-4, r^2)^2 and its roughness lobe flags.
+int apply_params(ana_ctx* c, const ana_diff_params* P) {
+    const size_t nm = c->h_mats.size(), nl = c->h_lights.size();
+    for (size_t i = 0; i < nm; ++i) {
+        ana::DevMaterial& m = c->h_mats[i];
+        if (P->albedo) m.albedo = make_float3(P->albedo[3 * i], P->albedo[3 * i + 1], P->albedo[3 * i + 2]);
+        if (P->roughness && m.type == ANA_MAT_STANDARD) {
+            const float r = P->roughness[i];
+            const float a = std::max(1e-4f, r * r);
+            m.rough = r;
+            m.alpha2 = a * a;
+            uint32_t f = 16u;
+            if (r < 0.001f) f |= 4u;
+            else if (r < 0.3f) f |= 2u;
+            else f |= 1u;
+            m.flags = f;
+            m.is_delta = (r < 0.001f && (m.metal > 0.999f || m.spec > 0.f)) ? 1 : 0;
+        }
+        if (P->emission && m.type == ANA_MAT_EMISSIVE)
+            m.emission = make_float3(P->emission[3 * i], P->emission[3 * i + 1], P->emission[3 * i + 2]);
+    }
+    for (size_t i = 0; i < nl; ++i)
+        if (P->light_le && c->h_lights[i].type == ANA_LIGHT_AREA)
+            c->h_lights[i].Le = make_float3(P->light_le[3 * i], P->light_le[3 * i + 1], P->light_le[3 * i + 2]);
+    bool emitters = false;
+    for (const ana::DevMaterial& m : c->h_mats)
+        if (m.emission.x != 0.f || m.emission.y != 0.f || m.emission.z != 0.f) emitters = true;
+    c->ds.has_emitters = emitters ? 1 : 0;
+    if (nm)
+        CK(cudaMemcpyAsync(c->d_scene + c->o_mats, c->h_mats.data(), nm * sizeof(ana::DevMaterial),
+                           cudaMemcpyHostToDevice, c->stream),
+           "materials H2D");
+    if (nl)
+        CK(cudaMemcpyAsync(c->d_scene + c->o_lights, c->h_lights.data(), nl * sizeof(ana::DevLight),
+                           cudaMemcpyHostToDevice, c->stream),
+           "lights H2D");
+    CK(cudaStreamSynchronize(c->stream), "parameter upload");
+    drop_graph(c);
     return ANA_OK;
 }
 
@@ -733,6 +909,8 @@ void ana_destroy(ana_ctx* c) {
     cudaFree(c->d_queues);
     cudaFree(c->d_counters);
     cudaFree(c->d_err);
+    cudaFree(c->d_adj);
+    cudaFree(c->d_adj_io);
     for (cudaEvent_t e : c->stage_ev) cudaEventDestroy(e);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
@@ -973,6 +1151,97 @@ int ana_trace_batch_noalloc(ana_ctx* c, const float* rays, size_t n, ana_hit* ou
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) return cuda_fail(c, e, "ana_trace_batch_noalloc");
     if (herr) return fail(c, ANA_ERR_DEVICE_CHECK, "ana_trace_batch_noalloc: traversal stack overflow on the device");
+    return ANA_OK;
+}
+
+int ana_diff_counts(ana_ctx* c, uint32_t* nm, uint32_t* nl) {
+    if (!c || !nm || !nl) return fail(c, ANA_ERR_INVALID_ARG, "ana_diff_counts: NULL argument");
+    if (!c->has_scene) return fail(c, ANA_ERR_STATE, "ana_diff_counts: no scene uploaded");
+    *nm = uint32_t(c->h_mats.size());
+    *nl = uint32_t(c->h_lights.size());
+    return ANA_OK;
+}
+
+int ana_diff_get_params(ana_ctx* c, ana_diff_params* out) {
+    if (!c || !out) return fail(c, ANA_ERR_INVALID_ARG, "ana_diff_get_params: NULL argument");
+    if (!c->has_scene) return fail(c, ANA_ERR_STATE, "ana_diff_get_params: no scene uploaded");
+    for (size_t i = 0; i < c->h_mats.size(); ++i) {
+        const ana::DevMaterial& m = c->h_mats[i];
+        const bool ss = m.type == ANA_MAT_STANDARD, em = m.type == ANA_MAT_EMISSIVE;
+        if (out->albedo) {
+            out->albedo[3 * i] = m.albedo.x;
+            out->albedo[3 * i + 1] = m.albedo.y;
+            out->albedo[3 * i + 2] = m.albedo.z;
+        }
+        if (out->roughness) out->roughness[i] = ss ? m.rough : 0.f;
+        if (out->emission) {
+            out->emission[3 * i] = em ? m.emission.x : 0.f;
+            out->emission[3 * i + 1] = em ? m.emission.y : 0.f;
+            out->emission[3 * i + 2] = em ? m.emission.z : 0.f;
+        }
+    }
+    for (size_t l = 0; l < c->h_lights.size(); ++l) {
+        const ana::DevLight& L = c->h_lights[l];
+        const bool area = L.type == ANA_LIGHT_AREA;
+        if (out->light_le) {
+            out->light_le[3 * l] = area ? L.Le.x : 0.f;
+            out->light_le[3 * l + 1] = area ? L.Le.y : 0.f;
+            out->light_le[3 * l + 2] = area ? L.Le.z : 0.f;
+        }
+    }
+    return ANA_OK;
+}
+
+int ana_forward(ana_ctx* c, const ana_render_desc* d, const ana_diff_params* params, float* image) {
+    if (!c || !d) return fail(c, ANA_ERR_INVALID_ARG, "ana_forward: NULL argument");
+    if (!c->has_scene) return fail(c, ANA_ERR_STATE, "ana_forward: no scene uploaded");
+    if (c->scenes.size() != 1)
+        return fail(c, ANA_ERR_UNSUPPORTED, "ana_forward: differentiable rendering takes one uploaded scene");
+    if (c->h_mats.size() >= 0xFFFF || c->h_lights.size() >= 0xFFFF)
+        return fail(c, ANA_ERR_UNSUPPORTED, "ana_forward: more than 65534 materials or lights");
+    CK(cudaSetDevice(c->device), "cudaSetDevice");
+    c->fwd_valid = false;
+    if (params) {
+        int rc = apply_params(c, params);
+        if (rc) return rc;
+    }
+    const uint32_t flags = ANA_RENDER_CLEAR_FILM | (d->flags & ANA_RENDER_GRAPH);
+    int rc = render_items(c, d, 1, flags);
+    if (rc) return rc;
+    c->fwd_desc = *d;
+    c->fwd_valid = true;
+    if (image) {
+        const size_t n = size_t(d->width) * d->height;
+        std::vector<ana_film_pixel> px(n);
+        CK(cudaMemcpy(px.data(), c->film, n * sizeof(ana_film_pixel), cudaMemcpyDeviceToHost), "film D2H");
+        for (size_t i = 0; i < n; ++i) {  // Film::getPixel
+            const float w = px[i].w;
+            image[3 * i] = w > 0.f ? px[i].r / w : 0.f;
+            image[3 * i + 1] = w > 0.f ? px[i].g / w : 0.f;
+            image[3 * i + 2] = w > 0.f ? px[i].b / w : 0.f;
+        }
+    }
+    return ANA_OK;
+}
+
+int ana_backward(ana_ctx* c, const float* d_image, ana_diff_params* out) {
+    if (!c || !d_image || !out) return fail(c, ANA_ERR_INVALID_ARG, "ana_backward: NULL argument");
+    if (!c->fwd_valid) return fail(c, ANA_ERR_STATE, "ana_backward: no ana_forward since the last scene change");
+    const size_t nm = c->h_mats.size(), nl = c->h_lights.size();
+    std::vector<float> g(8 * nm + 4 * nl, 0.f);
+    CK(cudaSetDevice(c->device), "cudaSetDevice");
+    int rc = render_items(c, &c->fwd_desc, 1, 0, d_image, g.data());
+    if (rc) return rc;
+    for (size_t i = 0; i < nm; ++i) {
+        for (int ch = 0; ch < 3; ++ch) {
+            if (out->albedo) out->albedo[3 * i + ch] = g[8 * i + ch];
+            if (out->emission) out->emission[3 * i + ch] = g[8 * i + 4 + ch];
+        }
+        if (out->roughness) out->roughness[i] = g[8 * i + 3];
+    }
+    for (size_t l = 0; l < nl; ++l)
+        for (int ch = 0; ch < 3; ++ch)
+            if (out->light_le) out->light_le[3 * l + ch] = g[8 * nm + 4 * l + ch];
     return ANA_OK;
 }
 

@@ -321,6 +321,49 @@ __device__ __forceinline__ float3 scene_env(const DevScene& S, const DevSceneRec
     return R.has_dome ? env_eval(S.env, d) : R.env_radiance;
 }
 
+// Sums v over the lanes of the warp that share `key` and adds the sums to
+// grad[key + j] with one atomic per distinct key (FP32 reduction before the
+// atomics). Every lane of the warp must call it; kNoKey lanes add nothing.
+template <int N>
+__device__ __forceinline__ void warp_accum(float* grad, uint32_t key, const float (&v)[N]) {
+    const uint32_t lane = threadIdx.x & 31u;
+    bool ok = key != kNoKey;
+#pragma unroll
+    for (int j = 0; j < N; ++j) ok = ok && isfinite(v[j]);
+    if (!ok) key = kNoKey;
+    uint32_t pending = __ballot_sync(0xFFFFFFFFu, key != kNoKey);
+    while (pending) {
+        const int leader = __ffs(pending) - 1;
+        const uint32_t k0 = __shfl_sync(0xFFFFFFFFu, key, leader);
+        const bool mine = key == k0;
+        pending &= ~__ballot_sync(0xFFFFFFFFu, mine);
+#pragma unroll
+        for (int j = 0; j < N; ++j) {
+            float s = mine ? v[j] : 0.f;
+            s += __shfl_xor_sync(0xFFFFFFFFu, s, 16);
+            s += __shfl_xor_sync(0xFFFFFFFFu, s, 8);
+            s += __shfl_xor_sync(0xFFFFFFFFu, s, 4);
+            s += __shfl_xor_sync(0xFFFFFFFFu, s, 2);
+            s += __shfl_xor_sync(0xFFFFFFFFu, s, 1);
+            if (lane == uint32_t(leader) && s != 0.f) atomicAdd(grad + k0 + j, s);
+        }
+    }
+}
+
+__device__ __forceinline__ float3 load3(const float* a, size_t i) { return f3(a[3 * i], a[3 * i + 1], a[3 * i + 2]); }
+__device__ __forceinline__ float sum3(float3 v) { return v.x + v.y + v.z; }
+
+// shade: one path vertex (PathIntegrator::Li, lines 81-176): emission,
+// estimateDirect's light sample (shadow queue) and BSDF sample (MIS queue),
+// and the continuation with Russian roulette (extend queue).
+// kAdj (the adjoint replay) adds, with the sampling untouched:
+//  - the pending continuation gradient of the previous vertex, now that its
+//    remaining radiance L_rem = L - (radiance gathered so far) is known:
+//    delta * (d log f / d theta) * L_rem;
+//  - the emission gradient delta * beta of an emissive hit that counts;
+//  - the NEE and MIS gradient payloads (resolved after their rays) and the
+//    pending gradient of this vertex's continuation.
+template <bool kAdj>
 __global__ void __launch_bounds__(kMaxStageBlock) k_shade(const __grid_constant__ Params p) {
     const uint32_t b = p.bounce;
     const uint32_t cur = b & 1u, nxt = cur ^ 1u;
@@ -331,6 +374,10 @@ __global__ void __launch_bounds__(kMaxStageBlock) k_shade(const __grid_constant_
         const uint32_t i = base + threadIdx.x;
         bool pushSh = false, pushMis = false, pushExt = false;
         float4 shO, shD, shC, mO, mD, mC, eO, eD, eB;
+        // adjoint: payloads of the pushed entries and this vertex's direct sums
+        float4 shG0, shG1, mG0, mG1, eG0, eG1;
+        uint32_t keyPend = kNoKey, keyEmit = kNoKey;
+        float vPend[4] = {0.f, 0.f, 0.f, 0.f}, vEmit[3] = {0.f, 0.f, 0.f};
         if (i < n) {
             float4 qo = p.q.ext_o[cur][i], qd = p.q.ext_d[cur][i], qb = p.q.ext_b[cur][i];
             float4 h0 = p.q.hit0[i];
@@ -343,6 +390,25 @@ __global__ void __launch_bounds__(kMaxStageBlock) k_shade(const __grid_constant_
             float3 o = f3(qo), d = f3(qd), beta = f3(qb);
             uint32_t prim = __float_as_uint(h0.y);
             float3 Ladd = f3(0.f, 0.f, 0.f);
+            float3 delta = f3(0.f, 0.f, 0.f);
+            bool adj = false;
+            if constexpr (kAdj) {
+                const size_t li = size_t(pid - p.chunk_first_path);
+                delta = load3(p.a.dL, li);
+                adj = !is_black(delta);
+                const float4 g0 = p.a.ext_g0[cur][i];
+                const uint32_t pm = __float_as_uint(g0.w);
+                if (adj && pm != kNoKey) {
+                    const float4 g1 = p.a.ext_g1[cur][i];
+                    const float3 Lrem = load3(p.a.Lp, li) - load3(p.q.L, li);
+                    const float3 wa = delta * Lrem * f3(g0), wr = delta * Lrem * f3(g1);
+                    keyPend = 8u * pm;
+                    vPend[0] = wa.x;
+                    vPend[1] = wa.y;
+                    vPend[2] = wa.z;
+                    vPend[3] = sum3(wr);
+                }
+            }
             if (prim == kMiss) {
                 if (bounce == 0 || spec) Ladd = beta * scene_env(S, R, d);
             } else {
@@ -358,6 +424,15 @@ __global__ void __launch_bounds__(kMaxStageBlock) k_shade(const __grid_constant_
                     ShadeCtx c = make_ctx(si, d);
                     float3 Le = mat_le(m);
                     if (!is_black(Le) && (bounce == 0 || spec)) Ladd = Ladd + beta * Le;
+                    if constexpr (kAdj) {
+                        if (adj && m.type == ANA_MAT_EMISSIVE && (bounce == 0 || spec)) {
+                            const float3 ge = delta * beta;
+                            keyEmit = 8u * uint32_t(mi) + 4u;
+                            vEmit[0] = ge.x;
+                            vEmit[1] = ge.y;
+                            vEmit[2] = ge.z;
+                        }
+                    }
                     if (!m.is_delta && nL > 0) {
                         float ul = ss.next();
                         uint32_t lidx = min(uint32_t(ul * float(nL)), nL - 1u);
@@ -386,6 +461,18 @@ __global__ void __launch_bounds__(kMaxStageBlock) k_shade(const __grid_constant_
                                 shO = pack_u(org, pid);
                                 shD = pack(dir, dist * (1.f - 1e-4f));
                                 shC = pack_u(contrib, sc);
+                                if constexpr (kAdj) {
+                                    // contrib = beta * f * Li * s, s = cosI w nL / pdf
+                                    const float s = cosI * w / ls.pdf * float(nL);
+                                    const BsdfGrad g = mat_grad(m, c, wo, ls.wi);
+                                    const float3 db = delta * beta * s;
+                                    const float3 ga = db * g.dfda * ls.Li;
+                                    const bool area = adj && L.type == ANA_LIGHT_AREA;
+                                    const float3 gl = area ? db * be.f : f3(0.f, 0.f, 0.f);
+                                    const uint32_t lid = area ? R.light_base + lidx : 0xFFFFu;
+                                    shG0 = make_float4(ga.x, ga.y, ga.z, sum3(db * g.dfdr * ls.Li));
+                                    shG1 = pack_u(gl, (adj ? uint32_t(mi) : 0xFFFFu) | (lid << 16));
+                                }
                             }
                         }
                         // BSDF sampling toward the light (non-delta lights)
@@ -403,6 +490,14 @@ __global__ void __launch_bounds__(kMaxStageBlock) k_shade(const __grid_constant_
                                 mO = pack_u(org, pid);
                                 mD = pack(bs.wi, 0.f);
                                 mC = pack_u(contrib, sc);
+                                if constexpr (kAdj) {
+                                    // bs.f = f |cos wi|: K = beta * f * |cos wi| * cosI w nL / pdf
+                                    const BsdfGrad g = mat_grad(m, c, wo, bs.wi);
+                                    const float s = fabsf(c.to_local(bs.wi).z) * cosI * w / bs.pdf * float(nL);
+                                    const float3 db = delta * beta * s;
+                                    mG0 = pack_u(db * g.dfda, adj ? uint32_t(mi) : kNoKey);
+                                    mG1 = pack(db * g.dfdr, 0.f);
+                                }
                             }
                         }
                     }
@@ -426,11 +521,28 @@ __global__ void __launch_bounds__(kMaxStageBlock) k_shade(const __grid_constant_
                             eO = pack_u(org, pid);
                             eD = pack_u(bs.wi, nm);
                             eB = pack_u(beta, sc);
+                            if constexpr (kAdj) {
+                                // beta' = beta * f |cos| / pdf (pdf and roulette detached):
+                                // d log beta' / d theta = (d f / d theta) / f per channel
+                                const BsdfGrad g = mat_grad(m, c, wo, bs.wi);
+                                auto ratio = [](float num, float den) { return den > 0.f ? num / den : 0.f; };
+                                const float3 la = f3(ratio(g.dfda.x, g.f.x), ratio(g.dfda.y, g.f.y),
+                                                     ratio(g.dfda.z, g.f.z));
+                                const float3 lr = f3(ratio(g.dfdr.x, g.f.x), ratio(g.dfdr.y, g.f.y),
+                                                     ratio(g.dfdr.z, g.f.z));
+                                const bool any = adj && (!is_black(la) || !is_black(lr));
+                                eG0 = pack_u(la, any ? uint32_t(mi) : kNoKey);
+                                eG1 = pack(lr, 0.f);
+                            }
                         }
                     }
                 }
             }
             if (!is_black(Ladd)) add_L(p, pid, Ladd);
+        }
+        if constexpr (kAdj) {
+            warp_accum(p.a.grad, keyPend, vPend);
+            warp_accum(p.a.grad, keyEmit, vEmit);
         }
         uint32_t* cb = p.counters + b * kCountersPerBounce;
         uint32_t k = block_push(pushSh, cb + 1);
@@ -438,25 +550,37 @@ __global__ void __launch_bounds__(kMaxStageBlock) k_shade(const __grid_constant_
             p.q.sh_o[k] = shO;
             p.q.sh_d[k] = shD;
             p.q.sh_c[k] = shC;
+            if constexpr (kAdj) {
+                p.a.sh_g0[k] = shG0;
+                p.a.sh_g1[k] = shG1;
+            }
         }
         k = block_push(pushMis, cb + 2);
         if (pushMis) {
             p.q.mis_o[k] = mO;
             p.q.mis_d[k] = mD;
             p.q.mis_c[k] = mC;
+            if constexpr (kAdj) {
+                p.a.mis_g0[k] = mG0;
+                p.a.mis_g1[k] = mG1;
+            }
         }
         k = block_push(pushExt, cb + kCountersPerBounce + 0);
         if (pushExt) {
             p.q.ext_o[nxt][k] = eO;
             p.q.ext_d[nxt][k] = eD;
             p.q.ext_b[nxt][k] = eB;
+            if constexpr (kAdj) {
+                p.a.ext_g0[nxt][k] = eG0;
+                p.a.ext_g1[nxt][k] = eG1;
+            }
         }
     }
 }
 
 // NEE shadow rays: shadowTransmittance (src/integrator/ShadowRay.h:26-61) for
 // opaque scenes — any blocker in [1e-4, tmax] makes the transmittance black.
-template <bool kCurves, bool kPersist>
+template <bool kCurves, bool kPersist, bool kAdj>
 __global__ void ANA_TRAVERSAL_BOUNDS k_shadow(const __grid_constant__ Params p) {
     uint32_t* cb = p.counters + p.bounce * kCountersPerBounce;
     run_traversal<true, false, kPersist>(
@@ -470,7 +594,9 @@ __global__ void ANA_TRAVERSAL_BOUNDS k_shadow(const __grid_constant__ Params p) 
             float4 o = p.q.sh_o[i], d = p.q.sh_d[i], c = p.q.sh_c[i];
             Ray r{f3(o), f3(d), 1e-4f, d.w};
             uint32_t segRoot = kCurves ? p.S.scenes[scene_bits(c.w)].seg_root : kNoRoot;
-            if (!finish_any<kCurves>(p.S, segRoot, r, T, p.err)) add_L(p, __float_as_uint(o.w), f3(c));
+            const bool occluded = finish_any<kCurves>(p.S, segRoot, r, T, p.err);
+            if (!occluded) add_L(p, __float_as_uint(o.w), f3(c));
+            if constexpr (kAdj) p.a.sh_vis[i] = occluded ? 0u : 1u;
         });
 }
 
@@ -479,7 +605,7 @@ __global__ void ANA_TRAVERSAL_BOUNDS k_shadow(const __grid_constant__ Params p) 
 // batch without emissive surfaces every hit contributes zero, so the ray only
 // needs to know whether anything is hit (kAny): identical result, cheaper
 // query.
-template <bool kAny, bool kCurves, bool kPersist>
+template <bool kAny, bool kCurves, bool kPersist, bool kAdj>
 __global__ void ANA_TRAVERSAL_BOUNDS k_mis(const __grid_constant__ Params p) {
     uint32_t* cb = p.counters + p.bounce * kCountersPerBounce;
     const DevScene& S = p.S;
@@ -496,6 +622,7 @@ __global__ void ANA_TRAVERSAL_BOUNDS k_mis(const __grid_constant__ Params p) {
             const DevSceneRec& R = S.scenes[scene_bits(c.w)];
             uint32_t segRoot = kCurves ? R.seg_root : kNoRoot;
             float3 Li;
+            int mi = -1;
             if (kAny) {
                 Li = finish_any<kCurves>(S, segRoot, r, T, p.err) ? f3(0.f, 0.f, 0.f) : scene_env(S, R, r.d);
             } else {
@@ -509,12 +636,92 @@ __global__ void ANA_TRAVERSAL_BOUNDS k_mis(const __grid_constant__ Params p) {
                     else
                         slot = __float_as_uint(ldg4(S.tri_shade + 4 * size_t(__float_as_uint(
                                                                        ldg4(S.tri_isect + 3 * size_t(h.prim)).w))).w);
-                    int mi = slot_material(S, R, slot);
+                    mi = slot_material(S, R, slot);
                     Li = mi >= 0 ? mat_le(S.materials[mi]) : f3(0.f, 0.f, 0.f);
                 }
             }
             if (!is_black(Li)) add_L(p, __float_as_uint(o.w), f3(c) * Li);
+            if constexpr (kAdj) p.a.mis_res[i] = pack_u(Li, mi >= 0 ? uint32_t(mi) : kNoKey);
         });
+}
+
+// Adjoint replay set-up, after generate: dLoss/dL of every path of the chunk
+// (the film keeps finite samples only, each with weight 1/spp of its pixel),
+// and no pending continuation gradient on the camera vertices.
+__global__ void __launch_bounds__(256) k_adj_init(const __grid_constant__ Params p) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < p.chunk_paths; i += gridDim.x * blockDim.x) {
+        const uint32_t gid = p.chunk_first_path + i;
+        const DevSceneRec& R = p.S.scenes[scene_of(p.S, gid)];
+        const uint32_t pixel = (gid - R.path_offset) / R.spp;
+        const float3 L = load3(p.a.Lp, i);
+        float3 dl = f3(0.f, 0.f, 0.f);
+        if (is_finite3(L)) dl = load3(p.a.d_image, size_t(R.film_offset) + pixel) * (1.f / float(R.spp));
+        p.a.dL[3 * size_t(i)] = dl.x;
+        p.a.dL[3 * size_t(i) + 1] = dl.y;
+        p.a.dL[3 * size_t(i) + 2] = dl.z;
+        p.a.ext_g0[0][i] = make_float4(0.f, 0.f, 0.f, __uint_as_float(kNoKey));
+    }
+}
+
+// Resolves the gradient payloads of one bounce once the shadow and MIS rays
+// are traced. NEE (unoccluded only): material albedo / roughness terms and
+// the area light's Le term. MIS: the material terms times the Li found, and
+// delta * K for the emissive material hit.
+__global__ void __launch_bounds__(256) k_adj_direct(const __grid_constant__ Params p) {
+    const uint32_t* cb = p.counters + p.bounce * kCountersPerBounce;
+    const uint32_t nsh = cb[1], nmis = cb[2], n = max(nsh, nmis);
+    const uint32_t lightBase = 8u * p.a.num_materials;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += stride) {
+        const uint32_t i = base + threadIdx.x;
+        uint32_t kMat = kNoKey, kLe = kNoKey;
+        float vMat[4] = {0.f, 0.f, 0.f, 0.f}, vLe[3] = {0.f, 0.f, 0.f};
+        if (i < nsh && p.a.sh_vis[i]) {
+            const float4 g0 = p.a.sh_g0[i], g1 = p.a.sh_g1[i];
+            const uint32_t ids = __float_as_uint(g1.w), m = ids & 0xFFFFu, l = ids >> 16;
+            if (m != 0xFFFFu) {
+                kMat = 8u * m;
+                vMat[0] = g0.x;
+                vMat[1] = g0.y;
+                vMat[2] = g0.z;
+                vMat[3] = g0.w;
+            }
+            if (l != 0xFFFFu) {
+                kLe = lightBase + 4u * l;
+                vLe[0] = g1.x;
+                vLe[1] = g1.y;
+                vLe[2] = g1.z;
+            }
+        }
+        warp_accum(p.a.grad, kMat, vMat);
+        warp_accum(p.a.grad, kLe, vLe);
+        kMat = kNoKey;
+        kLe = kNoKey;
+        if (i < nmis) {
+            const float4 res = p.a.mis_res[i], g0 = p.a.mis_g0[i];
+            const float3 Li = f3(res);
+            const uint32_t m = __float_as_uint(g0.w), hit = __float_as_uint(res.w);
+            if (m != kNoKey && !is_black(Li)) {
+                const float4 g1 = p.a.mis_g1[i];
+                kMat = 8u * m;
+                vMat[0] = g0.x * Li.x;
+                vMat[1] = g0.y * Li.y;
+                vMat[2] = g0.z * Li.z;
+                vMat[3] = sum3(f3(g1) * Li);
+            }
+            if (m != kNoKey && hit != kNoKey && p.S.materials[hit].type == ANA_MAT_EMISSIVE) {
+                const uint32_t pid = __float_as_uint(p.q.mis_o[i].w);
+                const float3 delta = load3(p.a.dL, size_t(pid - p.chunk_first_path));
+                const float3 ge = delta * f3(p.q.mis_c[i]);
+                kLe = 8u * hit + 4u;
+                vLe[0] = ge.x;
+                vLe[1] = ge.y;
+                vLe[2] = ge.z;
+            }
+        }
+        warp_accum(p.a.grad, kMat, vMat);
+        warp_accum(p.a.grad, kLe, vLe);
+    }
 }
 
 // Film accumulation (PathIntegrator.cpp:43-57 + Film::mergeTile, Film.cpp:34-56):
@@ -647,8 +854,11 @@ static void prime(K kernel) {
 
 void prime_kernels() {
     prime(k_generate);
-    prime(k_shade);
+    prime(k_shade<false>);
+    prime(k_shade<true>);
     prime(k_film);
+    prime(k_adj_init);
+    prime(k_adj_direct);
     prime(k_extend<false, false, false>);
     prime(k_extend<false, false, true>);
     prime(k_extend<false, true, false>);
@@ -657,18 +867,26 @@ void prime_kernels() {
     prime(k_extend<true, false, true>);
     prime(k_extend<true, true, false>);
     prime(k_extend<true, true, true>);
-    prime(k_shadow<false, false>);
-    prime(k_shadow<false, true>);
-    prime(k_shadow<true, false>);
-    prime(k_shadow<true, true>);
-    prime(k_mis<false, false, false>);
-    prime(k_mis<false, false, true>);
-    prime(k_mis<false, true, false>);
-    prime(k_mis<false, true, true>);
-    prime(k_mis<true, false, false>);
-    prime(k_mis<true, false, true>);
-    prime(k_mis<true, true, false>);
-    prime(k_mis<true, true, true>);
+    prime(k_shadow<false, false, false>);
+    prime(k_shadow<false, true, false>);
+    prime(k_shadow<true, false, false>);
+    prime(k_shadow<true, true, false>);
+    prime(k_shadow<false, false, true>);
+    prime(k_shadow<false, true, true>);
+    prime(k_shadow<true, false, true>);
+    prime(k_shadow<true, true, true>);
+    prime(k_mis<false, false, false, false>);
+    prime(k_mis<false, false, true, false>);
+    prime(k_mis<false, true, false, false>);
+    prime(k_mis<false, true, true, false>);
+    prime(k_mis<true, false, false, false>);
+    prime(k_mis<true, false, true, false>);
+    prime(k_mis<true, true, false, false>);
+    prime(k_mis<true, true, true, false>);
+    prime(k_mis<false, false, false, true>);
+    prime(k_mis<false, false, true, true>);
+    prime(k_mis<false, true, false, true>);
+    prime(k_mis<false, true, true, true>);
     prime(k_trace_batch<false, false, false>);
     prime(k_trace_batch<false, false, true>);
     prime(k_trace_batch<false, true, false>);
@@ -699,32 +917,53 @@ void launch_extend(const Params& p, const LaunchCfg& c, cudaStream_t s, bool cou
     }
 }
 void launch_shade(const Params& p, const LaunchCfg& c, cudaStream_t s) {
-    k_shade<<<c.grid_cap, c.block, 0, s>>>(p);
+    k_shade<false><<<c.grid_cap, c.block, 0, s>>>(p);
 }
-template <bool kCurves, bool kPersist>
+template <bool kCurves, bool kPersist, bool kAdj>
 static void sh_launch(const Params& p, const LaunchCfg& c, cudaStream_t s) {
-    auto k = k_shadow<kCurves, kPersist>;
+    auto k = k_shadow<kCurves, kPersist, kAdj>;
     k<<<traversal_grid<kPersist>(k, c), kPersistBlock, 0, s>>>(p);
 }
-void launch_shadow(const Params& p, const LaunchCfg& c, cudaStream_t s) {
+template <bool kAdj>
+static void shadow_dispatch(const Params& p, const LaunchCfg& c, cudaStream_t s) {
     const bool cv = p.S.has_curves != 0, ps = c.persistent != 0;
-    if (cv) ps ? sh_launch<true, true>(p, c, s) : sh_launch<true, false>(p, c, s);
-    else ps ? sh_launch<false, true>(p, c, s) : sh_launch<false, false>(p, c, s);
+    if (cv) ps ? sh_launch<true, true, kAdj>(p, c, s) : sh_launch<true, false, kAdj>(p, c, s);
+    else ps ? sh_launch<false, true, kAdj>(p, c, s) : sh_launch<false, false, kAdj>(p, c, s);
 }
-template <bool kAny, bool kCurves, bool kPersist>
+void launch_shadow(const Params& p, const LaunchCfg& c, cudaStream_t s) { shadow_dispatch<false>(p, c, s); }
+template <bool kAny, bool kCurves, bool kPersist, bool kAdj>
 static void mis_launch(const Params& p, const LaunchCfg& c, cudaStream_t s) {
-    auto k = k_mis<kAny, kCurves, kPersist>;
+    auto k = k_mis<kAny, kCurves, kPersist, kAdj>;
     k<<<traversal_grid<kPersist>(k, c), kPersistBlock, 0, s>>>(p);
 }
 void launch_mis(const Params& p, const LaunchCfg& c, cudaStream_t s) {
     const bool cv = p.S.has_curves != 0, ps = c.persistent != 0, any = !p.S.has_emitters;
     if (any) {
-        if (cv) ps ? mis_launch<true, true, true>(p, c, s) : mis_launch<true, true, false>(p, c, s);
-        else ps ? mis_launch<true, false, true>(p, c, s) : mis_launch<true, false, false>(p, c, s);
+        if (cv) ps ? mis_launch<true, true, true, false>(p, c, s) : mis_launch<true, true, false, false>(p, c, s);
+        else ps ? mis_launch<true, false, true, false>(p, c, s) : mis_launch<true, false, false, false>(p, c, s);
     } else {
-        if (cv) ps ? mis_launch<false, true, true>(p, c, s) : mis_launch<false, true, false>(p, c, s);
-        else ps ? mis_launch<false, false, true>(p, c, s) : mis_launch<false, false, false>(p, c, s);
+        if (cv) ps ? mis_launch<false, true, true, false>(p, c, s) : mis_launch<false, true, false, false>(p, c, s);
+        else ps ? mis_launch<false, false, true, false>(p, c, s) : mis_launch<false, false, false, false>(p, c, s);
     }
+}
+
+// Adjoint replay. The MIS rays always look for the surface they hit (the
+// emission gradient needs the emissive material), which gives the same Li as
+// the any-hit form the forward pass may use.
+void launch_adj_init(const Params& p, const LaunchCfg& c, cudaStream_t s) {
+    k_adj_init<<<blocks_for(p.chunk_paths, 256, c.grid_cap), 256, 0, s>>>(p);
+}
+void launch_shade_adj(const Params& p, const LaunchCfg& c, cudaStream_t s) {
+    k_shade<true><<<c.grid_cap, c.block, 0, s>>>(p);
+}
+void launch_shadow_adj(const Params& p, const LaunchCfg& c, cudaStream_t s) { shadow_dispatch<true>(p, c, s); }
+void launch_mis_adj(const Params& p, const LaunchCfg& c, cudaStream_t s) {
+    const bool cv = p.S.has_curves != 0, ps = c.persistent != 0;
+    if (cv) ps ? mis_launch<false, true, true, true>(p, c, s) : mis_launch<false, true, false, true>(p, c, s);
+    else ps ? mis_launch<false, false, true, true>(p, c, s) : mis_launch<false, false, false, true>(p, c, s);
+}
+void launch_adj_direct(const Params& p, const LaunchCfg& c, cudaStream_t s) {
+    k_adj_direct<<<c.grid_cap, 256, 0, s>>>(p);
 }
 void launch_film(const Params& p, const LaunchCfg& c, cudaStream_t s) {
     k_film<<<blocks_for(p.chunk_pixels, 256, c.grid_cap), 256, 0, s>>>(p);

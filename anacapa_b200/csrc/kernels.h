@@ -46,9 +46,41 @@ struct ChunkSeg {
     uint32_t pad[3];
 };
 
+// Path-replay adjoint state (used only by the backward pass). Gradient
+// accumulators: 8 floats per material (albedo rgb, roughness, emission rgb,
+// -), then 4 per light (Le rgb, -). Material and light ids in the payloads
+// are global indices; kNoKey marks an absent one.
+//   ext_g0/1: pending continuation gradient of the vertex that spawned the
+//             extend entry: d log f / d albedo (xyz), material (w bits);
+//             d log f / d roughness (xyz)
+//   sh_g0/1:  NEE term: delta * d contribution / d albedo (xyz), / d roughness
+//             summed over channels (w); delta * d contribution / d Le (xyz),
+//             material (low 16 bits) | light (high 16 bits) (w bits)
+//   mis_g0/1: MIS term without Li: delta * dK / d albedo (xyz), material (w
+//             bits); delta * dK / d roughness (xyz)
+//   sh_vis:   1 when the shadow ray was unoccluded
+//   mis_res:  Li of the MIS ray (xyz), material hit (w bits, kNoKey: none)
+struct AdjQueues {
+    float4* ext_g0[2];
+    float4* ext_g1[2];
+    float4* sh_g0;
+    float4* sh_g1;
+    float4* mis_g0;
+    float4* mis_g1;
+    uint32_t* sh_vis;
+    float4* mis_res;
+    const float* Lp;       // primal radiance of every path of the chunk (3 floats)
+    float* dL;             // dLoss / dL of every path of the chunk (3 floats)
+    const float* d_image;  // dLoss / d pixel, film layout (3 floats per pixel)
+    float* grad;
+    uint32_t num_materials;
+};
+constexpr uint32_t kNoKey = 0xFFFFFFFFu;
+
 struct Params {
     DevScene S;
     Queues q;
+    AdjQueues a;
     ana_film_pixel* film;      // batch film (all scenes)
     uint32_t* counters;        // this chunk's counters
     uint32_t* err;             // device error word (bit 0: traversal stack overflow)
@@ -76,6 +108,16 @@ void launch_shade(const Params& p, const LaunchCfg& c, cudaStream_t s);
 void launch_shadow(const Params& p, const LaunchCfg& c, cudaStream_t s);
 void launch_mis(const Params& p, const LaunchCfg& c, cudaStream_t s);
 void launch_film(const Params& p, const LaunchCfg& c, cudaStream_t s);
+
+// Adjoint replay stages: the shade / shadow / MIS kernels of the forward pass
+// with the gradient bookkeeping compiled in (identical sampling decisions),
+// the per-path delta set-up, and the resolution of the NEE and MIS gradient
+// payloads once their rays are traced.
+void launch_adj_init(const Params& p, const LaunchCfg& c, cudaStream_t s);
+void launch_shade_adj(const Params& p, const LaunchCfg& c, cudaStream_t s);
+void launch_shadow_adj(const Params& p, const LaunchCfg& c, cudaStream_t s);
+void launch_mis_adj(const Params& p, const LaunchCfg& c, cudaStream_t s);
+void launch_adj_direct(const Params& p, const LaunchCfg& c, cudaStream_t s);
 void launch_trace_batch(const DevScene& S, uint32_t scene, const float* rays, size_t n, ana_hit* out, int occlusion,
                         uint32_t* fetch, uint32_t* err, int persistent, cudaStream_t s);
 

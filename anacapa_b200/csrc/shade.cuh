@@ -552,6 +552,91 @@ __device__ __forceinline__ BsdfEval mat_eval(const DevMaterial& m, const ShadeCt
 // returns emission_color * emission; Lambert and hair emit nothing.
 __device__ __forceinline__ float3 mat_le(const DevMaterial& m) { return m.emission; }
 
+// ---- parameter derivatives of the BSDF value (path-replay adjoint) -------------
+// The pieces of eval_ggx that depend on alpha2: the Schlick weight
+// x5 = (1 - dot(wo, h))^5, dg = D G2 / (4 cosO cosI), and d(dg)/d(alpha2) from
+//   dD/da2  = (den - 2 a2 cosH^2) / (pi den^3),  den = cosH^2 (a2 - 1) + 1
+//   dG1/da2 = -c (1 - c^2) / (s (c + s)^2),       s = sqrt(a2 + (1 - a2) c^2)
+// under the same validity tests as eval_ggx (false where it returns zero).
+__device__ __forceinline__ bool ggx_parts(float3 wol, float3 wil, float a2, float& x5, float& dg, float& ddg) {
+    if (wol.z <= 0.f || wil.z <= 0.f) return false;
+    float3 wh = safe_normalize(wol + wil);
+    if (wh.z <= 0.f) return false;
+    const float dotVH = fmaxf(0.f, dot(wol, wh));
+    const float cosO = fabsf(wol.z), cosI = fabsf(wil.z);
+    if (cosO < 1e-6f || cosI < 1e-6f) return false;
+    const float x = 1.f - dotVH;
+    x5 = x * x * x * x * x;
+    const float c2 = wh.z * wh.z;
+    const float den = c2 * (a2 - 1.f) + 1.f;
+    const float D = a2 / (kPi * den * den);
+    const float dD = (den - 2.f * a2 * c2) / (kPi * den * den * den);
+    auto g1 = [a2](float c, float& g, float& dgc) {
+        const float cc = c * c, s = sqrtf(a2 + (1.f - a2) * cc);
+        g = 2.f * c / (c + s);
+        dgc = -c * (1.f - cc) / (s * (c + s) * (c + s));
+    };
+    float gO, dgO, gI, dgI;
+    g1(cosO, gO, dgO);
+    g1(cosI, gI, dgI);
+    const float inv = 1.f / (4.f * cosO * cosI);
+    dg = D * gO * gI * inv;
+    ddg = (dD * gO * gI + D * (dgO * gI + gO * dgI)) * inv;
+    return true;
+}
+
+// f(wo, wi) as mat_eval returns it (no cosine), with its derivatives by the
+// material's albedo (per channel: f_c depends on albedo_c alone) and by its
+// GGX roughness r. Lambert / emissive: f = albedo / pi. standard_surface: the
+// lobe weights depend on neither parameter; the metal lobe's Schlick F0 =
+// albedo * base and the diffuse lobe are affine in albedo; r enters the metal
+// and dielectric-specular lobes through alpha2 = max(1e-4, r^2)^2, so
+// d alpha2 / dr = 4 r^3 above the clamp and 0 below it. Hair has no
+// differentiable parameter here: both derivatives are zero.
+struct BsdfGrad {
+    float3 f, dfda, dfdr;
+};
+__device__ __forceinline__ BsdfGrad mat_grad(const DevMaterial& m, const ShadeCtx& c, float3 wo, float3 wi) {
+    BsdfGrad g{f3(0.f, 0.f, 0.f), f3(0.f, 0.f, 0.f), f3(0.f, 0.f, 0.f)};
+    const float3 wol = c.to_local(wo), wil = c.to_local(wi);
+    if (m.type == ANA_MAT_HAIR) {
+        g.f = mat_eval(m, c, wo, wi).f;
+        return g;
+    }
+    if (!(wol.z * wil.z > 0.f)) return g;
+    if (m.type != ANA_MAT_STANDARD) {
+        g.f = m.albedo * kInvPi;
+        g.dfda = f3(kInvPi, kInvPi, kInvPi);
+        return g;
+    }
+    LobeWeights w;
+    if (!ss_weights(m, wol.z, w)) return g;
+    float pdf;
+    g.f = ss_combined(m, wol, wil, w, pdf);
+    const float r = m.rough;
+    const float dA2 = r * r > 1e-4f ? 4.f * r * r * r : 0.f;
+    float x5, dg, ddg;
+    if ((w.metal > 0.f || w.spec > 0.f) && ggx_parts(wol, wil, m.alpha2, x5, dg, ddg)) {
+        const float3 one = f3(1.f, 1.f, 1.f);
+        if (w.metal > 0.f) {
+            const float3 F0 = m.albedo * m.base;
+            const float3 F = F0 + (one - F0) * x5;
+            g.dfda = g.dfda + one * (w.metal * m.base * (1.f - x5) * dg);
+            g.dfdr = g.dfdr + F * (w.metal * ddg * dA2);
+        }
+        if (w.spec > 0.f) {
+            const float3 F0 = m.spec_color * (m.spec * m.f0_dielectric);
+            const float3 F = F0 + (one - F0) * x5;
+            g.dfdr = g.dfdr + F * (w.spec * ddg * dA2);
+        }
+    }
+    if (w.diff > 0.f) {
+        const float k = m.base * kInvPi * w.diff;
+        g.dfda = g.dfda + f3(k, k, k);
+    }
+    return g;
+}
+
 // ---- lights ------------------------------------------------------------------------
 struct LightSample {
     float3 Li, wi;

@@ -328,6 +328,37 @@ int ana_trace_batch(ana_ctx* ctx, const float* rays, size_t n, ana_hit* out, int
 #define ANA_TRACE_NOALLOC_MAX_RAYS 65536
 int ana_trace_batch_noalloc(ana_ctx* ctx, const float* rays, size_t n, ana_hit* out, int occlusion_only);
 
+/* ---- differentiable rendering: path-replay adjoint ------------------------
+ * A forward/backward pair with autograd-Function semantics over the uploaded
+ * scene (one scene, not a batch). Parameters, by uploaded material index i
+ * and light index l (NULL arrays are left unchanged / not written):
+ *   albedo[i][3]     Lambert and emissive albedo, standard_surface base_color
+ *   roughness[i]     standard_surface specular_roughness (others: unused, 0)
+ *   emission[i][3]   emissive material Le (others: unused, 0)
+ *   light_le[l][3]   area light Le (dome: unused, 0)
+ * ana_forward writes the parameters into the scene, renders the frame of
+ * `desc` (as ana_render with ANA_RENDER_CLEAR_FILM) and returns the resolved
+ * image (width x height x 3 floats, Film::getPixel) when image_out is not
+ * NULL. It keeps only the frame description: the sample indices and seed fix
+ * every path. ana_backward takes dLoss/d image (same layout) and returns
+ * dLoss/d parameters: it replays every path of that frame twice, once for its
+ * radiance L and once to propagate the adjoint (Vicini, Speierer, Jakob 2021:
+ * sampling decisions, pdfs, MIS weights and roulette are held fixed), and
+ * reduces the per-path gradients per warp in FP32 before atomic adds. Hair
+ * parameters and the dome are not differentiated. */
+typedef struct ana_diff_params {
+    float* albedo;
+    float* roughness;
+    float* emission;
+    float* light_le;
+} ana_diff_params;
+
+int ana_diff_counts(ana_ctx* ctx, uint32_t* num_materials, uint32_t* num_lights);
+/* Current parameter values (as uploaded, or as last set by ana_forward). */
+int ana_diff_get_params(ana_ctx* ctx, ana_diff_params* out);
+int ana_forward(ana_ctx* ctx, const ana_render_desc* desc, const ana_diff_params* params, float* image_out);
+int ana_backward(ana_ctx* ctx, const float* d_image, ana_diff_params* grad_out);
+
 int ana_get_stats(ana_ctx* ctx, ana_stats* out);
 
 /* Copy the last error message of this context (or of the last failed

@@ -1044,6 +1044,221 @@ V3<T> Li(const Scene<T>& S, Ray<T> r, Halton& smp, uint32_t maxDepth, uint32_t m
     return L;
 }
 
+// ---- FP64 reference adjoint (test infrastructure) ------------------------------
+// dL/d theta of one path estimate by forward-mode accumulation along the path:
+// d beta and d L are dense over the parameters (3 channels each), in double.
+// Parameters: 8 per material (albedo rgb, roughness, emission rgb, -), then 4
+// per light (Le rgb, -). Sampling decisions, pdfs, MIS weights and Russian
+// roulette are held at the path's values: the estimator that a path-replay
+// adjoint differentiates. The path itself is traced in T exactly as Li does;
+// the local BSDF derivatives come from central differences of the BSDF value
+// in double at the path's local directions (independent of any hand-written
+// derivative).
+template <class T> Mat<double> matD(const Mat<T>& m) {
+    Mat<double> o;
+    o.type = m.type;
+    o.albedo = V3<double>(m.albedo.x, m.albedo.y, m.albedo.z);
+    o.emission = V3<double>(m.emission.x, m.emission.y, m.emission.z);
+    o.base = m.base;
+    o.metal = m.metal;
+    o.rough = m.rough;
+    o.spec = m.spec;
+    o.coat = m.coat;
+    o.coatRough = m.coatRough;
+    o.ior = m.ior;
+    o.specColor = V3<double>(m.specColor.x, m.specColor.y, m.specColor.z);
+    o.coatAlpha2 = m.coatAlpha2;
+    o.f0 = m.f0;
+    o.coatF0 = m.coatF0;
+    o.flags = m.flags;
+    o.delta = m.delta;
+    return o;
+}
+// BSDF value in the local frame, double (Lambert, emissive, standard; hair: 0).
+inline V3<double> bsdfLocal(const Mat<double>& m, V3<double> wo, V3<double> wi) {
+    if (!(wo.z * wi.z > 0.0)) return {};
+    if (m.type == MAT_LAMBERT || m.type == MAT_EMISSIVE) return m.albedo * kInvPi<double>;
+    if (m.type != MAT_STANDARD) return {};
+    W4<double> w;
+    if (!ssWeights(m, wo.z, w)) return {};
+    double pdf;
+    return ssCombined(m, wo, wi, w, pdf);
+}
+// J[k] = d f / d theta_k for theta = (albedo r, g, b, roughness), f in double.
+inline void bsdfJacobian(const Mat<double>& m0, V3<double> wo, V3<double> wi, V3<double> J[4]) {
+    for (int k = 0; k < 4; ++k) {
+        Mat<double> a = m0, b = m0;
+        double h;
+        if (k < 3) {
+            h = 1e-4;
+            double* pa = k == 0 ? &a.albedo.x : k == 1 ? &a.albedo.y : &a.albedo.z;
+            double* pb = k == 0 ? &b.albedo.x : k == 1 ? &b.albedo.y : &b.albedo.z;
+            *pa += h;
+            *pb -= h;
+        } else {
+            h = 1e-5;
+            a.rough += h;
+            b.rough -= h;
+        }
+        J[k] = (bsdfLocal(a, wo, wi) - bsdfLocal(b, wo, wi)) * (0.5 / h);
+    }
+}
+
+struct PathGrad {
+    size_t P;
+    std::vector<double> dbeta, dL;  // [param][channel]
+    explicit PathGrad(size_t p) : P(p), dbeta(3 * p, 0.0), dL(3 * p, 0.0) {}
+    // dL += dbeta * s (per channel)
+    void addScaled(const double s[3]) {
+        for (size_t k = 0; k < P; ++k)
+            for (int c = 0; c < 3; ++c) dL[3 * k + c] += dbeta[3 * k + c] * s[c];
+    }
+};
+
+template <class T>
+V3<T> LiGrad(const Scene<T>& S, Ray<T> r, Halton& smp, uint32_t maxDepth, PathGrad& G, uint32_t minDepth = 2) {
+    V3<T> L, beta(1, 1, 1);
+    bool spec = false;
+    const uint32_t nL = uint32_t(S.lights.size());
+    const size_t lightBase = 8 * S.mats.size();
+    auto u1 = [&]() { return T(smp.get1D()); };
+    auto d3 = [](V3<T> v) { return V3<double>(double(v.x), double(v.y), double(v.z)); };
+    // beta-weighted local derivative term: dL[param k of material mi] += beta * J_k * s
+    auto addLocal = [&](uint32_t mi, const V3<double> J[4], const double s[3]) {
+        const double b[3] = {double(beta.x), double(beta.y), double(beta.z)};
+        for (int k = 0; k < 4; ++k)
+            for (int c = 0; c < 3; ++c) G.dL[3 * (8 * mi + k) + c] += b[c] * J[k][c] * s[c];
+    };
+    for (uint32_t bounce = 0; bounce <= maxDepth; ++bounce) {
+        Hit<T> h = trace(S, r);
+        if (!h.hit) {
+            if (bounce == 0 || spec) {
+                V3<T> bg = envLe(S, r.d);
+                const double s[3] = {double(bg.x), double(bg.y), double(bg.z)};
+                G.addScaled(s);
+                L = L + beta * bg;
+            }
+            break;
+        }
+        SI<T> si = surface(S, r, h);
+        const Mat<T>* m = matOf(S, si.slot);
+        if (!m) break;
+        const uint32_t mi = uint32_t(m - S.mats.data());
+        const Mat<double> mD = matD(*m);
+        V3<T> wo = -r.d;
+        Ctx<T> c(si, r.d);
+        const V3<double> wol = d3(c.toLocal(wo));
+        if (!m->emission.black() && (bounce == 0 || spec)) {
+            const double s[3] = {double(m->emission.x), double(m->emission.y), double(m->emission.z)};
+            G.addScaled(s);
+            L = L + beta * m->emission;
+        }
+        if (m->type == MAT_EMISSIVE && (bounce == 0 || spec))
+            for (int ch = 0; ch < 3; ++ch) G.dL[3 * (8 * mi + 4 + ch) + ch] += double(beta[ch]);
+        if (!m->delta && nL > 0) {
+            uint32_t li = std::min(uint32_t(smp.get1D() * float(nL)), nL - 1);
+            const Light<T>& lt = S.lights[li];
+            V3<T> Ld;
+            {
+                T a = u1(), b = u1();
+                LS<T> ls = lt.type == 0 ? areaSample(lt, si.p, a, b) : envSample(S, a, b);
+                if (ls.pdf > T(0) && !ls.Li.black()) {
+                    BE<T> be = matEval(*m, c, wo, ls.wi);
+                    if (!be.f.black()) {
+                        Ray<T> sr = spawnRayTo(si.p, si.n, si.p + ls.wi * ls.dist);
+                        if (!trace(S, sr, true).hit) {
+                            T w = powerH(ls.pdf, be.pdf);
+                            T cosI = si.curve ? std::sqrt(std::max(T(0), T(1) - dot(ls.wi, c.t) * dot(ls.wi, c.t)))
+                                              : std::abs(dot(ls.wi, si.n));
+                            Ld = Ld + be.f * ls.Li * cosI * w / ls.pdf;
+                            const double k = double(cosI) * double(w) / double(ls.pdf) * double(nL);
+                            const double sf[3] = {double(be.f.x * ls.Li.x) * k, double(be.f.y * ls.Li.y) * k,
+                                                  double(be.f.z * ls.Li.z) * k};
+                            G.addScaled(sf);
+                            V3<double> J[4];
+                            bsdfJacobian(mD, wol, d3(c.toLocal(ls.wi)), J);
+                            const double sl[3] = {double(ls.Li.x) * k, double(ls.Li.y) * k, double(ls.Li.z) * k};
+                            addLocal(mi, J, sl);
+                            if (lt.type == 0)
+                                for (int ch = 0; ch < 3; ++ch)
+                                    G.dL[3 * (lightBase + 4 * li + ch) + ch] += double(beta[ch]) * double(be.f[ch]) * k;
+                        }
+                    }
+                }
+            }
+            {
+                T uc = u1();
+                T a = u1(), b = u1();
+                BS<T> bs = matSample(*m, c, wo, a, b, uc);
+                if (bs.valid()) {
+                    T lp = lt.type == 0 ? areaPdf(lt, si.p, bs.wi) : envPdf(S, bs.wi);
+                    if (lp > T(0)) {
+                        T w = bs.delta() ? T(1) : powerH(bs.pdf, lp);
+                        Ray<T> mr = spawnRay(si.p, si.ng, bs.wi);
+                        mr.tmax = T(1e10f);
+                        Hit<T> mh = trace(S, mr);
+                        V3<T> Lm;
+                        int hm = -1;
+                        if (!mh.hit) Lm = envLe(S, bs.wi);
+                        else {
+                            SI<T> ms = surface(S, mr, mh);
+                            const Mat<T>* hmat = matOf(S, ms.slot);
+                            if (hmat) {
+                                Lm = hmat->emission;
+                                hm = int(hmat - S.mats.data());
+                            }
+                        }
+                        const T cosN = std::abs(dot(bs.wi, si.n));
+                        if (!Lm.black()) Ld = Ld + bs.f * Lm * cosN * w / bs.pdf;
+                        const double k = double(cosN) * double(w) / double(bs.pdf) * double(nL);
+                        if (!Lm.black()) {
+                            const double sf[3] = {double(bs.f.x * Lm.x) * k, double(bs.f.y * Lm.y) * k,
+                                                  double(bs.f.z * Lm.z) * k};
+                            G.addScaled(sf);
+                            const V3<double> wil = d3(c.toLocal(bs.wi));
+                            V3<double> J[4];
+                            bsdfJacobian(mD, wol, wil, J);
+                            const double cl = std::abs(wil.z);
+                            const double sl[3] = {double(Lm.x) * k * cl, double(Lm.y) * k * cl, double(Lm.z) * k * cl};
+                            addLocal(mi, J, sl);
+                        }
+                        if (hm >= 0 && S.mats[size_t(hm)].type == MAT_EMISSIVE)
+                            for (int ch = 0; ch < 3; ++ch)
+                                G.dL[3 * (8 * size_t(hm) + 4 + ch) + ch] += double(beta[ch]) * double(bs.f[ch]) * k;
+                    }
+                }
+            }
+            L = L + beta * Ld * T(float(nL));
+        }
+        T uc = u1();
+        T a = u1(), b = u1();
+        BS<T> bs = matSample(*m, c, wo, a, b, uc);
+        if (!bs.valid()) break;
+        spec = bs.delta();
+        // d beta' = d beta * (f/pdf) + beta * (d f / d theta) |cos| / pdf, then the roulette factor
+        const V3<double> wil = d3(c.toLocal(bs.wi));
+        V3<double> J[4];
+        bsdfJacobian(mD, wol, wil, J);
+        const double cl = std::abs(wil.z);
+        const double wr[3] = {double(bs.f.x / bs.pdf), double(bs.f.y / bs.pdf), double(bs.f.z / bs.pdf)};
+        const double bOld[3] = {double(beta.x), double(beta.y), double(beta.z)};
+        for (size_t k = 0; k < G.P; ++k)
+            for (int ch = 0; ch < 3; ++ch) G.dbeta[3 * k + ch] *= wr[ch];
+        for (int k = 0; k < 4; ++k)
+            for (int ch = 0; ch < 3; ++ch) G.dbeta[3 * (8 * mi + k) + ch] += bOld[ch] * J[k][ch] * cl / double(bs.pdf);
+        beta = beta * (bs.f / bs.pdf);
+        r = spawnRay(si.p, si.n, bs.wi);
+        if (bounce >= minDepth) {
+            T q = T(1) - std::min(beta.maxc(), T(0.95f));
+            if (T(smp.get1D()) < q) break;
+            const T rr = T(1) / (T(1) - q);
+            beta = beta * rr;
+            for (double& v : G.dbeta) v *= double(rr);
+        }
+    }
+    return L;
+}
+
 // Camera::generateRay (IIntegrator.h:90-109), pinhole.
 template <class T> Ray<T> cameraRay(const Scene<T>& S, uint32_t px, uint32_t py, T jx, T jy) {
     T s = (T(px) + jx) / T(S.W);
@@ -1065,6 +1280,33 @@ V3<T> sampleLi(const Scene<T>& S, uint32_t px, uint32_t py, uint32_t sIdx, uint3
     h.get1D();
     h.get1D();
     return Li(S, cameraRay(S, px, py, jx, jy), h, maxDepth);
+}
+
+// Per-row sums of the path gradients of a frame, weighted by dLoss/dL =
+// dLoss/d pixel / spp for finite samples (the film drops the others).
+template <class T>
+void adjointRows(const Scene<T>& S, uint32_t W, uint32_t H, uint32_t spp, uint32_t s0, uint32_t maxDepth,
+                 uint64_t seed, const float* dimage, int threads, size_t P, std::vector<std::vector<double>>& rows) {
+    parallel_for(H, threads, [&](uint32_t py) {
+        std::vector<double>& acc = rows[py];
+        for (uint32_t px = 0; px < W; ++px) {
+            const float* dI = dimage + 3 * (size_t(py) * W + px);
+            for (uint32_t s = 0; s < spp; ++s) {
+                Halton hs;
+                hs.seed = seed;
+                hs.start(px, py, s0 + s);
+                T jx = T(hs.get1D()), jy = T(hs.get1D());
+                hs.get1D();
+                hs.get1D();
+                hs.get1D();
+                PathGrad G(P);
+                V3<T> L = LiGrad(S, cameraRay(S, px, py, jx, jy), hs, maxDepth, G);
+                if (!L.finite()) continue;
+                for (size_t k = 0; k < P; ++k)
+                    for (int c = 0; c < 3; ++c) acc[k] += double(dI[c]) / double(spp) * G.dL[3 * k + c];
+            }
+        }
+    });
 }
 
 }  // namespace po
@@ -1435,5 +1677,29 @@ void po_pcg(uint64_t seed, uint32_t n, uint32_t* out) {
 }
 
 float po_ggx_D(float c, float a2) { return D_GGX<float>(c, a2); }
+
+// Number of gradient entries of po_adjoint: 8 per material, 4 per light.
+uint64_t po_num_params(void* p) {
+    Handle* h = static_cast<Handle*>(p);
+    return h->precision == 64 ? 8 * h->d.mats.size() + 4 * h->d.lights.size()
+                              : 8 * h->f.mats.size() + 4 * h->f.lights.size();
+}
+
+// dLoss/d theta of a W x H x spp frame (samples s0 ..) given dLoss/d image
+// (3 per pixel; the image is the film's mean over finite samples), in double.
+// grad: po_num_params entries.
+void po_adjoint(void* p, uint32_t W, uint32_t H, uint32_t spp, uint32_t s0, uint32_t maxDepth, uint64_t seed,
+                const float* dimage, int threads, double* grad) {
+    Handle* h = static_cast<Handle*>(p);
+    const size_t P = po_num_params(p);
+    std::vector<std::vector<double>> rows(H, std::vector<double>(P, 0.0));
+    if (h->precision == 64) adjointRows(h->d, W, H, spp, s0, maxDepth, seed, dimage, threads, P, rows);
+    else adjointRows(h->f, W, H, spp, s0, maxDepth, seed, dimage, threads, P, rows);
+    for (size_t k = 0; k < P; ++k) {
+        double s = 0.0;
+        for (uint32_t y = 0; y < H; ++y) s += rows[y][k];
+        grad[k] = s;
+    }
+}
 
 }  // extern "C"

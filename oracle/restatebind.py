@@ -53,6 +53,10 @@ def lib():
         L.po_pcg.argtypes = [C.c_uint64, C.c_uint32, _U32]
         L.po_ggx_D.argtypes = [C.c_float, C.c_float]
         L.po_ggx_D.restype = C.c_float
+        L.po_num_params.argtypes = [_P]
+        L.po_num_params.restype = C.c_uint64
+        L.po_adjoint.argtypes = [_P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64,
+                                 _F, C.c_int, _D]
         _lib = L
     return _lib
 
@@ -125,6 +129,18 @@ class PoScene:
                          s.max_depth if max_depth is None else max_depth, threads, x0, y0, x1, y1, seed,
                          rgbw.ctypes.data_as(_D), lsq.ctypes.data_as(_D))
         return rgbw, lsq
+
+    def adjoint(self, d_image, spp=None, sample_start=0, max_depth=None, seed=0, threads=0):
+        """Reference dLoss/d theta (float64) of the frame for dLoss/d image
+        (H, W, 3): forward-mode along every path, parameters laid out 8 per
+        material (albedo rgb, roughness, emission rgb, -), 4 per light."""
+        s = self.scene
+        g = np.ascontiguousarray(np.asarray(d_image, np.float32).reshape(s.height, s.width, 3))
+        out = np.zeros(int(self.L.po_num_params(self.h)), np.float64)
+        self.L.po_adjoint(self.h, s.width, s.height, s.spp if spp is None else spp, sample_start,
+                          s.max_depth if max_depth is None else max_depth, seed, _fp(g), threads,
+                          out.ctypes.data_as(_D))
+        return out
 
     def li(self, q, max_depth=None, seed=0, threads=0):
         q = np.ascontiguousarray(np.asarray(q, np.uint32).reshape(-1, 3))

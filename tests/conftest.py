@@ -29,6 +29,14 @@ def lib_built():
 
 
 @pytest.fixture(scope="session")
+def restate_built():
+    """This repository's CPU restatement of the path (oracle/restate), built here."""
+    from oracle import restatebind as P
+    P.build()
+    return P
+
+
+@pytest.fixture(scope="session")
 def ref_built():
     """The reference hot path compiled from its own sources (oracle/_ref)."""
     from oracle import refbind as R
