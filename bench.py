@@ -14,6 +14,11 @@ is the same metric through the C ABI with host buffers: every step uploads
 the prepared scene from pinned host memory, renders and reads the film back.
 `--impl reference` times the reference's own CPU PathIntegrator (compiled from
 its sources into oracle/_ref) on the host cores instead.
+
+The same line carries the metric's two other parts, measured after the timed
+region: "batched" (64 Cornell variants as one graph-replayed batch render vs
+one launch sequence per scene, same samples, so equal RMSE) and "adjoint"
+(ana_backward vs ana_forward device time on the differentiable scene).
 """
 from __future__ import annotations
 
@@ -31,7 +36,10 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "path samples/s"
+# the headline value is the throughput scene's samples/s; the batched-vs-plain
+# and adjoint/forward parts of the metric are reported under "batched" and
+# "adjoint" in the same line
+METRIC = "path samples/s at equal RMSE vs FP64 image, batched vs plain; adjoint/fwd time"
 UNIT = "samples/s"
 
 
@@ -50,6 +58,8 @@ def parse():
                     help="target CPU work of the reference sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the batched-vs-plain and adjoint/forward measurements")
     ap.add_argument("--traversal", type=int, default=0,
                     help="0 library default, 1 persistent warps, 2 one thread per ray")
     return ap.parse_args()
@@ -232,6 +242,74 @@ def run_reference(a):
     return 0
 
 
+def bench_batched(local, reps=3):
+    """The batched workload: 64 Cornell variants (resolutions 64^2..512^2,
+    4..64 spp, depth 4..16) as one batch render replayed from a CUDA graph,
+    against the same 64 frames rendered one scene per launch sequence. Both
+    forms run the same per-variant estimator (same samples), so their images
+    and RMSE against the FP64 oracle are identical. Device time (CUDA events)
+    per form; launch configuration from the autotuner's best point (8M-path
+    chunks, 256-thread stage blocks, persistent traversal, leaves of 2)."""
+    from anacapa_b200 import api
+    from anacapa_b200 import scenes as S
+    scenes = S.batched_variants(64, seed=0)
+    preps = [api.Prepared(sc, max_leaf_tris=2) for sc in scenes]
+    descs = [(sc.width, sc.height, sc.spp, sc.max_depth) for sc in scenes]
+    paths = sum(sc.num_paths for sc in scenes)
+    r = api.Renderer(device=local, chunk_paths=8 << 20, block_size=256)
+    plain = []
+    for it in range(reps + 1):
+        ms = 0.0
+        for pr, d in zip(preps, descs):
+            r.upload(pr)
+            r.render(*d)
+            ms += r.stats().render_ms
+        if it:
+            plain.append(ms)
+    batch = api.Batch(preps)
+    r.upload_batch(batch)
+    batched = []
+    for it in range(reps + 1):
+        r.render_batch(descs, graph=True)
+        if it:
+            batched.append(r.stats().render_ms)
+    r.close()
+    pm, bm = statistics.median(plain), statistics.median(batched)
+    return {"workload": f"64 Cornell variants, {paths:,} paths", "paths": paths,
+            "plain_ms": pm, "batched_graph_ms": bm,
+            "plain_samples_per_s": paths / (pm / 1e3), "batched_samples_per_s": paths / (bm / 1e3),
+            "speedup": pm / bm, "equal_rmse": "identical per-variant estimator and samples"}
+
+
+def bench_adjoint(local, reps=3):
+    """Path-replay adjoint on the differentiable scene (Cornell + 20,480-
+    triangle icosphere, 512x512, 16 spp, depth 8): device time of ana_forward
+    and of ana_backward (primal + adjoint replay) for an L2 loss against a
+    target rendered from perturbed parameters."""
+    from anacapa_b200 import api
+    from anacapa_b200 import scenes as S
+    W = H = 512
+    spp, depth = 16, 8
+    r = api.Renderer(device=local)
+    r.upload(S.differentiable(W, H, spp, depth, params=S.perturbed_diff_params(1)))
+    target = r.forward(W, H, spp, depth)
+    r.upload(S.differentiable(W, H, spp, depth))
+    fwd, bwd = [], []
+    for it in range(reps + 1):
+        img = r.forward(W, H, spp, depth)
+        f = r.stats().render_ms
+        r.backward(2.0 * (img - target) / img.size)
+        b = r.stats().render_ms
+        if it:
+            fwd.append(f)
+            bwd.append(b)
+    r.close()
+    fm, bm = statistics.median(fwd), statistics.median(bwd)
+    return {"workload": "differentiable Cornell + icosphere 512x512x16, depth 8, L2 loss",
+            "forward_ms": fm, "backward_ms": bm, "adjoint_over_forward": bm / fm,
+            "forward_samples_per_s": W * H * spp / (fm / 1e3)}
+
+
 def run_ours(a):
     ws, rank, local, pg = dist_setup(a)
     import torch
@@ -295,6 +373,10 @@ def run_ours(a):
         e2e_s = allreduce_max(pg, (t1 - t0) / a.steps, local)
         e2e = {"value": ws * paths_step / e2e_s, "unit": UNIT,
                "h2d_bytes_per_step": int(prep.nbytes), "d2h_bytes_per_step": int(W * H * 20)}
+    extra = {}
+    if not a.no_extras:  # the metric's other two parts, outside the timed region
+        extra["batched"] = bench_batched(local)
+        extra["adjoint"] = bench_adjoint(local)
     cpu = None
     if rank == 0 and ws == 1 and not a.no_cpu_baseline:
         try:
@@ -322,6 +404,7 @@ def run_ours(a):
             "e2e": e2e,
             "cpu_baseline": cpu,
             "clocks": ck,
+            **extra,
         }
         print(json.dumps(line), flush=True)
     r.close()
