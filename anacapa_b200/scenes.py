@@ -335,8 +335,14 @@ def throughput(width=1920, height=1080, spp=64, max_depth=12, n_spheres=4096,
                                 metalness=float(metal[i]), coat=0.0))
         b.mesh(centers[i] + radii[i] * uv_, f_, m, nrm=uv_)
     mg = b.material(Material(MAT_STANDARD, base_color=(0.45, 0.45, 0.45), roughness=0.7))
-    g, y = 60.0, -10.6
-    b.quad([-g, y, -g], [-g, y, g], [g, y, g], [g, y, -g], [0, 1, 0], mg)
+    # The ground rises 0.1 over its 120-unit depth. An exactly level quad at
+    # |y| = 10.6 has a zero-thickness box once the reference's 1e-7 padding
+    # (BVHBackend.cpp, sahSplit) is rounded away, so its slab test never
+    # passes and the plane would be invisible to the reference and to us.
+    g, y0, y1 = 60.0, -10.6, -10.5
+    gn = np.array([0.0, 2.0 * g, -(y1 - y0)])
+    gn /= np.linalg.norm(gn)
+    b.quad([-g, y0, -g], [-g, y1, g], [g, y1, g], [g, y0, -g], gn, mg)
     dome = sky_dome(*dome_size)
     return b.scene("throughput", area_lights=[], dome_rgb=dome, dome_intensity=1.0,
                    cam_from=(0.0, 6.0, -32.0), cam_at=(0.0, -1.0, 0.0), cam_up=(0.0, 1.0, 0.0),
