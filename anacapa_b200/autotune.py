@@ -21,14 +21,14 @@ from . import scenes as S
 
 @dataclasses.dataclass(frozen=True)
 class Config:
-    chunk_paths: int = 1 << 22
+    chunk_paths: int = 1 << 25
     block_size: int = 256
     traversal: int = api.ANA_TRAVERSAL_PERSISTENT
     max_leaf_tris: int = 4
 
 
 SPACE = {
-    "chunk_paths": [1 << 20, 1 << 21, 1 << 22, 1 << 23],
+    "chunk_paths": [1 << 21, 1 << 22, 1 << 23, 1 << 24, 1 << 25, 1 << 26],
     "block_size": [128, 256, 512],
     "traversal": [api.ANA_TRAVERSAL_PERSISTENT, api.ANA_TRAVERSAL_PER_RAY],
     "max_leaf_tris": [2, 4, 8],

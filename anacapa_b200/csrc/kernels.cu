@@ -270,10 +270,11 @@ __global__ void ANA_TRAVERSAL_BOUNDS k_extend(const __grid_constant__ Params p) 
 
 // Surface interaction of a hit (BVHBackend::fillSurfaceInteraction,
 // BVHBackend.cpp:285-317; CurveBrute intersectOneSegment, CurveBrute.cpp:209-233).
+template <bool kCurves = true>
 __device__ __forceinline__ SurfInt surf_int(const DevScene& S, float3 o, float3 d, float t, uint32_t prim, float u,
                                             float v, float4 h1) {
     SurfInt si;
-    if (!(prim & 0x80000000u)) {
+    if (!kCurves || !(prim & 0x80000000u)) {
         const float4* tp = S.tri_isect + 3 * size_t(prim);
         float4 a = ldg4(tp), e1 = ldg4(tp + 1), e2 = ldg4(tp + 2);
         uint32_t orig = __float_as_uint(a.w);
@@ -363,7 +364,7 @@ __device__ __forceinline__ float sum3(float3 v) { return v.x + v.y + v.z; }
 //  - the emission gradient delta * beta of an emissive hit that counts;
 //  - the NEE and MIS gradient payloads (resolved after their rays) and the
 //    pending gradient of this vertex's continuation.
-template <bool kAdj>
+template <bool kAdj, bool kFiber>
 __global__ void __launch_bounds__(kMaxStageBlock) k_shade(const __grid_constant__ Params p) {
     const uint32_t b = p.bounce;
     const uint32_t cur = b & 1u, nxt = cur ^ 1u;
@@ -413,7 +414,7 @@ __global__ void __launch_bounds__(kMaxStageBlock) k_shade(const __grid_constant_
                 if (bounce == 0 || spec) Ladd = beta * scene_env(S, R, d);
             } else {
                 float4 h1 = (prim & 0x80000000u) ? p.q.hit1[i] : make_float4(0, 0, 0, 0);
-                SurfInt si = surf_int(S, o, d, h0.x, prim, h0.z, h0.w, h1);
+                SurfInt si = surf_int<kFiber>(S, o, d, h0.x, prim, h0.z, h0.w, h1);
                 int mi = slot_material(S, R, si.slot);
                 if (mi >= 0) {
                     const DevMaterial m = S.materials[mi];
@@ -441,7 +442,7 @@ __global__ void __launch_bounds__(kMaxStageBlock) k_shade(const __grid_constant_
                         float lu0 = ss.next(), lu1 = ss.next();
                         LightSample ls = light_sample(S, L, si.p, lu0, lu1);
                         if (ls.pdf > 0.f && !is_black(ls.Li)) {
-                            BsdfEval be = mat_eval(m, c, wo, ls.wi);
+                            BsdfEval be = mat_eval<kFiber>(m, c, wo, ls.wi);
                             if (!is_black(be.f)) {
                                 float3 target = si.p + ls.wi * ls.dist;
                                 float3 dir = target - si.p;
@@ -464,7 +465,7 @@ __global__ void __launch_bounds__(kMaxStageBlock) k_shade(const __grid_constant_
                                 if constexpr (kAdj) {
                                     // contrib = beta * f * Li * s, s = cosI w nL / pdf
                                     const float s = cosI * w / ls.pdf * float(nL);
-                                    const BsdfGrad g = mat_grad(m, c, wo, ls.wi);
+                                    const BsdfGrad g = mat_grad<kFiber>(m, c, wo, ls.wi);
                                     const float3 db = delta * beta * s;
                                     const float3 ga = db * g.dfda * ls.Li;
                                     const bool area = adj && L.type == ANA_LIGHT_AREA;
@@ -478,7 +479,7 @@ __global__ void __launch_bounds__(kMaxStageBlock) k_shade(const __grid_constant_
                         // BSDF sampling toward the light (non-delta lights)
                         float uc = ss.next();
                         float bu0 = ss.next(), bu1 = ss.next();
-                        BsdfSample bs = mat_sample(m, c, wo, bu0, bu1, uc);
+                        BsdfSample bs = mat_sample<kFiber>(m, c, wo, bu0, bu1, uc);
                         if (bs.valid()) {
                             float lp = light_pdf(S, L, si.p, bs.wi);
                             if (lp > 0.f) {
@@ -492,7 +493,7 @@ __global__ void __launch_bounds__(kMaxStageBlock) k_shade(const __grid_constant_
                                 mC = pack_u(contrib, sc);
                                 if constexpr (kAdj) {
                                     // bs.f = f |cos wi|: K = beta * f * |cos wi| * cosI w nL / pdf
-                                    const BsdfGrad g = mat_grad(m, c, wo, bs.wi);
+                                    const BsdfGrad g = mat_grad<kFiber>(m, c, wo, bs.wi);
                                     const float s = fabsf(c.to_local(bs.wi).z) * cosI * w / bs.pdf * float(nL);
                                     const float3 db = delta * beta * s;
                                     mG0 = pack_u(db * g.dfda, adj ? uint32_t(mi) : kNoKey);
@@ -504,7 +505,7 @@ __global__ void __launch_bounds__(kMaxStageBlock) k_shade(const __grid_constant_
                     // continuation
                     float uc = ss.next();
                     float u0 = ss.next(), u1 = ss.next();
-                    BsdfSample bs = mat_sample(m, c, wo, u0, u1, uc);
+                    BsdfSample bs = mat_sample<kFiber>(m, c, wo, u0, u1, uc);
                     if (bs.valid()) {
                         spec = bs.delta();
                         beta = beta * (bs.f / bs.pdf);
@@ -524,7 +525,7 @@ __global__ void __launch_bounds__(kMaxStageBlock) k_shade(const __grid_constant_
                             if constexpr (kAdj) {
                                 // beta' = beta * f |cos| / pdf (pdf and roulette detached):
                                 // d log beta' / d theta = (d f / d theta) / f per channel
-                                const BsdfGrad g = mat_grad(m, c, wo, bs.wi);
+                                const BsdfGrad g = mat_grad<kFiber>(m, c, wo, bs.wi);
                                 auto ratio = [](float num, float den) { return den > 0.f ? num / den : 0.f; };
                                 const float3 la = f3(ratio(g.dfda.x, g.f.x), ratio(g.dfda.y, g.f.y),
                                                      ratio(g.dfda.z, g.f.z));
@@ -854,8 +855,10 @@ static void prime(K kernel) {
 
 void prime_kernels() {
     prime(k_generate);
-    prime(k_shade<false>);
-    prime(k_shade<true>);
+    prime(k_shade<false, false>);
+    prime(k_shade<false, true>);
+    prime(k_shade<true, false>);
+    prime(k_shade<true, true>);
     prime(k_film);
     prime(k_adj_init);
     prime(k_adj_direct);
@@ -917,7 +920,8 @@ void launch_extend(const Params& p, const LaunchCfg& c, cudaStream_t s, bool cou
     }
 }
 void launch_shade(const Params& p, const LaunchCfg& c, cudaStream_t s) {
-    k_shade<false><<<c.grid_cap, c.block, 0, s>>>(p);
+    if (p.S.has_fibers) k_shade<false, true><<<c.grid_cap, c.block, 0, s>>>(p);
+    else k_shade<false, false><<<c.grid_cap, c.block, 0, s>>>(p);
 }
 template <bool kCurves, bool kPersist, bool kAdj>
 static void sh_launch(const Params& p, const LaunchCfg& c, cudaStream_t s) {
@@ -954,7 +958,8 @@ void launch_adj_init(const Params& p, const LaunchCfg& c, cudaStream_t s) {
     k_adj_init<<<blocks_for(p.chunk_paths, 256, c.grid_cap), 256, 0, s>>>(p);
 }
 void launch_shade_adj(const Params& p, const LaunchCfg& c, cudaStream_t s) {
-    k_shade<true><<<c.grid_cap, c.block, 0, s>>>(p);
+    if (p.S.has_fibers) k_shade<true, true><<<c.grid_cap, c.block, 0, s>>>(p);
+    else k_shade<true, false><<<c.grid_cap, c.block, 0, s>>>(p);
 }
 void launch_shadow_adj(const Params& p, const LaunchCfg& c, cudaStream_t s) { shadow_dispatch<true>(p, c, s); }
 void launch_mis_adj(const Params& p, const LaunchCfg& c, cudaStream_t s) {

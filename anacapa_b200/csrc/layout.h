@@ -124,7 +124,7 @@ struct DevScene {
     uint32_t num_scenes;
     uint32_t has_curves;    // any scene has curve segments
     uint32_t has_emitters;  // any material reachable from a slot emits (Le != 0)
-    uint32_t pad;
+    uint32_t has_fibers;    // curve segments or hair materials: shading needs the fiber code
     DevEnv env;             // the (single) dome of the batch
 };
 
