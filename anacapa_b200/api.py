@@ -95,7 +95,8 @@ class AnaStats(C.Structure):
                 ("shade_ms", C.c_float), ("shadow_ms", C.c_float), ("mis_ms", C.c_float),
                 ("film_ms", C.c_float), ("bounces", C.c_uint32), ("chunks", C.c_uint32),
                 ("kernel_launches", C.c_uint64), ("extend_launches", C.c_uint64),
-                ("node_fetches", C.c_uint64), ("tri_tests", C.c_uint64), ("seg_tests", C.c_uint64)]
+                ("node_fetches", C.c_uint64), ("tri_tests", C.c_uint64), ("seg_tests", C.c_uint64),
+                ("curve_node_fetches", C.c_uint64)]
 
 
 class AnaDiffParams(C.Structure):

@@ -101,7 +101,7 @@ int build_blob(const ana::Prepared* const* list, uint32_t n, Blob& B, std::strin
         off = align_up(off + bytes);
         return o;
     };
-    B.o_tri_nodes = take(nNodes * sizeof(ana::BvhNode));
+    B.o_tri_nodes = take(nNodes * sizeof(ana::Bvh4Node));
     B.o_tri_isect = take(nTris * 48);
     B.o_tri_shade = take(nTris * 64);
     B.o_seg_nodes = take(nSegNodes * sizeof(ana::BvhNode));
@@ -133,7 +133,7 @@ int build_blob(const ana::Prepared* const* list, uint32_t n, Blob& B, std::strin
     }
     B.mem = static_cast<unsigned char*>(mem);
     std::memset(B.mem, 0, B.size);
-    auto* nodes = reinterpret_cast<ana::BvhNode*>(B.mem + B.o_tri_nodes);
+    auto* nodes = reinterpret_cast<ana::Bvh4Node*>(B.mem + B.o_tri_nodes);
     auto* isect = reinterpret_cast<float4*>(B.mem + B.o_tri_isect);
     auto* shade = reinterpret_cast<float4*>(B.mem + B.o_tri_shade);
     auto* snodes = reinterpret_cast<ana::BvhNode*>(B.mem + B.o_seg_nodes);
@@ -142,7 +142,17 @@ int build_blob(const ana::Prepared* const* list, uint32_t n, Blob& B, std::strin
     auto* mats = reinterpret_cast<ana::DevMaterial*>(B.mem + B.o_mats);
     auto* slots = reinterpret_cast<int32_t*>(B.mem + B.o_slots);
     auto* lights = reinterpret_cast<ana::DevLight*>(B.mem + B.o_lights);
-    // child refs: interior nodes shift by the scene's node base, leaves by its primitive base
+    // 4-wide triangle nodes: interior refs shift by the scene's node base, the
+    // first-triangle field of leaf entries (bits 0..24) by its primitive base
+    auto fix_node4 = [](ana::Bvh4Node nd, uint32_t nodeBase, uint32_t primBase) {
+        uint32_t* ref = &nd.ref.x;
+        for (int k = 0; k < 4; ++k) {
+            if (ref[k] == ana::kEmptyChild) continue;
+            ref[k] += (ref[k] & 0x80000000u) ? primBase : nodeBase;
+        }
+        return nd;
+    };
+    // binary curve nodes: likewise, with refs and leaf counts in n3
     auto fix_node = [](ana::BvhNode nd, uint32_t nodeBase, uint32_t primBase) {
         float* n3 = &nd.n3.x;
         for (int ch = 0; ch < 2; ++ch) {
@@ -161,7 +171,7 @@ int build_blob(const ana::Prepared* const* list, uint32_t n, Blob& B, std::strin
         const uint32_t nodeBase = uint32_t(iN), triBase = uint32_t(iT), sNodeBase = uint32_t(iSN),
                        segBase = uint32_t(iS), strBase = uint32_t(iStr), matBase = uint32_t(iM);
         st.tri_root = (P.num_tris && !P.tri_nodes.empty()) ? nodeBase : ana::kNoRoot;
-        for (const ana::BvhNode& nd : P.tri_nodes) nodes[iN++] = fix_node(nd, nodeBase, triBase);
+        for (const ana::Bvh4Node& nd : P.tri_nodes) nodes[iN++] = fix_node4(nd, nodeBase, triBase);
         for (uint32_t t = 0; t < P.num_tris; ++t) {
             float4 a = P.tri_isect[3 * size_t(t)];
             a.w = fbits(ubits(a.w) + triBase);  // index into the batch's shading array
@@ -375,7 +385,7 @@ int upload_blob(ana_ctx* c, const Blob& B) {
     unsigned char* b = c->d_scene;
     ana::DevScene& S = c->ds;
     S = ana::DevScene{};
-    S.tri_nodes = reinterpret_cast<const ana::BvhNode*>(b + B.o_tri_nodes);
+    S.tri_nodes = reinterpret_cast<const ana::Bvh4Node*>(b + B.o_tri_nodes);
     S.tri_isect = reinterpret_cast<const float4*>(b + B.o_tri_isect);
     S.tri_shade = reinterpret_cast<const float4*>(b + B.o_tri_shade);
     S.seg_nodes = reinterpret_cast<const ana::BvhNode*>(b + B.o_seg_nodes);
@@ -694,7 +704,7 @@ int render_items(ana_ctx* c, const ana_render_desc* descs, uint32_t n, uint32_t 
         if (clear) cudaMemsetAsync(c->film, 0, totalPixels * sizeof(ana_film_pixel), c->stream);
         cudaMemsetAsync(c->d_counters, 0, ncount * 4, c->stream);
         cudaMemsetAsync(c->d_err, 0, 4, c->stream);
-        if (count_work) cudaMemsetAsync(c->d_work, 0, 3 * sizeof(unsigned long long), c->stream);
+        if (count_work) cudaMemsetAsync(c->d_work, 0, 4 * sizeof(unsigned long long), c->stream);
         for (uint32_t k = 0; k < nchunks; ++k) {
             const ChunkPlan& cp = chunks[k];
             p.chunk_first_path = cp.first_path;
@@ -759,7 +769,7 @@ int render_items(ana_ctx* c, const ana_render_desc* descs, uint32_t n, uint32_t 
     }
     CK(cudaGetLastError(), "kernel launch");
     CK(cudaEventRecord(c->ev1, c->stream), "event");
-    unsigned long long hwork[3] = {0, 0, 0};
+    unsigned long long hwork[4] = {0, 0, 0, 0};
     if (count_work)
         CK(cudaMemcpyAsync(hwork, c->d_work, sizeof(hwork), cudaMemcpyDeviceToHost, c->stream), "work D2H");
     c->h_counters.resize(ncountAll);
@@ -791,6 +801,7 @@ int render_items(ana_ctx* c, const ana_render_desc* descs, uint32_t n, uint32_t 
     st.node_fetches = hwork[0];
     st.tri_tests = hwork[1];
     st.seg_tests = hwork[2];
+    st.curve_node_fetches = hwork[3];
     if (timing) {
         float acc[5] = {0, 0, 0, 0, 0};
         for (size_t i = 0; i < ev_i; ++i) {

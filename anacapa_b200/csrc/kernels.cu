@@ -198,16 +198,18 @@ __device__ __forceinline__ bool finish_any(const DevScene& S, uint32_t segRoot, 
 }
 
 __device__ __forceinline__ void warp_add_work(unsigned long long* work, const Counters& cnt) {
-    unsigned long long a = cnt.nodes, b = cnt.prims, c = cnt.segs;
+    unsigned long long a = cnt.nodes, b = cnt.prims, c = cnt.segs, e = cnt.cnodes;
     for (int off = 16; off > 0; off >>= 1) {
         a += __shfl_down_sync(0xFFFFFFFFu, a, off);
         b += __shfl_down_sync(0xFFFFFFFFu, b, off);
         c += __shfl_down_sync(0xFFFFFFFFu, c, off);
+        e += __shfl_down_sync(0xFFFFFFFFu, e, off);
     }
     if ((threadIdx.x & 31u) == 0) {
         atomicAdd(work + 0, a);
         atomicAdd(work + 1, b);
         atomicAdd(work + 2, c);
+        atomicAdd(work + 3, e);
     }
 }
 
@@ -221,8 +223,8 @@ __device__ __forceinline__ void run_traversal(const DevScene& S, uint32_t n, uin
     if constexpr (kPersist) {
         persistent_traverse<kAny, kCount>(S, n, fetch, err, cnt, load, done);
     } else {
-        uint32_t stack[kMaxStack];
-        float stackT[kMaxStack];
+        uint32_t stack[kMaxStack4];
+        float stackT[kMaxStack4];
         for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
             Ray ray;
             uint32_t root;
@@ -249,7 +251,7 @@ template <bool kCount, bool kCurves, bool kPersist>
 __global__ void ANA_TRAVERSAL_BOUNDS k_extend(const __grid_constant__ Params p) {
     const uint32_t cur = p.bounce & 1u;
     uint32_t* cb = p.counters + p.bounce * kCountersPerBounce;
-    Counters cnt{0, 0, 0};
+    Counters cnt{0, 0, 0, 0};
     run_traversal<false, kCount, kPersist>(
         p.S, cb[0], cb + 3, p.err, &cnt,
         [&](uint32_t i, Ray& r, uint32_t& root) {

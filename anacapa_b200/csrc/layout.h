@@ -30,7 +30,24 @@ struct BvhNode {
 };
 static_assert(sizeof(BvhNode) == 64, "BvhNode must be 64 bytes");
 
-constexpr uint32_t kMaxStack = 64;   // traversal stack depth (reference: 64)
+constexpr uint32_t kMaxStack = 64;   // curve traversal stack depth (reference: 64)
+
+// 4-wide triangle BVH node (128 bytes, one L2 line): the four children's
+// boxes as structure of arrays (child k in component k) and their references
+// (an interior node index, a leaf entry: bit 31 | (count-1) << 25 | first
+// triangle, or kEmptyChild). The nodes are the reference's binary SAH tree
+// collapsed: every child box is a box of that tree, bit for bit.
+struct Bvh4Node {
+    float4 lox, hix, loy, hiy, loz, hiz;
+    uint4 ref;
+    uint4 pad;
+};
+static_assert(sizeof(Bvh4Node) == 128, "Bvh4Node must be 128 bytes");
+constexpr uint32_t kEmptyChild = 0xFFFFFFFFu;
+// Triangle traversal stack: a 4-wide step pushes up to three entries, so the
+// build bounds the worst root-to-leaf sum of pushes by this (prepare_scene
+// rejects a deeper tree).
+constexpr uint32_t kMaxStack4 = 128;
 
 // Material, flattened with the derived constants each reference class
 // precomputes in its constructor.
@@ -110,7 +127,7 @@ struct DevSceneRec {
 };
 
 struct DevScene {
-    const BvhNode* tri_nodes;
+    const Bvh4Node* tri_nodes;
     const float4* tri_isect;
     const float4* tri_shade;
     const BvhNode* seg_nodes;

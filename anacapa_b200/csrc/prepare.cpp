@@ -70,8 +70,9 @@ struct Box {
 };
 
 // ---------------------------------------------------------------------------
-// Binary BVH build tree (both builders produce this, then flatten_bvh2 lays
-// it out as 64-byte nodes).
+// Binary BVH build tree (both builders produce this; flatten_bvh4 lays the
+// triangle tree out as 128-byte 4-wide nodes, flatten_bvh2 the curve tree as
+// 64-byte binary nodes).
 // ---------------------------------------------------------------------------
 struct BuildNode {
     Box box;
@@ -319,6 +320,97 @@ void flatten_bvh2(const NodePool& pool, uint32_t root, std::vector<BvhNode>& out
     }
 }
 
+// ---------------------------------------------------------------------------
+// Collapse a binary build tree into 4-wide nodes. A node's children start as
+// its binary node's two children; the interior child of largest surface area
+// is replaced by its own two children until there are four or only leaves
+// remain. Every child box is therefore a box of the binary tree, bit for bit,
+// and a box contains its descendants' boxes, so a ray that passes a child's
+// slab test passes every skipped ancestor's: the triangles tested are those
+// the binary traversal would test. Nodes are laid out depth-first; returns the
+// worst root-to-leaf sum of (children - 1), the traversal stack bound.
+// ---------------------------------------------------------------------------
+template <class EmitLeaf>
+uint32_t flatten_bvh4(const NodePool& pool, uint32_t root, std::vector<Bvh4Node>& out, bool& rootEmpty,
+                      EmitLeaf emit_leaf) {
+    out.clear();
+    auto set_child = [](Bvh4Node& n, int k, const Box& b, uint32_t ref) {
+        (&n.lox.x)[k] = b.lo[0];
+        (&n.hix.x)[k] = b.hi[0];
+        (&n.loy.x)[k] = b.lo[1];
+        (&n.hiy.x)[k] = b.hi[1];
+        (&n.loz.x)[k] = b.lo[2];
+        (&n.hiz.x)[k] = b.hi[2];
+        (&n.ref.x)[k] = ref;
+    };
+    auto empty_node = [&]() {
+        Bvh4Node n;
+        std::memset(&n, 0, sizeof(n));
+        Box e;
+        for (int k = 0; k < 4; ++k) set_child(n, k, e, kEmptyChild);
+        return n;
+    };
+    auto area = [](const Box& b) {
+        float dx = b.hi[0] - b.lo[0], dy = b.hi[1] - b.lo[1], dz = b.hi[2] - b.lo[2];
+        return dx * dy + dy * dz + dz * dx;
+    };
+    const BuildNode& R = pool.nodes[root];
+    if (R.count > 0 || R.left < 0) {
+        rootEmpty = R.count == 0;
+        Bvh4Node n = empty_node();
+        if (R.count) set_child(n, 0, R.box, 0x80000000u | ((R.count - 1u) << 25) | emit_leaf(R.start, R.count));
+        out.push_back(n);
+        return 0;
+    }
+    rootEmpty = false;
+    struct Item {
+        uint32_t bn;
+        int32_t parent;
+        int slot;
+        uint32_t depth;  // pushes on the way from the root to this node
+    };
+    std::vector<Item> stack;
+    stack.push_back({root, -1, 0, 0});
+    uint32_t bound = 0;
+    while (!stack.empty()) {
+        const Item it = stack.back();
+        stack.pop_back();
+        const BuildNode& b = pool.nodes[it.bn];
+        if (b.count > 0) {
+            const uint32_t off = emit_leaf(b.start, b.count);
+            set_child(out[size_t(it.parent)], it.slot, b.box, 0x80000000u | ((b.count - 1u) << 25) | off);
+            bound = std::max(bound, it.depth);
+            continue;
+        }
+        const uint32_t idx = uint32_t(out.size());
+        out.push_back(empty_node());
+        if (it.parent >= 0) set_child(out[size_t(it.parent)], it.slot, b.box, idx);
+        uint32_t kids[4] = {uint32_t(b.left), uint32_t(b.right), 0, 0};
+        int nk = 2;
+        while (nk < 4) {
+            int pick = -1;
+            float best = -1.f;
+            for (int k = 0; k < nk; ++k) {
+                const BuildNode& c = pool.nodes[kids[k]];
+                if (c.count == 0 && c.left >= 0 && area(c.box) > best) {
+                    best = area(c.box);
+                    pick = k;
+                }
+            }
+            if (pick < 0) break;
+            const BuildNode& c = pool.nodes[kids[pick]];
+            for (int k = nk; k > pick + 1; --k) kids[k] = kids[k - 1];  // keep left-to-right order
+            kids[pick] = uint32_t(c.left);
+            kids[pick + 1] = uint32_t(c.right);
+            ++nk;
+        }
+        const uint32_t d = it.depth + uint32_t(nk - 1);
+        // push in reverse so the leftmost child is placed (and its leaves emitted) first
+        for (int k = nk - 1; k >= 0; --k) stack.push_back({kids[k], int32_t(idx), k, d});
+    }
+    return bound;
+}
+
 // StrandDesc::widthAt (include/anacapa/accel/CurvePool.h:45-54)
 float width_at(const float* w, uint32_t n, float v) {
     if (n == 0) return 0.001f;
@@ -349,7 +441,7 @@ bool finite3(const float* p) { return std::isfinite(p[0]) && std::isfinite(p[1])
 }  // namespace
 
 uint64_t Prepared::bytes() const {
-    return tri_nodes.size() * sizeof(BvhNode) + tri_isect.size() * 16 + tri_shade.size() * 16 +
+    return tri_nodes.size() * sizeof(Bvh4Node) + tri_isect.size() * 16 + tri_shade.size() * 16 +
            seg_nodes.size() * sizeof(BvhNode) + segs.size() * 16 + strand_color.size() * 4 +
            materials.size() * sizeof(DevMaterial) + slot_material.size() * 4 +
            lights.size() * sizeof(DevLight) +
@@ -482,12 +574,13 @@ int prepare_scene(const ana_scene_desc& d, Prepared& P, std::string& err) {
         NodePool pool(2 * size_t(T) + 1);
         uint32_t root = sah_build(pi, 0, T, maxLeafT, pool, 0);
         P.tri_isect.reserve(size_t(T) * 3);
-        flatten_bvh2(pool, root, P.tri_nodes, P.tri_root_is_empty, [&](uint32_t s, uint32_t c) {
+        const uint32_t stackBound = flatten_bvh4(pool, root, P.tri_nodes, P.tri_root_is_empty, [&](uint32_t s, uint32_t c) {
             uint32_t off = uint32_t(P.tri_isect.size() / 3);
             for (uint32_t i = s; i < s + c; ++i)
                 for (int k = 0; k < 3; ++k) P.tri_isect.push_back(isect[3 * size_t(pi[i].idx) + k]);
             return off;
         });
+        if (stackBound > kMaxStack4) return unsupported("triangle BVH deeper than the traversal stack");
     } else {
         P.tri_nodes.clear();
         P.tri_root_is_empty = true;

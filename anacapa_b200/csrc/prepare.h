@@ -21,7 +21,7 @@ struct HostEnv {
 };
 
 struct Prepared {
-    std::vector<BvhNode> tri_nodes;
+    std::vector<Bvh4Node> tri_nodes;
     std::vector<float4> tri_isect;   // 3 per triangle, leaf order
     std::vector<float4> tri_shade;   // 4 per triangle, mesh order
     bool tri_root_is_empty = true;

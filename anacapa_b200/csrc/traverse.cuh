@@ -88,7 +88,7 @@ struct TriHit {
 };
 
 struct Counters {
-    uint32_t nodes, prims, segs;
+    uint32_t nodes, prims, segs, cnodes;  // triangle nodes, triangles, segments, curve nodes
 };
 
 // ---------------------------------------------------------------------------
@@ -139,35 +139,68 @@ __device__ __forceinline__ bool trav_pop(Traversal& T, const uint32_t* stack, co
     return false;
 }
 
-// Interior step: one node fetch and two child-box tests.
+// Interior step: one 128-byte node fetch and four child-box tests. The
+// children entered are ordered by entry distance with a 4-key sorting
+// network; the nearest becomes the current node, the others are pushed
+// farthest first (popped nearest first, and skipped once a closer hit is
+// known).
+__device__ __forceinline__ void cswap(float& ka, uint32_t& va, float& kb, uint32_t& vb) {
+    if (kb < ka) {
+        const float k = ka;
+        ka = kb;
+        kb = k;
+        const uint32_t v = va;
+        va = vb;
+        vb = v;
+    }
+}
+
 template <bool kAny, bool kCount>
 __device__ __forceinline__ void trav_interior(Traversal& T, const DevScene& S, uint32_t* stack, float* stackT,
                                               uint32_t* err, Counters* cnt) {
     const float4* np = reinterpret_cast<const float4*>(S.tri_nodes + T.cur);
-    float4 n0 = ldg4(np), n1 = ldg4(np + 1), n2 = ldg4(np + 2), n3 = ldg4(np + 3);
+    const float4 lx = ldg4(np), hx = ldg4(np + 1), ly = ldg4(np + 2), hy = ldg4(np + 3), lz = ldg4(np + 4),
+                 hz = ldg4(np + 5), rf = ldg4(np + 6);
     if (kCount) cnt->nodes++;
-    float tn0, tn1;
     const float cull = kAny ? T.r.tmax : T.closest;
-    bool h0 = box_hit(T.r, n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, cull, tn0);
-    bool h1 = box_hit(T.r, n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, cull, tn1);
-    uint32_t c0 = fbits_u(n3.z) ? leaf_entry(fbits_u(n3.x), fbits_u(n3.z)) : fbits_u(n3.x);
-    uint32_t c1 = fbits_u(n3.w) ? leaf_entry(fbits_u(n3.y), fbits_u(n3.w)) : fbits_u(n3.y);
-    if (h0 && h1) {
-        bool swap = !(tn0 < tn1);
-        if (T.sp >= int(kMaxStack)) {
-            atomicOr(err, 1u);
-            T.exhausted = true;
-            return;
+    float key[4];
+    uint32_t ref[4] = {fbits_u(rf.x), fbits_u(rf.y), fbits_u(rf.z), fbits_u(rf.w)};
+    {
+        const float l0[4] = {lx.x, lx.y, lx.z, lx.w}, h0[4] = {hx.x, hx.y, hx.z, hx.w};
+        const float l1[4] = {ly.x, ly.y, ly.z, ly.w}, h1[4] = {hy.x, hy.y, hy.z, hy.w};
+        const float l2[4] = {lz.x, lz.y, lz.z, lz.w}, h2[4] = {hz.x, hz.y, hz.z, hz.w};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            float tn;
+            const bool h = ref[k] != kEmptyChild && box_hit(T.r, l0[k], h0[k], l1[k], h1[k], l2[k], h2[k], cull, tn);
+            key[k] = h ? tn : INFINITY;
         }
-        stack[T.sp] = swap ? c0 : c1;
-        stackT[T.sp] = swap ? tn0 : tn1;
-        ++T.sp;
-        T.cur = swap ? c1 : c0;
-    } else if (h0 || h1) {
-        T.cur = h0 ? c0 : c1;
-    } else if (!trav_pop(T, stack, stackT)) {
-        T.exhausted = true;
     }
+    const int n = int(key[0] < INFINITY) + int(key[1] < INFINITY) + int(key[2] < INFINITY) + int(key[3] < INFINITY);
+    if (n == 0) {
+        if (!trav_pop(T, stack, stackT)) T.exhausted = true;
+        return;
+    }
+    // misses carry key +inf, so the n children entered come first
+    cswap(key[0], ref[0], key[1], ref[1]);
+    cswap(key[2], ref[2], key[3], ref[3]);
+    cswap(key[0], ref[0], key[2], ref[2]);
+    cswap(key[1], ref[1], key[3], ref[3]);
+    cswap(key[1], ref[1], key[2], ref[2]);
+    if (T.sp + n - 1 > int(kMaxStack4)) {
+        atomicOr(err, 1u);
+        T.exhausted = true;
+        return;
+    }
+#pragma unroll
+    for (int k = 3; k >= 1; --k) {
+        if (k < n) {
+            stack[T.sp] = ref[k];
+            stackT[T.sp] = key[k];
+            ++T.sp;
+        }
+    }
+    T.cur = ref[0];
 }
 
 // Leaf step: test the leaf's triangles, then pop.
@@ -202,8 +235,8 @@ __device__ __forceinline__ void persistent_traverse(const DevScene& S, uint32_t 
                                                     Counters* cnt, Load load, Done done) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t ltmask = (1u << lane) - 1u;
-    uint32_t stack[kMaxStack];
-    float stackT[kMaxStack];
+    uint32_t stack[kMaxStack4];
+    float stackT[kMaxStack4];
     Traversal T;
     bool active = false, drained = false;
     uint32_t idx = 0;
@@ -406,7 +439,7 @@ __device__ __forceinline__ CurveHit trace_curves(const DevScene& S, uint32_t roo
         if (!(cur & 0x80000000u)) {
             const float4* np = reinterpret_cast<const float4*>(S.seg_nodes + cur);
             float4 n0 = ldg4(np), n1 = ldg4(np + 1), n2 = ldg4(np + 2), n3 = ldg4(np + 3);
-            if (kCount) cnt->nodes++;
+            if (kCount) cnt->cnodes++;
             float tn0 = 0.f, tn1 = 0.f;
             bool h0 = curve_box_hit(ray, inv, n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, ch.t, tn0);
             bool h1 = curve_box_hit(ray, inv, n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, ch.t, tn1);

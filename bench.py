@@ -353,7 +353,7 @@ def run_ours(a):
     launches = int(sum(s.kernel_launches for s in stats))
     # roofline of the dominant kernel (closest-hit traversal)
     ext_launches = stats[0].extend_launches
-    alg_bytes = (64 * work.node_fetches + 48 * work.tri_tests + 80 * work.seg_tests
+    alg_bytes = (128 * work.node_fetches + 64 * work.curve_node_fetches + 48 * work.tri_tests + 80 * work.seg_tests
                  + (32 + 16) * work.extend_rays)
     peak, peak_kind = measured_peaks()
     achieved = (alg_bytes / ext_launches) / ((ext_ms / ext_launches) / 1e3) / 1e9 if ext_ms > 0 else None
@@ -393,6 +393,7 @@ def run_ours(a):
             "data": "synthetic (seeded numpy scene generator)",
             "config": workload_config(a, scene),
             "rays_per_s": ws * rays / (ms_step / 1e3),
+            "extend_rays_per_step": int(stats[0].extend_rays),
             "stage_ms": {"extend": ext_ms, "shade": shade_ms, "shadow": shadow_ms, "mis": mis_ms},
             "roofline": {"bound": "hbm", "kernel": "k_extend (closest-hit BVH traversal)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -221,9 +221,11 @@ typedef struct ana_stats {
     uint32_t chunks;            /* path chunks of the last render               */
     uint64_t kernel_launches;   /* kernels this library launched in the render  */
     uint64_t extend_launches;   /* of which closest-hit (extend) launches       */
-    uint64_t node_fetches;      /* ANA_RENDER_COUNT_WORK: 64-byte BVH node loads */
+    uint64_t node_fetches;      /* ANA_RENDER_COUNT_WORK: 128-byte triangle BVH
+                                   node loads (4-wide nodes)                     */
     uint64_t tri_tests;         /*   triangle tests (48 bytes each)              */
     uint64_t seg_tests;         /*   curve segment tests (80 bytes each)         */
+    uint64_t curve_node_fetches;/*   64-byte curve BVH node loads                */
 } ana_stats;
 
 typedef struct ana_ctx ana_ctx;
