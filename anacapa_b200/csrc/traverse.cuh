@@ -96,10 +96,17 @@ struct Counters {
 // warp loops over
 //   1. refill: lanes without a ray take the next queue entries (one
 //      warp-aggregated atomicAdd on the stage's fetch counter);
-//   2. interior phase: every lane descends interior nodes until it reaches a
-//      leaf or runs out of nodes; the phase ends when no lane needs another
-//      interior step, so lanes stay converged on the node-test code;
-//   3. leaf phase: one leaf's triangles per lane.
+//   2. interior phase: lanes descend interior nodes until they reach a
+//      leaf; the phase ends when every lane has a leaf to test (or nothing
+//      left), or when no lane can take another interior step, so lanes stay
+//      converged on the node-test code. Any-hit queries are speculative
+//      (Aila and Laine, "Understanding the efficiency of ray traversal on
+//      GPUs", 2009): a lane that reaches a leaf parks it and keeps descending
+//      from its next stack entry. Closest-hit queries do not speculate: a
+//      leaf tested early shortens the ray and culls later nodes (measured on
+//      the throughput frame: speculation cost closest hit 3 %, saved any hit
+//      8-12 %);
+//   3. leaf phase: the parked leaf's (else the current leaf's) triangles.
 // A lane whose stack is exhausted (or, for occlusion, that found a blocker)
 // reports its ray and picks up a new one at the next refill, so finished rays
 // do not idle the warp until its slowest ray completes. Box and triangle
@@ -203,11 +210,11 @@ __device__ __forceinline__ void trav_interior(Traversal& T, const DevScene& S, u
     T.cur = ref[0];
 }
 
-// Leaf step: test the leaf's triangles, then pop.
+// Tests the triangles of leaf entry `leaf`; true when an any-hit query found
+// its blocker.
 template <bool kAny, bool kCount>
-__device__ __forceinline__ void trav_leaf(Traversal& T, const DevScene& S, const uint32_t* stack,
-                                          const float* stackT, Counters* cnt) {
-    uint32_t off = T.cur & 0x01FFFFFFu, c = ((T.cur >> 25) & 63u) + 1u;
+__device__ __forceinline__ bool leaf_test(Traversal& T, const DevScene& S, uint32_t leaf, Counters* cnt) {
+    const uint32_t off = leaf & 0x01FFFFFFu, c = ((leaf >> 25) & 63u) + 1u;
     for (uint32_t i = off; i < off + c; ++i) {
         const float4* tp = S.tri_isect + 3 * size_t(i);
         float4 a = ldg4(tp), b = ldg4(tp + 1), e = ldg4(tp + 2);
@@ -218,11 +225,19 @@ __device__ __forceinline__ void trav_leaf(Traversal& T, const DevScene& S, const
             T.u = u;
             T.v = v;
             T.tri = int32_t(i);
-            if (kAny) {
-                T.exhausted = true;
-                return;
-            }
+            if (kAny) return true;
         }
+    }
+    return false;
+}
+
+// Leaf step of the one-thread-per-ray schedule: test the current leaf, then pop.
+template <bool kAny, bool kCount>
+__device__ __forceinline__ void trav_leaf(Traversal& T, const DevScene& S, const uint32_t* stack,
+                                          const float* stackT, Counters* cnt) {
+    if (leaf_test<kAny, kCount>(T, S, T.cur, cnt)) {
+        T.exhausted = true;
+        return;
     }
     if (!trav_pop(T, stack, stackT)) T.exhausted = true;
 }
@@ -239,7 +254,7 @@ __device__ __forceinline__ void persistent_traverse(const DevScene& S, uint32_t 
     float stackT[kMaxStack4];
     Traversal T;
     bool active = false, drained = false;
-    uint32_t idx = 0;
+    uint32_t idx = 0, parked = kEmptyChild;
     while (true) {
         // 1. refill idle lanes
         if (!drained) {
@@ -262,15 +277,28 @@ __device__ __forceinline__ void persistent_traverse(const DevScene& S, uint32_t 
             }
         }
         if (!__any_sync(0xFFFFFFFFu, active)) break;
-        // 2. interior phase
+        // 2. interior phase (speculative)
         while (true) {
-            bool want = active && !T.exhausted && !(T.cur & 0x80000000u);
-            if (!__any_sync(0xFFFFFFFFu, want)) break;
+            if (kAny && active && !T.exhausted && (T.cur & 0x80000000u) && parked == kEmptyChild) {
+                parked = T.cur;
+                if (!trav_pop(T, stack, stackT)) T.exhausted = true;
+            }
+            const bool want = active && !T.exhausted && !(T.cur & 0x80000000u);
+            const bool ready = !active || T.exhausted || (kAny ? parked != kEmptyChild : bool(T.cur & 0x80000000u));
+            if (!__any_sync(0xFFFFFFFFu, want) || __all_sync(0xFFFFFFFFu, ready)) break;
             if (want) trav_interior<kAny, kCount>(T, S, stack, stackT, err, cnt);
         }
-        // 3. leaf phase
-        if (active && !T.exhausted) trav_leaf<kAny, kCount>(T, S, stack, stackT, cnt);
-        if (active && T.exhausted) {
+        // 3. leaf phase: one leaf per lane
+        if (active) {
+            if (parked != kEmptyChild) {
+                if (leaf_test<kAny, kCount>(T, S, parked, cnt)) T.exhausted = true;
+                parked = kEmptyChild;
+            } else if (!T.exhausted && (T.cur & 0x80000000u)) {
+                if (leaf_test<kAny, kCount>(T, S, T.cur, cnt)) T.exhausted = true;
+                else if (!trav_pop(T, stack, stackT)) T.exhausted = true;
+            }
+        }
+        if (active && T.exhausted && parked == kEmptyChild) {
             done(idx, T);
             active = false;
         }
