@@ -622,6 +622,7 @@ int render_items(ana_ctx* c, const ana_render_desc* descs, uint32_t n, uint32_t 
     cfg.persistent = c->opts.traversal == ANA_TRAVERSAL_PER_RAY ? 0 : 1;
     const long long gcap = ((long long)cap + cfg.block - 1) / cfg.block;
     cfg.grid_cap = int(std::max<long long>(1, std::min<long long>(gcap, 1 << 20)));
+    cfg.stage_grid = std::max(1, 4 * c->num_sms * (2048 / cfg.block));
     const size_t launches = backward ? size_t(nchunks) * (3 + 9 * size_t(maxDepth + 1))
                                      : size_t(nchunks) * (2 + 4 * size_t(maxDepth + 1));
     if (timing && c->stage_ev.size() < 2 * launches) {

@@ -19,6 +19,7 @@
 // with a block-level allocation: warp ballots give each lane its rank, one
 // shared-memory scan over the block's warps and a single atomicAdd per block
 // reserve a contiguous range, so every warp writes a contiguous, coalesced run.
+#include <algorithm>
 #include <map>
 #include <mutex>
 #include <utility>
@@ -36,30 +37,41 @@ constexpr int kPersistBlock = 256;    // traversal kernels: 8 warps per block
 constexpr int kPersistMinBlocks = 4;  // persistent schedule: 4 resident blocks/SM (<= 64 registers)
 constexpr int kMaxStageBlock = 512;   // largest block of k_shade (the tunable stage kernel)
 
-// Reserve one slot per thread with want == true; returns the slot (valid only
-// for those threads). Must be reached by every thread of the block.
-__device__ __forceinline__ uint32_t block_push(bool want, uint32_t* counter) {
-    __shared__ uint32_t s_cnt[kMaxBlock / 32];
-    __shared__ uint32_t s_base;
+// Reserves one slot per thread and queue where that thread's want flag is
+// set, for three queues at once: warp ballots give each lane its rank, threads
+// 0-2 scan the block's warp counts of one queue each and reserve the block's
+// range with one atomicAdd. Must be reached by every thread of the block.
+__device__ __forceinline__ void block_push3(bool w0, bool w1, bool w2, uint32_t* c0, uint32_t* c1, uint32_t* c2,
+                                            uint32_t& k0, uint32_t& k1, uint32_t& k2) {
+    __shared__ uint32_t s_cnt[3][kMaxBlock / 32];
+    __shared__ uint32_t s_base[3];
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t nwarps = (blockDim.x + 31u) >> 5;
-    uint32_t mask = __ballot_sync(0xFFFFFFFFu, want);
-    uint32_t rank = __popc(mask & ((1u << lane) - 1u));
-    if (lane == 0) s_cnt[warp] = __popc(mask);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        uint32_t run = 0;
-        for (uint32_t w = 0; w < nwarps; ++w) {
-            uint32_t c = s_cnt[w];
-            s_cnt[w] = run;
-            run += c;
-        }
-        s_base = run ? atomicAdd(counter, run) : 0u;
+    const uint32_t lt = (1u << lane) - 1u;
+    const uint32_t m0 = __ballot_sync(0xFFFFFFFFu, w0), m1 = __ballot_sync(0xFFFFFFFFu, w1),
+                   m2 = __ballot_sync(0xFFFFFFFFu, w2);
+    if (lane == 0) {
+        s_cnt[0][warp] = __popc(m0);
+        s_cnt[1][warp] = __popc(m1);
+        s_cnt[2][warp] = __popc(m2);
     }
     __syncthreads();
-    uint32_t slot = s_base + s_cnt[warp] + rank;
+    if (threadIdx.x < 3) {
+        uint32_t* cnt = s_cnt[threadIdx.x];
+        uint32_t run = 0;
+        for (uint32_t w = 0; w < nwarps; ++w) {
+            const uint32_t c = cnt[w];
+            cnt[w] = run;
+            run += c;
+        }
+        uint32_t* ctr = threadIdx.x == 0 ? c0 : (threadIdx.x == 1 ? c1 : c2);
+        s_base[threadIdx.x] = run ? atomicAdd(ctr, run) : 0u;
+    }
+    __syncthreads();
+    k0 = s_base[0] + s_cnt[0][warp] + __popc(m0 & lt);
+    k1 = s_base[1] + s_cnt[1][warp] + __popc(m1 & lt);
+    k2 = s_base[2] + s_cnt[2][warp] + __popc(m2 & lt);
     __syncthreads();  // s_cnt / s_base are reused by the next call
-    return slot;
 }
 
 __device__ __forceinline__ float4 pack(float3 v, float w) { return make_float4(v.x, v.y, v.z, w); }
@@ -548,7 +560,8 @@ __global__ void __launch_bounds__(kMaxStageBlock) k_shade(const __grid_constant_
             warp_accum(p.a.grad, keyEmit, vEmit);
         }
         uint32_t* cb = p.counters + b * kCountersPerBounce;
-        uint32_t k = block_push(pushSh, cb + 1);
+        uint32_t k, kMis, kExt;
+        block_push3(pushSh, pushMis, pushExt, cb + 1, cb + 2, cb + kCountersPerBounce + 0, k, kMis, kExt);
         if (pushSh) {
             p.q.sh_o[k] = shO;
             p.q.sh_d[k] = shD;
@@ -558,7 +571,7 @@ __global__ void __launch_bounds__(kMaxStageBlock) k_shade(const __grid_constant_
                 p.a.sh_g1[k] = shG1;
             }
         }
-        k = block_push(pushMis, cb + 2);
+        k = kMis;
         if (pushMis) {
             p.q.mis_o[k] = mO;
             p.q.mis_d[k] = mD;
@@ -568,7 +581,7 @@ __global__ void __launch_bounds__(kMaxStageBlock) k_shade(const __grid_constant_
                 p.a.mis_g1[k] = mG1;
             }
         }
-        k = block_push(pushExt, cb + kCountersPerBounce + 0);
+        k = kExt;
         if (pushExt) {
             p.q.ext_o[nxt][k] = eO;
             p.q.ext_d[nxt][k] = eD;
@@ -922,8 +935,9 @@ void launch_extend(const Params& p, const LaunchCfg& c, cudaStream_t s, bool cou
     }
 }
 void launch_shade(const Params& p, const LaunchCfg& c, cudaStream_t s) {
-    if (p.S.has_fibers) k_shade<false, true><<<c.grid_cap, c.block, 0, s>>>(p);
-    else k_shade<false, false><<<c.grid_cap, c.block, 0, s>>>(p);
+    const int g = std::min(c.grid_cap, c.stage_grid);
+    if (p.S.has_fibers) k_shade<false, true><<<g, c.block, 0, s>>>(p);
+    else k_shade<false, false><<<g, c.block, 0, s>>>(p);
 }
 template <bool kCurves, bool kPersist, bool kAdj>
 static void sh_launch(const Params& p, const LaunchCfg& c, cudaStream_t s) {
@@ -960,8 +974,9 @@ void launch_adj_init(const Params& p, const LaunchCfg& c, cudaStream_t s) {
     k_adj_init<<<blocks_for(p.chunk_paths, 256, c.grid_cap), 256, 0, s>>>(p);
 }
 void launch_shade_adj(const Params& p, const LaunchCfg& c, cudaStream_t s) {
-    if (p.S.has_fibers) k_shade<true, true><<<c.grid_cap, c.block, 0, s>>>(p);
-    else k_shade<true, false><<<c.grid_cap, c.block, 0, s>>>(p);
+    const int g = std::min(c.grid_cap, c.stage_grid);
+    if (p.S.has_fibers) k_shade<true, true><<<g, c.block, 0, s>>>(p);
+    else k_shade<true, false><<<g, c.block, 0, s>>>(p);
 }
 void launch_shadow_adj(const Params& p, const LaunchCfg& c, cudaStream_t s) { shadow_dispatch<true>(p, c, s); }
 void launch_mis_adj(const Params& p, const LaunchCfg& c, cudaStream_t s) {
@@ -970,7 +985,7 @@ void launch_mis_adj(const Params& p, const LaunchCfg& c, cudaStream_t s) {
     else ps ? mis_launch<false, false, true, true>(p, c, s) : mis_launch<false, false, false, true>(p, c, s);
 }
 void launch_adj_direct(const Params& p, const LaunchCfg& c, cudaStream_t s) {
-    k_adj_direct<<<c.grid_cap, 256, 0, s>>>(p);
+    k_adj_direct<<<std::min(c.grid_cap, c.stage_grid), 256, 0, s>>>(p);
 }
 void launch_film(const Params& p, const LaunchCfg& c, cudaStream_t s) {
     k_film<<<blocks_for(p.chunk_pixels, 256, c.grid_cap), 256, 0, s>>>(p);

@@ -95,6 +95,10 @@ struct Params {
 struct LaunchCfg {
     int block;       // threads per block for the stage kernels
     int grid_cap;    // blocks for grid-stride kernels over the chunk capacity
+    int stage_grid;  // blocks for stage kernels whose item count is only known on
+                     // the device (shade, adjoint resolution): four waves of
+                     // the most blocks an SM can hold, so sparse late bounces do
+                     // not pay for launching blocks sized for a full chunk
     int persistent;  // traversal schedule: 1 persistent warps with refill, 0 thread per ray
 };
 

@@ -58,6 +58,9 @@ def parse():
                     help="target CPU work of the reference sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--chunk-paths", type=int, default=1 << 27,
+                    help="paths in flight per wavefront chunk; the default is the autotuner's best "
+                         "point for this frame (all 132,710,400 paths in one chunk, ~31 GB of queues)")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batched-vs-plain and adjoint/forward measurements")
     ap.add_argument("--traversal", type=int, default=0,
@@ -72,8 +75,10 @@ def workload_config(a, scene):
                      f"{a.width}x{a.height}, {a.spp} spp, max depth {a.depth}"),
         "paths_per_step": scene.num_paths,
         "triangles": scene.num_triangles,
-        "l2": "inputs larger than L2 (scene arrays + wavefront queues ~1.7 GB vs 126 MB L2)",
+        "l2": "inputs larger than L2 (706 MB of scene arrays + GBs of wavefront queues vs 126 MB L2)",
         "sampler": "scrambled Halton seed 0",
+        "chunk_paths": min(a.chunk_paths, scene.num_paths),
+        "launch": "stage block 256, persistent traversal, BVH leaves of 4 (the reference's)",
     }
 
 
@@ -319,7 +324,7 @@ def run_ours(a):
         torch.cuda.set_device(local)
     scene = S.throughput(a.width, a.height, a.spp, a.depth, n_spheres=a.n_spheres)
     prep = api.Prepared(scene)
-    r = api.Renderer(device=local, timing=True, traversal=a.traversal)
+    r = api.Renderer(device=local, timing=True, traversal=a.traversal, chunk_paths=a.chunk_paths)
     r.upload(prep)
     W, H, spp = scene.width, scene.height, scene.spp
     start = rank * spp  # each rank renders its own disjoint sample range of the frame
