@@ -174,39 +174,32 @@ struct SceneHit {
     float tseg;
 };
 
-// Completes a triangle traversal with the curve pass (strictly closer ribbon
-// hits win) and packs the result. kCurves = false compiles the curve code out
-// of kernels for triangle-only batches.
+// Packs a finished traversal (triangles, then strictly closer ribbons when
+// kCurves). kCurves = false compiles the curve code out of kernels for
+// triangle-only batches.
 template <bool kCurves>
-__device__ __forceinline__ SceneHit finish_closest(const DevScene& S, uint32_t segRoot, const Ray& r,
-                                                   const Traversal& T, uint32_t* err) {
+__device__ __forceinline__ SceneHit finish_closest(const Traversal& T, float tmax) {
     SceneHit h;
-    h.t = T.tri >= 0 ? T.closest : r.tmax;
+    h.t = T.tri >= 0 ? T.closest : tmax;
     h.u = T.u;
     h.v = T.v;
     h.prim = T.tri >= 0 ? uint32_t(T.tri) : kMiss;
     h.tang = f3(0.f, 0.f, 0.f);
     h.tseg = 0.f;
-    if (kCurves) {
-        CurveHit ch = trace_curves(S, segRoot, r, T.tri >= 0 ? T.closest : r.tmax, false, err);
-        if (ch.seg >= 0) {
-            h.t = ch.t;
-            h.prim = 0x80000000u | uint32_t(ch.seg);
-            h.tang = ch.tang;
-            h.tseg = ch.tSeg;
-            h.u = 0.f;
-            h.v = ch.tSeg;
-        }
+    if (kCurves && T.seg >= 0) {
+        h.t = T.closest;
+        h.prim = 0x80000000u | uint32_t(T.seg);
+        h.tang = T.tang;
+        h.tseg = T.tseg;
+        h.u = 0.f;
+        h.v = T.tseg;
     }
     return h;
 }
 
 template <bool kCurves>
-__device__ __forceinline__ bool finish_any(const DevScene& S, uint32_t segRoot, const Ray& r, const Traversal& T,
-                                           uint32_t* err) {
-    if (T.tri >= 0) return true;
-    if (kCurves) return trace_curves(S, segRoot, r, r.tmax, true, err).seg >= 0;
-    return false;
+__device__ __forceinline__ bool finish_any(const Traversal& T) {
+    return T.tri >= 0 || (kCurves && T.seg >= 0);
 }
 
 __device__ __forceinline__ void warp_add_work(unsigned long long* work, const Counters& cnt) {
@@ -229,30 +222,41 @@ __device__ __forceinline__ void warp_add_work(unsigned long long* work, const Co
 //   kPersist: persistent warps with per-lane refill (persistent_traverse);
 //   otherwise one thread per ray over a grid-stride loop.
 // Both use the same interior/leaf steps, so results are identical.
-template <bool kAny, bool kCount, bool kPersist, class Load, class Done>
+template <bool kAny, bool kCount, bool kPersist, bool kCurves, class Load, class Done>
 __device__ __forceinline__ void run_traversal(const DevScene& S, uint32_t n, uint32_t* fetch, uint32_t* err,
                                               Counters* cnt, Load load, Done done) {
     if constexpr (kPersist) {
-        persistent_traverse<kAny, kCount>(S, n, fetch, err, cnt, load, done);
+        persistent_traverse<kAny, kCount, kCurves>(S, n, fetch, err, cnt, load, done);
     } else {
         uint32_t stack[kMaxStack4];
         float stackT[kMaxStack4];
         for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
             Ray ray;
-            uint32_t root;
-            load(i, ray, root);
+            uint32_t root, segRoot;
+            load(i, ray, root, segRoot);
             Traversal T;
             trav_init(T, ray, root);
-            while (!T.exhausted) {
-                if (!(T.cur & 0x80000000u)) trav_interior<kAny, kCount>(T, S, stack, stackT, err, cnt);
-                else trav_leaf<kAny, kCount>(T, S, stack, stackT, cnt);
+            while (true) {
+                while (!T.exhausted) {
+                    if (!(T.cur & 0x80000000u)) {
+                        node_step<kAny, kCount, kCurves>(T, S, stack, stackT, err, cnt);
+                    } else if (leaf_step<kAny, kCount, kCurves>(T, S, T.cur, cnt)) {
+                        T.exhausted = true;
+                    } else if (!trav_pop(T, stack, stackT)) {
+                        T.exhausted = true;
+                    }
+                }
+                if (stage_done<kAny, kCurves>(T, ray.d, segRoot)) break;
             }
             done(i, T);
         }
     }
 }
 
-#define ANA_TRAVERSAL_BOUNDS __launch_bounds__(kPersistBlock, kPersist ? kPersistMinBlocks : 1)
+// Persistent triangle kernels fit 4 blocks per SM (64 registers); with the
+// curve stage they take 2 (128 registers: the ribbon test's state).
+#define ANA_TRAVERSAL_BOUNDS \
+    __launch_bounds__(kPersistBlock, kPersist ? (kCurves ? 2 : kPersistMinBlocks) : 1)
 
 __device__ __forceinline__ uint32_t scene_bits(float w) { return __float_as_uint(w); }
 
@@ -264,18 +268,17 @@ __global__ void ANA_TRAVERSAL_BOUNDS k_extend(const __grid_constant__ Params p) 
     const uint32_t cur = p.bounce & 1u;
     uint32_t* cb = p.counters + p.bounce * kCountersPerBounce;
     Counters cnt{0, 0, 0, 0};
-    run_traversal<false, kCount, kPersist>(
+    run_traversal<false, kCount, kPersist, kCurves>(
         p.S, cb[0], cb + 3, p.err, &cnt,
-        [&](uint32_t i, Ray& r, uint32_t& root) {
+        [&](uint32_t i, Ray& r, uint32_t& root, uint32_t& segRoot) {
             float4 o = p.q.ext_o[cur][i], d = p.q.ext_d[cur][i];
             r = Ray{f3(o), f3(d), 1e-4f, INFINITY};
-            root = p.S.scenes[scene_bits(p.q.ext_b[cur][i].w)].tri_root;
+            const DevSceneRec& R = p.S.scenes[scene_bits(p.q.ext_b[cur][i].w)];
+            root = R.tri_root;
+            segRoot = kCurves ? R.seg_root : kNoRoot;
         },
         [&](uint32_t i, const Traversal& T) {
-            float4 o = p.q.ext_o[cur][i], d = p.q.ext_d[cur][i];
-            Ray r{f3(o), f3(d), 1e-4f, INFINITY};
-            uint32_t segRoot = kCurves ? p.S.scenes[scene_bits(p.q.ext_b[cur][i].w)].seg_root : kNoRoot;
-            SceneHit h = finish_closest<kCurves>(p.S, segRoot, r, T, p.err);
+            SceneHit h = finish_closest<kCurves>(T, INFINITY);
             p.q.hit0[i] = make_float4(h.t, __uint_as_float(h.prim), h.u, h.v);
             if (kCurves && h.prim != kMiss && (h.prim & 0x80000000u)) p.q.hit1[i] = pack(h.tang, h.tseg);
         });
@@ -599,18 +602,18 @@ __global__ void __launch_bounds__(kMaxStageBlock) k_shade(const __grid_constant_
 template <bool kCurves, bool kPersist, bool kAdj>
 __global__ void ANA_TRAVERSAL_BOUNDS k_shadow(const __grid_constant__ Params p) {
     uint32_t* cb = p.counters + p.bounce * kCountersPerBounce;
-    run_traversal<true, false, kPersist>(
+    run_traversal<true, false, kPersist, kCurves>(
         p.S, cb[1], cb + 4, p.err, nullptr,
-        [&](uint32_t i, Ray& r, uint32_t& root) {
+        [&](uint32_t i, Ray& r, uint32_t& root, uint32_t& segRoot) {
             float4 o = p.q.sh_o[i], d = p.q.sh_d[i];
             r = Ray{f3(o), f3(d), 1e-4f, d.w};
-            root = p.S.scenes[scene_bits(p.q.sh_c[i].w)].tri_root;
+            const DevSceneRec& R = p.S.scenes[scene_bits(p.q.sh_c[i].w)];
+            root = R.tri_root;
+            segRoot = kCurves ? R.seg_root : kNoRoot;
         },
         [&](uint32_t i, const Traversal& T) {
-            float4 o = p.q.sh_o[i], d = p.q.sh_d[i], c = p.q.sh_c[i];
-            Ray r{f3(o), f3(d), 1e-4f, d.w};
-            uint32_t segRoot = kCurves ? p.S.scenes[scene_bits(c.w)].seg_root : kNoRoot;
-            const bool occluded = finish_any<kCurves>(p.S, segRoot, r, T, p.err);
+            float4 o = p.q.sh_o[i], c = p.q.sh_c[i];
+            const bool occluded = finish_any<kCurves>(T);
             if (!occluded) add_L(p, __float_as_uint(o.w), f3(c));
             if constexpr (kAdj) p.a.sh_vis[i] = occluded ? 0u : 1u;
         });
@@ -625,26 +628,27 @@ template <bool kAny, bool kCurves, bool kPersist, bool kAdj>
 __global__ void ANA_TRAVERSAL_BOUNDS k_mis(const __grid_constant__ Params p) {
     uint32_t* cb = p.counters + p.bounce * kCountersPerBounce;
     const DevScene& S = p.S;
-    run_traversal<kAny, false, kPersist>(
+    run_traversal<kAny, false, kPersist, kCurves>(
         S, cb[2], cb + 5, p.err, nullptr,
-        [&](uint32_t i, Ray& r, uint32_t& root) {
+        [&](uint32_t i, Ray& r, uint32_t& root, uint32_t& segRoot) {
             float4 o = p.q.mis_o[i], d = p.q.mis_d[i];
             r = Ray{f3(o), f3(d), 1e-4f, 1e10f};
-            root = S.scenes[scene_bits(p.q.mis_c[i].w)].tri_root;
+            const DevSceneRec& R = S.scenes[scene_bits(p.q.mis_c[i].w)];
+            root = R.tri_root;
+            segRoot = kCurves ? R.seg_root : kNoRoot;
         },
         [&](uint32_t i, const Traversal& T) {
             float4 o = p.q.mis_o[i], d = p.q.mis_d[i], c = p.q.mis_c[i];
-            Ray r{f3(o), f3(d), 1e-4f, 1e10f};
+            const float3 rd = f3(d);
             const DevSceneRec& R = S.scenes[scene_bits(c.w)];
-            uint32_t segRoot = kCurves ? R.seg_root : kNoRoot;
             float3 Li;
             int mi = -1;
             if (kAny) {
-                Li = finish_any<kCurves>(S, segRoot, r, T, p.err) ? f3(0.f, 0.f, 0.f) : scene_env(S, R, r.d);
+                Li = finish_any<kCurves>(T) ? f3(0.f, 0.f, 0.f) : scene_env(S, R, rd);
             } else {
-                SceneHit h = finish_closest<kCurves>(S, segRoot, r, T, p.err);
+                SceneHit h = finish_closest<kCurves>(T, 1e10f);
                 if (h.prim == kMiss) {
-                    Li = scene_env(S, R, r.d);
+                    Li = scene_env(S, R, rd);
                 } else {
                     uint32_t slot;
                     if (h.prim & 0x80000000u)
@@ -784,21 +788,20 @@ __global__ void ANA_TRAVERSAL_BOUNDS k_trace_batch(const __grid_constant__ DevSc
                                                    const float* rays, uint32_t n, ana_hit* out, uint32_t* fetch,
                                                    uint32_t* err) {
     const uint32_t triRoot = S.scenes[scene].tri_root, segRoot = S.scenes[scene].seg_root;
-    auto load = [&](uint32_t i, Ray& r, uint32_t& root) {
+    auto load = [&](uint32_t i, Ray& r, uint32_t& root, uint32_t& sroot) {
         const float4* rp = reinterpret_cast<const float4*>(rays + 8 * size_t(i));
         float4 a = rp[0], b = rp[1];
         r = Ray{f3(a), f3(b), a.w, b.w};
         root = triRoot;
+        sroot = kCurves ? segRoot : kNoRoot;
     };
-    run_traversal<kAny, false, kPersist>(S, n, fetch, err, nullptr, load, [&](uint32_t i, const Traversal& T) {
-        Ray r;
-        uint32_t root;
-        load(i, r, root);
+    run_traversal<kAny, false, kPersist, kCurves>(S, n, fetch, err, nullptr, load, [&](uint32_t i, const Traversal& T) {
         ana_hit h{0, -1, -1, -1, 0.f, 0.f, 0.f, 0.f};
         if (kAny) {
-            h.hit = finish_any<kCurves>(S, segRoot, r, T, err) ? 1 : 0;
+            h.hit = finish_any<kCurves>(T) ? 1 : 0;
         } else {
-            SceneHit sh = finish_closest<kCurves>(S, segRoot, r, T, err);
+            const float tmax = reinterpret_cast<const float4*>(rays + 8 * size_t(i))[1].w;
+            SceneHit sh = finish_closest<kCurves>(T, tmax);
             if (sh.prim != kMiss) {
                 h.hit = 1;
                 h.t = sh.t;

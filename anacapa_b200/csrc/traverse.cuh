@@ -119,6 +119,13 @@ struct Traversal {
     uint32_t cur;
     int sp;
     bool exhausted;
+    // curve stage (scenes with curves): the triangle BVH is traversed first,
+    // then the curve BVH from the triangle hit distance (CurveBrute::trace)
+    uint32_t stage;  // 0 triangles, 1 curves
+    int32_t seg;     // leaf-order segment of the closest ribbon hit, -1 if none
+    float tseg;
+    float3 tang;
+    float3 cd, fx, fy, cinv;  // exact direction, ray-space frame x/y, 1/d
 };
 
 // Starts a traversal at a scene's root (kNoRoot: the scene has no triangles).
@@ -134,6 +141,8 @@ __device__ __forceinline__ void trav_init(Traversal& T, const Ray& ray, uint32_t
     T.cur = root;
     T.sp = 0;
     T.exhausted = root == kNoRoot;
+    T.stage = 0;
+    T.seg = -1;
 }
 
 __device__ __forceinline__ bool trav_pop(Traversal& T, const uint32_t* stack, const float* stackT) {
@@ -240,69 +249,6 @@ __device__ __forceinline__ void trav_leaf(Traversal& T, const DevScene& S, const
         return;
     }
     if (!trav_pop(T, stack, stackT)) T.exhausted = true;
-}
-
-// Runs the persistent loop. Load(i, ray, root) reads queue entry i and its
-// scene's BVH root; Done(i, T) consumes the finished traversal of entry i (a
-// lane-local call).
-template <bool kAny, bool kCount, class Load, class Done>
-__device__ __forceinline__ void persistent_traverse(const DevScene& S, uint32_t n, uint32_t* fetch, uint32_t* err,
-                                                    Counters* cnt, Load load, Done done) {
-    const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t ltmask = (1u << lane) - 1u;
-    uint32_t stack[kMaxStack4];
-    float stackT[kMaxStack4];
-    Traversal T;
-    bool active = false, drained = false;
-    uint32_t idx = 0, parked = kEmptyChild;
-    while (true) {
-        // 1. refill idle lanes
-        if (!drained) {
-            uint32_t need = __ballot_sync(0xFFFFFFFFu, !active);
-            if (need) {
-                uint32_t leader = __ffs(need) - 1u, base = 0;
-                if (lane == leader) base = atomicAdd(fetch, __popc(need));
-                base = __shfl_sync(0xFFFFFFFFu, base, leader);
-                if (base >= n) drained = true;
-                if (!active) {
-                    idx = base + __popc(need & ltmask);
-                    if (idx < n) {
-                        Ray ray;
-                        uint32_t root;
-                        load(idx, ray, root);
-                        trav_init(T, ray, root);
-                        active = true;
-                    }
-                }
-            }
-        }
-        if (!__any_sync(0xFFFFFFFFu, active)) break;
-        // 2. interior phase (speculative)
-        while (true) {
-            if (kAny && active && !T.exhausted && (T.cur & 0x80000000u) && parked == kEmptyChild) {
-                parked = T.cur;
-                if (!trav_pop(T, stack, stackT)) T.exhausted = true;
-            }
-            const bool want = active && !T.exhausted && !(T.cur & 0x80000000u);
-            const bool ready = !active || T.exhausted || (kAny ? parked != kEmptyChild : bool(T.cur & 0x80000000u));
-            if (!__any_sync(0xFFFFFFFFu, want) || __all_sync(0xFFFFFFFFu, ready)) break;
-            if (want) trav_interior<kAny, kCount>(T, S, stack, stackT, err, cnt);
-        }
-        // 3. leaf phase: one leaf per lane
-        if (active) {
-            if (parked != kEmptyChild) {
-                if (leaf_test<kAny, kCount>(T, S, parked, cnt)) T.exhausted = true;
-                parked = kEmptyChild;
-            } else if (!T.exhausted && (T.cur & 0x80000000u)) {
-                if (leaf_test<kAny, kCount>(T, S, T.cur, cnt)) T.exhausted = true;
-                else if (!trav_pop(T, stack, stackT)) T.exhausted = true;
-            }
-        }
-        if (active && T.exhausted && parked == kEmptyChild) {
-            done(idx, T);
-            active = false;
-        }
-    }
 }
 
 // ===========================================================================
@@ -444,76 +390,168 @@ __device__ __forceinline__ bool ribbon_hit(const RayFrame& fr, float tmin, float
     return hit;
 }
 
-struct CurveHit {
-    int32_t seg;   // leaf-order segment index, -1 if none
-    float t, tSeg;
-    float3 tang;
-};
+// ---------------------------------------------------------------------------
+// Curve stage of a traversal (CurveBrute::trace's curve pass,
+// CurveBrute.cpp:398-440): after the triangle BVH, the curve BVH is traversed
+// from the triangle hit distance, keeping only strictly closer ribbon hits.
+// Node and leaf steps mirror the triangle ones, so both stages share the
+// converged interior / leaf phases and the stack.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void curve_begin(Traversal& T, float3 d, uint32_t segRoot) {
+    T.stage = 1;
+    T.cd = d;
+    onb_exact(d, T.fx, T.fy);
+    T.cinv = f3(xdiv(1.f, d.x), xdiv(1.f, d.y), xdiv(1.f, d.z));
+    T.cur = segRoot;
+    T.sp = 0;
+    T.exhausted = segRoot == kNoRoot;
+}
 
-// Curve BVH pass of CurveBrute::trace (CurveBrute.cpp:398-440): starts from the
-// triangle hit distance and keeps only strictly closer ribbon hits.
-template <bool kCount = false>
-__device__ __forceinline__ CurveHit trace_curves(const DevScene& S, uint32_t root, const Ray& ray, float bestT,
-                                                 bool anyHit, uint32_t* err, Counters* cnt = nullptr) {
-    CurveHit ch{-1, bestT, 0.f, f3(0.f, 0.f, 0.f)};
-    if (root == kNoRoot) return ch;
-    RayFrame fr = make_frame(ray);
-    float3 inv = f3(xdiv(1.f, ray.d.x), xdiv(1.f, ray.d.y), xdiv(1.f, ray.d.z));
-    uint32_t stack[kMaxStack];
-    float stackT[kMaxStack];
-    int sp = 0;
-    uint32_t cur = root;
+// One curve-BVH node: two child boxes (CurveBrute::aabbHit), nearer first.
+template <bool kCount>
+__device__ __forceinline__ void curve_interior(Traversal& T, const DevScene& S, uint32_t* stack, float* stackT,
+                                               uint32_t* err, Counters* cnt) {
+    const Ray ray{T.r.o, T.cd, T.r.tmin, T.r.tmax};
+    const float4* np = reinterpret_cast<const float4*>(S.seg_nodes + T.cur);
+    const float4 n0 = ldg4(np), n1 = ldg4(np + 1), n2 = ldg4(np + 2), n3 = ldg4(np + 3);
+    if (kCount) cnt->cnodes++;
+    float tn0 = 0.f, tn1 = 0.f;
+    const bool h0 = curve_box_hit(ray, T.cinv, n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, T.closest, tn0);
+    const bool h1 = curve_box_hit(ray, T.cinv, n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, T.closest, tn1);
+    const uint32_t c0 = fbits_u(n3.z) ? leaf_entry(fbits_u(n3.x), fbits_u(n3.z)) : fbits_u(n3.x);
+    const uint32_t c1 = fbits_u(n3.w) ? leaf_entry(fbits_u(n3.y), fbits_u(n3.w)) : fbits_u(n3.y);
+    if (h0 && h1) {
+        const bool swap = !(tn0 < tn1);
+        if (T.sp >= int(kMaxStack4)) {
+            atomicOr(err, 1u);
+            T.exhausted = true;
+            return;
+        }
+        stack[T.sp] = swap ? c0 : c1;
+        stackT[T.sp] = swap ? tn0 : tn1;
+        ++T.sp;
+        T.cur = swap ? c1 : c0;
+    } else if (h0 || h1) {
+        T.cur = h0 ? c0 : c1;
+    } else if (!trav_pop(T, stack, stackT)) {
+        T.exhausted = true;
+    }
+}
+
+// Ribbon tests of one curve leaf; true when an any-hit query found its blocker.
+template <bool kAny, bool kCount>
+__device__ __forceinline__ bool curve_leaf_test(Traversal& T, const DevScene& S, uint32_t leaf, Counters* cnt) {
+    const RayFrame fr{T.r.o, T.fx, T.fy, T.cd};
+    const uint32_t off = leaf & 0x01FFFFFFu, c = ((leaf >> 25) & 63u) + 1u;
+    for (uint32_t i = off; i < off + c; ++i) {
+        const float4* sp4 = S.segs + 5 * size_t(i);
+        const float4 a = ldg4(sp4), b = ldg4(sp4 + 1), e = ldg4(sp4 + 2), g = ldg4(sp4 + 3);
+        if (kCount) cnt->segs++;
+        float ts, bt = T.closest;
+        float3 tg;
+        if (ribbon_hit(fr, T.r.tmin, f3(a), f3(b), f3(e), f3(g), a.w, b.w, e.w, g.w, bt, ts, tg)) {
+            T.seg = int32_t(i);
+            T.closest = bt;
+            T.tseg = ts;
+            T.tang = tg;
+            if (kAny) return true;
+        }
+    }
+    return false;
+}
+
+// Stage dispatch of the node and leaf steps.
+template <bool kAny, bool kCount, bool kCurves>
+__device__ __forceinline__ void node_step(Traversal& T, const DevScene& S, uint32_t* stack, float* stackT,
+                                          uint32_t* err, Counters* cnt) {
+    if (kCurves && T.stage) curve_interior<kCount>(T, S, stack, stackT, err, cnt);
+    else trav_interior<kAny, kCount>(T, S, stack, stackT, err, cnt);
+}
+template <bool kAny, bool kCount, bool kCurves>
+__device__ __forceinline__ bool leaf_step(Traversal& T, const DevScene& S, uint32_t leaf, Counters* cnt) {
+    if (kCurves && T.stage) return curve_leaf_test<kAny, kCount>(T, S, leaf, cnt);
+    return leaf_test<kAny, kCount>(T, S, leaf, cnt);
+}
+
+// A lane whose triangle traversal ended moves on to the curve BVH (unless an
+// any-hit query already found a blocker). Returns true when the ray is done.
+template <bool kAny, bool kCurves>
+__device__ __forceinline__ bool stage_done(Traversal& T, float3 d, uint32_t segRoot) {
+    if (kCurves && T.stage == 0 && !(kAny && T.tri >= 0)) curve_begin(T, d, segRoot);
+    return T.exhausted;
+}
+
+// Runs the persistent loop. Load(i, ray, root, segRoot) reads queue entry i
+// and its scene's triangle and curve BVH roots; Done(i, T) consumes the
+// finished traversal of entry i (a lane-local call). With kCurves a lane that
+// finishes the triangle BVH continues with the curve BVH in the same phases.
+template <bool kAny, bool kCount, bool kCurves, class Load, class Done>
+__device__ __forceinline__ void persistent_traverse(const DevScene& S, uint32_t n, uint32_t* fetch, uint32_t* err,
+                                                    Counters* cnt, Load load, Done done) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t ltmask = (1u << lane) - 1u;
+    uint32_t stack[kMaxStack4];
+    float stackT[kMaxStack4];
+    Traversal T;
+    bool active = false, drained = false;
+    uint32_t idx = 0, parked = kEmptyChild;
     while (true) {
-        if (!(cur & 0x80000000u)) {
-            const float4* np = reinterpret_cast<const float4*>(S.seg_nodes + cur);
-            float4 n0 = ldg4(np), n1 = ldg4(np + 1), n2 = ldg4(np + 2), n3 = ldg4(np + 3);
-            if (kCount) cnt->cnodes++;
-            float tn0 = 0.f, tn1 = 0.f;
-            bool h0 = curve_box_hit(ray, inv, n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, ch.t, tn0);
-            bool h1 = curve_box_hit(ray, inv, n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, ch.t, tn1);
-            uint32_t c0 = fbits_u(n3.z) ? leaf_entry(fbits_u(n3.x), fbits_u(n3.z)) : fbits_u(n3.x);
-            uint32_t c1 = fbits_u(n3.w) ? leaf_entry(fbits_u(n3.y), fbits_u(n3.w)) : fbits_u(n3.y);
-            if (h0 && h1) {
-                bool swap = !(tn0 < tn1);
-                if (sp >= int(kMaxStack)) { atomicOr(err, 1u); return ch; }
-                stack[sp] = swap ? c0 : c1;
-                stackT[sp] = swap ? tn0 : tn1;
-                ++sp;
-                cur = swap ? c1 : c0;
-                continue;
-            } else if (h0 || h1) {
-                cur = h0 ? c0 : c1;
-                continue;
-            }
-        } else {
-            uint32_t off = cur & 0x01FFFFFFu, c = ((cur >> 25) & 63u) + 1u;
-            for (uint32_t i = off; i < off + c; ++i) {
-                const float4* sp4 = S.segs + 5 * size_t(i);
-                float4 a = ldg4(sp4), b = ldg4(sp4 + 1), e = ldg4(sp4 + 2), g = ldg4(sp4 + 3);
-                if (kCount) cnt->segs++;
-                float ts;
-                float3 tg;
-                float bt = ch.t;
-                if (ribbon_hit(fr, ray.tmin, f3(a), f3(b), f3(e), f3(g), a.w, b.w, e.w, g.w, bt, ts, tg)) {
-                    ch.seg = int32_t(i);
-                    ch.t = bt;
-                    ch.tSeg = ts;
-                    ch.tang = tg;
-                    if (anyHit) return ch;
+        // 1. refill idle lanes
+        if (!drained) {
+            uint32_t need = __ballot_sync(0xFFFFFFFFu, !active);
+            if (need) {
+                uint32_t leader = __ffs(need) - 1u, base = 0;
+                if (lane == leader) base = atomicAdd(fetch, __popc(need));
+                base = __shfl_sync(0xFFFFFFFFu, base, leader);
+                if (base >= n) drained = true;
+                if (!active) {
+                    idx = base + __popc(need & ltmask);
+                    if (idx < n) {
+                        Ray ray;
+                        uint32_t root, segRoot;
+                        load(idx, ray, root, segRoot);
+                        trav_init(T, ray, root);
+                        active = true;
+                    }
                 }
             }
         }
-        bool found = false;
-        while (sp > 0) {
-            --sp;
-            if (stackT[sp] > ch.t) continue;
-            cur = stack[sp];
-            found = true;
-            break;
+        if (!__any_sync(0xFFFFFFFFu, active)) break;
+        // 2. interior phase (speculative)
+        while (true) {
+            if (kAny && active && !T.exhausted && (T.cur & 0x80000000u) && parked == kEmptyChild) {
+                parked = T.cur;
+                if (!trav_pop(T, stack, stackT)) T.exhausted = true;
+            }
+            const bool want = active && !T.exhausted && !(T.cur & 0x80000000u);
+            const bool ready = !active || T.exhausted || (kAny ? parked != kEmptyChild : bool(T.cur & 0x80000000u));
+            if (!__any_sync(0xFFFFFFFFu, want) || __all_sync(0xFFFFFFFFu, ready)) break;
+            if (want) node_step<kAny, kCount, kCurves>(T, S, stack, stackT, err, cnt);
         }
-        if (!found) break;
+        // 3. leaf phase: one leaf per lane
+        if (active) {
+            if (parked != kEmptyChild) {
+                if (leaf_step<kAny, kCount, kCurves>(T, S, parked, cnt)) T.exhausted = true;
+                parked = kEmptyChild;
+            } else if (!T.exhausted && (T.cur & 0x80000000u)) {
+                if (leaf_step<kAny, kCount, kCurves>(T, S, T.cur, cnt)) T.exhausted = true;
+                else if (!trav_pop(T, stack, stackT)) T.exhausted = true;
+            }
+        }
+        if (active && T.exhausted && parked == kEmptyChild) {
+            bool finished = true;
+            if (kCurves && T.stage == 0) {  // the curve BVH follows (the entry is read again for d)
+                Ray ray;
+                uint32_t root, segRoot;
+                load(idx, ray, root, segRoot);
+                finished = stage_done<kAny, kCurves>(T, ray.d, segRoot);
+            }
+            if (finished) {
+                done(idx, T);
+                active = false;
+            }
+        }
     }
-    return ch;
 }
 
 }  // namespace ana

@@ -18,7 +18,9 @@ its sources into oracle/_ref) on the host cores instead.
 The same line carries the metric's two other parts, measured after the timed
 region: "batched" (64 Cornell variants as one graph-replayed batch render vs
 one launch sequence per scene, same samples, so equal RMSE) and "adjoint"
-(ana_backward vs ana_forward device time on the differentiable scene).
+(ana_backward vs ana_forward device time on the differentiable scene);
+"other_configs" times single frames of the Cornell and hair configurations
+and of a 938-sphere (about 1.2M-triangle) throughput frame.
 """
 from __future__ import annotations
 
@@ -286,6 +288,45 @@ def bench_batched(local, reps=3):
             "speedup": pm / bm, "equal_rmse": "identical per-variant estimator and samples"}
 
 
+def bench_frame(local, scene, reps=3, chunk_paths=0):
+    """Device time of one frame of `scene` (median of reps after one warm-up)."""
+    from anacapa_b200 import api
+    r = api.Renderer(device=local, chunk_paths=chunk_paths)
+    r.upload(api.Prepared(scene))
+    times = []
+    for it in range(reps + 1):
+        r.render_scene(scene)
+        if it:
+            times.append(r.stats().render_ms)
+    st = r.stats()
+    r.close()
+    ms = statistics.median(times)
+    rays = st.extend_rays + st.shadow_rays + st.mis_rays
+    return {"paths": scene.num_paths, "ms": ms, "samples_per_s": scene.num_paths / (ms / 1e3),
+            "rays_per_s": rays / (ms / 1e3)}
+
+
+def bench_configs(local):
+    """The other single-frame configurations: Cornell 256x256x16 (depth 8),
+    hair 200k strands 1280x720x32 (depth 10), and the throughput frame with
+    938 spheres (about 1.2M triangles, the triangle count the throughput
+    configuration states; its generator gives 5.24M with 4096 spheres)."""
+    from anacapa_b200 import scenes as S
+    out = {}
+    cornell = S.cornell(256, 256, 16, 8)
+    out["cornell_256x256x16"] = {"workload": "Cornell box, 36 triangles, Lambert, area light; depth 8",
+                                 **bench_frame(local, cornell)}
+    hair = S.hair(1280, 720, 32, 10)
+    out["hair_1280x720x32"] = {"workload": f"hair: 200,000 strands, {hair.num_segments:,} cubic segments, "
+                                           "Kajiya-Kay as the reference executes it, one area light; depth 10",
+                               **bench_frame(local, hair, chunk_paths=1 << 25)}
+    thr = S.throughput(n_spheres=938)
+    out["throughput_938_spheres"] = {"workload": f"throughput scene with 938 spheres: {thr.num_triangles:,} "
+                                                 "triangles, 1920x1080x64, depth 12",
+                                     **bench_frame(local, thr, chunk_paths=1 << 27)}
+    return out
+
+
 def bench_adjoint(local, reps=3):
     """Path-replay adjoint on the differentiable scene (Cornell + 20,480-
     triangle icosphere, 512x512, 16 spp, depth 8): device time of ana_forward
@@ -382,6 +423,7 @@ def run_ours(a):
     if not a.no_extras:  # the metric's other two parts, outside the timed region
         extra["batched"] = bench_batched(local)
         extra["adjoint"] = bench_adjoint(local)
+        extra["other_configs"] = bench_configs(local)
     cpu = None
     if rank == 0 and ws == 1 and not a.no_cpu_baseline:
         try:
