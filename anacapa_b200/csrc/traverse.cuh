@@ -310,8 +310,10 @@ __device__ __forceinline__ float3 project(const RayFrame& f, float3 p) {
 }
 
 struct SubSeg {
-    float3 P0, P1, P2, P3;
+    float3 P0, P1, P2, P3;  // world-space control points (further splits, tangent)
+    float3 c0, c3;          // projected end points
     float hw0, hw3, toff, tscale;
+    float zlo;              // zMin - maxHalfW: the test that depends on bestT
     int depth;
 };
 
@@ -333,45 +335,64 @@ __device__ __forceinline__ float max4(float a, float b, float c, float d) {
     return fmaxf(fmaxf(a, b), fmaxf(c, d));
 }
 
-// subdivide (CurveBrute.cpp:85-176) as an explicit depth-first stack (left
-// half first, as the recursion visits it). Updates bestT on a closer hit.
+// The bounds tests of subdivide (CurveBrute.cpp:97-117) on projected control
+// points: depth range against [tmin, bestT], and the projected box's distance
+// from the ray axis against the larger half-width. zlo receives zMin - maxHalfW.
+__device__ __forceinline__ bool ribbon_bounds(float3 c0, float3 c1, float3 c2, float3 c3, float hw0, float hw3,
+                                              float tmin, float bestT, float& zlo) {
+    const float maxHalfW = fmaxf(hw0, hw3);
+    const float zMin = min4(c0.z, c1.z, c2.z, c3.z), zMax = max4(c0.z, c1.z, c2.z, c3.z);
+    zlo = xsub(zMin, maxHalfW);
+    if (zlo > bestT) return false;
+    if (xadd(zMax, maxHalfW) < tmin) return false;
+    const float xMin = min4(c0.x, c1.x, c2.x, c3.x), xMax = max4(c0.x, c1.x, c2.x, c3.x);
+    const float yMin = min4(c0.y, c1.y, c2.y, c3.y), yMax = max4(c0.y, c1.y, c2.y, c3.y);
+    const float cx = (0.f < xMin) ? xMin : (0.f > xMax ? xMax : 0.f);
+    const float cy = (0.f < yMin) ? yMin : (0.f > yMax ? yMax : 0.f);
+    return !(xadd(xmul(cx, cx), xmul(cy, cy)) > xmul(maxHalfW, maxHalfW));
+}
+
+// subdivide (CurveBrute.cpp:85-176): depth-6 de Casteljau subdivision in ray
+// space, the left half first, updating bestT on a closer hit. The reference
+// projects a node's four control points when it visits the node; a child
+// shares two of them with its parent and one with its sibling, so here a split
+// projects the five new points once (the same world points give the same
+// projections), both children are bounds-tested at once and only survivors are
+// pushed. The one test that depends on bestT (which only decreases) is
+// repeated when a child is popped, so every node is accepted or culled, and
+// every leaf evaluated, exactly as in the recursion and in the same order.
 __device__ __forceinline__ bool ribbon_hit(const RayFrame& fr, float tmin, float3 P0, float3 P1, float3 P2,
                                            float3 P3, float hw0, float hw3, float toff, float tscale,
                                            float& bestT, float& tSeg, float3& tang) {
     SubSeg st[8];
     int sp = 0;
-    st[sp++] = SubSeg{P0, P1, P2, P3, hw0, hw3, toff, tscale, 6};
+    {
+        const float3 c0 = project(fr, P0), c1 = project(fr, P1), c2 = project(fr, P2), c3 = project(fr, P3);
+        float zlo;
+        if (!ribbon_bounds(c0, c1, c2, c3, hw0, hw3, tmin, bestT, zlo)) return false;
+        st[sp++] = SubSeg{P0, P1, P2, P3, c0, c3, hw0, hw3, toff, tscale, zlo, 6};
+    }
     bool hit = false;
     while (sp > 0) {
-        SubSeg s = st[--sp];
-        float3 c0 = project(fr, s.P0), c1 = project(fr, s.P1), c2 = project(fr, s.P2),
-               c3 = project(fr, s.P3);
-        float maxHalfW = fmaxf(s.hw0, s.hw3);
-        float zMin = min4(c0.z, c1.z, c2.z, c3.z), zMax = max4(c0.z, c1.z, c2.z, c3.z);
-        if (xsub(zMin, maxHalfW) > bestT) continue;
-        if (xadd(zMax, maxHalfW) < tmin) continue;
-        float xMin = min4(c0.x, c1.x, c2.x, c3.x), xMax = max4(c0.x, c1.x, c2.x, c3.x);
-        float yMin = min4(c0.y, c1.y, c2.y, c3.y), yMax = max4(c0.y, c1.y, c2.y, c3.y);
-        float cx = (0.f < xMin) ? xMin : (0.f > xMax ? xMax : 0.f);
-        float cy = (0.f < yMin) ? yMin : (0.f > yMax ? yMax : 0.f);
-        if (xadd(xmul(cx, cx), xmul(cy, cy)) > xmul(maxHalfW, maxHalfW)) continue;
+        const SubSeg s = st[--sp];
+        if (s.zlo > bestT) continue;
         if (s.depth == 0) {
-            float ax = c0.x, ay = c0.y, bx = c3.x, by = c3.y;
-            float dx = xsub(bx, ax), dy = xsub(by, ay);
-            float lenSq = xadd(xmul(dx, dx), xmul(dy, dy));
+            const float ax = s.c0.x, ay = s.c0.y, bx = s.c3.x, by = s.c3.y;
+            const float dx = xsub(bx, ax), dy = xsub(by, ay);
+            const float lenSq = xadd(xmul(dx, dx), xmul(dy, dy));
             float tLine;
             if (lenSq < 1e-12f) tLine = 0.f;
             else
                 tLine = fmaxf(0.f, fminf(1.f, xdiv(xsub(xmul(-ax, dx), xmul(ay, dy)), lenSq)));
-            float px = xadd(ax, xmul(dx, tLine)), py = xadd(ay, xmul(dy, tLine));
-            float dist2 = xadd(xmul(px, px), xmul(py, py));
-            float halfW = xadd(xmul(s.hw0, xsub(1.f, tLine)), xmul(s.hw3, tLine));
+            const float px = xadd(ax, xmul(dx, tLine)), py = xadd(ay, xmul(dy, tLine));
+            const float dist2 = xadd(xmul(px, px), xmul(py, py));
+            const float halfW = xadd(xmul(s.hw0, xsub(1.f, tLine)), xmul(s.hw3, tLine));
             if (dist2 > xmul(halfW, halfW)) continue;
-            float tRay = xadd(c0.z, xmul(xsub(c3.z, c0.z), tLine));
+            const float tRay = xadd(s.c0.z, xmul(xsub(s.c3.z, s.c0.z), tLine));
             if (tRay < tmin || tRay >= bestT) continue;
             float3 tg = bezier_tangent(s.P0, s.P1, s.P2, s.P3, tLine);
             if (xdot(tg, tg) < 1e-12f) tg = xsub3(s.P3, s.P0);
-            float len = __fsqrt_rn(xdot(tg, tg));
+            const float len = __fsqrt_rn(xdot(tg, tg));
             tg = len > 1e-8f ? xmul3(tg, xdiv(1.f, len)) : f3(0.f, 0.f, 1.f);
             bestT = tRay;
             tSeg = xadd(s.toff, xmul(tLine, s.tscale));
@@ -380,12 +401,17 @@ __device__ __forceinline__ bool ribbon_hit(const RayFrame& fr, float tmin, float
             continue;
         }
         // bezierSplitMid (CurveBrute.cpp:66-80)
-        float3 Q01 = xmid(s.P0, s.P1), Q12 = xmid(s.P1, s.P2), Q23 = xmid(s.P2, s.P3);
-        float3 R01 = xmid(Q01, Q12), R12 = xmid(Q12, Q23), M = xmid(R01, R12);
-        float hwMid = xmul(xadd(s.hw0, s.hw3), 0.5f);
-        float tsh = xmul(s.tscale, 0.5f);
-        st[sp++] = SubSeg{M, R12, Q23, s.P3, hwMid, s.hw3, xadd(s.toff, tsh), tsh, s.depth - 1};
-        st[sp++] = SubSeg{s.P0, Q01, R01, M, s.hw0, hwMid, s.toff, tsh, s.depth - 1};
+        const float3 Q01 = xmid(s.P0, s.P1), Q12 = xmid(s.P1, s.P2), Q23 = xmid(s.P2, s.P3);
+        const float3 R01 = xmid(Q01, Q12), R12 = xmid(Q12, Q23), M = xmid(R01, R12);
+        const float3 cq01 = project(fr, Q01), cr01 = project(fr, R01), cm = project(fr, M),
+                     cr12 = project(fr, R12), cq23 = project(fr, Q23);
+        const float hwMid = xmul(xadd(s.hw0, s.hw3), 0.5f);
+        const float tsh = xmul(s.tscale, 0.5f);
+        float zl, zr;
+        const bool okL = ribbon_bounds(s.c0, cq01, cr01, cm, s.hw0, hwMid, tmin, bestT, zl);
+        const bool okR = ribbon_bounds(cm, cr12, cq23, s.c3, hwMid, s.hw3, tmin, bestT, zr);
+        if (okR) st[sp++] = SubSeg{M, R12, Q23, s.P3, cm, s.c3, hwMid, s.hw3, xadd(s.toff, tsh), tsh, zr, s.depth - 1};
+        if (okL) st[sp++] = SubSeg{s.P0, Q01, R01, M, s.c0, cm, s.hw0, hwMid, s.toff, tsh, zl, s.depth - 1};
     }
     return hit;
 }
