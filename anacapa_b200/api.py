@@ -99,6 +99,11 @@ class AnaStats(C.Structure):
                 ("curve_node_fetches", C.c_uint64)]
 
 
+class AnaTile(C.Structure):
+    _fields_ = [("x0", C.c_uint32), ("y0", C.c_uint32), ("width", C.c_uint32), ("height", C.c_uint32),
+                ("sample_start", C.c_uint32), ("sample_count", C.c_uint32)]
+
+
 class AnaDiffParams(C.Structure):
     _fields_ = [("albedo", _P), ("roughness", _P), ("emission", _P), ("light_le", _P)]
 
@@ -119,7 +124,7 @@ EXPORTS = ["ana_create", "ana_destroy", "ana_upload_scene", "ana_prepare_scene",
            "ana_get_stats", "ana_last_error", "ana_version", "ana_batch_create", "ana_batch_free",
            "ana_batch_bytes", "ana_upload_batch", "ana_render_batch", "ana_batch_film_read",
            "ana_prepared_digest", "ana_trace_batch_noalloc", "ana_diff_counts", "ana_diff_get_params",
-           "ana_forward", "ana_backward"]
+           "ana_forward", "ana_backward", "ana_render_tiles", "ana_render_adaptive"]
 ANA_RENDER_GRAPH = 4
 
 _lib = None
@@ -168,6 +173,8 @@ def lib():
     L.ana_batch_film_read.argtypes = [_P, C.c_uint32, _P, C.c_size_t]
     L.ana_prepared_digest.argtypes = [_P]
     L.ana_prepared_digest.restype = C.c_uint64
+    L.ana_render_tiles.argtypes = [_P, C.POINTER(AnaRenderDesc), C.POINTER(AnaTile), C.c_uint32]
+    L.ana_render_adaptive.argtypes = [_P, C.POINTER(AnaRenderDesc), C.c_uint32, C.c_uint32, _P, C.c_uint32]
     L.ana_diff_counts.argtypes = [_P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
     L.ana_diff_get_params.argtypes = [_P, C.POINTER(AnaDiffParams)]
     L.ana_forward.argtypes = [_P, C.POINTER(AnaRenderDesc), C.POINTER(AnaDiffParams), _P]
@@ -359,6 +366,23 @@ class Renderer:
     def render_scene(self, sc: S.Scene, spp=None, clear=True, sample_start=0, seed=0, count_work=False):
         self.render(sc.width, sc.height, sc.spp if spp is None else spp, sc.max_depth,
                     sample_start=sample_start, seed=seed, clear=clear, count_work=count_work)
+
+    def render_tiles(self, width, height, max_depth, tiles, clear=False, min_depth=2, seed=0):
+        """ana_render_tiles: tiles = [(x0, y0, w, h, sample_start, sample_count), ...]
+        of one width x height frame, accumulated into the film."""
+        arr = (AnaTile * max(1, len(tiles)))(*[AnaTile(*map(int, t)) for t in tiles])
+        r = AnaRenderDesc(width, height, 0, 0, max_depth, min_depth, seed,
+                          ANA_RENDER_CLEAR_FILM if clear else 0)
+        self._check(lib().ana_render_tiles(self.h, C.byref(r), arr, len(tiles)))
+
+    def render_adaptive(self, width, height, spp, max_depth, tile_size=64, base_spp=0, min_depth=2, seed=0):
+        """ana_render_adaptive: the two-pass tile-adaptive schedule; returns the
+        extra samples given to each tile (row-major)."""
+        nt = (-(-width // tile_size)) * (-(-height // tile_size))
+        extra = np.zeros(nt, np.uint32)
+        r = AnaRenderDesc(width, height, 0, spp, max_depth, min_depth, seed, ANA_RENDER_CLEAR_FILM)
+        self._check(lib().ana_render_adaptive(self.h, C.byref(r), tile_size, base_spp, extra.ctypes.data, nt))
+        return extra
 
     def film(self, width, height) -> np.ndarray:
         """(H, W, 5) float32: pre-weighted r, g, b, weight, sum of lum^2."""

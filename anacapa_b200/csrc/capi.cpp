@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -469,25 +470,32 @@ int ensure_adjoint(ana_ctx* c, uint32_t cap) {
 // path-replay adjoint instead: per chunk a primal replay of the same paths
 // (their radiance L) and an adjoint replay that accumulates dLoss / d theta
 // into adj_grad (host, 8 floats per material then 4 per light).
-int render_items(ana_ctx* c, const ana_render_desc* descs, uint32_t n, uint32_t flags,
+// One render item: the pixels [x0, x0 + rw) x [y0, y0 + rh) of the width x
+// height film of uploaded scene `scene`, sample indices [sample_start,
+// sample_start + spp), accumulated at film_offset of the context's film. A
+// frame is one item covering its film; PathIntegrator::renderTile's tiles
+// are items that share one film.
+struct Item {
+    uint32_t scene, width, height, x0, y0, rw, rh, sample_start, spp, max_depth, min_depth;
+    uint64_t seed, film_offset;
+};
+
+// The batch render of `items` into a film of totalPixels pixels.
+int render_items(ana_ctx* c, const std::vector<Item>& items, uint64_t totalPixels, uint32_t flags,
                  const float* adj_image = nullptr, float* adj_grad = nullptr) {
     const bool backward = adj_image != nullptr;
     if (backward) flags &= ~uint32_t(ANA_RENDER_GRAPH | ANA_RENDER_COUNT_WORK);
-    if (!c || !descs || n == 0) return fail(c, ANA_ERR_INVALID_ARG, "ana_render: NULL argument or no items");
-    if (!c->has_scene) return fail(c, ANA_ERR_STATE, "ana_render: no scene uploaded");
-    if (n != c->scenes.size())
-        return fail(c, ANA_ERR_INVALID_ARG, "ana_render_batch: one desc per uploaded scene is required");
-    uint64_t totalPaths = 0, totalPixels = 0;
+    const uint32_t n = uint32_t(items.size());
+    if (n == 0) return fail(c, ANA_ERR_INVALID_ARG, "ana_render: no items");
+    uint64_t totalPaths = 0;
     uint32_t maxSpp = 0, maxDepth = 0;
-    for (uint32_t k = 0; k < n; ++k) {
-        const ana_render_desc& r = descs[k];
-        if (r.width == 0 || r.height == 0 || r.sample_count == 0)
+    for (const Item& it : items) {
+        if (it.rw == 0 || it.rh == 0 || it.spp == 0)
             return fail(c, ANA_ERR_INVALID_ARG, "ana_render: empty frame or zero samples");
-        if (r.max_depth > 255) return fail(c, ANA_ERR_INVALID_ARG, "ana_render: max_depth > 255");
-        totalPixels += uint64_t(r.width) * r.height;
-        totalPaths += uint64_t(r.width) * r.height * r.sample_count;
-        maxSpp = std::max(maxSpp, r.sample_count);
-        maxDepth = std::max(maxDepth, r.max_depth);
+        if (it.max_depth > 255) return fail(c, ANA_ERR_INVALID_ARG, "ana_render: max_depth > 255");
+        totalPaths += uint64_t(it.rw) * it.rh * it.spp;
+        maxSpp = std::max(maxSpp, it.spp);
+        maxDepth = std::max(maxDepth, it.max_depth);
     }
     if (totalPaths >= (1ull << 32))
         return fail(c, ANA_ERR_INVALID_ARG, "ana_render: total width*height*sample_count must be < 2^32");
@@ -519,15 +527,13 @@ int render_items(ana_ctx* c, const ana_render_desc* descs, uint32_t n, uint32_t 
     if (rc) return rc;
     if (c->film_pixels != totalPixels) flags |= ANA_RENDER_CLEAR_FILM;
     c->film_pixels = totalPixels;
-    c->item_film_offset.assign(n, 0);
-    c->item_film_pixels.assign(n, 0);
     // scene records, path offsets, chunk plan
     std::vector<ana::DevSceneRec> recs(n);
     std::vector<uint32_t> pathOff(n + 1, 0);
-    uint64_t pix = 0, path = 0;
+    uint64_t path = 0;
     for (uint32_t k = 0; k < n; ++k) {
-        const ana_render_desc& r = descs[k];
-        const SceneStatic& st = c->scenes[k];
+        const Item& r = items[k];
+        const SceneStatic& st = c->scenes[r.scene];
         ana::DevSceneRec& R = recs[k];
         std::memset(&R, 0, sizeof(R));
         R.tri_root = st.tri_root;
@@ -536,21 +542,22 @@ int render_items(ana_ctx* c, const ana_render_desc* descs, uint32_t n, uint32_t 
         R.num_slots = st.num_slots;
         R.light_base = st.light_base;
         R.num_lights = st.num_lights;
-        R.spp = r.sample_count;
+        R.spp = r.spp;
         R.sample_start = r.sample_start;
         R.max_depth = r.max_depth;
         R.min_depth = r.min_depth;
-        R.film_offset = uint32_t(pix);
+        R.film_offset = uint32_t(r.film_offset);
         R.path_offset = uint32_t(path);
         R.seed = r.seed;
         R.env_radiance = make_float3(st.env_radiance[0], st.env_radiance[1], st.env_radiance[2]);
         R.has_dome = st.has_dome ? 1 : 0;
         R.cam = ana::make_camera(st.camera, r.width, r.height);
-        c->item_film_offset[k] = pix;
-        c->item_film_pixels[k] = size_t(r.width) * r.height;
+        R.rect_x0 = r.x0;
+        R.rect_y0 = r.y0;
+        R.rect_w = r.rw;
+        R.film_w = r.width;
         pathOff[k] = uint32_t(path);
-        pix += uint64_t(r.width) * r.height;
-        path += uint64_t(r.width) * r.height * r.sample_count;
+        path += uint64_t(r.rw) * r.rh * r.spp;
     }
     pathOff[n] = uint32_t(path);
     // chunks: cut the global path space at pixel boundaries, `cap` paths each
@@ -560,8 +567,8 @@ int render_items(ana_ctx* c, const ana_render_desc* descs, uint32_t n, uint32_t 
         ChunkPlan cp{0, 0, 0, 0, 0};
         uint32_t gpath = 0;
         for (uint32_t k = 0; k < n; ++k) {
-            const uint32_t spp = descs[k].sample_count;
-            const uint32_t npx = descs[k].width * descs[k].height;
+            const uint32_t spp = items[k].spp;
+            const uint32_t npx = items[k].rw * items[k].rh;
             uint32_t px = 0;
             while (px < npx) {
                 uint32_t fit = std::min(npx - px, (cap - cp.paths) / spp);
@@ -820,6 +827,33 @@ int render_items(ana_ctx* c, const ana_render_desc* descs, uint32_t n, uint32_t 
     return ANA_OK;
 }
 
+// Whole frames: descs[k] renders uploaded scene k into its own film, the
+// films back to back.
+int render_descs(ana_ctx* c, const ana_render_desc* descs, uint32_t n, uint32_t flags,
+                 const float* adj_image = nullptr, float* adj_grad = nullptr) {
+    if (!c || !descs || n == 0) return fail(c, ANA_ERR_INVALID_ARG, "ana_render: NULL argument or no items");
+    if (!c->has_scene) return fail(c, ANA_ERR_STATE, "ana_render: no scene uploaded");
+    if (n != c->scenes.size())
+        return fail(c, ANA_ERR_INVALID_ARG, "ana_render_batch: one desc per uploaded scene is required");
+    std::vector<Item> items(n);
+    std::vector<size_t> offs(n), pixels(n);
+    uint64_t pix = 0;
+    for (uint32_t k = 0; k < n; ++k) {
+        const ana_render_desc& r = descs[k];
+        items[k] = Item{k, r.width, r.height, 0, 0, r.width, r.height, r.sample_start, r.sample_count,
+                        r.max_depth, r.min_depth, r.seed, pix};
+        offs[k] = pix;
+        pixels[k] = size_t(r.width) * r.height;
+        pix += uint64_t(r.width) * r.height;
+    }
+    const int rc = render_items(c, items, pix, flags, adj_image, adj_grad);
+    if (rc == ANA_OK) {
+        c->item_film_offset = offs;
+        c->item_film_pixels = pixels;
+    }
+    return rc;
+}
+
 // Writes differentiable parameters into the host material / light tables and
 // copies both tables to the device. Derived fields follow prepare_scene:
 // standard_surface alpha2 = max(1e-4, r^2)^2 and its roughness lobe flags.
@@ -1033,11 +1067,118 @@ int ana_render(ana_ctx* c, const ana_render_desc* r) {
     if (!c || !r) return fail(c, ANA_ERR_INVALID_ARG, "ana_render: NULL argument");
     if (c->has_scene && c->scenes.size() != 1)
         return fail(c, ANA_ERR_STATE, "ana_render: a batch is uploaded; use ana_render_batch");
-    return render_items(c, r, 1, r->flags);
+    return render_descs(c, r, 1, r->flags);
 }
 
 int ana_render_batch(ana_ctx* c, const ana_render_desc* descs, uint32_t count, uint32_t flags) {
-    return render_items(c, descs, count, flags);
+    return render_descs(c, descs, count, flags);
+}
+
+int ana_render_tiles(ana_ctx* c, const ana_render_desc* f, const ana_tile* tiles, uint32_t n) {
+    if (!c || !f || (!tiles && n)) return fail(c, ANA_ERR_INVALID_ARG, "ana_render_tiles: NULL argument");
+    if (!c->has_scene) return fail(c, ANA_ERR_STATE, "ana_render_tiles: no scene uploaded");
+    if (c->scenes.size() != 1)
+        return fail(c, ANA_ERR_UNSUPPORTED, "ana_render_tiles: tiles render one uploaded scene, not a batch");
+    const uint32_t W = f->width, H = f->height;
+    if (W == 0 || H == 0) return fail(c, ANA_ERR_INVALID_ARG, "ana_render_tiles: empty frame");
+    std::vector<uint8_t> cover(size_t(W) * H, 0);
+    std::vector<Item> items;
+    items.reserve(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        const ana_tile& t = tiles[i];
+        if (uint64_t(t.x0) + t.width > W || uint64_t(t.y0) + t.height > H)
+            return fail(c, ANA_ERR_INVALID_ARG, "ana_render_tiles: tile " + std::to_string(i) + " outside the frame");
+        if (t.width == 0 || t.height == 0 || t.sample_count == 0) continue;  // nothing to render
+        for (uint32_t y = t.y0; y < t.y0 + t.height; ++y)
+            for (uint32_t x = t.x0; x < t.x0 + t.width; ++x) {
+                uint8_t& m = cover[size_t(y) * W + x];
+                if (m) return fail(c, ANA_ERR_INVALID_ARG, "ana_render_tiles: tiles overlap");
+                m = 1;
+            }
+        items.push_back(Item{0, W, H, t.x0, t.y0, t.width, t.height, t.sample_start, t.sample_count, f->max_depth,
+                             f->min_depth, f->seed, 0});
+    }
+    const uint32_t flags = f->flags & (ANA_RENDER_CLEAR_FILM | ANA_RENDER_COUNT_WORK);
+    if (items.empty()) return (flags & ANA_RENDER_CLEAR_FILM) ? ana_film_clear(c, W, H) : ANA_OK;
+    const int rc = render_items(c, items, uint64_t(W) * H, flags);
+    if (rc == ANA_OK) {
+        c->item_film_offset.assign(1, 0);
+        c->item_film_pixels.assign(1, size_t(W) * H);
+    }
+    return rc;
+}
+
+int ana_render_adaptive(ana_ctx* c, const ana_render_desc* f, uint32_t ts, uint32_t baseSpp, uint32_t* extraOut,
+                        uint32_t extraCap) {
+    if (!c || !f) return fail(c, ANA_ERR_INVALID_ARG, "ana_render_adaptive: NULL argument");
+    if (ts == 0) return fail(c, ANA_ERR_INVALID_ARG, "ana_render_adaptive: tile_size is 0");
+    const uint32_t W = f->width, H = f->height, total = f->sample_count;
+    if (W == 0 || H == 0 || total == 0) return fail(c, ANA_ERR_INVALID_ARG, "ana_render_adaptive: empty frame");
+    uint32_t base = baseSpp > 0 ? baseSpp : std::min(32u, std::max(16u, total / 16));
+    base = std::min(base, total);
+    const uint32_t extra = total - base;
+    // scheduleTiles: row-major tiles of ts x ts pixels, clipped at the frame
+    std::vector<ana_tile> tiles;
+    for (uint32_t y = 0; y < H; y += ts)
+        for (uint32_t x = 0; x < W; x += ts) tiles.push_back(ana_tile{x, y, std::min(ts, W - x), std::min(ts, H - y), 0, 0});
+    const uint32_t nt = uint32_t(tiles.size());
+    // base pass over every pixel (the base tiles cover the frame exactly)
+    ana_render_desc b = *f;
+    b.sample_start = 0;
+    b.sample_count = base;
+    b.flags = ANA_RENDER_CLEAR_FILM;
+    int rc = render_descs(c, &b, 1, b.flags);
+    if (rc) return rc;
+    std::vector<uint32_t> extraPerTile(nt, 0);
+    if (extra > 0) {
+        std::vector<ana_film_pixel> px(size_t(W) * H);
+        CK(cudaMemcpyAsync(px.data(), c->film, px.size() * sizeof(ana_film_pixel), cudaMemcpyDeviceToHost,
+                           c->stream),
+           "film D2H");
+        CK(cudaStreamSynchronize(c->stream), "film D2H");
+        // Film::varianceAt: the mean luminance with Rec.709 weights against the
+        // sum of squared integrator luminances, both per unit weight
+        auto variance_at = [&](uint32_t x, uint32_t y) {
+            const ana_film_pixel& p = px[size_t(y) * W + x];
+            const float w = p.w;
+            if (w <= 0.f) return 0.f;
+            const float invW = 1.f / w;
+            const float meanL = (p.r * 0.2126f + p.g * 0.7152f + p.b * 0.0722f) * invW;
+            const float eLsq = p.sum_lum_sq * invW;
+            return std::max(0.f, eLsq - meanL * meanL);
+        };
+        std::vector<float> logWeight(nt);
+        for (uint32_t i = 0; i < nt; ++i) {
+            const ana_tile& t = tiles[i];
+            float sum = 0.f;
+            for (uint32_t ty = 0; ty < t.height; ++ty)
+                for (uint32_t tx = 0; tx < t.width; ++tx) sum += variance_at(t.x0 + tx, t.y0 + ty);
+            const float tileVar = sum / static_cast<float>(t.width * t.height);
+            logWeight[i] = std::log(1.f + tileVar);
+        }
+        float totalW = 0.f;
+        for (float v : logWeight) totalW += v;
+        const uint32_t uniformHalf = extra / 2, bonusHalf = extra - uniformHalf;
+        for (uint32_t i = 0; i < nt; ++i) {
+            uint32_t bonus = 0;
+            if (totalW > 1e-6f) {
+                const float frac = logWeight[i] / totalW;
+                bonus = static_cast<uint32_t>(std::round(frac * static_cast<float>(bonusHalf * nt)));
+            }
+            extraPerTile[i] = std::min(uniformHalf + bonus, extra);
+        }
+        for (uint32_t i = 0; i < nt; ++i) {
+            tiles[i].sample_start = base;
+            tiles[i].sample_count = extraPerTile[i];
+        }
+        ana_render_desc e = *f;
+        e.flags = 0;
+        rc = ana_render_tiles(c, &e, tiles.data(), nt);
+        if (rc) return rc;
+    }
+    if (extraOut)
+        for (uint32_t i = 0; i < std::min(nt, extraCap); ++i) extraOut[i] = extraPerTile[i];
+    return ANA_OK;
 }
 
 int ana_film_clear(ana_ctx* c, uint32_t w, uint32_t h) {
@@ -1227,7 +1368,7 @@ int ana_forward(ana_ctx* c, const ana_render_desc* d, const ana_diff_params* par
         if (rc) return rc;
     }
     const uint32_t flags = ANA_RENDER_CLEAR_FILM | (d->flags & ANA_RENDER_GRAPH);
-    int rc = render_items(c, d, 1, flags);
+    int rc = render_descs(c, d, 1, flags);
     if (rc) return rc;
     c->fwd_desc = *d;
     c->fwd_valid = true;
@@ -1251,7 +1392,7 @@ int ana_backward(ana_ctx* c, const float* d_image, ana_diff_params* out) {
     const size_t nm = c->h_mats.size(), nl = c->h_lights.size();
     std::vector<float> g(8 * nm + 4 * nl, 0.f);
     CK(cudaSetDevice(c->device), "cudaSetDevice");
-    int rc = render_items(c, &c->fwd_desc, 1, 0, d_image, g.data());
+    int rc = render_descs(c, &c->fwd_desc, 1, 0, d_image, g.data());
     if (rc) return rc;
     for (size_t i = 0; i < nm; ++i) {
         for (int ch = 0; ch < 3; ++ch) {

@@ -95,8 +95,15 @@ __device__ __forceinline__ void path_coords(const DevSceneRec& R, uint32_t gid, 
     uint32_t local = gid - R.path_offset;
     uint32_t pixel = local / R.spp;
     sidx = R.sample_start + (local - pixel * R.spp);
-    py = pixel / R.cam.width;
-    px = pixel - py * R.cam.width;
+    const uint32_t ly = pixel / R.rect_w;
+    px = R.rect_x0 + (pixel - ly * R.rect_w);
+    py = R.rect_y0 + ly;
+}
+
+// Film index of an item's pixel (its index within the item's rectangle).
+__device__ __forceinline__ size_t film_index(const DevSceneRec& R, uint32_t pixel) {
+    const uint32_t ly = pixel / R.rect_w;
+    return size_t(R.film_offset) + size_t(R.rect_y0 + ly) * R.film_w + R.rect_x0 + (pixel - ly * R.rect_w);
 }
 
 __device__ __forceinline__ void add_L(const Params& p, uint32_t gid, float3 v) {
@@ -675,7 +682,7 @@ __global__ void __launch_bounds__(256) k_adj_init(const __grid_constant__ Params
         const uint32_t pixel = (gid - R.path_offset) / R.spp;
         const float3 L = load3(p.a.Lp, i);
         float3 dl = f3(0.f, 0.f, 0.f);
-        if (is_finite3(L)) dl = load3(p.a.d_image, size_t(R.film_offset) + pixel) * (1.f / float(R.spp));
+        if (is_finite3(L)) dl = load3(p.a.d_image, film_index(R, pixel)) * (1.f / float(R.spp));
         p.a.dL[3 * size_t(i)] = dl.x;
         p.a.dL[3 * size_t(i) + 1] = dl.y;
         p.a.dL[3 * size_t(i) + 2] = dl.z;
@@ -771,7 +778,7 @@ __global__ void __launch_bounds__(256) k_film(const __grid_constant__ Params p) 
             }
         }
         const float invSPP = 1.f / float(spp);
-        ana_film_pixel& f = p.film[R.film_offset + sg.first_pixel + k];
+        ana_film_pixel& f = p.film[film_index(R, sg.first_pixel + k)];
         float w = float(spp);
         f.r += (acc.x * invSPP) * w;
         f.g += (acc.y * invSPP) * w;

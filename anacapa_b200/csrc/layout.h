@@ -124,6 +124,9 @@ struct DevSceneRec {
     float3 env_radiance;             // SceneView::envRadiance (no dome)
     uint32_t has_dome;
     DevCamera cam;                   // includes the film size
+    // The item's pixels: a rect_w-wide rectangle at (rect_x0, rect_y0) of a
+    // film_w-wide film (a TileRequest; a whole frame is the full rectangle).
+    uint32_t rect_x0, rect_y0, rect_w, film_w;
 };
 
 struct DevScene {

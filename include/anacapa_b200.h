@@ -330,6 +330,37 @@ int ana_trace_batch(ana_ctx* ctx, const float* rays, size_t n, ana_hit* out, int
 #define ANA_TRACE_NOALLOC_MAX_RAYS 65536
 int ana_trace_batch_noalloc(ana_ctx* ctx, const float* rays, size_t n, ana_hit* out, int occlusion_only);
 
+/* ---- tiles and adaptive sampling ------------------------------------------ */
+/* A tile of a frame (TileRequest, include/anacapa/integrator/IIntegrator.h):
+ * pixels [x0, x0 + width) x [y0, y0 + height), sample indices
+ * [sample_start, sample_start + sample_count). */
+typedef struct ana_tile {
+    uint32_t x0, y0, width, height;
+    uint32_t sample_start, sample_count;
+} ana_tile;
+
+/* PathIntegrator::renderTile (src/integrator/PathIntegrator.cpp:8-69) over n
+ * tiles of one frame, in one launch sequence, each merged into the frame's
+ * film as Film::mergeTile does (Film.cpp:34-73). frame gives the film size,
+ * depths and seed; its sample_start/sample_count are unused; with
+ * ANA_RENDER_CLEAR_FILM the film is cleared first. Tiles must lie inside the
+ * frame and must not overlap (ANA_ERR_INVALID_ARG). */
+int ana_render_tiles(ana_ctx* ctx, const ana_render_desc* frame, const ana_tile* tiles, uint32_t n);
+
+/* RenderSession::render's adaptive two-pass schedule for a tile-rendering
+ * integrator (src/render/RenderSession.cpp:548-653): tiles of tile_size
+ * pixels in row-major order (scheduleTiles, RenderSession.cpp:380-397); a base
+ * pass of base_spp samples per pixel (0: min(32, max(16, spp / 16)), at most
+ * spp); the mean Film::varianceAt (Film.cpp:80-90) of each tile; then every
+ * tile gets extra/2 + round(log(1 + var) / sum log(1 + var) * (extra - extra/2)
+ * * tiles) more samples (at most extra = spp - base), from sample index base.
+ * frame->sample_count is the total spp; the film is cleared first. When
+ * extra_out is not NULL it receives the extra samples of each tile
+ * (extra_capacity entries at most; the tile count is
+ * ceil(W / tile_size) * ceil(H / tile_size)). */
+int ana_render_adaptive(ana_ctx* ctx, const ana_render_desc* frame, uint32_t tile_size, uint32_t base_spp,
+                        uint32_t* extra_out, uint32_t extra_capacity);
+
 /* ---- differentiable rendering: path-replay adjoint ------------------------
  * A forward/backward pair with autograd-Function semantics over the uploaded
  * scene (one scene, not a batch). Parameters, by uploaded material index i
