@@ -45,7 +45,8 @@ class AnaMaterial(C.Structure):
 
 
 class AnaLight(C.Structure):
-    _fields_ = [("type", C.c_uint32), ("center", F3), ("u", F3), ("v", F3), ("Le", F3)]
+    _fields_ = [("type", C.c_uint32), ("center", F3), ("u", F3), ("v", F3), ("Le", F3),
+                ("half_angle_deg", C.c_float)]
 
 
 class AnaCamera(C.Structure):
@@ -265,6 +266,13 @@ class SceneDesc:
             l.u[:] = a.u
             l.v[:] = a.v
             l.Le[:] = a.Le
+            lights.append(l)
+        for a in sc.dir_lights:
+            l = AnaLight()
+            l.type = S.LIGHT_DIRECTIONAL
+            l.u[:] = a.direction
+            l.Le[:] = a.Le
+            l.half_angle_deg = a.half_angle_deg
             lights.append(l)
         if sc.dome_rgb is not None:
             l = AnaLight()

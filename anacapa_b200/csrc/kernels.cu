@@ -473,7 +473,7 @@ __global__ void __launch_bounds__(kMaxStageBlock) k_shade(const __grid_constant_
                                 float dist = length(dir);
                                 dir = dir * (1.f / dist);
                                 float3 org = spawn_origin(si.p, si.n, dir);
-                                float w = power_heuristic(ls.pdf, be.pdf);
+                                float w = ls.delta ? 1.f : power_heuristic(ls.pdf, be.pdf);
                                 float cosI;
                                 if (si.is_curve) {
                                     float dt = dot(ls.wi, c.t);
@@ -500,10 +500,17 @@ __global__ void __launch_bounds__(kMaxStageBlock) k_shade(const __grid_constant_
                                 }
                             }
                         }
-                        // BSDF sampling toward the light (non-delta lights)
-                        float uc = ss.next();
-                        float bu0 = ss.next(), bu1 = ss.next();
-                        BsdfSample bs = mat_sample<kFiber>(m, c, wo, bu0, bu1, uc);
+                        // BSDF sampling toward the light: non-delta lights only,
+                        // and only then are its sample dimensions drawn
+                        // (estimateDirect, PathIntegrator.cpp:210)
+                        const bool deltaLight = L.type == ANA_LIGHT_DIRECTIONAL;
+                        float uc = 0.f, bu0 = 0.f, bu1 = 0.f;
+                        if (!deltaLight) {
+                            uc = ss.next();
+                            bu0 = ss.next();
+                            bu1 = ss.next();
+                        }
+                        BsdfSample bs = deltaLight ? no_sample() : mat_sample<kFiber>(m, c, wo, bu0, bu1, uc);
                         if (bs.valid()) {
                             float lp = light_pdf(S, L, si.p, bs.wi);
                             if (lp > 0.f) {

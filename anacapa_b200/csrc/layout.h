@@ -82,7 +82,7 @@ struct DevLight {
     float3 center, u, v, normal, Le;
     float area;
     float uLen2, vLen2;  // |u|^2, |v|^2 as AreaLight::pdf computes them
-    float pad2;
+    float cos_cone;      // directional: cos of the angular radius (normal = direction to it)
 };
 
 // Equirect dome with its 2-D piecewise-constant distribution

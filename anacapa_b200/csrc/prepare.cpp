@@ -755,6 +755,12 @@ int prepare_scene(const ana_scene_desc& d, Prepared& P, std::string& err) {
         } else if (l.type == ANA_LIGHT_DOME) {
             if (hasDome) return bad("more than one dome light");
             hasDome = true;
+        } else if (l.type == ANA_LIGHT_DIRECTIONAL) {  // DirectionalLight.h:33-45
+            const V3 dir = safeNormalize(load3(l.u));
+            o.normal = make_float3(dir.x, dir.y, dir.z);
+            o.Le = make_float3(l.Le[0], l.Le[1], l.Le[2]);
+            const float kPi = 3.14159265358979323846f;
+            o.cos_cone = std::cos(l.half_angle_deg * kPi / 180.f);
         } else {
             return bad("unknown light type");
         }

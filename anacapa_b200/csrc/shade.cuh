@@ -652,6 +652,7 @@ __device__ __forceinline__ BsdfGrad mat_grad(const DevMaterial& m, const ShadeCt
 struct LightSample {
     float3 Li, wi;
     float pdf, dist;
+    bool delta;  // LightSample::isDelta: MIS weight 1
 };
 
 // Distribution1D::sample (DomeLight.h:167-181): lower_bound over the cdf.
@@ -785,11 +786,40 @@ __device__ __forceinline__ float area_pdf(const DevLight& L, float3 p, float3 wi
     return (t * t) / (denom * L.area);
 }
 
+// DirectionalLight::sample (DirectionalLight.h:52-78): the direction toward the
+// light, jittered inside its cone when it has an angular radius; pdf 1 and
+// delta either way, so Li / pdf = Le.
+__device__ __forceinline__ LightSample dir_sample(const DevLight& L, float ux, float uy) {
+    LightSample s;
+    s.Li = L.Le;
+    s.pdf = 1.f;
+    s.dist = 1e10f;
+    s.delta = true;
+    if (L.cos_cone >= 1.f - 1e-6f) {
+        s.wi = L.normal;
+    } else {
+        const float cosT = 1.f - ux * (1.f - L.cos_cone);
+        const float sinT = sqrtf(fmaxf(0.f, 1.f - cosT * cosT));
+        const float phi = 2.f * kPi * uy;
+        float sp, cp;
+        sincosf(phi, &sp, &cp);
+        float3 t, bt;
+        onb(L.normal, t, bt);
+        s.wi = safe_normalize(t * (sinT * cp) + bt * (sinT * sp) + L.normal * cosT);
+    }
+    return s;
+}
+
 __device__ __forceinline__ LightSample light_sample(const DevScene& S, const DevLight& L, float3 p, float ux,
                                                     float uy) {
-    return L.type == ANA_LIGHT_AREA ? area_sample(L, p, ux, uy) : env_sample(S.env, ux, uy);
+    if (L.type == ANA_LIGHT_DIRECTIONAL) return dir_sample(L, ux, uy);
+    LightSample s = L.type == ANA_LIGHT_AREA ? area_sample(L, p, ux, uy) : env_sample(S.env, ux, uy);
+    s.delta = false;
+    return s;
 }
+// ILight::pdf; a directional light is delta (DirectionalLight::pdf returns 0).
 __device__ __forceinline__ float light_pdf(const DevScene& S, const DevLight& L, float3 p, float3 wi) {
+    if (L.type == ANA_LIGHT_DIRECTIONAL) return 0.f;
     return L.type == ANA_LIGHT_AREA ? area_pdf(L, p, wi) : env_pdf(S.env, wi);
 }
 

@@ -20,6 +20,7 @@
 #include "shading/MarschnerHair.h"
 #include "shading/StandardSurface.h"
 #include "shading/lights/AreaLight.h"
+#include "shading/lights/DirectionalLight.h"
 #include "shading/lights/DomeLight.h"
 
 namespace anacapa_b200 {
@@ -219,6 +220,18 @@ bool flatten(const SceneView& scene, uint32_t width, uint32_t height, Flat& F, s
             area_axis(*a, false, al.u);
             area_axis(*a, true, al.v);
             put3(al.Le, a->sampleLe({0.5f, 0.5f}, {0.5f, 0.5f}).Le);
+        } else if (auto* sun = dynamic_cast<const DirectionalLight*>(l)) {
+            // DirectionalLight keeps its direction and cone private. sample()
+            // returns the direction itself for u.x = 0 (the whole cone
+            // collapses to it; for a hard light exactly, DirectionalLight.h:
+            // 60-62) and a direction on the cone's edge for u.x = 1.
+            const LightSample s0 = sun->sample({}, {}, {0.f, 0.f});
+            const LightSample s1 = sun->sample({}, {}, {1.f, 0.f});
+            const float c = std::min(1.f, dot(s0.wi, s1.wi));
+            al.type = ANA_LIGHT_DIRECTIONAL;
+            put3(al.u, s0.wi);
+            put3(al.Le, s0.Li);
+            al.half_angle_deg = c >= 1.f - 1e-6f ? 0.f : std::acos(c) * 180.f / 3.14159265358979323846f;
         } else if (auto* dl = dynamic_cast<const DomeLight*>(l)) {
             if (dl != dome) {
                 err = "a dome light in SceneView::lights must be SceneView::envLight";
@@ -226,7 +239,7 @@ bool flatten(const SceneView& scene, uint32_t width, uint32_t height, Flat& F, s
             }
             al.type = ANA_LIGHT_DOME;
         } else {
-            err = "unsupported light class (directional lights are not implemented)";
+            err = "unsupported light class";
             return false;
         }
         F.lights.push_back(al);

@@ -33,6 +33,7 @@ MAT_HAIR = 3
 
 LIGHT_AREA = 0
 LIGHT_DOME = 1
+LIGHT_DIRECTIONAL = 2
 
 
 @dataclasses.dataclass
@@ -78,6 +79,15 @@ class AreaLight:
 
 
 @dataclasses.dataclass
+class DirLight:
+    """DirectionalLight (src/shading/lights/DirectionalLight.h): direction
+    toward the light, radiance, angular radius in degrees (0: hard shadows)."""
+    direction: tuple
+    Le: tuple
+    half_angle_deg: float = 0.0
+
+
+@dataclasses.dataclass
 class Scene:
     name: str
     # meshes, concatenated: vertex/triangle ranges per mesh
@@ -114,6 +124,8 @@ class Scene:
     # each), apertureRadius, focalDistance, shutterOpen, shutterClose. None:
     # built from cam_from/cam_at/cam_up/vfov.
     cam_basis: Optional[tuple] = None
+    # SceneView::lights after the area lights, before the dome
+    dir_lights: List[DirLight] = dataclasses.field(default_factory=list)
 
     @property
     def num_meshes(self) -> int:
@@ -467,3 +479,42 @@ def perturbed_diff_params(seed=1):
     p["roughness"] = np.clip(p["roughness"] + rng.uniform(-0.15, 0.15, 6), 0.05, 1.0
                              ).astype(np.float32)
     return p
+
+
+def sunlit(width=256, height=192, spp=16, max_depth=8, half_angle_deg=0.0, n_spheres=12, seed=3) -> Scene:
+    """A ground quad and n_spheres subdivision-2 icospheres (standard_surface,
+    random base colour and roughness, a third metallic) lit by a
+    DirectionalLight (DirectionalLight.h; half_angle_deg 0: hard shadows, else a
+    soft cone) and a small area light, under a constant environment radiance.
+    Light selection alternates between a delta light (no BSDF-sampled MIS ray)
+    and an area light (with one)."""
+    rng = np.random.default_rng(seed)
+    b = _Builder()
+    mg = b.material(Material(MAT_LAMBERT, albedo=(0.5, 0.5, 0.5)))
+    # The ground rises 0.1 over its depth and the area light tilts by 0.02:
+    # an exactly level quad has a zero-thickness box once the reference's
+    # 1e-7 padding (BVHBackend.cpp, sahSplit) rounds away against |y| - |oy|,
+    # and its slab test then rejects every ray.
+    g, y0, y1 = 6.0, 0.0, 0.1
+    gn = np.array([0.0, 2.0 * g, -(y1 - y0)])
+    gn /= np.linalg.norm(gn)
+    b.quad([-g, y0, -g], [-g, y1, g], [g, y1, g], [g, y0, -g], gn, mg)
+    v, f = icosphere(2)
+    for _ in range(n_spheres):
+        m = b.material(Material(MAT_STANDARD, base_color=tuple(map(float, rng.uniform(0.1, 0.9, 3))),
+                                roughness=float(rng.uniform(0.1, 0.9)),
+                                metalness=float(rng.uniform() < 0.33)))
+        r = float(rng.uniform(0.3, 0.8))
+        c = np.array([rng.uniform(-3, 3), r + 0.05, rng.uniform(-3, 3)])
+        b.mesh(c + r * v, f, m, nrm=v)
+    le = (6.0, 5.0, 4.0)
+    ml = b.material(Material(MAT_EMISSIVE, albedo=(0.0, 0.0, 0.0), emission=le))
+    lc, lu, lv = np.array([2.0, 3.5, 1.0]), np.array([0.4, 0.0, 0.0]), np.array([0.0, 0.02, 0.3])
+    ln = np.cross(lu, lv)
+    ln /= np.linalg.norm(ln)
+    b.quad(lc - lu - lv, lc + lu - lv, lc + lu + lv, lc - lu + lv, ln, ml)
+    return b.scene("sunlit", area_lights=[AreaLight(tuple(lc), tuple(lu), tuple(lv), le)],
+                   dir_lights=[DirLight((-0.4, 0.8, -0.3), (3.0, 2.8, 2.5), half_angle_deg)],
+                   env_radiance=(0.05, 0.07, 0.1),
+                   cam_from=(0.0, 4.0, -9.0), cam_at=(0.0, 0.5, 0.0), cam_up=(0.0, 1.0, 0.0),
+                   vfov=45.0, width=width, height=height, spp=spp, max_depth=max_depth)

@@ -83,8 +83,11 @@ typedef struct ana_material {
 enum {
     ANA_LIGHT_AREA = 0,  /* AreaLight src/shading/lights/AreaLight.h:17-125: quad centre,
                             half-extent axes u and v, radiance Le                     */
-    ANA_LIGHT_DOME = 1   /* DomeLight src/shading/lights/DomeLight.h:205: the scene's
+    ANA_LIGHT_DOME = 1,  /* DomeLight src/shading/lights/DomeLight.h:205: the scene's
                             equirect environment (ana_scene_desc.env_*)               */
+    ANA_LIGHT_DIRECTIONAL = 2 /* DirectionalLight src/shading/lights/DirectionalLight.h:24-160:
+                            a delta light at infinity; u = direction toward the light,
+                            Le, half_angle_deg = angular radius (0: hard shadows)     */
 };
 
 typedef struct ana_light {
@@ -93,6 +96,7 @@ typedef struct ana_light {
     float u[3];
     float v[3];
     float Le[3];
+    float half_angle_deg;
 } ana_light;
 
 /* ---- camera (Camera, include/anacapa/integrator/IIntegrator.h:27-144) ------ */

@@ -38,6 +38,7 @@
 #include "shading/StandardSurface.h"
 #include "shading/Texture.h"
 #include "shading/lights/AreaLight.h"
+#include "shading/lights/DirectionalLight.h"
 #include "shading/lights/DomeLight.h"
 
 #include <chrono>
@@ -223,6 +224,14 @@ void ref_set_slot(void* sp, uint32_t slot, int matHandle) {
 int ref_light_area(void* sp, const float* c, const float* u, const float* v, const float* Le) {
     auto* s = static_cast<RefScene*>(sp);
     s->lights.push_back(std::make_unique<AreaLight>(v3(c), v3(u), v3(v), v3(Le)));
+    s->view.lights.push_back(s->lights.back().get());
+    return int(s->lights.size() - 1);
+}
+
+// DirectionalLight (its scene radius and centre only place BDPT's emission disk).
+int ref_light_directional(void* sp, const float* dir, const float* Le, float halfAngleDeg) {
+    auto* s = static_cast<RefScene*>(sp);
+    s->lights.push_back(std::make_unique<DirectionalLight>(v3(dir), v3(Le), 10.f, Vec3f{}, halfAngleDeg));
     s->view.lights.push_back(s->lights.back().get());
     return int(s->lights.size() - 1);
 }

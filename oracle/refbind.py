@@ -69,6 +69,7 @@ def lib(variant="record"):
     L.ref_mat_marschner.argtypes = [_P, C.c_float, _F, C.c_float, C.c_float, C.c_float]
     L.ref_set_slot.argtypes = [_P, C.c_uint32, C.c_int]
     L.ref_light_area.argtypes = [_P, _F, _F, _F, _F]
+    L.ref_light_directional.argtypes = [_P, _F, _F, C.c_float]
     L.ref_light_dome.argtypes = [_P, _F, C.c_uint32, C.c_uint32, C.c_float, C.c_int]
     L.ref_set_env_radiance.argtypes = [_P, _F]
     L.ref_set_camera.argtypes = [_P, _F, _F, _F, C.c_float, C.c_uint32, C.c_uint32]
@@ -154,6 +155,9 @@ class RefScene:
         for a in scene.area_lights:
             self.light_handles.append(L.ref_light_area(h, _fp(f32(a.center)), _fp(f32(a.u)),
                                                        _fp(f32(a.v)), _fp(f32(a.Le))))
+        for a in scene.dir_lights:
+            self.light_handles.append(L.ref_light_directional(h, _fp(f32(a.direction)), _fp(f32(a.Le)),
+                                                              float(a.half_angle_deg)))
         if scene.dome_rgb is not None:
             d = f32(scene.dome_rgb)
             self.light_handles.append(L.ref_light_dome(h, _fp(d), d.shape[1], d.shape[0],

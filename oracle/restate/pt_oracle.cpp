@@ -96,9 +96,10 @@ struct Mat {
 
 template <class T>
 struct Light {
-    int type = 0;  // 0 area, 1 dome
+    int type = 0;  // 0 area, 1 dome, 2 directional (n = direction toward it)
     V3<T> c, u, v, n, Le;
     T area = 1;
+    T cosCone = 1;
 };
 
 template <class T>
@@ -960,6 +961,26 @@ template <class T> T areaPdf(const Light<T>& L, V3<T> p, V3<T> wi) {  // AreaLig
 
 template <class T> T powerH(T f, T g) { return (f * f) / (f * f + g * g); }
 
+// DirectionalLight::sample (DirectionalLight.h:52-78): delta, pdf 1, the
+// direction toward the light jittered inside its cone when it has one.
+template <class T> LS<T> dirSample(const Light<T>& L, T ux, T uy) {
+    LS<T> ls;
+    ls.Li = L.Le;
+    ls.pdf = T(1);
+    ls.dist = T(1e10f);
+    if (L.cosCone >= T(1) - T(1e-6f)) {
+        ls.wi = L.n;
+    } else {
+        T ct = T(1) - ux * (T(1) - L.cosCone);
+        T st = std::sqrt(std::max(T(0), T(1) - ct * ct));
+        T phi = T(2) * kPi<T> * uy;
+        V3<T> t, bt;
+        onb(L.n, t, bt);
+        ls.wi = safeNormalize(t * (st * std::cos(phi)) + bt * (st * std::sin(phi)) + L.n * ct);
+    }
+    return ls;
+}
+
 template <class T> const Mat<T>* matOf(const Scene<T>& S, uint32_t slot) {
     if (slot >= S.slots.size() || S.slots[slot] < 0) return nullptr;
     return &S.mats[size_t(S.slots[slot])];
@@ -990,13 +1011,14 @@ V3<T> Li(const Scene<T>& S, Ray<T> r, Halton& smp, uint32_t maxDepth, uint32_t m
             V3<T> Ld;
             {
                 T a = u1(), b = u1();
-                LS<T> ls = lt.type == 0 ? areaSample(lt, si.p, a, b) : envSample(S, a, b);
+                LS<T> ls = lt.type == 0 ? areaSample(lt, si.p, a, b)
+                           : lt.type == 2 ? dirSample(lt, a, b) : envSample(S, a, b);
                 if (ls.pdf > T(0) && !ls.Li.black()) {
                     BE<T> be = matEval(*m, c, wo, ls.wi);
                     if (!be.f.black()) {
                         Ray<T> sr = spawnRayTo(si.p, si.n, si.p + ls.wi * ls.dist);
                         if (!trace(S, sr, true).hit) {
-                            T w = powerH(ls.pdf, be.pdf);
+                            T w = lt.type == 2 ? T(1) : powerH(ls.pdf, be.pdf);
                             T cosI = si.curve ? std::sqrt(std::max(T(0), T(1) - dot(ls.wi, c.t) * dot(ls.wi, c.t)))
                                               : std::abs(dot(ls.wi, si.n));
                             Ld = Ld + be.f * ls.Li * cosI * w / ls.pdf;
@@ -1004,7 +1026,7 @@ V3<T> Li(const Scene<T>& S, Ray<T> r, Halton& smp, uint32_t maxDepth, uint32_t m
                     }
                 }
             }
-            {
+            if (lt.type != 2) {  // BSDF sampling for non-delta lights only (PathIntegrator.cpp:210)
                 T uc = u1();  // right-to-left argument evaluation of sample(ctx, wo, get2D(), get1D())
                 T a = u1(), b = u1();
                 BS<T> bs = matSample(*m, c, wo, a, b, uc);
@@ -1161,13 +1183,14 @@ V3<T> LiGrad(const Scene<T>& S, Ray<T> r, Halton& smp, uint32_t maxDepth, PathGr
             V3<T> Ld;
             {
                 T a = u1(), b = u1();
-                LS<T> ls = lt.type == 0 ? areaSample(lt, si.p, a, b) : envSample(S, a, b);
+                LS<T> ls = lt.type == 0 ? areaSample(lt, si.p, a, b)
+                           : lt.type == 2 ? dirSample(lt, a, b) : envSample(S, a, b);
                 if (ls.pdf > T(0) && !ls.Li.black()) {
                     BE<T> be = matEval(*m, c, wo, ls.wi);
                     if (!be.f.black()) {
                         Ray<T> sr = spawnRayTo(si.p, si.n, si.p + ls.wi * ls.dist);
                         if (!trace(S, sr, true).hit) {
-                            T w = powerH(ls.pdf, be.pdf);
+                            T w = lt.type == 2 ? T(1) : powerH(ls.pdf, be.pdf);
                             T cosI = si.curve ? std::sqrt(std::max(T(0), T(1) - dot(ls.wi, c.t) * dot(ls.wi, c.t)))
                                               : std::abs(dot(ls.wi, si.n));
                             Ld = Ld + be.f * ls.Li * cosI * w / ls.pdf;
@@ -1186,7 +1209,7 @@ V3<T> LiGrad(const Scene<T>& S, Ray<T> r, Halton& smp, uint32_t maxDepth, PathGr
                     }
                 }
             }
-            {
+            if (lt.type != 2) {
                 T uc = u1();
                 T a = u1(), b = u1();
                 BS<T> bs = matSample(*m, c, wo, a, b, uc);
@@ -1582,6 +1605,21 @@ void po_light_area(void* p, const float* c, const float* u, const float* v, cons
         L.Le = ld<T>(Le);
         L.n = safeNormalize(cross(L.u, L.v));
         L.area = cross(L.u, L.v).length() * T(4);
+        S.lights.push_back(L);
+    };
+    if (h->precision == 64) add(h->d);
+    else add(h->f);
+}
+
+void po_light_directional(void* p, const float* dir, const float* Le, float halfAngleDeg) {
+    Handle* h = static_cast<Handle*>(p);
+    auto add = [&](auto& S) {
+        using T = std::decay_t<decltype(S.env[0])>;
+        Light<T> L;
+        L.type = 2;
+        L.n = safeNormalize(ld<T>(dir));
+        L.Le = ld<T>(Le);
+        L.cosCone = T(std::cos(halfAngleDeg * 3.14159265358979323846f / 180.f));
         S.lights.push_back(L);
     };
     if (h->precision == 64) add(h->d);

@@ -41,6 +41,7 @@ def lib():
         L.po_add_material.argtypes = [_P, C.c_int, _F, _F, _F, _F]
         L.po_set_slots.argtypes = [_P, _I32, C.c_uint32]
         L.po_light_area.argtypes = [_P, _F, _F, _F, _F]
+        L.po_light_directional.argtypes = [_P, _F, _F, C.c_float]
         L.po_light_dome.argtypes = [_P, _F, C.c_uint32, C.c_uint32, C.c_float]
         L.po_set_env_radiance.argtypes = [_P, _F]
         L.po_set_camera.argtypes = [_P, _F, _F, _F, C.c_float, C.c_uint32, C.c_uint32]
@@ -98,6 +99,8 @@ class PoScene:
         L.po_set_slots(h, slots.ctypes.data_as(_I32), len(slots))
         for a in scene.area_lights:
             L.po_light_area(h, _fp(f32(a.center)), _fp(f32(a.u)), _fp(f32(a.v)), _fp(f32(a.Le)))
+        for a in scene.dir_lights:
+            L.po_light_directional(h, _fp(f32(a.direction)), _fp(f32(a.Le)), float(a.half_angle_deg))
         if scene.dome_rgb is not None:
             d = f32(scene.dome_rgb)
             L.po_light_dome(h, _fp(d), d.shape[1], d.shape[0], scene.dome_intensity)

@@ -22,8 +22,9 @@ def dropin(gpu, ref_built):
 
 @pytest.mark.parametrize("make", [lambda: S.cornell(128, 128, 8),
                                   lambda: S.hair(96, 54, 4, 10, n_strands=5000),
-                                  lambda: S.throughput(96, 54, 4, 12, n_spheres=64)],
-                         ids=["cornell", "hair", "throughput_small"])
+                                  lambda: S.throughput(96, 54, 4, 12, n_spheres=64),
+                                  lambda: S.sunlit(96, 72, 8)],
+                         ids=["cornell", "hair", "throughput_small", "sunlit"])
 def test_dropin_matches_direct_render(dropin, make):
     sc = make()
     rs = dropin.RefScene(sc, variant="dropin")
@@ -37,5 +38,9 @@ def test_dropin_matches_direct_render(dropin, make):
     r.render_scene(sc)
     direct = r.image(sc.width, sc.height)
     r.close()
-    assert np.allclose(rgb, direct, rtol=1e-5, atol=1e-6), np.abs(rgb - direct).max()
+    # DirectionalLight normalises its direction in float and prepare
+    # normalises the probed direction again, one ulp away from the direct
+    # scene's single normalisation: that case gets a 1e-4 band.
+    tol = (1e-4, 1e-4) if sc.dir_lights else (1e-5, 1e-6)
+    assert np.allclose(rgb, direct, rtol=tol[0], atol=tol[1]), np.abs(rgb - direct).max()
     assert np.isfinite(var).all() and (var >= 0).all()

@@ -239,3 +239,18 @@ def test_restatement64_radiance_close(ref_built):
     from oracle import restatebind as P
     li = P.PoScene(S.cornell(), 64).li(GOLD["cornell_li_q"])
     assert np.max(np.abs(li - GOLD["cornell_li"])) < 1e-5 * max(1.0, float(np.abs(GOLD["cornell_li"]).max()))
+
+
+@pytest.mark.parametrize("half_angle", [0.0, 2.0], ids=["hard", "cone"])
+def test_restatement_directional_light_matches_reference(ref_built, half_angle):
+    """The restatement's DirectionalLight and its skipped BSDF-sampling branch
+    (PathIntegrator.cpp:210) against the reference built without FMA
+    contraction: per-sample radiance bit for bit."""
+    from oracle import restatebind as P
+    sc = S.sunlit(64, 48, 1, 8, half_angle_deg=half_angle)
+    rng = np.random.default_rng(11)
+    q = np.stack([rng.integers(0, sc.width, 300), rng.integers(0, sc.height, 300),
+                  rng.integers(0, 8, 300)], 1).astype(np.uint32)
+    ref = ref_built.RefScene(sc, variant="nocontract").li(q)
+    li = P.PoScene(sc, 32).li(q).astype(np.float32)
+    assert np.array_equal(li, ref)
