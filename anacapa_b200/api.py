@@ -41,7 +41,7 @@ class AnaMaterial(C.Structure):
                 ("coat", C.c_float), ("coat_roughness", C.c_float), ("transmission", C.c_float),
                 ("emission_weight", C.c_float), ("emission_color", F3), ("alpha_mask", C.c_uint32),
                 ("eta", C.c_float), ("sigma_a", F3), ("beta_m", C.c_float), ("beta_n", C.c_float),
-                ("alpha_deg", C.c_float), ("hair_mode", C.c_uint32)]
+                ("alpha_deg", C.c_float), ("hair_mode", C.c_uint32), ("opacity", C.c_float)]
 
 
 class AnaLight(C.Structure):
@@ -216,7 +216,8 @@ def material_struct(m: S.Material) -> AnaMaterial:
     s.transmission = m.transmission
     s.emission_weight = m.emission_w
     s.emission_color[:] = m.emission_color
-    s.alpha_mask = 0
+    s.alpha_mask = 1 if m.alpha_mask else 0
+    s.opacity = m.opacity
     s.eta = m.eta
     s.sigma_a[:] = m.sigma_a
     s.beta_m = m.beta_m

@@ -58,7 +58,7 @@ struct Blob {
     size_t o_tri_nodes = 0, o_tri_isect = 0, o_tri_shade = 0, o_seg_nodes = 0, o_segs = 0, o_scol = 0, o_mats = 0,
            o_slots = 0, o_lights = 0, o_env_rgb = 0, o_cf = 0, o_cc = 0, o_ci = 0, o_mf = 0, o_mc = 0;
     std::vector<SceneStatic> scenes;
-    bool has_curves = false, has_emitters = false;
+    bool has_curves = false, has_emitters = false, has_transmit = false;
     size_t n_mats = 0, n_lights = 0;
     ana::HostEnv env_meta;  // scalars only
     Blob() = default;
@@ -166,6 +166,7 @@ int build_blob(const ana::Prepared* const* list, uint32_t n, Blob& B, std::strin
     B.scenes.assign(n, SceneStatic{});
     B.has_curves = false;
     B.has_emitters = false;
+    B.has_transmit = false;
     for (uint32_t k = 0; k < n; ++k) {
         const ana::Prepared& P = *list[k];
         SceneStatic& st = B.scenes[k];
@@ -206,6 +207,7 @@ int build_blob(const ana::Prepared* const* list, uint32_t n, Blob& B, std::strin
         std::memcpy(st.env_radiance, P.env.radiance, sizeof(st.env_radiance));
         st.camera = P.camera;
         if (P.has_emitters) B.has_emitters = true;
+        if (P.has_transmit) B.has_transmit = true;
     }
     if (dome) {
         std::memcpy(B.mem + B.o_env_rgb, dome->env.rgb.data(), dome->env.rgb.size() * 4);
@@ -397,6 +399,7 @@ int upload_blob(ana_ctx* c, const Blob& B) {
     S.lights = reinterpret_cast<const ana::DevLight*>(b + B.o_lights);
     S.has_curves = B.has_curves ? 1 : 0;
     S.has_emitters = B.has_emitters ? 1 : 0;
+    S.has_transmit = B.has_transmit ? 1 : 0;
     S.has_fibers = S.has_curves;
     {
         const auto* mats = reinterpret_cast<const ana::DevMaterial*>(B.mem + B.o_mats);
@@ -855,24 +858,16 @@ int render_descs(ana_ctx* c, const ana_render_desc* descs, uint32_t n, uint32_t 
 }
 
 // Writes differentiable parameters into the host material / light tables and
-// copies both tables to the device. Derived fields follow prepare_scene:
-// standard_surface alpha2 = max(1e-4, r^2)^2 and its roughness lobe flags.
+// copies both tables to the device. Derived fields follow prepare_scene
+// (derive_standard: GGX alpha2, flags, isDelta).
 int apply_params(ana_ctx* c, const ana_diff_params* P) {
     const size_t nm = c->h_mats.size(), nl = c->h_lights.size();
     for (size_t i = 0; i < nm; ++i) {
         ana::DevMaterial& m = c->h_mats[i];
         if (P->albedo) m.albedo = make_float3(P->albedo[3 * i], P->albedo[3 * i + 1], P->albedo[3 * i + 2]);
         if (P->roughness && m.type == ANA_MAT_STANDARD) {
-            const float r = P->roughness[i];
-            const float a = std::max(1e-4f, r * r);
-            m.rough = r;
-            m.alpha2 = a * a;
-            uint32_t f = 16u;
-            if (r < 0.001f) f |= 4u;
-            else if (r < 0.3f) f |= 2u;
-            else f |= 1u;
-            m.flags = f;
-            m.is_delta = (r < 0.001f && (m.metal > 0.999f || m.spec > 0.f)) ? 1 : 0;
+            m.rough = P->roughness[i];
+            ana::derive_standard(m);
         }
         if (P->emission && m.type == ANA_MAT_EMISSIVE)
             m.emission = make_float3(P->emission[3 * i], P->emission[3 * i + 1], P->emission[3 * i + 2]);
@@ -1361,6 +1356,9 @@ int ana_forward(ana_ctx* c, const ana_render_desc* d, const ana_diff_params* par
         return fail(c, ANA_ERR_UNSUPPORTED, "ana_forward: differentiable rendering takes one uploaded scene");
     if (c->h_mats.size() >= 0xFFFF || c->h_lights.size() >= 0xFFFF)
         return fail(c, ANA_ERR_UNSUPPORTED, "ana_forward: more than 65534 materials or lights");
+    for (const ana::DevMaterial& m : c->h_mats)
+        if (m.transmission > 0.001f || m.opacity < 1.f || m.tint.x != 0.f || m.tint.y != 0.f || m.tint.z != 0.f)
+            return fail(c, ANA_ERR_UNSUPPORTED, "ana_forward: glass and alpha-masked materials are not differentiated");
     CK(cudaSetDevice(c->device), "cudaSetDevice");
     c->fwd_valid = false;
     if (params) {

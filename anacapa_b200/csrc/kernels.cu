@@ -244,18 +244,22 @@ __device__ __forceinline__ void run_traversal(const DevScene& S, uint32_t n, uin
             Traversal T;
             trav_init(T, ray, root);
             while (true) {
-                while (!T.exhausted) {
-                    if (!(T.cur & 0x80000000u)) {
-                        node_step<kAny, kCount, kCurves>(T, S, stack, stackT, err, cnt);
-                    } else if (leaf_step<kAny, kCount, kCurves>(T, S, T.cur, cnt)) {
-                        T.exhausted = true;
-                    } else if (!trav_pop(T, stack, stackT)) {
-                        T.exhausted = true;
+                while (true) {
+                    while (!T.exhausted) {
+                        if (!(T.cur & 0x80000000u)) {
+                            node_step<kAny, kCount, kCurves>(T, S, stack, stackT, err, cnt);
+                        } else if (leaf_step<kAny, kCount, kCurves>(T, S, T.cur, cnt)) {
+                            T.exhausted = true;
+                        } else if (!trav_pop(T, stack, stackT)) {
+                            T.exhausted = true;
+                        }
                     }
+                    if (stage_done<kAny, kCurves>(T, ray.d, segRoot)) break;
                 }
-                if (stage_done<kAny, kCurves>(T, ray.d, segRoot)) break;
+                Ray next;
+                if (!trace_again(done, i, T, next)) break;
+                trav_init(T, next, root);
             }
-            done(i, T);
         }
     }
 }
@@ -339,6 +343,13 @@ __device__ __forceinline__ SurfInt surf_int(const DevScene& S, float3 o, float3 
 // SceneView::materials[meshID] of a scene (-1: no material).
 __device__ __forceinline__ int slot_material(const DevScene& S, const DevSceneRec& R, uint32_t slot) {
     return slot < R.num_slots ? __ldg(S.slot_material + R.slot_base + slot) : -1;
+}
+
+// Mesh or strand slot (SurfaceInteraction::meshID) of a hit primitive.
+__device__ __forceinline__ uint32_t hit_slot(const DevScene& S, uint32_t prim) {
+    if (prim & 0x80000000u) return __float_as_uint(ldg4(S.segs + 5 * size_t(prim & 0x7FFFFFFFu) + 4).z);
+    const uint32_t orig = __float_as_uint(ldg4(S.tri_isect + 3 * size_t(prim)).w);
+    return __float_as_uint(ldg4(S.tri_shade + 4 * size_t(orig)).w);
 }
 
 // Environment radiance seen along a direction that leaves the scene.
@@ -445,126 +456,145 @@ __global__ void __launch_bounds__(kMaxStageBlock) k_shade(const __grid_constant_
                     uint32_t px, py, sidx;
                     path_coords(R, pid, px, py, sidx);
                     SampleStream ss{R.seed, px, py, sidx, meta >> 16};
-                    float3 wo = -d;
-                    ShadeCtx c = make_ctx(si, d);
-                    float3 Le = mat_le(m);
-                    if (!is_black(Le) && (bounce == 0 || spec)) Ladd = Ladd + beta * Le;
-                    if constexpr (kAdj) {
-                        if (adj && m.type == ANA_MAT_EMISSIVE && (bounce == 0 || spec)) {
-                            const float3 ge = delta * beta;
-                            keyEmit = 8u * uint32_t(mi) + 4u;
-                            vEmit[0] = ge.x;
-                            vEmit[1] = ge.y;
-                            vEmit[2] = ge.z;
-                        }
-                    }
-                    if (!m.is_delta && nL > 0) {
-                        float ul = ss.next();
-                        uint32_t lidx = min(uint32_t(ul * float(nL)), nL - 1u);
-                        const DevLight L = S.lights[R.light_base + lidx];
-                        // light sampling
-                        float lu0 = ss.next(), lu1 = ss.next();
-                        LightSample ls = light_sample(S, L, si.p, lu0, lu1);
-                        if (ls.pdf > 0.f && !is_black(ls.Li)) {
-                            BsdfEval be = mat_eval<kFiber>(m, c, wo, ls.wi);
-                            if (!is_black(be.f)) {
-                                float3 target = si.p + ls.wi * ls.dist;
-                                float3 dir = target - si.p;
-                                float dist = length(dir);
-                                dir = dir * (1.f / dist);
-                                float3 org = spawn_origin(si.p, si.n, dir);
-                                float w = ls.delta ? 1.f : power_heuristic(ls.pdf, be.pdf);
-                                float cosI;
-                                if (si.is_curve) {
-                                    float dt = dot(ls.wi, c.t);
-                                    cosI = sqrtf(fmaxf(0.f, 1.f - dt * dt));
-                                } else {
-                                    cosI = absdot(ls.wi, si.n);
-                                }
-                                float3 contrib = beta * (be.f * ls.Li * cosI * w / ls.pdf) * float(nL);
-                                pushSh = true;
-                                shO = pack_u(org, pid);
-                                shD = pack(dir, dist * (1.f - 1e-4f));
-                                shC = pack_u(contrib, sc);
-                                if constexpr (kAdj) {
-                                    // contrib = beta * f * Li * s, s = cosI w nL / pdf
-                                    const float s = cosI * w / ls.pdf * float(nL);
-                                    const BsdfGrad g = mat_grad<kFiber>(m, c, wo, ls.wi);
-                                    const float3 db = delta * beta * s;
-                                    const float3 ga = db * g.dfda * ls.Li;
-                                    const bool area = adj && L.type == ANA_LIGHT_AREA;
-                                    const float3 gl = area ? db * be.f : f3(0.f, 0.f, 0.f);
-                                    const uint32_t lid = area ? R.light_base + lidx : 0xFFFFu;
-                                    shG0 = make_float4(ga.x, ga.y, ga.z, sum3(db * g.dfdr * ls.Li));
-                                    shG1 = pack_u(gl, (adj ? uint32_t(mi) : 0xFFFFu) | (lid << 16));
-                                }
-                            }
-                        }
-                        // BSDF sampling toward the light: non-delta lights only,
-                        // and only then are its sample dimensions drawn
-                        // (estimateDirect, PathIntegrator.cpp:210)
-                        const bool deltaLight = L.type == ANA_LIGHT_DIRECTIONAL;
-                        float uc = 0.f, bu0 = 0.f, bu1 = 0.f;
-                        if (!deltaLight) {
-                            uc = ss.next();
-                            bu0 = ss.next();
-                            bu1 = ss.next();
-                        }
-                        BsdfSample bs = deltaLight ? no_sample() : mat_sample<kFiber>(m, c, wo, bu0, bu1, uc);
-                        if (bs.valid()) {
-                            float lp = light_pdf(S, L, si.p, bs.wi);
-                            if (lp > 0.f) {
-                                float w = bs.delta() ? 1.f : power_heuristic(bs.pdf, lp);
-                                float3 org = spawn_origin(si.p, si.ng, bs.wi);
-                                float cosI = absdot(bs.wi, si.n);
-                                float3 contrib = beta * (bs.f * cosI * w / bs.pdf) * float(nL);
-                                pushMis = true;
-                                mO = pack_u(org, pid);
-                                mD = pack(bs.wi, 0.f);
-                                mC = pack_u(contrib, sc);
-                                if constexpr (kAdj) {
-                                    // bs.f = f |cos wi|: K = beta * f * |cos wi| * cosI w nL / pdf
-                                    const BsdfGrad g = mat_grad<kFiber>(m, c, wo, bs.wi);
-                                    const float s = fabsf(c.to_local(bs.wi).z) * cosI * w / bs.pdf * float(nL);
-                                    const float3 db = delta * beta * s;
-                                    mG0 = pack_u(db * g.dfda, adj ? uint32_t(mi) : kNoKey);
-                                    mG1 = pack(db * g.dfdr, 0.f);
-                                }
-                            }
-                        }
-                    }
-                    // continuation
-                    float uc = ss.next();
-                    float u0 = ss.next(), u1 = ss.next();
-                    BsdfSample bs = mat_sample<kFiber>(m, c, wo, u0, u1, uc);
-                    if (bs.valid()) {
-                        spec = bs.delta();
-                        beta = beta * (bs.f / bs.pdf);
-                        float3 org = spawn_origin(si.p, si.n, bs.wi);
-                        bool alive = true;
-                        if (bounce >= R.min_depth) {
-                            float q = 1.f - fminf(max_comp(beta), 0.95f);
-                            if (ss.next() < q) alive = false;
-                            else beta = beta * (1.f / (1.f - q));
-                        }
-                        if (alive && bounce + 1u <= R.max_depth) {
+                    // alpha test (PathIntegrator.cpp:103-118): a cut-out point
+                    // continues the ray unshaded, one bounce later, drawing a
+                    // sample dimension only for partial opacity
+                    bool cut = false;
+                    if (m.opacity < 1.f) cut = m.opacity <= 0.f || ss.next() >= m.opacity;
+                    if (cut) {
+                        if (bounce + 1u <= R.max_depth) {
                             pushExt = true;
-                            uint32_t nm = (bounce + 1u) | (spec ? 0x100u : 0u) | (ss.dim << 16);
-                            eO = pack_u(org, pid);
-                            eD = pack_u(bs.wi, nm);
+                            const uint32_t nm = (bounce + 1u) | (spec ? 0x100u : 0u) | (ss.dim << 16);
+                            eO = pack_u(spawn_origin(si.p, si.ng, d), pid);
+                            eD = pack_u(d, nm);
                             eB = pack_u(beta, sc);
                             if constexpr (kAdj) {
-                                // beta' = beta * f |cos| / pdf (pdf and roulette detached):
-                                // d log beta' / d theta = (d f / d theta) / f per channel
-                                const BsdfGrad g = mat_grad<kFiber>(m, c, wo, bs.wi);
-                                auto ratio = [](float num, float den) { return den > 0.f ? num / den : 0.f; };
-                                const float3 la = f3(ratio(g.dfda.x, g.f.x), ratio(g.dfda.y, g.f.y),
-                                                     ratio(g.dfda.z, g.f.z));
-                                const float3 lr = f3(ratio(g.dfdr.x, g.f.x), ratio(g.dfdr.y, g.f.y),
-                                                     ratio(g.dfdr.z, g.f.z));
-                                const bool any = adj && (!is_black(la) || !is_black(lr));
-                                eG0 = pack_u(la, any ? uint32_t(mi) : kNoKey);
-                                eG1 = pack(lr, 0.f);
+                                eG0 = make_float4(0.f, 0.f, 0.f, __uint_as_float(kNoKey));
+                                eG1 = make_float4(0.f, 0.f, 0.f, 0.f);
+                            }
+                        }
+                    } else {
+                        float3 wo = -d;
+                        ShadeCtx c = make_ctx(si, d);
+                        float3 Le = mat_le(m);
+                        if (!is_black(Le) && (bounce == 0 || spec)) Ladd = Ladd + beta * Le;
+                        if constexpr (kAdj) {
+                            if (adj && m.type == ANA_MAT_EMISSIVE && (bounce == 0 || spec)) {
+                                const float3 ge = delta * beta;
+                                keyEmit = 8u * uint32_t(mi) + 4u;
+                                vEmit[0] = ge.x;
+                                vEmit[1] = ge.y;
+                                vEmit[2] = ge.z;
+                            }
+                        }
+                        if (!m.is_delta && nL > 0) {
+                            float ul = ss.next();
+                            uint32_t lidx = min(uint32_t(ul * float(nL)), nL - 1u);
+                            const DevLight L = S.lights[R.light_base + lidx];
+                            // light sampling
+                            float lu0 = ss.next(), lu1 = ss.next();
+                            LightSample ls = light_sample(S, L, si.p, lu0, lu1);
+                            if (ls.pdf > 0.f && !is_black(ls.Li)) {
+                                BsdfEval be = mat_eval<kFiber>(m, c, wo, ls.wi);
+                                if (!is_black(be.f)) {
+                                    float3 target = si.p + ls.wi * ls.dist;
+                                    float3 dir = target - si.p;
+                                    float dist = length(dir);
+                                    dir = dir * (1.f / dist);
+                                    float3 org = spawn_origin(si.p, si.n, dir);
+                                    float w = ls.delta ? 1.f : power_heuristic(ls.pdf, be.pdf);
+                                    float cosI;
+                                    if (si.is_curve) {
+                                        float dt = dot(ls.wi, c.t);
+                                        cosI = sqrtf(fmaxf(0.f, 1.f - dt * dt));
+                                    } else {
+                                        cosI = absdot(ls.wi, si.n);
+                                    }
+                                    float3 contrib = beta * (be.f * ls.Li * cosI * w / ls.pdf) * float(nL);
+                                    pushSh = true;
+                                    shO = pack_u(org, pid);
+                                    shD = pack(dir, dist * (1.f - 1e-4f));
+                                    shC = pack_u(contrib, sc);
+                                    if constexpr (kAdj) {
+                                        // contrib = beta * f * Li * s, s = cosI w nL / pdf
+                                        const float s = cosI * w / ls.pdf * float(nL);
+                                        const BsdfGrad g = mat_grad<kFiber>(m, c, wo, ls.wi);
+                                        const float3 db = delta * beta * s;
+                                        const float3 ga = db * g.dfda * ls.Li;
+                                        const bool area = adj && L.type == ANA_LIGHT_AREA;
+                                        const float3 gl = area ? db * be.f : f3(0.f, 0.f, 0.f);
+                                        const uint32_t lid = area ? R.light_base + lidx : 0xFFFFu;
+                                        shG0 = make_float4(ga.x, ga.y, ga.z, sum3(db * g.dfdr * ls.Li));
+                                        shG1 = pack_u(gl, (adj ? uint32_t(mi) : 0xFFFFu) | (lid << 16));
+                                    }
+                                }
+                            }
+                            // BSDF sampling toward the light: non-delta lights only,
+                            // and only then are its sample dimensions drawn
+                            // (estimateDirect, PathIntegrator.cpp:210)
+                            const bool deltaLight = L.type == ANA_LIGHT_DIRECTIONAL;
+                            float uc = 0.f, bu0 = 0.f, bu1 = 0.f;
+                            if (!deltaLight) {
+                                uc = ss.next();
+                                bu0 = ss.next();
+                                bu1 = ss.next();
+                            }
+                            BsdfSample bs = deltaLight ? no_sample() : mat_sample<kFiber>(m, c, wo, bu0, bu1, uc);
+                            if (bs.valid()) {
+                                float lp = light_pdf(S, L, si.p, bs.wi);
+                                if (lp > 0.f) {
+                                    float w = bs.delta() ? 1.f : power_heuristic(bs.pdf, lp);
+                                    float3 org = spawn_origin(si.p, si.ng, bs.wi);
+                                    float cosI = absdot(bs.wi, si.n);
+                                    float3 contrib = beta * (bs.f * cosI * w / bs.pdf) * float(nL);
+                                    pushMis = true;
+                                    mO = pack_u(org, pid);
+                                    mD = pack(bs.wi, 0.f);
+                                    mC = pack_u(contrib, sc);
+                                    if constexpr (kAdj) {
+                                        // bs.f = f |cos wi|: K = beta * f * |cos wi| * cosI w nL / pdf
+                                        const BsdfGrad g = mat_grad<kFiber>(m, c, wo, bs.wi);
+                                        const float s = fabsf(c.to_local(bs.wi).z) * cosI * w / bs.pdf * float(nL);
+                                        const float3 db = delta * beta * s;
+                                        mG0 = pack_u(db * g.dfda, adj ? uint32_t(mi) : kNoKey);
+                                        mG1 = pack(db * g.dfdr, 0.f);
+                                    }
+                                }
+                            }
+                        }
+                        // continuation
+                        float uc = ss.next();
+                        float u0 = ss.next(), u1 = ss.next();
+                        BsdfSample bs = mat_sample<kFiber>(m, c, wo, u0, u1, uc);
+                        if (bs.valid()) {
+                            spec = bs.delta();
+                            beta = beta * (bs.f / bs.pdf);
+                            float3 org = spawn_origin(si.p, si.n, bs.wi);
+                            bool alive = true;
+                            if (bounce >= R.min_depth) {
+                                float q = 1.f - fminf(max_comp(beta), 0.95f);
+                                if (ss.next() < q) alive = false;
+                                else beta = beta * (1.f / (1.f - q));
+                            }
+                            if (alive && bounce + 1u <= R.max_depth) {
+                                pushExt = true;
+                                uint32_t nm = (bounce + 1u) | (spec ? 0x100u : 0u) | (ss.dim << 16);
+                                eO = pack_u(org, pid);
+                                eD = pack_u(bs.wi, nm);
+                                eB = pack_u(beta, sc);
+                                if constexpr (kAdj) {
+                                    // beta' = beta * f |cos| / pdf (pdf and roulette detached):
+                                    // d log beta' / d theta = (d f / d theta) / f per channel
+                                    const BsdfGrad g = mat_grad<kFiber>(m, c, wo, bs.wi);
+                                    auto ratio = [](float num, float den) { return den > 0.f ? num / den : 0.f; };
+                                    const float3 la = f3(ratio(g.dfda.x, g.f.x), ratio(g.dfda.y, g.f.y),
+                                                         ratio(g.dfda.z, g.f.z));
+                                    const float3 lr = f3(ratio(g.dfdr.x, g.f.x), ratio(g.dfdr.y, g.f.y),
+                                                         ratio(g.dfdr.z, g.f.z));
+                                    const bool any = adj && (!is_black(la) || !is_black(lr));
+                                    eG0 = pack_u(la, any ? uint32_t(mi) : kNoKey);
+                                    eG1 = pack(lr, 0.f);
+                                }
                             }
                         }
                     }
@@ -664,18 +694,136 @@ __global__ void ANA_TRAVERSAL_BOUNDS k_mis(const __grid_constant__ Params p) {
                 if (h.prim == kMiss) {
                     Li = scene_env(S, R, rd);
                 } else {
-                    uint32_t slot;
-                    if (h.prim & 0x80000000u)
-                        slot = __float_as_uint(ldg4(S.segs + 5 * size_t(h.prim & 0x7FFFFFFFu) + 4).z);
-                    else
-                        slot = __float_as_uint(ldg4(S.tri_shade + 4 * size_t(__float_as_uint(
-                                                                       ldg4(S.tri_isect + 3 * size_t(h.prim)).w))).w);
-                    mi = slot_material(S, R, slot);
+                    mi = slot_material(S, R, hit_slot(S, h.prim));
                     Li = mi >= 0 ? mat_le(S.materials[mi]) : f3(0.f, 0.f, 0.f);
                 }
             }
             if (!is_black(Li)) add_L(p, __float_as_uint(o.w), f3(c) * Li);
             if constexpr (kAdj) p.a.mis_res[i] = pack_u(Li, mi >= 0 ? uint32_t(mi) : kNoKey);
+        });
+}
+
+// Rays that step through transmissive surfaces (batches whose materials
+// include glass or alpha masks). Each lane keeps its entry's step state: the
+// product of the tints passed, the current origin and tMax, and the surfaces
+// passed. A transmissive closest hit multiplies the tint in and, unless less
+// than 1e-4 of the distance remains or 8 surfaces have been traced, the ray
+// is traced again from spawnRay(p, ng, d) with tMax = remaining - 1e-4.
+struct StepState {
+    float3 tr, org;
+    float tmax;
+    uint32_t steps;
+    bool fresh;
+    __device__ void begin(float3 o, float tm) {
+        if (!fresh) return;
+        tr = f3(1.f, 1.f, 1.f);
+        org = o;
+        tmax = tm;
+        steps = 0;
+        fresh = false;
+    }
+    // After a transmissive hit with tr still non-black: true (and `next`) if
+    // the ray continues past the surface.
+    template <bool kCurves>
+    __device__ bool advance(const DevScene& S, const SceneHit& h, float3 d, bool& tooClose, Ray& next) {
+        const float remaining = tmax - h.t;
+        tooClose = remaining <= 1e-4f;
+        if (tooClose || steps >= 7u) return false;
+        const float4 h1 = make_float4(h.tang.x, h.tang.y, h.tang.z, h.tseg);
+        const SurfInt si = surf_int<kCurves>(S, org, d, h.t, h.prim, h.u, h.v, h1);
+        next = Ray{spawn_origin(si.p, si.ng, d), d, 1e-4f, remaining - 1e-4f};
+        org = next.o;
+        tmax = next.tmax;
+        ++steps;
+        return true;
+    }
+};
+
+// NEE shadow rays with transmissive surfaces: shadowTransmittance
+// (src/integrator/ShadowRay.h:26-61) — an opaque surface (black
+// transmittanceColor) blocks, glass and alpha-masked surfaces tint; after 8
+// surfaces the tint so far is returned.
+template <bool kCurves, bool kPersist>
+__global__ void ANA_TRAVERSAL_BOUNDS k_shadow_step(const __grid_constant__ Params p) {
+    uint32_t* cb = p.counters + p.bounce * kCountersPerBounce;
+    const DevScene& S = p.S;
+    StepState st;
+    st.fresh = true;
+    run_traversal<false, false, kPersist, kCurves>(
+        S, cb[1], cb + 4, p.err, nullptr,
+        [&](uint32_t i, Ray& r, uint32_t& root, uint32_t& segRoot) {
+            float4 o = p.q.sh_o[i], d = p.q.sh_d[i];
+            r = Ray{f3(o), f3(d), 1e-4f, d.w};
+            st.begin(r.o, r.tmax);
+            const DevSceneRec& R = S.scenes[scene_bits(p.q.sh_c[i].w)];
+            root = R.tri_root;
+            segRoot = kCurves ? R.seg_root : kNoRoot;
+        },
+        [&](uint32_t i, const Traversal& T, Ray& next) -> bool {
+            const float4 c = p.q.sh_c[i];
+            const SceneHit h = finish_closest<kCurves>(T, st.tmax);
+            bool lit = true;
+            if (h.prim != kMiss) {
+                const DevSceneRec& R = S.scenes[scene_bits(c.w)];
+                const int mi = slot_material(S, R, hit_slot(S, h.prim));
+                const float3 tint = mi >= 0 ? S.materials[mi].tint : f3(0.f, 0.f, 0.f);
+                st.tr = st.tr * tint;
+                lit = !is_black(tint) && !is_black(st.tr);
+                bool tooClose;
+                if (lit && st.advance<kCurves>(S, h, f3(p.q.sh_d[i]), tooClose, next)) return true;
+            }
+            if (lit) add_L(p, __float_as_uint(p.q.sh_o[i].w), f3(c) * st.tr);
+            st.fresh = true;
+            return false;
+        });
+}
+
+// BSDF-sampled MIS rays with transmissive surfaces (PathIntegrator.cpp:
+// 214-259): the first non-transmissive surface within 1e10 (or the 8th
+// transmissive one) gives Le, a miss or a last step closer than 1e-4 the
+// environment, times the tint of the surfaces passed.
+template <bool kCurves, bool kPersist>
+__global__ void ANA_TRAVERSAL_BOUNDS k_mis_step(const __grid_constant__ Params p) {
+    uint32_t* cb = p.counters + p.bounce * kCountersPerBounce;
+    const DevScene& S = p.S;
+    StepState st;
+    st.fresh = true;
+    run_traversal<false, false, kPersist, kCurves>(
+        S, cb[2], cb + 5, p.err, nullptr,
+        [&](uint32_t i, Ray& r, uint32_t& root, uint32_t& segRoot) {
+            float4 o = p.q.mis_o[i], d = p.q.mis_d[i];
+            r = Ray{f3(o), f3(d), 1e-4f, 1e10f};
+            st.begin(r.o, r.tmax);
+            const DevSceneRec& R = S.scenes[scene_bits(p.q.mis_c[i].w)];
+            root = R.tri_root;
+            segRoot = kCurves ? R.seg_root : kNoRoot;
+        },
+        [&](uint32_t i, const Traversal& T, Ray& next) -> bool {
+            const float4 c = p.q.mis_c[i];
+            const float3 rd = f3(p.q.mis_d[i]);
+            const DevSceneRec& R = S.scenes[scene_bits(c.w)];
+            const SceneHit h = finish_closest<kCurves>(T, st.tmax);
+            float3 Li = f3(0.f, 0.f, 0.f);
+            if (h.prim == kMiss) {
+                Li = scene_env(S, R, rd);
+            } else {
+                const int mi = slot_material(S, R, hit_slot(S, h.prim));
+                if (mi < 0) {
+                    st.tr = f3(0.f, 0.f, 0.f);
+                } else {
+                    const DevMaterial& m = S.materials[mi];
+                    const float3 tint = m.tint;
+                    bool tooClose = false;
+                    if (!is_black(tint)) {
+                        st.tr = st.tr * tint;
+                        if (!is_black(st.tr) && st.advance<kCurves>(S, h, rd, tooClose, next)) return true;
+                    }
+                    Li = tooClose ? scene_env(S, R, rd) : mat_le(m);
+                }
+            }
+            if (!is_black(Li) && !is_black(st.tr)) add_L(p, __float_as_uint(p.q.mis_o[i].w), f3(c) * (Li * st.tr));
+            st.fresh = true;
+            return false;
         });
 }
 
@@ -922,6 +1070,14 @@ void prime_kernels() {
     prime(k_mis<false, false, true, true>);
     prime(k_mis<false, true, false, true>);
     prime(k_mis<false, true, true, true>);
+    prime(k_shadow_step<false, false>);
+    prime(k_shadow_step<false, true>);
+    prime(k_shadow_step<true, false>);
+    prime(k_shadow_step<true, true>);
+    prime(k_mis_step<false, false>);
+    prime(k_mis_step<false, true>);
+    prime(k_mis_step<true, false>);
+    prime(k_mis_step<true, true>);
     prime(k_trace_batch<false, false, false>);
     prime(k_trace_batch<false, false, true>);
     prime(k_trace_batch<false, true, false>);
@@ -967,7 +1123,20 @@ static void shadow_dispatch(const Params& p, const LaunchCfg& c, cudaStream_t s)
     if (cv) ps ? sh_launch<true, true, kAdj>(p, c, s) : sh_launch<true, false, kAdj>(p, c, s);
     else ps ? sh_launch<false, true, kAdj>(p, c, s) : sh_launch<false, false, kAdj>(p, c, s);
 }
-void launch_shadow(const Params& p, const LaunchCfg& c, cudaStream_t s) { shadow_dispatch<false>(p, c, s); }
+template <bool kCurves, bool kPersist>
+static void step_launch(const Params& p, const LaunchCfg& c, cudaStream_t s, bool mis) {
+    auto k = mis ? k_mis_step<kCurves, kPersist> : k_shadow_step<kCurves, kPersist>;
+    k<<<traversal_grid<kPersist>(k, c), kPersistBlock, 0, s>>>(p);
+}
+static void step_dispatch(const Params& p, const LaunchCfg& c, cudaStream_t s, bool mis) {
+    const bool cv = p.S.has_curves != 0, ps = c.persistent != 0;
+    if (cv) ps ? step_launch<true, true>(p, c, s, mis) : step_launch<true, false>(p, c, s, mis);
+    else ps ? step_launch<false, true>(p, c, s, mis) : step_launch<false, false>(p, c, s, mis);
+}
+void launch_shadow(const Params& p, const LaunchCfg& c, cudaStream_t s) {
+    if (p.S.has_transmit) step_dispatch(p, c, s, false);
+    else shadow_dispatch<false>(p, c, s);
+}
 template <bool kAny, bool kCurves, bool kPersist, bool kAdj>
 static void mis_launch(const Params& p, const LaunchCfg& c, cudaStream_t s) {
     auto k = k_mis<kAny, kCurves, kPersist, kAdj>;
@@ -975,7 +1144,9 @@ static void mis_launch(const Params& p, const LaunchCfg& c, cudaStream_t s) {
 }
 void launch_mis(const Params& p, const LaunchCfg& c, cudaStream_t s) {
     const bool cv = p.S.has_curves != 0, ps = c.persistent != 0, any = !p.S.has_emitters;
-    if (any) {
+    if (p.S.has_transmit) {
+        step_dispatch(p, c, s, true);
+    } else if (any) {
         if (cv) ps ? mis_launch<true, true, true, false>(p, c, s) : mis_launch<true, true, false, false>(p, c, s);
         else ps ? mis_launch<true, false, true, false>(p, c, s) : mis_launch<true, false, false, false>(p, c, s);
     } else {

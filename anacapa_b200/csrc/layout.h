@@ -73,7 +73,13 @@ struct DevMaterial {
     float s;             // azimuthal logistic scale
     float alpha_shift[3];// lobe shift angles (radians)
     float beta_m;
-    float pad0, pad1;
+    // standard_surface glass and alpha (StandardSurface.h:197-218, 245-414)
+    float transmission;  // Params::transmission
+    float ior;           // Params::specular_IOR (eta of the glass lobes)
+    float alpha2_t;      // (r^2)^2 unclamped: evaluate()'s transmission lobe
+    float opacity;       // evalOpacity: opacity when alphaMask, else 1
+    float3 tint;         // transmittanceColor (black: opaque to shadow rays)
+    float pad0;
 };
 
 struct DevLight {
@@ -145,6 +151,8 @@ struct DevScene {
     uint32_t has_curves;    // any scene has curve segments
     uint32_t has_emitters;  // any material reachable from a slot emits (Le != 0)
     uint32_t has_fibers;    // curve segments or hair materials: shading needs the fiber code
+    uint32_t has_transmit;  // a material passes shadow rays (non-black transmittanceColor):
+                            // shadow and MIS rays step through surfaces
     DevEnv env;             // the (single) dome of the batch
 };
 

@@ -494,6 +494,23 @@ DevCamera make_camera(const ana_camera& c, uint32_t width, uint32_t height) {
     return d;
 }
 
+void derive_standard(DevMaterial& o) {
+    const float r = o.rough;
+    const float a = std::max(1e-4f, r * r);  // sample/evaluate: max(1e-4, rough^2)
+    o.alpha2 = a * a;
+    float at = r * r;  // evaluate(), transmission lobe: rough^2 squared, no clamp
+    at *= at;
+    o.alpha2_t = at;
+    uint32_t f = 16u;
+    if (o.transmission > 0.001f) f |= 8u;
+    if (r < 0.001f) f |= 4u;
+    else if (r < 0.3f) f |= 2u;
+    else f |= 1u;
+    o.flags = f;
+    const bool smoothGlass = r < 0.001f && o.transmission > 0.001f && o.metal < 0.001f;
+    o.is_delta = (smoothGlass || (r < 0.001f && (o.metal > 0.999f || o.spec > 0.f))) ? 1 : 0;
+}
+
 int prepare_scene(const ana_scene_desc& d, Prepared& P, std::string& err) {
     auto bad = [&](const char* m) {
         err = m;
@@ -658,6 +675,7 @@ int prepare_scene(const ana_scene_desc& d, Prepared& P, std::string& err) {
         DevMaterial& o = P.materials[i];
         std::memset(&o, 0, sizeof(o));
         o.type = m.type;
+        o.opacity = 1.f;  // IMaterial::evalOpacity's default
         switch (m.type) {
             case ANA_MAT_LAMBERT:
             case ANA_MAT_EMISSIVE:  // Lambertian.h:29-99
@@ -666,10 +684,7 @@ int prepare_scene(const ana_scene_desc& d, Prepared& P, std::string& err) {
                 if (m.type == ANA_MAT_EMISSIVE)
                     o.emission = make_float3(m.emission[0], m.emission[1], m.emission[2]);
                 break;
-            case ANA_MAT_STANDARD: {  // StandardSurface.h:152-181
-                if (m.transmission > 0.001f)
-                    return unsupported("standard_surface transmission (glass) is not implemented");
-                if (m.alpha_mask) return unsupported("alpha-masked materials are not implemented");
+            case ANA_MAT_STANDARD: {  // StandardSurface.h:152-218
                 o.albedo = make_float3(m.base_color[0], m.base_color[1], m.base_color[2]);
                 o.base = m.base;
                 o.metal = m.metalness;
@@ -677,8 +692,9 @@ int prepare_scene(const ana_scene_desc& d, Prepared& P, std::string& err) {
                 o.spec = m.specular;
                 o.spec_color = make_float3(m.specular_color[0], m.specular_color[1], m.specular_color[2]);
                 o.coat = m.coat;
-                float a = std::max(1e-4f, m.roughness * m.roughness);
-                o.alpha2 = a * a;
+                o.transmission = m.transmission;
+                o.ior = m.specular_ior;
+                derive_standard(o);
                 float ca = std::max(1e-4f, m.coat_roughness * m.coat_roughness);
                 o.coat_alpha2 = ca * ca;
                 float r = (1.f - m.specular_ior) / (1.f + m.specular_ior);
@@ -689,12 +705,20 @@ int prepare_scene(const ana_scene_desc& d, Prepared& P, std::string& err) {
                     o.emission = make_float3(m.emission_color[0] * m.emission_weight,
                                              m.emission_color[1] * m.emission_weight,
                                              m.emission_color[2] * m.emission_weight);
-                uint32_t f = 16u;
-                if (m.roughness < 0.001f) f |= 4u;
-                else if (m.roughness < 0.3f) f |= 2u;
-                else f |= 1u;
-                o.flags = f;
-                o.is_delta = (m.roughness < 0.001f && (m.metalness > 0.999f || m.specular > 0.f)) ? 1 : 0;
+                // evalOpacity and transmittanceColor (StandardSurface.h:197-218)
+                o.opacity = m.alpha_mask ? m.opacity : 1.f;
+                if (m.alpha_mask) {
+                    const float t = 1.f - m.opacity;
+                    if (t > 0.f) o.tint = make_float3(t, t, t);
+                } else if (m.transmission >= 0.001f && !(m.metalness > 0.001f)) {
+                    // Fresnel reflectance at normal incidence, fresnelDielectric(1, IOR)
+                    const float eta = m.specular_ior;
+                    const float Rs = (1.f - eta * 1.f) / (1.f + eta * 1.f);
+                    const float Rp = (eta * 1.f - 1.f) / (eta * 1.f + 1.f);
+                    const float Fr = 0.5f * (Rs * Rs + Rp * Rp);
+                    const float k = m.transmission * (1.f - Fr);
+                    o.tint = make_float3(m.base_color[0] * k, m.base_color[1] * k, m.base_color[2] * k);
+                }
                 break;
             }
             case ANA_MAT_HAIR: {  // MarschnerHair.h:200-216
@@ -723,11 +747,14 @@ int prepare_scene(const ana_scene_desc& d, Prepared& P, std::string& err) {
     }
     P.slot_material.assign(d.slot_material, d.slot_material + d.num_slots);
     P.has_emitters = false;
+    P.has_transmit = false;
     for (int32_t s : P.slot_material) {
         if (s >= int32_t(d.num_materials)) return bad("slot refers to a missing material");
         if (s >= 0) {
             const float3 e = P.materials[size_t(s)].emission;
             if (e.x != 0.f || e.y != 0.f || e.z != 0.f) P.has_emitters = true;
+            const float3 t = P.materials[size_t(s)].tint;
+            if (t.x != 0.f || t.y != 0.f || t.z != 0.f) P.has_transmit = true;
         }
     }
 

@@ -35,8 +35,15 @@ struct Prepared {
     ana_camera camera{};
     uint32_t num_tris = 0, num_segs = 0;
     bool has_emitters = false;
+    bool has_transmit = false;  // a slot's material has a non-black shadow tint
     uint64_t bytes() const;
 };
+
+// The roughness-derived fields of a standard_surface material (rough, metal,
+// spec and transmission set): GGX alpha2 of sample/evaluate, the unclamped
+// alpha2 of the transmission lobe, flags() and isDelta()
+// (StandardSurface.h:152-181, 384).
+void derive_standard(DevMaterial& m);
 
 // Returns ANA_OK or an error code with a message in err.
 int prepare_scene(const ana_scene_desc& d, Prepared& out, std::string& err);

@@ -241,10 +241,118 @@ __device__ __forceinline__ bool ss_sample_ggx(float3 wol, float ux, float uy, fl
     return pdf > 0.f && !is_black(f);
 }
 
+// ---- standard_surface glass (StandardSurface.h:245-340) --------------------
+// The sample path of a transmissive non-metal: Fresnel chooses between mirror
+// reflection and Snell refraction (roughness < 0.001, delta), or between GGX
+// reflection and Walter et al. microfacet refraction about a sampled
+// half-vector. eta = IOR entering the front face, 1/IOR leaving; f carries
+// |cos| (importance transport, no eta^2).
+__device__ __forceinline__ bool ss_glass(const DevMaterial& m) { return m.transmission > 0.001f && m.metal < 0.001f; }
+
+__device__ __forceinline__ BsdfSample glass_sample(const DevMaterial& m, const ShadeCtx& c, float3 wol, float ux,
+                                                   float uy, float uc) {
+    const float eta = c.front ? m.ior : (1.f / m.ior);
+    BsdfSample s;
+    if (m.rough < 0.001f) {
+        const float cosI = wol.z;
+        const float Fr = fresnel_dielectric(cosI, eta);
+        if (uc < Fr) {
+            s.wi = c.to_world(f3(-wol.x, -wol.y, wol.z));
+            s.f = m.albedo * Fr;
+            s.pdf = Fr;
+            s.flags = kFlagSpecular | kFlagReflection;
+        } else {
+            const float sin2T = fmaxf(0.f, 1.f - cosI * cosI) / (eta * eta);
+            const float cosT = sqrtf(fmaxf(0.f, 1.f - sin2T));
+            s.wi = c.to_world(f3(-wol.x / eta, -wol.y / eta, -cosT));
+            s.f = m.albedo * (1.f - Fr);
+            s.pdf = 1.f - Fr;
+            s.flags = kFlagSpecular | kFlagTransmission;
+        }
+        return s;
+    }
+    const float a2 = m.alpha2;
+    const float3 wh = sample_ggx_h(ux, uy, a2);
+    if (wh.z <= 0.f) return no_sample();
+    const float cosIH = fmaxf(0.f, dot(wol, wh));
+    if (cosIH <= 0.f) return no_sample();
+    const float Fr = fresnel_dielectric(cosIH, eta);
+    if (uc < Fr) {
+        const float3 wil = wh * (2.f * cosIH) - wol;
+        if (wil.z <= 0.f) return no_sample();
+        const float D = d_ggx(wh.z, a2);
+        const float G2 = g2_sep(wol.z, wil.z, a2);
+        s.wi = c.to_world(wil);
+        s.f = f3(Fr, Fr, Fr) * (D * G2 / (4.f * wol.z)) * m.albedo;
+        s.pdf = Fr * pdf_ggx_refl(wh.z, a2, cosIH);
+        s.flags = kFlagGlossy | kFlagReflection;
+        return s;
+    }
+    const float sin2T = fmaxf(0.f, 1.f - cosIH * cosIH) / (eta * eta);
+    if (sin2T >= 1.f) return no_sample();  // total internal reflection
+    const float cosTH = sqrtf(1.f - sin2T);
+    const float3 wil = wol * (-1.f / eta) + wh * (cosIH / eta - cosTH);
+    if (wil.z >= 0.f) return no_sample();
+    const float cosO = wol.z;
+    const float D = d_ggx(wh.z, a2);
+    const float G2 = g2_sep(cosO, fabsf(wil.z), a2);
+    const float denom = cosIH + eta * fabsf(dot(wil, wh));
+    if (denom < 1e-6f) return no_sample();
+    const float absT = fabsf(dot(wil, wh));
+    const float jac = eta * eta * absT / (denom * denom);
+    s.wi = c.to_world(wil);
+    s.f = m.albedo * ((1.f - Fr) * D * G2 * cosIH * absT / (cosO * denom * denom));
+    s.pdf = (1.f - Fr) * (D * wh.z) * jac;
+    s.flags = kFlagGlossy | kFlagTransmission;
+    return s;
+}
+
+// evaluate() of glass (StandardSurface.h:380-438): the microfacet
+// transmission lobe for directions on opposite sides (its alpha2 unclamped),
+// Fresnel-weighted GGX reflection on the same side; smooth glass has no
+// finite density.
+__device__ __forceinline__ BsdfEval glass_eval_t(const DevMaterial& m, const ShadeCtx& c, float3 wol, float3 wil) {
+    BsdfEval e{f3(0.f, 0.f, 0.f), 0.f};
+    if (m.transmission < 0.001f || m.rough < 0.001f || m.metal > 0.001f) return e;
+    const float eta = c.front ? m.ior : (1.f / m.ior);
+    const float a2 = m.alpha2_t;
+    float3 wh = safe_normalize(wol + wil * eta);
+    if (wh.z < 0.f) wh = -wh;
+    const float cosIH = fmaxf(0.f, dot(wol, wh));
+    const float cosTH = fabsf(dot(wil, wh));
+    const float Fr = fresnel_dielectric(cosIH, eta);
+    const float D = d_ggx(wh.z, a2);
+    const float G2 = g2_sep(wol.z, fabsf(wil.z), a2);
+    const float denom = cosIH + eta * cosTH;
+    if (denom < 1e-6f) return e;
+    const float bsdf = (1.f - Fr) * D * G2 * cosIH * cosTH / (wol.z * fabsf(wil.z) * denom * denom);
+    const float jac = eta * eta * cosTH / (denom * denom);
+    e.f = m.albedo * bsdf;
+    e.pdf = (1.f - Fr) * D * wh.z * jac;
+    return e;
+}
+__device__ __forceinline__ BsdfEval glass_eval_r(const DevMaterial& m, const ShadeCtx& c, float3 wol, float3 wil) {
+    BsdfEval e{f3(0.f, 0.f, 0.f), 0.f};
+    if (m.rough < 0.001f) return e;
+    const float eta = c.front ? m.ior : (1.f / m.ior);
+    const float a2 = m.alpha2;
+    const float3 wh = safe_normalize(wol + wil);
+    if (wh.z < 0.f) return e;
+    const float cosIH = fmaxf(0.f, dot(wol, wh));
+    const float Fr = fresnel_dielectric(cosIH, eta);
+    const float D = d_ggx(wh.z, a2);
+    const float G2 = g2_sep(wol.z, wil.z, a2);
+    const float cosR = wil.z;
+    e.pdf = Fr > 0.f ? Fr * pdf_ggx_refl(wh.z, a2, cosIH) : 0.f;
+    e.f = m.albedo * (Fr * D * G2 / (4.f * wol.z * cosR));
+    return e;
+}
+
 __device__ __forceinline__ BsdfSample ss_sample(const DevMaterial& m, const ShadeCtx& c, float3 wo, float ux,
                                                 float uy, float uc) {
     float3 wol = c.to_local(wo);
     if (wol.z <= 0.f) return no_sample();
+    if (ss_glass(m)) return glass_sample(m, c, wol, ux, uy, uc);
     LobeWeights w;
     if (!ss_weights(m, wol.z, w)) return no_sample();
     float3 wil;
@@ -284,7 +392,8 @@ __device__ __forceinline__ BsdfSample ss_sample(const DevMaterial& m, const Shad
 __device__ __forceinline__ BsdfEval ss_eval(const DevMaterial& m, const ShadeCtx& c, float3 wo, float3 wi) {
     float3 wol = c.to_local(wo), wil = c.to_local(wi);
     BsdfEval e{f3(0.f, 0.f, 0.f), 0.f};
-    if (!(wol.z * wil.z > 0.f)) return e;  // opaque: no transmission lobe
+    if (!(wol.z * wil.z > 0.f)) return glass_eval_t(m, c, wol, wil);  // opaque: black
+    if (ss_glass(m)) return glass_eval_r(m, c, wol, wil);
     LobeWeights w;
     if (!ss_weights(m, wol.z, w)) return e;
     e.f = ss_combined(m, wol, wil, w, e.pdf);

@@ -9,6 +9,7 @@
 // CurveBrute::trace's aabbHit and the ray-ribbon subdivide
 // (src/accel/CurveBrute.cpp:85-234, 478-498).
 #pragma once
+#include <type_traits>
 #include "dmath.cuh"
 #include "layout.h"
 
@@ -507,10 +508,24 @@ __device__ __forceinline__ bool stage_done(Traversal& T, float3 d, uint32_t segR
     return T.exhausted;
 }
 
+// Done(i, T) consumes a finished traversal; Done(i, T, next) -> bool may
+// instead ask for entry i to be traced again along `next` (same direction:
+// a ray stepping through a transmissive surface) by returning true.
+template <class Done>
+__device__ __forceinline__ bool trace_again(Done& done, uint32_t i, const Traversal& T, Ray& next) {
+    if constexpr (std::is_invocable_r_v<bool, Done&, uint32_t, const Traversal&, Ray&>) {
+        return done(i, T, next);
+    } else {
+        done(i, T);
+        return false;
+    }
+}
+
 // Runs the persistent loop. Load(i, ray, root, segRoot) reads queue entry i
-// and its scene's triangle and curve BVH roots; Done(i, T) consumes the
-// finished traversal of entry i (a lane-local call). With kCurves a lane that
-// finishes the triangle BVH continues with the curve BVH in the same phases.
+// and its scene's triangle and curve BVH roots; Done consumes the finished
+// traversal of entry i (a lane-local call, see trace_again: a lane asked to
+// trace again keeps its entry). With kCurves a lane that finishes the
+// triangle BVH continues with the curve BVH in the same phases.
 template <bool kAny, bool kCount, bool kCurves, class Load, class Done>
 __device__ __forceinline__ void persistent_traverse(const DevScene& S, uint32_t n, uint32_t* fetch, uint32_t* err,
                                                     Counters* cnt, Load load, Done done) {
@@ -573,8 +588,15 @@ __device__ __forceinline__ void persistent_traverse(const DevScene& S, uint32_t 
                 finished = stage_done<kAny, kCurves>(T, ray.d, segRoot);
             }
             if (finished) {
-                done(idx, T);
-                active = false;
+                Ray next;
+                if (trace_again(done, idx, T, next)) {
+                    Ray ray;
+                    uint32_t root, segRoot;
+                    load(idx, ray, root, segRoot);
+                    trav_init(T, next, root);
+                } else {
+                    active = false;
+                }
             }
         }
     }

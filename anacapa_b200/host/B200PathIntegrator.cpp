@@ -106,10 +106,6 @@ bool material_of(const IMaterial* m, ana_material& o, std::string& err) {
             err = "standard_surface with image textures is not supported";
             return false;
         }
-        if (p.transmission > 0.001f || p.alphaMask) {
-            err = "standard_surface glass / alpha masks are not supported";
-            return false;
-        }
         o.type = ANA_MAT_STANDARD;
         put3(o.base_color, p.base_color.value);
         o.base = p.base;
@@ -123,6 +119,8 @@ bool material_of(const IMaterial* m, ana_material& o, std::string& err) {
         o.transmission = p.transmission;
         o.emission_weight = p.emission;
         put3(o.emission_color, p.emission_color.value);
+        o.alpha_mask = p.alphaMask ? 1u : 0u;
+        o.opacity = p.opacity.value;
         return true;
     }
     if (auto* hm = dynamic_cast<const MarschnerHairMaterial*>(m)) {

@@ -11,7 +11,7 @@
 // sampleStart + sampleCount) samples per pixel and merges the result into the
 // Film as one full-frame TileBuffer (Film::mergeTile), returning true.
 // There is no CPU fallback: unsupported scene content (motion blur,
-// textures, glass, alpha masks, a rotated dome) makes
+// textures, a rotated dome) makes
 // prepare/renderFrame fail with a message in lastError(); renderTile throws.
 #pragma once
 

@@ -52,6 +52,8 @@ class Material:
     coat: float = 0.0
     coat_roughness: float = 0.1
     transmission: float = 0.0
+    alpha_mask: bool = False
+    opacity: float = 1.0
     emission_w: float = 0.0
     emission_color: tuple = (0.0, 0.0, 0.0)
     # hair (src/shading/MarschnerHair.h:192-198 defaults)
@@ -63,11 +65,13 @@ class Material:
     hair_mode: int = 0  # 0: as the reference executes it (Kajiya-Kay); 1: Marschner lobes
 
     def standard_packed(self) -> np.ndarray:
-        """18-float packing used by the reference harness."""
+        """20-float packing used by the reference harness (the restatement
+        reads the first 18)."""
         return np.array([*self.base_color, self.base, self.metalness, self.roughness,
                          self.specular, *self.specular_color, self.specular_ior, self.coat,
                          self.coat_roughness, self.transmission, self.emission_w,
-                         *self.emission_color], dtype=np.float32)
+                         *self.emission_color, float(self.alpha_mask), self.opacity],
+                        dtype=np.float32)
 
 
 @dataclasses.dataclass
@@ -517,4 +521,75 @@ def sunlit(width=256, height=192, spp=16, max_depth=8, half_angle_deg=0.0, n_sph
                    dir_lights=[DirLight((-0.4, 0.8, -0.3), (3.0, 2.8, 2.5), half_angle_deg)],
                    env_radiance=(0.05, 0.07, 0.1),
                    cam_from=(0.0, 4.0, -9.0), cam_at=(0.0, 0.5, 0.0), cam_up=(0.0, 1.0, 0.0),
+                   vfov=45.0, width=width, height=height, spp=spp, max_depth=max_depth)
+
+
+def glass(width=192, height=144, spp=16, max_depth=8, seed=5) -> Scene:
+    """Transmission and alpha testing (StandardSurface.h:197-414,
+    PathIntegrator.cpp:103-118, ShadowRay.h): on the tilted ground of `sunlit`,
+    a smooth glass sphere (IOR 1.5, delta), a rough glass sphere (roughness
+    0.3, GGX transmission), a smooth tinted water sphere (IOR 1.33), a smooth
+    mirror (roughness 0, metal: a delta opaque material), two alpha-masked
+    cards (opacity 0.4: stochastic, one sample dimension per test; opacity 0:
+    cut out without one) and two glass panes, lit by an area light, a
+    directional light and a constant environment. Cards and panes are turned
+    about y so that no box is flat."""
+    rng = np.random.default_rng(seed)
+    b = _Builder()
+    mg = b.material(Material(MAT_LAMBERT, albedo=(0.55, 0.5, 0.45)))
+    g, y0, y1 = 6.0, 0.0, 0.1
+    gn = np.array([0.0, 2.0 * g, -(y1 - y0)])
+    gn /= np.linalg.norm(gn)
+    b.quad([-g, y0, -g], [-g, y1, g], [g, y1, g], [g, y0, -g], gn, mg)
+    v, f = icosphere(3)
+    spheres = [
+        (Material(MAT_STANDARD, base_color=(1.0, 1.0, 1.0), roughness=0.0, transmission=1.0,
+                  specular_ior=1.5), (-1.6, 0.8, 0.2), 0.75),
+        (Material(MAT_STANDARD, base_color=(0.9, 0.95, 1.0), roughness=0.3, transmission=1.0,
+                  specular_ior=1.5), (0.4, 0.7, 0.9), 0.6),
+        (Material(MAT_STANDARD, base_color=(0.7, 0.9, 0.8), roughness=0.0, transmission=0.9,
+                  specular_ior=1.33), (1.9, 0.55, -0.6), 0.5),
+        (Material(MAT_STANDARD, base_color=(0.9, 0.85, 0.7), roughness=0.0, metalness=1.0),
+         (-0.2, 0.45, -1.3), 0.4),
+        (Material(MAT_STANDARD, base_color=(0.8, 0.3, 0.2), roughness=0.4), (2.6, 0.5, 1.8), 0.45),
+    ]
+    for m, c, r in spheres:
+        b.mesh(np.asarray(c) + r * v, f, b.material(m), nrm=v)
+
+    def card(mat, c, half_w, half_h, yaw_deg):
+        a = np.radians(yaw_deg)
+        u = np.array([np.cos(a), 0.0, np.sin(a)]) * half_w
+        w = np.array([0.05, 1.0, 0.03]) * half_h
+        c = np.asarray(c, np.float64)
+        n = np.cross(u, w)
+        b.quad(c - u - w, c + u - w, c + u + w, c - u + w, n / np.linalg.norm(n), mat)
+
+    leaf = b.material(Material(MAT_STANDARD, base_color=(0.3, 0.6, 0.2), roughness=0.6, alpha_mask=True,
+                               opacity=0.4))
+    cutout = b.material(Material(MAT_STANDARD, base_color=(0.9, 0.1, 0.1), roughness=0.5, alpha_mask=True,
+                                 opacity=0.0))
+    pane = b.material(Material(MAT_STANDARD, base_color=(0.95, 0.9, 0.8), roughness=0.0, transmission=1.0,
+                               specular_ior=1.5))
+    frosted = b.material(Material(MAT_STANDARD, base_color=(0.9, 0.9, 1.0), roughness=0.15, transmission=1.0,
+                                  specular_ior=1.5))
+    card(leaf, (-0.6, 1.0, -2.4), 0.8, 0.9, 25.0)
+    card(cutout, (1.2, 0.9, -2.2), 0.6, 0.8, -30.0)
+    card(pane, (0.9, 1.1, 2.6), 1.1, 1.0, 15.0)
+    card(frosted, (-2.4, 1.0, 1.9), 0.8, 0.9, -40.0)
+    for _ in range(6):
+        m = b.material(Material(MAT_STANDARD, base_color=tuple(map(float, rng.uniform(0.1, 0.9, 3))),
+                                roughness=float(rng.uniform(0.1, 0.9))))
+        r = float(rng.uniform(0.2, 0.35))
+        c = np.array([rng.uniform(-4, 4), r + 0.05, rng.uniform(-4, 4)])
+        b.mesh(c + r * icosphere(1)[0], icosphere(1)[1], m, nrm=icosphere(1)[0])
+    le = (7.0, 6.0, 5.0)
+    ml = b.material(Material(MAT_EMISSIVE, albedo=(0.0, 0.0, 0.0), emission=le))
+    lc, lu, lv = np.array([-1.0, 3.2, -0.5]), np.array([0.5, 0.0, 0.0]), np.array([0.0, 0.03, 0.4])
+    ln = np.cross(lu, lv)
+    ln /= np.linalg.norm(ln)
+    b.quad(lc - lu - lv, lc + lu - lv, lc + lu + lv, lc - lu + lv, ln, ml)
+    return b.scene("glass", area_lights=[AreaLight(tuple(lc), tuple(lu), tuple(lv), le)],
+                   dir_lights=[DirLight((0.5, 0.7, -0.4), (2.5, 2.4, 2.2), 1.5)],
+                   env_radiance=(0.15, 0.18, 0.25),
+                   cam_from=(0.0, 3.2, -7.5), cam_at=(0.0, 0.6, 0.0), cam_up=(0.0, 1.0, 0.0),
                    vfov=45.0, width=width, height=height, spp=spp, max_depth=max_depth)

@@ -66,10 +66,11 @@ typedef struct ana_material {
     float specular_ior;
     float coat;
     float coat_roughness;
-    float transmission;    /* must be <= 0.001: glass is outside the implemented path */
+    float transmission;    /* > 0.001: dielectric glass (smooth below roughness 0.001, else
+                              GGX transmission), StandardSurface.h:245-340, 380-414 */
     float emission_weight; /* Params::emission */
     float emission_color[3];
-    uint32_t alpha_mask;   /* must be 0 */
+    uint32_t alpha_mask;   /* Params::alphaMask: opacity below drives alpha testing */
     /* hair, MarschnerHairMaterial::Params (MarschnerHair.h:192-198) */
     float eta;
     float sigma_a[3];
@@ -77,6 +78,9 @@ typedef struct ana_material {
     float beta_n;
     float alpha_deg;
     uint32_t hair_mode;    /* ANA_HAIR_* */
+    /* standard_surface Params::opacity (constant), read when alpha_mask is set:
+     * evalOpacity and the shadow tint 1 - opacity (StandardSurface.h:197-218) */
+    float opacity;
 } ana_material;
 
 /* ---- lights (include/anacapa/shading/ILight.h) ----------------------------- */

@@ -115,9 +115,9 @@ private:
 };
 
 StandardSurfaceMaterial::Params ssParams(const float* p) {
-    // Packed layout (18 floats): base_color[3], base, metalness, roughness,
+    // Packed layout (20 floats): base_color[3], base, metalness, roughness,
     // specular, specular_color[3], specular_IOR, coat, coat_roughness,
-    // transmission, emission, emission_color[3]
+    // transmission, emission, emission_color[3], alphaMask (0/1), opacity
     StandardSurfaceMaterial::Params q;
     q.base_color = SpectrumTOV(Vec3f{p[0], p[1], p[2]});
     q.base = p[3];
@@ -131,6 +131,8 @@ StandardSurfaceMaterial::Params ssParams(const float* p) {
     q.transmission = p[13];
     q.emission = p[14];
     q.emission_color = SpectrumTOV(Vec3f{p[15], p[16], p[17]});
+    q.alphaMask = p[18] != 0.f;
+    q.opacity = FloatTOV(p[19]);
     return q;
 }
 
@@ -195,9 +197,9 @@ int ref_mat_emissive(void* sp, const float* albedo, const float* emission) {
     return int(s->mats.size() - 1);
 }
 
-int ref_mat_standard(void* sp, const float* packed18) {
+int ref_mat_standard(void* sp, const float* packed20) {
     auto* s = static_cast<RefScene*>(sp);
-    s->mats.push_back(std::make_unique<StandardSurfaceMaterial>(ssParams(packed18)));
+    s->mats.push_back(std::make_unique<StandardSurfaceMaterial>(ssParams(packed20)));
     return int(s->mats.size() - 1);
 }
 

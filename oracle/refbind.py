@@ -215,12 +215,14 @@ class RefScene:
             raise RuntimeError(f"drop-in render failed ({rc}): {err.value.decode()}")
         return rgb, var
 
-    def dropin_prepare(self):
+    def dropin_prepare(self, size=None):
         """The drop-in's host-side prepare of this scene (variant "dropin"
-        only): a raw ana_prepared handle, freed by the caller."""
+        only) for a film of `size` (default: the scene's): a raw ana_prepared
+        handle, freed by the caller."""
         s = self.scene
+        w, h = size if size is not None else (s.width, s.height)
         err = C.create_string_buffer(512)
-        p = self.L.ref_dropin_prepare(self.h, s.width, s.height, err, len(err))
+        p = self.L.ref_dropin_prepare(self.h, w, h, err, len(err))
         if not p:
             raise RuntimeError(f"drop-in prepare failed: {err.value.decode()}")
         return p

@@ -80,6 +80,8 @@ class PoScene:
             if m.type in (S.MAT_LAMBERT, S.MAT_EMISSIVE):
                 L.po_add_material(h, m.type, _fp(f32(m.albedo)), _fp(f32(m.emission)), None, None)
             elif m.type == S.MAT_STANDARD:
+                if m.transmission > 0.001 or m.alpha_mask:
+                    raise NotImplementedError("the restatement covers opaque materials without alpha masks")
                 L.po_add_material(h, m.type, None, None, _fp(m.standard_packed()), None)
             else:
                 hv = f32([m.eta, *m.sigma_a, m.beta_m, m.beta_n, m.alpha_deg, m.hair_mode])

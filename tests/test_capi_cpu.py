@@ -2,6 +2,7 @@
 include/anacapa_b200.h declares, and the host-side scene preparation (BVH
 builds, validation, error codes) behaves."""
 import ctypes as C
+import dataclasses
 import os
 import re
 
@@ -88,7 +89,11 @@ def test_prepare_rejects_bad_input(lib_built):
     glass = S.cornell()
     glass.materials = list(glass.materials)
     glass.materials[0] = S.Material(S.MAT_STANDARD, transmission=1.0, roughness=0.0)
-    assert _prepare_rc(glass) == api.ANA_ERR_UNSUPPORTED
+    assert _prepare_rc(glass) == api.ANA_OK
+    weird = S.cornell()
+    weird.materials = list(weird.materials)
+    weird.materials[0] = dataclasses.replace(weird.materials[0], type=7)
+    assert _prepare_rc(weird) == api.ANA_ERR_INVALID_ARG
     assert _prepare_rc(sc, max_leaf_tris=65) == api.ANA_ERR_INVALID_ARG
     assert _prepare_rc(sc, max_leaf_tris=8) == api.ANA_OK
     h = C.c_void_p()

@@ -31,8 +31,11 @@ def dropin(lib_built, ref_built):
 
 @pytest.mark.parametrize("make", [lambda: S.cornell(128, 128, 8),
                                   lambda: S.hair(96, 54, 4, 10, n_strands=5000),
-                                  lambda: S.throughput(96, 54, 4, 12, n_spheres=64)],
-                         ids=["cornell", "hair", "throughput_small"])
+                                  lambda: S.throughput(96, 54, 4, 12, n_spheres=64),
+                                  # the directional light is recovered by probing, an ulp
+                                  # away from the description's: left out of the digest
+                                  lambda: dataclasses.replace(S.glass(96, 72, 4), dir_lights=[])],
+                         ids=["cornell", "hair", "throughput_small", "glass"])
 def test_dropin_prepares_the_same_layout(dropin, make):
     sc = make()
     rs = dropin.RefScene(sc, variant="dropin")
@@ -48,8 +51,6 @@ def test_dropin_prepares_the_same_layout(dropin, make):
 
 def test_dropin_rejects_unsupported_content(dropin):
     sc = S.throughput(32, 32, 1, 4, n_spheres=8)
-    sc = dataclasses.replace(sc, materials=[dataclasses.replace(m, transmission=0.5)
-                                            if m.type == S.MAT_STANDARD else m for m in sc.materials])
     rs = dropin.RefScene(sc, variant="dropin")
-    with pytest.raises(RuntimeError, match="glass"):
-        rs.dropin_prepare()
+    with pytest.raises(RuntimeError, match="another film size"):
+        rs.dropin_prepare(size=(48, 32))

@@ -23,8 +23,9 @@ def dropin(gpu, ref_built):
 @pytest.mark.parametrize("make", [lambda: S.cornell(128, 128, 8),
                                   lambda: S.hair(96, 54, 4, 10, n_strands=5000),
                                   lambda: S.throughput(96, 54, 4, 12, n_spheres=64),
-                                  lambda: S.sunlit(96, 72, 8)],
-                         ids=["cornell", "hair", "throughput_small", "sunlit"])
+                                  lambda: S.sunlit(96, 72, 8),
+                                  lambda: S.glass(96, 72, 8)],
+                         ids=["cornell", "hair", "throughput_small", "sunlit", "glass"])
 def test_dropin_matches_direct_render(dropin, make):
     sc = make()
     rs = dropin.RefScene(sc, variant="dropin")
