@@ -97,7 +97,8 @@ class AnaStats(C.Structure):
                 ("film_ms", C.c_float), ("bounces", C.c_uint32), ("chunks", C.c_uint32),
                 ("kernel_launches", C.c_uint64), ("extend_launches", C.c_uint64),
                 ("node_fetches", C.c_uint64), ("tri_tests", C.c_uint64), ("seg_tests", C.c_uint64),
-                ("curve_node_fetches", C.c_uint64)]
+                ("curve_node_fetches", C.c_uint64),
+                ("upload_ms", C.c_float), ("build_ms", C.c_float * 4), ("build_levels", C.c_uint32)]
 
 
 class AnaTile(C.Structure):
@@ -125,7 +126,8 @@ EXPORTS = ["ana_create", "ana_destroy", "ana_upload_scene", "ana_prepare_scene",
            "ana_get_stats", "ana_last_error", "ana_version", "ana_batch_create", "ana_batch_free",
            "ana_batch_bytes", "ana_upload_batch", "ana_render_batch", "ana_batch_film_read",
            "ana_prepared_digest", "ana_trace_batch_noalloc", "ana_diff_counts", "ana_diff_get_params",
-           "ana_forward", "ana_backward", "ana_render_tiles", "ana_render_adaptive"]
+           "ana_forward", "ana_backward", "ana_render_tiles", "ana_render_adaptive",
+           "ana_upload_scene_device", "ana_scene_digest"]
 ANA_RENDER_GRAPH = 4
 
 _lib = None
@@ -149,6 +151,8 @@ def lib():
     L.ana_destroy.argtypes = [_P]
     L.ana_destroy.restype = None
     L.ana_upload_scene.argtypes = [_P, C.POINTER(AnaSceneDesc)]
+    L.ana_upload_scene_device.argtypes = [_P, C.POINTER(AnaSceneDesc)]
+    L.ana_scene_digest.argtypes = [_P, C.POINTER(C.c_uint64)]
     L.ana_prepare_scene.argtypes = [C.POINTER(AnaSceneDesc), C.POINTER(_P)]
     L.ana_upload_prepared.argtypes = [_P, _P]
     L.ana_prepared_bytes.argtypes = [_P]
@@ -358,13 +362,22 @@ class Renderer:
     def _check(self, rc):
         check(rc, self.h)
 
-    def upload(self, sc_or_prep, **kw):
+    def upload(self, sc_or_prep, device_build=False, **kw):
+        """ana_upload_scene (host BVH build), ana_upload_scene_device with
+        device_build, or ana_upload_prepared for a Prepared scene."""
         if isinstance(sc_or_prep, Prepared):
             self._check(lib().ana_upload_prepared(self.h, sc_or_prep.h))
         else:
             d = SceneDesc(sc_or_prep, **kw)
-            self._check(lib().ana_upload_scene(self.h, C.byref(d.desc)))
+            fn = lib().ana_upload_scene_device if device_build else lib().ana_upload_scene
+            self._check(fn(self.h, C.byref(d.desc)))
             self.scene = sc_or_prep
+
+    def scene_digest(self) -> int:
+        """ana_scene_digest: FNV-1a 64 of the uploaded scene arena."""
+        out = C.c_uint64()
+        self._check(lib().ana_scene_digest(self.h, C.byref(out)))
+        return int(out.value)
 
     def render(self, width, height, spp, max_depth, sample_start=0, min_depth=2, seed=0, clear=True,
                count_work=False):

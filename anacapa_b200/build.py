@@ -26,8 +26,9 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 SOURCES = {
     "kernels.cu": ["kernels.cu", "kernels.h", "layout.h", "dmath.cuh", "sampler.cuh", "shade.cuh",
                    "traverse.cuh"],
+    "build.cu": ["build.cu", "build.h", "layout.h"],
     "prepare.cpp": ["prepare.cpp", "prepare.h", "layout.h"],
-    "capi.cpp": ["capi.cpp", "kernels.h", "prepare.h", "layout.h"],
+    "capi.cpp": ["capi.cpp", "kernels.h", "prepare.h", "build.h", "layout.h"],
 }
 
 
@@ -60,6 +61,8 @@ def build(force=False, verbose=False, ptxas_info=False):
         if src.endswith(".cu"):
             cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
                    "--expt-relaxed-constexpr", *inc, "-c", path, "-o", obj]
+            if src == "build.cu":  # every float operation rounds on its own
+                cmd.insert(1, "-fmad=false")
             if ptxas_info:
                 cmd.insert(1, "-Xptxas=-v")
         else:

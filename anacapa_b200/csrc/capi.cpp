@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -13,6 +14,7 @@
 #include <vector>
 
 #include "../../include/anacapa_b200.h"
+#include "build.h"
 #include "kernels.h"
 #include "prepare.h"
 
@@ -52,8 +54,9 @@ struct SceneStatic {
 // One or more prepared scenes laid out as a single device arena in pinned
 // host memory (256-byte aligned sections), so an upload is one copy.
 struct Blob {
-    unsigned char* mem = nullptr;
+    unsigned char* mem = nullptr;  // host copy of [host_base, size)
     size_t size = 0;
+    size_t host_base = 0;  // > 0: the triangle sections come from a device build
     bool pinned = false;
     size_t o_tri_nodes = 0, o_tri_isect = 0, o_tri_shade = 0, o_seg_nodes = 0, o_segs = 0, o_scol = 0, o_mats = 0,
            o_slots = 0, o_lights = 0, o_env_rgb = 0, o_cf = 0, o_cc = 0, o_ci = 0, o_mf = 0, o_mc = 0;
@@ -61,6 +64,7 @@ struct Blob {
     bool has_curves = false, has_emitters = false, has_transmit = false;
     size_t n_mats = 0, n_lights = 0;
     ana::HostEnv env_meta;  // scalars only
+    unsigned char* at(size_t off) const { return mem + (off - host_base); }
     Blob() = default;
     Blob(const Blob&) = delete;
     Blob& operator=(const Blob&) = delete;
@@ -76,7 +80,11 @@ int build_blob(const ana::Prepared* const* list, uint32_t n, Blob& B, std::strin
     const ana::Prepared* dome = nullptr;
     for (uint32_t k = 0; k < n; ++k) {
         const ana::Prepared& P = *list[k];
-        nNodes += P.tri_nodes.size();
+        if (P.tris_on_device && n != 1) {
+            err = "a scene built on the device is uploaded on its own";
+            return ANA_ERR_INVALID_ARG;
+        }
+        nNodes += P.tris_on_device ? size_t(P.dev_tri_nodes) : P.tri_nodes.size();
         nTris += P.num_tris;
         nSegNodes += P.seg_nodes.size();
         nSegs += P.num_segs;
@@ -120,12 +128,16 @@ int build_blob(const ana::Prepared* const* list, uint32_t n, Blob& B, std::strin
     B.o_mf = take(dome ? dome->env.marg_func.size() * 4 : 0);
     B.o_mc = take(dome ? dome->env.marg_cdf.size() * 4 : 0);
     B.size = std::max<size_t>(off, kAlign);
+    bool devTris = false;
+    for (uint32_t k = 0; k < n; ++k) devTris = devTris || list[k]->tris_on_device;
+    B.host_base = devTris ? B.o_seg_nodes : 0;
+    const size_t hostBytes = std::max<size_t>(B.size - B.host_base, kAlign);
     void* mem = nullptr;
-    if (cudaHostAlloc(&mem, B.size, cudaHostAllocPortable) == cudaSuccess) {
+    if (cudaHostAlloc(&mem, hostBytes, cudaHostAllocPortable) == cudaSuccess) {
         B.pinned = true;
     } else {
         cudaGetLastError();
-        mem = std::aligned_alloc(kAlign, B.size);
+        mem = std::aligned_alloc(kAlign, hostBytes);
         B.pinned = false;
         if (!mem) {
             err = "host allocation failed";
@@ -133,16 +145,16 @@ int build_blob(const ana::Prepared* const* list, uint32_t n, Blob& B, std::strin
         }
     }
     B.mem = static_cast<unsigned char*>(mem);
-    std::memset(B.mem, 0, B.size);
-    auto* nodes = reinterpret_cast<ana::Bvh4Node*>(B.mem + B.o_tri_nodes);
-    auto* isect = reinterpret_cast<float4*>(B.mem + B.o_tri_isect);
-    auto* shade = reinterpret_cast<float4*>(B.mem + B.o_tri_shade);
-    auto* snodes = reinterpret_cast<ana::BvhNode*>(B.mem + B.o_seg_nodes);
-    auto* segs = reinterpret_cast<float4*>(B.mem + B.o_segs);
-    auto* scol = reinterpret_cast<float*>(B.mem + B.o_scol);
-    auto* mats = reinterpret_cast<ana::DevMaterial*>(B.mem + B.o_mats);
-    auto* slots = reinterpret_cast<int32_t*>(B.mem + B.o_slots);
-    auto* lights = reinterpret_cast<ana::DevLight*>(B.mem + B.o_lights);
+    std::memset(B.mem, 0, hostBytes);
+    auto* nodes = devTris ? nullptr : reinterpret_cast<ana::Bvh4Node*>(B.at(B.o_tri_nodes));
+    auto* isect = devTris ? nullptr : reinterpret_cast<float4*>(B.at(B.o_tri_isect));
+    auto* shade = devTris ? nullptr : reinterpret_cast<float4*>(B.at(B.o_tri_shade));
+    auto* snodes = reinterpret_cast<ana::BvhNode*>(B.at(B.o_seg_nodes));
+    auto* segs = reinterpret_cast<float4*>(B.at(B.o_segs));
+    auto* scol = reinterpret_cast<float*>(B.at(B.o_scol));
+    auto* mats = reinterpret_cast<ana::DevMaterial*>(B.at(B.o_mats));
+    auto* slots = reinterpret_cast<int32_t*>(B.at(B.o_slots));
+    auto* lights = reinterpret_cast<ana::DevLight*>(B.at(B.o_lights));
     // 4-wide triangle nodes: interior refs shift by the scene's node base, the
     // first-triangle field of leaf entries (bits 0..24) by its primitive base
     auto fix_node4 = [](ana::Bvh4Node nd, uint32_t nodeBase, uint32_t primBase) {
@@ -172,9 +184,14 @@ int build_blob(const ana::Prepared* const* list, uint32_t n, Blob& B, std::strin
         SceneStatic& st = B.scenes[k];
         const uint32_t nodeBase = uint32_t(iN), triBase = uint32_t(iT), sNodeBase = uint32_t(iSN),
                        segBase = uint32_t(iS), strBase = uint32_t(iStr), matBase = uint32_t(iM);
-        st.tri_root = (P.num_tris && !P.tri_nodes.empty()) ? nodeBase : ana::kNoRoot;
+        if (P.tris_on_device) {  // sections copied from the device build
+            st.tri_root = nodeBase;
+            iN += P.dev_tri_nodes;
+        } else {
+            st.tri_root = (P.num_tris && !P.tri_nodes.empty()) ? nodeBase : ana::kNoRoot;
+        }
         for (const ana::Bvh4Node& nd : P.tri_nodes) nodes[iN++] = fix_node4(nd, nodeBase, triBase);
-        for (uint32_t t = 0; t < P.num_tris; ++t) {
+        for (uint32_t t = 0; t < (P.tris_on_device ? 0u : P.num_tris); ++t) {
             float4 a = P.tri_isect[3 * size_t(t)];
             a.w = fbits(ubits(a.w) + triBase);  // index into the batch's shading array
             isect[3 * (size_t(triBase) + t)] = a;
@@ -210,12 +227,12 @@ int build_blob(const ana::Prepared* const* list, uint32_t n, Blob& B, std::strin
         if (P.has_transmit) B.has_transmit = true;
     }
     if (dome) {
-        std::memcpy(B.mem + B.o_env_rgb, dome->env.rgb.data(), dome->env.rgb.size() * 4);
-        std::memcpy(B.mem + B.o_cf, dome->env.cond_func.data(), dome->env.cond_func.size() * 4);
-        std::memcpy(B.mem + B.o_cc, dome->env.cond_cdf.data(), dome->env.cond_cdf.size() * 4);
-        std::memcpy(B.mem + B.o_ci, dome->env.cond_int.data(), dome->env.cond_int.size() * 4);
-        std::memcpy(B.mem + B.o_mf, dome->env.marg_func.data(), dome->env.marg_func.size() * 4);
-        std::memcpy(B.mem + B.o_mc, dome->env.marg_cdf.data(), dome->env.marg_cdf.size() * 4);
+        std::memcpy(B.at(B.o_env_rgb), dome->env.rgb.data(), dome->env.rgb.size() * 4);
+        std::memcpy(B.at(B.o_cf), dome->env.cond_func.data(), dome->env.cond_func.size() * 4);
+        std::memcpy(B.at(B.o_cc), dome->env.cond_cdf.data(), dome->env.cond_cdf.size() * 4);
+        std::memcpy(B.at(B.o_ci), dome->env.cond_int.data(), dome->env.cond_int.size() * 4);
+        std::memcpy(B.at(B.o_mf), dome->env.marg_func.data(), dome->env.marg_func.size() * 4);
+        std::memcpy(B.at(B.o_mc), dome->env.marg_cdf.data(), dome->env.marg_cdf.size() * 4);
         B.env_meta.present = true;
         B.env_meta.width = dome->env.width;
         B.env_meta.height = dome->env.height;
@@ -252,6 +269,7 @@ struct ana_ctx {
     // scenes
     unsigned char* d_scene = nullptr;
     size_t d_scene_size = 0;
+    size_t scene_bytes = 0;  // bytes of the uploaded arena in use
     ana::DevScene ds{};
     std::vector<SceneStatic> scenes;
     bool has_scene = false;
@@ -380,11 +398,31 @@ int ensure_queues(ana_ctx* c, uint32_t cap) {
     return ANA_OK;
 }
 
-int upload_blob(ana_ctx* c, const Blob& B) {
+// Copies a blob into the device arena. With `dt` the triangle sections come
+// from a device build (device-to-device) and the blob holds the rest.
+int upload_blob(ana_ctx* c, const Blob& B, const ana::DeviceTris* dt = nullptr) {
     CK(cudaSetDevice(c->device), "cudaSetDevice");
     int rc = ensure_buffer(c, &c->d_scene, &c->d_scene_size, B.size, "cudaMalloc(scene)");
     if (rc) return rc;
-    CK(cudaMemcpyAsync(c->d_scene, B.mem, B.size, cudaMemcpyHostToDevice, c->stream), "scene upload");
+    if (dt) {
+        CK(cudaMemsetAsync(c->d_scene, 0, B.o_seg_nodes, c->stream), "scene clear");
+        CK(cudaMemcpyAsync(c->d_scene + B.o_tri_nodes, dt->nodes, size_t(dt->num_nodes) * sizeof(ana::Bvh4Node),
+                           cudaMemcpyDeviceToDevice, c->stream),
+           "triangle nodes D2D");
+        CK(cudaMemcpyAsync(c->d_scene + B.o_tri_isect, dt->isect, size_t(dt->num_tris) * 48, cudaMemcpyDeviceToDevice,
+                           c->stream),
+           "triangle records D2D");
+        CK(cudaMemcpyAsync(c->d_scene + B.o_tri_shade, dt->shade, size_t(dt->num_tris) * 64, cudaMemcpyDeviceToDevice,
+                           c->stream),
+           "triangle shading D2D");
+        CK(cudaMemcpyAsync(c->d_scene + B.o_seg_nodes, B.at(B.o_seg_nodes), B.size - B.o_seg_nodes,
+                           cudaMemcpyHostToDevice, c->stream),
+           "scene upload");
+    } else {
+        if (B.host_base) return fail(c, ANA_ERR_STATE, "scene upload: the triangle sections are missing");
+        CK(cudaMemcpyAsync(c->d_scene, B.mem, B.size, cudaMemcpyHostToDevice, c->stream), "scene upload");
+    }
+    c->scene_bytes = B.size;
     unsigned char* b = c->d_scene;
     ana::DevScene& S = c->ds;
     S = ana::DevScene{};
@@ -402,7 +440,7 @@ int upload_blob(ana_ctx* c, const Blob& B) {
     S.has_transmit = B.has_transmit ? 1 : 0;
     S.has_fibers = S.has_curves;
     {
-        const auto* mats = reinterpret_cast<const ana::DevMaterial*>(B.mem + B.o_mats);
+        const auto* mats = reinterpret_cast<const ana::DevMaterial*>(B.at(B.o_mats));
         for (size_t i = 0; i < B.n_mats; ++i)
             if (mats[i].type == ANA_MAT_HAIR) S.has_fibers = 1;
     }
@@ -421,8 +459,8 @@ int upload_blob(ana_ctx* c, const Blob& B) {
     c->scenes = B.scenes;
     c->has_scene = true;
     c->upload_serial++;
-    const auto* hm = reinterpret_cast<const ana::DevMaterial*>(B.mem + B.o_mats);
-    const auto* hl = reinterpret_cast<const ana::DevLight*>(B.mem + B.o_lights);
+    const auto* hm = reinterpret_cast<const ana::DevMaterial*>(B.at(B.o_mats));
+    const auto* hl = reinterpret_cast<const ana::DevLight*>(B.at(B.o_lights));
     c->h_mats.assign(hm, hm + B.n_mats);
     c->h_lights.assign(hl, hl + B.n_lights);
     c->o_mats = B.o_mats;
@@ -795,7 +833,11 @@ int render_items(ana_ctx* c, const std::vector<Item>& items, uint64_t totalPixel
     float ms = 0.f;
     cudaEventElapsedTime(&ms, c->ev0, c->ev1);
     ana_stats& st = c->stats;
+    const ana_stats up = st;  // the upload fields describe the last upload
     st = ana_stats{};
+    st.upload_ms = up.upload_ms;
+    for (int k = 0; k < 4; ++k) st.build_ms[k] = up.build_ms[k];
+    st.build_levels = up.build_levels;
     st.paths = totalPaths;
     for (uint32_t k = 0; k < nchunks * (backward ? 2u : 1u); ++k)
         for (uint32_t b = 0; b < rows; ++b) {
@@ -1013,6 +1055,7 @@ int ana_upload_prepared(ana_ctx* c, const ana_prepared* p) {
 
 int ana_upload_scene(ana_ctx* c, const ana_scene_desc* d) {
     if (!c || !d) return fail(c, ANA_ERR_INVALID_ARG, "ana_upload_scene: NULL argument");
+    const auto t0 = std::chrono::steady_clock::now();
     ana_prepared* p = nullptr;
     int rc = ana_prepare_scene(d, &p);
     if (rc != ANA_OK) {
@@ -1026,7 +1069,68 @@ int ana_upload_scene(ana_ctx* c, const ana_scene_desc* d) {
         if (e != cudaSuccess) rc = cuda_fail(c, e, "scene upload sync");
     }
     ana_prepared_free(p);
+    for (int k = 0; k < 4; ++k) c->stats.build_ms[k] = 0.f;
+    c->stats.build_levels = 0;
+    c->stats.upload_ms =
+        std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
     return rc;
+}
+
+int ana_upload_scene_device(ana_ctx* c, const ana_scene_desc* d) {
+    if (!c || !d) return fail(c, ANA_ERR_INVALID_ARG, "ana_upload_scene_device: NULL argument");
+    const auto t0 = std::chrono::steady_clock::now();
+    CK(cudaSetDevice(c->device), "cudaSetDevice");
+    std::unique_ptr<ana_prepared> pp(new (std::nothrow) ana_prepared());
+    if (!pp) return fail(c, ANA_ERR_OOM, "ana_upload_scene_device: host allocation failed");
+    std::string err;
+    ana::DeviceTris dt;
+    int rc;
+    try {
+        rc = ana::prepare_scene(*d, pp->P, err, true);
+        if (rc == ANA_OK && pp->P.tris_on_device) {
+            const uint32_t maxLeaf = d->max_leaf_tris ? d->max_leaf_tris : 4;
+            rc = ana::build_tris_on_device(*d, maxLeaf, c->stream, dt, err);
+            pp->P.dev_tri_nodes = dt.num_nodes;
+        }
+        if (rc == ANA_OK) {
+            const ana::Prepared* one = &pp->P;
+            rc = build_blob(&one, 1, pp->blob, err);
+        }
+    } catch (const std::bad_alloc&) {
+        return fail(c, ANA_ERR_OOM, "ana_upload_scene_device: host allocation failed");
+    }
+    if (rc != ANA_OK) {
+        cudaStreamSynchronize(c->stream);
+        return fail(c, rc, "ana_upload_scene_device: " + err);
+    }
+    rc = upload_blob(c, pp->blob, pp->P.tris_on_device ? &dt : nullptr);
+    cudaError_t e = cudaStreamSynchronize(c->stream);  // before the build buffers are freed
+    if (rc == ANA_OK && e != cudaSuccess) rc = cuda_fail(c, e, "scene upload sync");
+    for (int k = 0; k < 4; ++k) c->stats.build_ms[k] = dt.ms[k];
+    c->stats.build_levels = dt.levels;
+    c->stats.upload_ms =
+        std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return rc;
+}
+
+static uint64_t fnv1a(const unsigned char* p, size_t n) {
+    uint64_t h = 1469598103934665603ULL;
+    for (size_t i = 0; i < n; ++i) {
+        h ^= p[i];
+        h *= 1099511628211ULL;
+    }
+    return h;
+}
+
+int ana_scene_digest(ana_ctx* c, uint64_t* out) {
+    if (!c || !out) return fail(c, ANA_ERR_INVALID_ARG, "ana_scene_digest: NULL argument");
+    if (!c->has_scene) return fail(c, ANA_ERR_STATE, "ana_scene_digest: no scene uploaded");
+    CK(cudaSetDevice(c->device), "cudaSetDevice");
+    std::vector<unsigned char> h(c->scene_bytes);
+    CK(cudaMemcpyAsync(h.data(), c->d_scene, h.size(), cudaMemcpyDeviceToHost, c->stream), "scene D2H");
+    CK(cudaStreamSynchronize(c->stream), "scene D2H sync");
+    *out = fnv1a(h.data(), h.size());
+    return ANA_OK;
 }
 
 int ana_batch_create(const ana_prepared* const* scenes, uint32_t count, ana_batch** out) {

@@ -511,7 +511,7 @@ void derive_standard(DevMaterial& o) {
     o.is_delta = (smoothGlass || (r < 0.001f && (o.metal > 0.999f || o.spec > 0.f))) ? 1 : 0;
 }
 
-int prepare_scene(const ana_scene_desc& d, Prepared& P, std::string& err) {
+int prepare_scene(const ana_scene_desc& d, Prepared& P, std::string& err, bool tris_on_device) {
     auto bad = [&](const char* m) {
         err = m;
         return int(ANA_ERR_INVALID_ARG);
@@ -535,10 +535,17 @@ int prepare_scene(const ana_scene_desc& d, Prepared& P, std::string& err) {
     // Leaf references carry the first primitive in 25 bits (traverse.cuh).
     if (T >= (1u << 25)) return bad("more than 2^25 triangles");
     P.num_tris = T;
-    std::vector<float4> isect(size_t(T) * 3);  // build order = mesh order first
-    P.tri_shade.assign(size_t(T) * 4, make_float4(0, 0, 0, 0));
-    std::vector<PrimInfo> pi(T);
-    for (uint32_t m = 0; m < d.num_meshes; ++m) {
+    P.tris_on_device = tris_on_device && T > 0;
+    P.dev_tri_nodes = 0;
+    if (P.tris_on_device) {
+        for (uint32_t m = 0; m < d.num_meshes; ++m)
+            if (d.mesh_vert_offset[m + 1] < d.mesh_vert_offset[m] || d.mesh_tri_offset[m + 1] < d.mesh_tri_offset[m])
+                return bad("mesh offsets not monotone");
+    }
+    std::vector<float4> isect(P.tris_on_device ? 0 : size_t(T) * 3);  // build order = mesh order first
+    P.tri_shade.assign(P.tris_on_device ? 0 : size_t(T) * 4, make_float4(0, 0, 0, 0));
+    std::vector<PrimInfo> pi(P.tris_on_device ? 0 : T);
+    for (uint32_t m = 0; m < (P.tris_on_device ? 0u : d.num_meshes); ++m) {
         uint32_t v0i = d.mesh_vert_offset[m], v1i = d.mesh_vert_offset[m + 1];
         uint32_t t0 = d.mesh_tri_offset[m], t1 = d.mesh_tri_offset[m + 1];
         if (v1i < v0i || t1 < t0) return bad("mesh offsets not monotone");
@@ -587,7 +594,10 @@ int prepare_scene(const ana_scene_desc& d, Prepared& P, std::string& err) {
     uint32_t maxLeafS = d.max_leaf_segments ? d.max_leaf_segments : 4;
     if (maxLeafT > 64 || maxLeafS > 64) return bad("leaf size > 64");
     P.tri_isect.clear();
-    if (T > 0) {
+    if (P.tris_on_device) {
+        P.tri_nodes.clear();
+        P.tri_root_is_empty = false;
+    } else if (T > 0) {
         NodePool pool(2 * size_t(T) + 1);
         uint32_t root = sah_build(pi, 0, T, maxLeafT, pool, 0);
         P.tri_isect.reserve(size_t(T) * 3);

@@ -36,6 +36,11 @@ struct Prepared {
     uint32_t num_tris = 0, num_segs = 0;
     bool has_emitters = false;
     bool has_transmit = false;  // a slot's material has a non-black shadow tint
+    // Triangle sections built on the device (build_tris_on_device): tri_nodes,
+    // tri_isect and tri_shade stay empty, num_tris is set and the node count
+    // is filled in once the device build has run.
+    bool tris_on_device = false;
+    uint32_t dev_tri_nodes = 0;
     uint64_t bytes() const;
 };
 
@@ -45,8 +50,10 @@ struct Prepared {
 // (StandardSurface.h:152-181, 384).
 void derive_standard(DevMaterial& m);
 
-// Returns ANA_OK or an error code with a message in err.
-int prepare_scene(const ana_scene_desc& d, Prepared& out, std::string& err);
+// Returns ANA_OK or an error code with a message in err. With
+// tris_on_device the triangle sections are left to the device build (the
+// mesh offsets are still validated here).
+int prepare_scene(const ana_scene_desc& d, Prepared& out, std::string& err, bool tris_on_device = false);
 
 // Camera::makePinhole (include/anacapa/integrator/IIntegrator.h:49-74) for a film size.
 DevCamera make_camera(const ana_camera& c, uint32_t width, uint32_t height);

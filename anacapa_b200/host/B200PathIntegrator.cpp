@@ -359,11 +359,11 @@ bool B200PathIntegrator::upload(const SceneView& scene) {
     // rebuilt per frame from the film size
     uint32_t w = scene.camera ? scene.camera->imageWidth : 1, h = scene.camera ? scene.camera->imageHeight : 1;
     std::string err;
-    ana_prepared* p = prepareHost(scene, w, h, err);
-    if (!p) return fail(err);
-    const int rc = ana_upload_prepared(m_ctx, p);
-    ana_prepared_free(p);
-    if (rc != ANA_OK) return fail(ana_message(m_ctx));
+    Flat F;
+    if (!flatten(scene, w, h, F, err)) return fail("B200PathIntegrator: " + err);
+    // triangle setup and SAH build on the device: the bytes prepareHost's
+    // layout would upload, without the host build (BVHBackend::commit)
+    if (ana_upload_scene_device(m_ctx, &F.d) != ANA_OK) return fail(ana_message(m_ctx));
     m_prepared = &scene;
     return true;
 }

@@ -234,6 +234,11 @@ typedef struct ana_stats {
     uint64_t tri_tests;         /*   triangle tests (48 bytes each)              */
     uint64_t seg_tests;         /*   curve segment tests (80 bytes each)         */
     uint64_t curve_node_fetches;/*   64-byte curve BVH node loads                */
+    float upload_ms;            /* wall time of the last scene upload call      */
+    float build_ms[4];          /* ana_upload_scene_device phases (wall time):
+                                   inputs + triangle setup, SAH levels, small
+                                   subtrees, 4-wide collapse + layout           */
+    uint32_t build_levels;      /* SAH levels run over the large nodes          */
 } ana_stats;
 
 typedef struct ana_ctx ana_ctx;
@@ -263,6 +268,18 @@ void ana_destroy(ana_ctx* ctx);
  * src/accel/CurveBrute.cpp:247-396). Replaces IIntegrator::prepare
  * (include/anacapa/integrator/IIntegrator.h:177) + IAccelerationStructure::commit. */
 int ana_upload_scene(ana_ctx* ctx, const ana_scene_desc* scene);
+
+/* ana_upload_scene with the triangle setup and SAH BVH build of
+ * BVHBackend::commit (src/accel/BVHBackend.cpp:17-228) run on the device:
+ * level-synchronous binned SAH over the large nodes, one thread per small
+ * subtree, the 4-wide collapse on the device. The uploaded bytes equal
+ * ana_upload_scene's (ana_scene_digest). Curves, materials, lights and the
+ * dome are prepared on the host as there. */
+int ana_upload_scene_device(ana_ctx* ctx, const ana_scene_desc* scene);
+
+/* FNV-1a 64 of the uploaded scene arena (no counterpart in the reference):
+ * equals ana_prepared_digest of the same scene prepared on the host. */
+int ana_scene_digest(ana_ctx* ctx, uint64_t* out);
 
 /* Host-side scene preparation split from the device copy, so a caller can
  * build once and re-upload: ana_prepare_scene builds the device layout on the
