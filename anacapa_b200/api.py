@@ -70,7 +70,8 @@ class AnaSceneDesc(C.Structure):
                 ("slot_material", _P), ("num_lights", C.c_uint32), ("lights", _P),
                 ("env_rgb", _P), ("env_width", C.c_uint32), ("env_height", C.c_uint32),
                 ("env_intensity", C.c_float), ("env_radiance", F3), ("camera", AnaCamera),
-                ("max_leaf_tris", C.c_uint32), ("max_leaf_segments", C.c_uint32)]
+                ("max_leaf_tris", C.c_uint32), ("max_leaf_segments", C.c_uint32),
+                ("mesh_motion_offset", _P), ("motion_keys", _P)]
 
 
 class AnaRenderDesc(C.Structure):
@@ -299,6 +300,7 @@ class SceneDesc:
         cam.at[:] = sc.cam_at
         cam.up[:] = sc.cam_up
         cam.vfov_deg = sc.vfov
+        cam.shutter_open, cam.shutter_close = sc.shutter
         if sc.cam_basis is not None:
             b = [float(x) for x in sc.cam_basis]
             cam.explicit_basis = 1
@@ -308,6 +310,15 @@ class SceneDesc:
         d.camera = cam
         d.max_leaf_tris = max_leaf_tris
         d.max_leaf_segments = max_leaf_segments
+        if sc.mesh_motion is not None and any(k for k in sc.mesh_motion):
+            off = np.zeros(sc.num_meshes + 1, np.uint32)
+            rows = []
+            for m in range(sc.num_meshes):
+                keys = sc.mesh_motion[m] or []
+                off[m + 1] = off[m] + len(keys)
+                rows += [[t, *np.asarray(M, np.float32).reshape(16)] for t, M in keys]
+            d.mesh_motion_offset = _ptr(arr(off, np.uint32))
+            d.motion_keys = _ptr(arr(np.asarray(rows, np.float32).reshape(-1, 17), np.float32))
         self.desc = d
         self._keep = keep
 

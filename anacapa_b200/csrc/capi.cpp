@@ -59,9 +59,10 @@ struct Blob {
     size_t host_base = 0;  // > 0: the triangle sections come from a device build
     bool pinned = false;
     size_t o_tri_nodes = 0, o_tri_isect = 0, o_tri_shade = 0, o_seg_nodes = 0, o_segs = 0, o_scol = 0, o_mats = 0,
-           o_slots = 0, o_lights = 0, o_env_rgb = 0, o_cf = 0, o_cc = 0, o_ci = 0, o_mf = 0, o_mc = 0;
+           o_slots = 0, o_lights = 0, o_env_rgb = 0, o_cf = 0, o_cc = 0, o_ci = 0, o_mf = 0, o_mc = 0,
+           o_motion = 0, o_keys = 0;
     std::vector<SceneStatic> scenes;
-    bool has_curves = false, has_emitters = false, has_transmit = false;
+    bool has_curves = false, has_emitters = false, has_transmit = false, has_motion = false;
     size_t n_mats = 0, n_lights = 0;
     ana::HostEnv env_meta;  // scalars only
     unsigned char* at(size_t off) const { return mem + (off - host_base); }
@@ -76,7 +77,8 @@ struct Blob {
 };
 
 int build_blob(const ana::Prepared* const* list, uint32_t n, Blob& B, std::string& err) {
-    size_t nNodes = 0, nTris = 0, nSegNodes = 0, nSegs = 0, nStr = 0, nMats = 0, nSlots = 0, nLights = 0;
+    size_t nNodes = 0, nTris = 0, nSegNodes = 0, nSegs = 0, nStr = 0, nMats = 0, nSlots = 0, nLights = 0,
+           nMotion = 0, nKeyVec = 0;
     const ana::Prepared* dome = nullptr;
     for (uint32_t k = 0; k < n; ++k) {
         const ana::Prepared& P = *list[k];
@@ -92,6 +94,8 @@ int build_blob(const ana::Prepared* const* list, uint32_t n, Blob& B, std::strin
         nMats += P.materials.size();
         nSlots += P.slot_material.size();
         nLights += P.lights.size();
+        nMotion += P.mesh_motion.size();
+        nKeyVec += P.motion_keys.size();
         if (P.env.present) {
             if (dome) {
                 err = "a batch may hold at most one dome light";
@@ -127,6 +131,8 @@ int build_blob(const ana::Prepared* const* list, uint32_t n, Blob& B, std::strin
     B.o_ci = take(dome ? dome->env.cond_int.size() * 4 : 0);
     B.o_mf = take(dome ? dome->env.marg_func.size() * 4 : 0);
     B.o_mc = take(dome ? dome->env.marg_cdf.size() * 4 : 0);
+    B.o_motion = take(nMotion * sizeof(uint2));
+    B.o_keys = take(nKeyVec * 16);
     B.size = std::max<size_t>(off, kAlign);
     bool devTris = false;
     for (uint32_t k = 0; k < n; ++k) devTris = devTris || list[k]->tris_on_device;
@@ -155,6 +161,8 @@ int build_blob(const ana::Prepared* const* list, uint32_t n, Blob& B, std::strin
     auto* mats = reinterpret_cast<ana::DevMaterial*>(B.at(B.o_mats));
     auto* slots = reinterpret_cast<int32_t*>(B.at(B.o_slots));
     auto* lights = reinterpret_cast<ana::DevLight*>(B.at(B.o_lights));
+    auto* motion = reinterpret_cast<uint2*>(B.at(B.o_motion));
+    auto* keys = reinterpret_cast<float4*>(B.at(B.o_keys));
     // 4-wide triangle nodes: interior refs shift by the scene's node base, the
     // first-triangle field of leaf entries (bits 0..24) by its primitive base
     auto fix_node4 = [](ana::Bvh4Node nd, uint32_t nodeBase, uint32_t primBase) {
@@ -174,8 +182,9 @@ int build_blob(const ana::Prepared* const* list, uint32_t n, Blob& B, std::strin
         }
         return nd;
     };
-    size_t iN = 0, iT = 0, iSN = 0, iS = 0, iStr = 0, iM = 0, iSl = 0, iL = 0;
+    size_t iN = 0, iT = 0, iSN = 0, iS = 0, iStr = 0, iM = 0, iSl = 0, iL = 0, iMo = 0, iK = 0;
     B.scenes.assign(n, SceneStatic{});
+    B.has_motion = nMotion > 0;
     B.has_curves = false;
     B.has_emitters = false;
     B.has_transmit = false;
@@ -191,15 +200,20 @@ int build_blob(const ana::Prepared* const* list, uint32_t n, Blob& B, std::strin
             st.tri_root = (P.num_tris && !P.tri_nodes.empty()) ? nodeBase : ana::kNoRoot;
         }
         for (const ana::Bvh4Node& nd : P.tri_nodes) nodes[iN++] = fix_node4(nd, nodeBase, triBase);
+        const uint32_t motionBase = uint32_t(iMo), keyBase = uint32_t(iK / 5);
         for (uint32_t t = 0; t < (P.tris_on_device ? 0u : P.num_tris); ++t) {
             float4 a = P.tri_isect[3 * size_t(t)];
-            a.w = fbits(ubits(a.w) + triBase);  // index into the batch's shading array
+            float4 e1 = P.tri_isect[3 * size_t(t) + 1];
+            a.w = fbits(ubits(a.w) + triBase);  // index into the batch's shading array (bit 31 kept)
+            if (ubits(a.w) & 0x80000000u) e1.w = fbits(ubits(e1.w) + motionBase);  // batch motion mesh
             isect[3 * (size_t(triBase) + t)] = a;
-            isect[3 * (size_t(triBase) + t) + 1] = P.tri_isect[3 * size_t(t) + 1];
+            isect[3 * (size_t(triBase) + t) + 1] = e1;
             isect[3 * (size_t(triBase) + t) + 2] = P.tri_isect[3 * size_t(t) + 2];
             for (int j = 0; j < 4; ++j) shade[4 * (size_t(triBase) + t) + j] = P.tri_shade[4 * size_t(t) + j];
         }
         iT += P.num_tris;
+        for (const uint2& mo : P.mesh_motion) motion[iMo++] = make_uint2(mo.x + keyBase, mo.y);
+        for (const float4& k4 : P.motion_keys) keys[iK++] = k4;
         st.seg_root = (P.num_segs && !P.seg_nodes.empty()) ? sNodeBase : ana::kNoRoot;
         if (P.num_segs) B.has_curves = true;
         for (const ana::BvhNode& nd : P.seg_nodes) snodes[iSN++] = fix_node(nd, sNodeBase, segBase);
@@ -438,6 +452,9 @@ int upload_blob(ana_ctx* c, const Blob& B, const ana::DeviceTris* dt = nullptr) 
     S.has_curves = B.has_curves ? 1 : 0;
     S.has_emitters = B.has_emitters ? 1 : 0;
     S.has_transmit = B.has_transmit ? 1 : 0;
+    S.mesh_motion = reinterpret_cast<const uint2*>(b + B.o_motion);
+    S.motion_keys = reinterpret_cast<const float4*>(b + B.o_keys);
+    S.has_motion = B.has_motion ? 1 : 0;
     S.has_fibers = S.has_curves;
     {
         const auto* mats = reinterpret_cast<const ana::DevMaterial*>(B.at(B.o_mats));
@@ -1463,6 +1480,8 @@ int ana_forward(ana_ctx* c, const ana_render_desc* d, const ana_diff_params* par
     for (const ana::DevMaterial& m : c->h_mats)
         if (m.transmission > 0.001f || m.opacity < 1.f || m.tint.x != 0.f || m.tint.y != 0.f || m.tint.z != 0.f)
             return fail(c, ANA_ERR_UNSUPPORTED, "ana_forward: glass and alpha-masked materials are not differentiated");
+    if (c->ds.has_motion)
+        return fail(c, ANA_ERR_UNSUPPORTED, "ana_forward: motion-blurred meshes are not differentiated");
     CK(cudaSetDevice(c->device), "cudaSetDevice");
     c->fwd_valid = false;
     if (params) {

@@ -100,6 +100,17 @@ __device__ __forceinline__ void path_coords(const DevSceneRec& R, uint32_t gid, 
     py = R.rect_y0 + ly;
 }
 
+// The ray time of a path: Camera::generateRay's shutterOpen + timeU *
+// (shutterClose - shutterOpen) with timeU its sample dimension 4; every ray of
+// the path carries it (PathIntegrator.cpp:148-149, 185, 221).
+__device__ __forceinline__ float path_time(const DevSceneRec& R, uint32_t gid) {
+    uint32_t px, py, sidx;
+    path_coords(R, gid, px, py, sidx);
+    SampleStream ss{R.seed, px, py, sidx, 4};
+    const float u = ss.next();
+    return xadd(R.cam.shutter_open, xmul(u, xsub(R.cam.shutter_close, R.cam.shutter_open)));
+}
+
 // Film index of an item's pixel (its index within the item's rectangle).
 __device__ __forceinline__ size_t film_index(const DevSceneRec& R, uint32_t pixel) {
     const uint32_t ly = pixel / R.rect_w;
@@ -229,11 +240,11 @@ __device__ __forceinline__ void warp_add_work(unsigned long long* work, const Co
 //   kPersist: persistent warps with per-lane refill (persistent_traverse);
 //   otherwise one thread per ray over a grid-stride loop.
 // Both use the same interior/leaf steps, so results are identical.
-template <bool kAny, bool kCount, bool kPersist, bool kCurves, class Load, class Done>
+template <bool kAny, bool kCount, bool kPersist, bool kCurves, bool kMotion = false, class Load, class Done>
 __device__ __forceinline__ void run_traversal(const DevScene& S, uint32_t n, uint32_t* fetch, uint32_t* err,
                                               Counters* cnt, Load load, Done done) {
     if constexpr (kPersist) {
-        persistent_traverse<kAny, kCount, kCurves>(S, n, fetch, err, cnt, load, done);
+        persistent_traverse<kAny, kCount, kCurves, kMotion>(S, n, fetch, err, cnt, load, done);
     } else {
         uint32_t stack[kMaxStack4];
         float stackT[kMaxStack4];
@@ -248,7 +259,7 @@ __device__ __forceinline__ void run_traversal(const DevScene& S, uint32_t n, uin
                     while (!T.exhausted) {
                         if (!(T.cur & 0x80000000u)) {
                             node_step<kAny, kCount, kCurves>(T, S, stack, stackT, err, cnt);
-                        } else if (leaf_step<kAny, kCount, kCurves>(T, S, T.cur, cnt)) {
+                        } else if (leaf_step<kAny, kCount, kCurves, kMotion>(T, S, T.cur, cnt)) {
                             T.exhausted = true;
                         } else if (!trav_pop(T, stack, stackT)) {
                             T.exhausted = true;
@@ -274,17 +285,18 @@ __device__ __forceinline__ uint32_t scene_bits(float w) { return __float_as_uint
 // extend: closest hit of every live path (PathIntegrator::Li, line 81).
 // kCount: the same traversal, counting node fetches and primitive tests
 // (warp-aggregated into p.work) to derive the stage's algorithmic bytes.
-template <bool kCount, bool kCurves, bool kPersist>
+template <bool kCount, bool kCurves, bool kPersist, bool kMotion = false>
 __global__ void ANA_TRAVERSAL_BOUNDS k_extend(const __grid_constant__ Params p) {
     const uint32_t cur = p.bounce & 1u;
     uint32_t* cb = p.counters + p.bounce * kCountersPerBounce;
     Counters cnt{0, 0, 0, 0};
-    run_traversal<false, kCount, kPersist, kCurves>(
+    run_traversal<false, kCount, kPersist, kCurves, kMotion>(
         p.S, cb[0], cb + 3, p.err, &cnt,
         [&](uint32_t i, Ray& r, uint32_t& root, uint32_t& segRoot) {
             float4 o = p.q.ext_o[cur][i], d = p.q.ext_d[cur][i];
             r = Ray{f3(o), f3(d), 1e-4f, INFINITY};
             const DevSceneRec& R = p.S.scenes[scene_bits(p.q.ext_b[cur][i].w)];
+            if constexpr (kMotion) r.time = path_time(R, __float_as_uint(o.w));
             root = R.tri_root;
             segRoot = kCurves ? R.seg_root : kNoRoot;
         },
@@ -300,21 +312,31 @@ __global__ void ANA_TRAVERSAL_BOUNDS k_extend(const __grid_constant__ Params p) 
 // BVHBackend.cpp:285-317; CurveBrute intersectOneSegment, CurveBrute.cpp:209-233).
 template <bool kCurves = true>
 __device__ __forceinline__ SurfInt surf_int(const DevScene& S, float3 o, float3 d, float t, uint32_t prim, float u,
-                                            float v, float4 h1) {
+                                            float v, float4 h1, float time = 0.f) {
     SurfInt si;
     if (!kCurves || !(prim & 0x80000000u)) {
         const float4* tp = S.tri_isect + 3 * size_t(prim);
         float4 a = ldg4(tp), e1 = ldg4(tp + 1), e2 = ldg4(tp + 2);
-        uint32_t orig = __float_as_uint(a.w);
+        const uint32_t ow = __float_as_uint(a.w), orig = ow & 0x01FFFFFFu;
         const float4* sp = S.tri_shade + 4 * size_t(orig);
         float4 s0 = ldg4(sp), s1 = ldg4(sp + 1), s2 = ldg4(sp + 2), s3 = ldg4(sp + 3);
         float w = 1.f - u - v;
         si.p = f3(a) + f3(e1) * u + f3(e2) * v;
         si.ng = f3(s0);
         float3 sn = safe_normalize(f3(s1) * w + f3(s2) * u + f3(s3) * v);
+        si.dpdu = f3(e1);
+        if (ow & 0x80000000u) {
+            // object-space triangle (fillSurfaceInteraction with worldXfm,
+            // BVHBackend.cpp:290-300): objectToWorld at the ray's time
+            M4 M;
+            o2w_at(S, __float_as_uint(e1.w), time, M);
+            si.p = m4_point(M, si.p);
+            si.ng = xsafe_normalize(m4_normal(M, si.ng));
+            sn = xsafe_normalize(m4_normal(M, sn));
+            si.dpdu = m4_vector(M, si.dpdu);
+        }
         if (dot(sn, si.ng) < 0.f) sn = -sn;
         si.n = sn;
-        si.dpdu = f3(e1);
         si.slot = __float_as_uint(s0.w);
         si.color = f3(1.f, 1.f, 1.f);
         si.is_curve = false;
@@ -348,7 +370,7 @@ __device__ __forceinline__ int slot_material(const DevScene& S, const DevSceneRe
 // Mesh or strand slot (SurfaceInteraction::meshID) of a hit primitive.
 __device__ __forceinline__ uint32_t hit_slot(const DevScene& S, uint32_t prim) {
     if (prim & 0x80000000u) return __float_as_uint(ldg4(S.segs + 5 * size_t(prim & 0x7FFFFFFFu) + 4).z);
-    const uint32_t orig = __float_as_uint(ldg4(S.tri_isect + 3 * size_t(prim)).w);
+    const uint32_t orig = __float_as_uint(ldg4(S.tri_isect + 3 * size_t(prim)).w) & 0x01FFFFFFu;
     return __float_as_uint(ldg4(S.tri_shade + 4 * size_t(orig)).w);
 }
 
@@ -449,7 +471,8 @@ __global__ void __launch_bounds__(kMaxStageBlock) k_shade(const __grid_constant_
                 if (bounce == 0 || spec) Ladd = beta * scene_env(S, R, d);
             } else {
                 float4 h1 = (prim & 0x80000000u) ? p.q.hit1[i] : make_float4(0, 0, 0, 0);
-                SurfInt si = surf_int<kFiber>(S, o, d, h0.x, prim, h0.z, h0.w, h1);
+                const float time = S.has_motion ? path_time(R, pid) : 0.f;
+                SurfInt si = surf_int<kFiber>(S, o, d, h0.x, prim, h0.z, h0.w, h1, time);
                 int mi = slot_material(S, R, si.slot);
                 if (mi >= 0) {
                     const DevMaterial m = S.materials[mi];
@@ -643,15 +666,16 @@ __global__ void __launch_bounds__(kMaxStageBlock) k_shade(const __grid_constant_
 
 // NEE shadow rays: shadowTransmittance (src/integrator/ShadowRay.h:26-61) for
 // opaque scenes — any blocker in [1e-4, tmax] makes the transmittance black.
-template <bool kCurves, bool kPersist, bool kAdj>
+template <bool kCurves, bool kPersist, bool kAdj, bool kMotion = false>
 __global__ void ANA_TRAVERSAL_BOUNDS k_shadow(const __grid_constant__ Params p) {
     uint32_t* cb = p.counters + p.bounce * kCountersPerBounce;
-    run_traversal<true, false, kPersist, kCurves>(
+    run_traversal<true, false, kPersist, kCurves, kMotion>(
         p.S, cb[1], cb + 4, p.err, nullptr,
         [&](uint32_t i, Ray& r, uint32_t& root, uint32_t& segRoot) {
             float4 o = p.q.sh_o[i], d = p.q.sh_d[i];
             r = Ray{f3(o), f3(d), 1e-4f, d.w};
             const DevSceneRec& R = p.S.scenes[scene_bits(p.q.sh_c[i].w)];
+            if constexpr (kMotion) r.time = path_time(R, __float_as_uint(o.w));
             root = R.tri_root;
             segRoot = kCurves ? R.seg_root : kNoRoot;
         },
@@ -668,16 +692,17 @@ __global__ void ANA_TRAVERSAL_BOUNDS k_shadow(const __grid_constant__ Params p) 
 // batch without emissive surfaces every hit contributes zero, so the ray only
 // needs to know whether anything is hit (kAny): identical result, cheaper
 // query.
-template <bool kAny, bool kCurves, bool kPersist, bool kAdj>
+template <bool kAny, bool kCurves, bool kPersist, bool kAdj, bool kMotion = false>
 __global__ void ANA_TRAVERSAL_BOUNDS k_mis(const __grid_constant__ Params p) {
     uint32_t* cb = p.counters + p.bounce * kCountersPerBounce;
     const DevScene& S = p.S;
-    run_traversal<kAny, false, kPersist, kCurves>(
+    run_traversal<kAny, false, kPersist, kCurves, kMotion>(
         S, cb[2], cb + 5, p.err, nullptr,
         [&](uint32_t i, Ray& r, uint32_t& root, uint32_t& segRoot) {
             float4 o = p.q.mis_o[i], d = p.q.mis_d[i];
             r = Ray{f3(o), f3(d), 1e-4f, 1e10f};
             const DevSceneRec& R = S.scenes[scene_bits(p.q.mis_c[i].w)];
+            if constexpr (kMotion) r.time = path_time(R, __float_as_uint(o.w));
             root = R.tri_root;
             segRoot = kCurves ? R.seg_root : kNoRoot;
         },
@@ -711,14 +736,15 @@ __global__ void ANA_TRAVERSAL_BOUNDS k_mis(const __grid_constant__ Params p) {
 // is traced again from spawnRay(p, ng, d) with tMax = remaining - 1e-4.
 struct StepState {
     float3 tr, org;
-    float tmax;
+    float tmax, time;
     uint32_t steps;
     bool fresh;
-    __device__ void begin(float3 o, float tm) {
+    __device__ void begin(float3 o, float tm, float t) {
         if (!fresh) return;
         tr = f3(1.f, 1.f, 1.f);
         org = o;
         tmax = tm;
+        time = t;
         steps = 0;
         fresh = false;
     }
@@ -730,8 +756,8 @@ struct StepState {
         tooClose = remaining <= 1e-4f;
         if (tooClose || steps >= 7u) return false;
         const float4 h1 = make_float4(h.tang.x, h.tang.y, h.tang.z, h.tseg);
-        const SurfInt si = surf_int<kCurves>(S, org, d, h.t, h.prim, h.u, h.v, h1);
-        next = Ray{spawn_origin(si.p, si.ng, d), d, 1e-4f, remaining - 1e-4f};
+        const SurfInt si = surf_int<kCurves>(S, org, d, h.t, h.prim, h.u, h.v, h1, time);
+        next = Ray{spawn_origin(si.p, si.ng, d), d, 1e-4f, remaining - 1e-4f, time};
         org = next.o;
         tmax = next.tmax;
         ++steps;
@@ -743,19 +769,19 @@ struct StepState {
 // (src/integrator/ShadowRay.h:26-61) — an opaque surface (black
 // transmittanceColor) blocks, glass and alpha-masked surfaces tint; after 8
 // surfaces the tint so far is returned.
-template <bool kCurves, bool kPersist>
+template <bool kCurves, bool kPersist, bool kMotion = false>
 __global__ void ANA_TRAVERSAL_BOUNDS k_shadow_step(const __grid_constant__ Params p) {
     uint32_t* cb = p.counters + p.bounce * kCountersPerBounce;
     const DevScene& S = p.S;
     StepState st;
     st.fresh = true;
-    run_traversal<false, false, kPersist, kCurves>(
+    run_traversal<false, false, kPersist, kCurves, kMotion>(
         S, cb[1], cb + 4, p.err, nullptr,
         [&](uint32_t i, Ray& r, uint32_t& root, uint32_t& segRoot) {
             float4 o = p.q.sh_o[i], d = p.q.sh_d[i];
-            r = Ray{f3(o), f3(d), 1e-4f, d.w};
-            st.begin(r.o, r.tmax);
             const DevSceneRec& R = S.scenes[scene_bits(p.q.sh_c[i].w)];
+            r = Ray{f3(o), f3(d), 1e-4f, d.w, kMotion ? path_time(R, __float_as_uint(o.w)) : 0.f};
+            st.begin(r.o, r.tmax, r.time);
             root = R.tri_root;
             segRoot = kCurves ? R.seg_root : kNoRoot;
         },
@@ -782,19 +808,19 @@ __global__ void ANA_TRAVERSAL_BOUNDS k_shadow_step(const __grid_constant__ Param
 // 214-259): the first non-transmissive surface within 1e10 (or the 8th
 // transmissive one) gives Le, a miss or a last step closer than 1e-4 the
 // environment, times the tint of the surfaces passed.
-template <bool kCurves, bool kPersist>
+template <bool kCurves, bool kPersist, bool kMotion = false>
 __global__ void ANA_TRAVERSAL_BOUNDS k_mis_step(const __grid_constant__ Params p) {
     uint32_t* cb = p.counters + p.bounce * kCountersPerBounce;
     const DevScene& S = p.S;
     StepState st;
     st.fresh = true;
-    run_traversal<false, false, kPersist, kCurves>(
+    run_traversal<false, false, kPersist, kCurves, kMotion>(
         S, cb[2], cb + 5, p.err, nullptr,
         [&](uint32_t i, Ray& r, uint32_t& root, uint32_t& segRoot) {
             float4 o = p.q.mis_o[i], d = p.q.mis_d[i];
-            r = Ray{f3(o), f3(d), 1e-4f, 1e10f};
-            st.begin(r.o, r.tmax);
             const DevSceneRec& R = S.scenes[scene_bits(p.q.mis_c[i].w)];
+            r = Ray{f3(o), f3(d), 1e-4f, 1e10f, kMotion ? path_time(R, __float_as_uint(o.w)) : 0.f};
+            st.begin(r.o, r.tmax, r.time);
             root = R.tri_root;
             segRoot = kCurves ? R.seg_root : kNoRoot;
         },
@@ -945,7 +971,7 @@ __global__ void __launch_bounds__(256) k_film(const __grid_constant__ Params p) 
 
 // IAccelerationStructure::traceBatch / occludedBatch over CurveBrute semantics,
 // against one scene of the batch.
-template <bool kAny, bool kCurves, bool kPersist>
+template <bool kAny, bool kCurves, bool kPersist, bool kMotion = false>
 __global__ void ANA_TRAVERSAL_BOUNDS k_trace_batch(const __grid_constant__ DevScene S, uint32_t scene,
                                                    const float* rays, uint32_t n, ana_hit* out, uint32_t* fetch,
                                                    uint32_t* err) {
@@ -957,7 +983,8 @@ __global__ void ANA_TRAVERSAL_BOUNDS k_trace_batch(const __grid_constant__ DevSc
         root = triRoot;
         sroot = kCurves ? segRoot : kNoRoot;
     };
-    run_traversal<kAny, false, kPersist, kCurves>(S, n, fetch, err, nullptr, load, [&](uint32_t i, const Traversal& T) {
+    // rays carry no time: Ray::time's default 0 (Types.h:259)
+    run_traversal<kAny, false, kPersist, kCurves, kMotion>(S, n, fetch, err, nullptr, load, [&](uint32_t i, const Traversal& T) {
         ana_hit h{0, -1, -1, -1, 0.f, 0.f, 0.f, 0.f};
         if (kAny) {
             h.hit = finish_any<kCurves>(T) ? 1 : 0;
@@ -975,7 +1002,7 @@ __global__ void ANA_TRAVERSAL_BOUNDS k_trace_batch(const __grid_constant__ DevSc
                     h.prim_id = int32_t(__float_as_uint(rec.y));
                     h.strand_id = int32_t(__float_as_uint(rec.x) - __float_as_uint(rec.w));
                 } else {
-                    uint32_t orig = __float_as_uint(ldg4(S.tri_isect + 3 * size_t(sh.prim)).w);
+                    uint32_t orig = __float_as_uint(ldg4(S.tri_isect + 3 * size_t(sh.prim)).w) & 0x01FFFFFFu;
                     const float4* sp = S.tri_shade + 4 * size_t(orig);
                     h.mesh_id = int32_t(__float_as_uint(ldg4(sp).w));
                     h.prim_id = int32_t(__float_as_uint(ldg4(sp + 1).w));
@@ -1078,6 +1105,22 @@ void prime_kernels() {
     prime(k_mis_step<false, true>);
     prime(k_mis_step<true, false>);
     prime(k_mis_step<true, true>);
+    prime(k_extend<false, false, true, true>);
+    prime(k_extend<false, true, true, true>);
+    prime(k_shadow<false, true, false, true>);
+    prime(k_shadow<true, true, false, true>);
+    prime(k_mis<false, false, true, false, true>);
+    prime(k_mis<false, true, true, false, true>);
+    prime(k_mis<true, false, true, false, true>);
+    prime(k_mis<true, true, true, false, true>);
+    prime(k_shadow_step<false, true, true>);
+    prime(k_shadow_step<true, true, true>);
+    prime(k_mis_step<false, true, true>);
+    prime(k_mis_step<true, true, true>);
+    prime(k_trace_batch<false, false, true, true>);
+    prime(k_trace_batch<false, true, true, true>);
+    prime(k_trace_batch<true, false, true, true>);
+    prime(k_trace_batch<true, true, true, true>);
     prime(k_trace_batch<false, false, false>);
     prime(k_trace_batch<false, false, true>);
     prime(k_trace_batch<false, true, false>);
@@ -1092,14 +1135,18 @@ void launch_generate(const Params& p, const LaunchCfg& c, cudaStream_t s) {
     k_generate<<<blocks_for(p.chunk_paths, 256, c.grid_cap), 256, 0, s>>>(p);
 }
 
-template <bool kCount, bool kCurves, bool kPersist>
+// Batches with motion-blurred meshes take the persistent schedule (their
+// kernels are instantiated for it only) without work counting.
+template <bool kCount, bool kCurves, bool kPersist, bool kMotion = false>
 static void ext_launch(const Params& p, const LaunchCfg& c, cudaStream_t s) {
-    auto k = k_extend<kCount, kCurves, kPersist>;
+    auto k = k_extend<kCount, kCurves, kPersist, kMotion>;
     k<<<traversal_grid<kPersist>(k, c), kPersistBlock, 0, s>>>(p);
 }
 void launch_extend(const Params& p, const LaunchCfg& c, cudaStream_t s, bool count_work) {
     const bool cv = p.S.has_curves != 0, ps = c.persistent != 0;
-    if (count_work) {
+    if (p.S.has_motion) {
+        cv ? ext_launch<false, true, true, true>(p, c, s) : ext_launch<false, false, true, true>(p, c, s);
+    } else if (count_work) {
         if (cv) ps ? ext_launch<true, true, true>(p, c, s) : ext_launch<true, true, false>(p, c, s);
         else ps ? ext_launch<true, false, true>(p, c, s) : ext_launch<true, false, false>(p, c, s);
     } else {
@@ -1112,40 +1159,47 @@ void launch_shade(const Params& p, const LaunchCfg& c, cudaStream_t s) {
     if (p.S.has_fibers) k_shade<false, true><<<g, c.block, 0, s>>>(p);
     else k_shade<false, false><<<g, c.block, 0, s>>>(p);
 }
-template <bool kCurves, bool kPersist, bool kAdj>
+template <bool kCurves, bool kPersist, bool kAdj, bool kMotion = false>
 static void sh_launch(const Params& p, const LaunchCfg& c, cudaStream_t s) {
-    auto k = k_shadow<kCurves, kPersist, kAdj>;
+    auto k = k_shadow<kCurves, kPersist, kAdj, kMotion>;
     k<<<traversal_grid<kPersist>(k, c), kPersistBlock, 0, s>>>(p);
 }
 template <bool kAdj>
 static void shadow_dispatch(const Params& p, const LaunchCfg& c, cudaStream_t s) {
     const bool cv = p.S.has_curves != 0, ps = c.persistent != 0;
-    if (cv) ps ? sh_launch<true, true, kAdj>(p, c, s) : sh_launch<true, false, kAdj>(p, c, s);
+    if (!kAdj && p.S.has_motion)
+        cv ? sh_launch<true, true, false, true>(p, c, s) : sh_launch<false, true, false, true>(p, c, s);
+    else if (cv) ps ? sh_launch<true, true, kAdj>(p, c, s) : sh_launch<true, false, kAdj>(p, c, s);
     else ps ? sh_launch<false, true, kAdj>(p, c, s) : sh_launch<false, false, kAdj>(p, c, s);
 }
-template <bool kCurves, bool kPersist>
+template <bool kCurves, bool kPersist, bool kMotion = false>
 static void step_launch(const Params& p, const LaunchCfg& c, cudaStream_t s, bool mis) {
-    auto k = mis ? k_mis_step<kCurves, kPersist> : k_shadow_step<kCurves, kPersist>;
+    auto k = mis ? k_mis_step<kCurves, kPersist, kMotion> : k_shadow_step<kCurves, kPersist, kMotion>;
     k<<<traversal_grid<kPersist>(k, c), kPersistBlock, 0, s>>>(p);
 }
 static void step_dispatch(const Params& p, const LaunchCfg& c, cudaStream_t s, bool mis) {
     const bool cv = p.S.has_curves != 0, ps = c.persistent != 0;
-    if (cv) ps ? step_launch<true, true>(p, c, s, mis) : step_launch<true, false>(p, c, s, mis);
+    if (p.S.has_motion)
+        cv ? step_launch<true, true, true>(p, c, s, mis) : step_launch<false, true, true>(p, c, s, mis);
+    else if (cv) ps ? step_launch<true, true>(p, c, s, mis) : step_launch<true, false>(p, c, s, mis);
     else ps ? step_launch<false, true>(p, c, s, mis) : step_launch<false, false>(p, c, s, mis);
 }
 void launch_shadow(const Params& p, const LaunchCfg& c, cudaStream_t s) {
     if (p.S.has_transmit) step_dispatch(p, c, s, false);
     else shadow_dispatch<false>(p, c, s);
 }
-template <bool kAny, bool kCurves, bool kPersist, bool kAdj>
+template <bool kAny, bool kCurves, bool kPersist, bool kAdj, bool kMotion = false>
 static void mis_launch(const Params& p, const LaunchCfg& c, cudaStream_t s) {
-    auto k = k_mis<kAny, kCurves, kPersist, kAdj>;
+    auto k = k_mis<kAny, kCurves, kPersist, kAdj, kMotion>;
     k<<<traversal_grid<kPersist>(k, c), kPersistBlock, 0, s>>>(p);
 }
 void launch_mis(const Params& p, const LaunchCfg& c, cudaStream_t s) {
     const bool cv = p.S.has_curves != 0, ps = c.persistent != 0, any = !p.S.has_emitters;
     if (p.S.has_transmit) {
         step_dispatch(p, c, s, true);
+    } else if (p.S.has_motion) {
+        if (any) cv ? mis_launch<true, true, true, false, true>(p, c, s) : mis_launch<true, false, true, false, true>(p, c, s);
+        else cv ? mis_launch<false, true, true, false, true>(p, c, s) : mis_launch<false, false, true, false, true>(p, c, s);
     } else if (any) {
         if (cv) ps ? mis_launch<true, true, true, false>(p, c, s) : mis_launch<true, true, false, false>(p, c, s);
         else ps ? mis_launch<true, false, true, false>(p, c, s) : mis_launch<true, false, false, false>(p, c, s);
@@ -1178,10 +1232,10 @@ void launch_adj_direct(const Params& p, const LaunchCfg& c, cudaStream_t s) {
 void launch_film(const Params& p, const LaunchCfg& c, cudaStream_t s) {
     k_film<<<blocks_for(p.chunk_pixels, 256, c.grid_cap), 256, 0, s>>>(p);
 }
-template <bool kAny, bool kCurves, bool kPersist>
+template <bool kAny, bool kCurves, bool kPersist, bool kMotion = false>
 static void tb_launch(const DevScene& S, uint32_t scene, const float* rays, uint32_t n, ana_hit* out,
                       uint32_t* fetch, uint32_t* err, int grid, cudaStream_t s) {
-    auto k = k_trace_batch<kAny, kCurves, kPersist>;
+    auto k = k_trace_batch<kAny, kCurves, kPersist, kMotion>;
     int g = kPersist ? resident_grid(k) : grid;
     k<<<g, kPersistBlock, 0, s>>>(S, scene, rays, n, out, fetch, err);
 }
@@ -1190,7 +1244,12 @@ void launch_trace_batch(const DevScene& S, uint32_t scene, const float* rays, si
     const bool cv = S.has_curves != 0;
     int grid = blocks_for(uint32_t(n), kPersistBlock, 1 << 20);
     uint32_t nn = uint32_t(n);
-    if (occlusion) {
+    if (S.has_motion) {
+        if (occlusion) cv ? tb_launch<true, true, true, true>(S, scene, rays, nn, out, fetch, err, grid, s)
+                          : tb_launch<true, false, true, true>(S, scene, rays, nn, out, fetch, err, grid, s);
+        else cv ? tb_launch<false, true, true, true>(S, scene, rays, nn, out, fetch, err, grid, s)
+                : tb_launch<false, false, true, true>(S, scene, rays, nn, out, fetch, err, grid, s);
+    } else if (occlusion) {
         if (cv) persistent ? tb_launch<true, true, true>(S, scene, rays, nn, out, fetch, err, grid, s)
                            : tb_launch<true, true, false>(S, scene, rays, nn, out, fetch, err, grid, s);
         else persistent ? tb_launch<true, false, true>(S, scene, rays, nn, out, fetch, err, grid, s)

@@ -153,6 +153,13 @@ struct DevScene {
     uint32_t has_fibers;    // curve segments or hair materials: shading needs the fiber code
     uint32_t has_transmit;  // a material passes shadow rays (non-black transmittanceColor):
                             // shadow and MIS rays step through surfaces
+    // Motion blur: an object-space triangle has bit 31 set in its tri_isect
+    // index word and its motion mesh in the e1 record's w; mesh_motion[m] =
+    // (first key, key count), each key 5 float4 in motion_keys: (time, -, -,
+    // -) and the object-to-world rows.
+    const uint2* mesh_motion;
+    const float4* motion_keys;
+    uint32_t has_motion;
     DevEnv env;             // the (single) dome of the batch
 };
 

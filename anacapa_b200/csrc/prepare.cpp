@@ -39,6 +39,14 @@ inline V3 safeNormalize(V3 v, V3 fb = {0.f, 0.f, 1.f}) {
     return len > 1e-8f ? mul(v, 1.f / len) : fb;
 }
 inline V3 load3(const float* p) { return {p[0], p[1], p[2]}; }
+// Mat4f::transformPoint (Types.h:144-150), row-major m
+inline V3 xform_point(const float* m, V3 p) {
+    float x = m[0] * p.x + m[1] * p.y + m[2] * p.z + m[3];
+    float y = m[4] * p.x + m[5] * p.y + m[6] * p.z + m[7];
+    float z = m[8] * p.x + m[9] * p.y + m[10] * p.z + m[11];
+    float w = m[12] * p.x + m[13] * p.y + m[14] * p.z + m[15];
+    return {x / w, y / w, z / w};
+}
 inline float4 f4(V3 v, float w) { return make_float4(v.x, v.y, v.z, w); }
 inline float bits(uint32_t u) {
     float f;
@@ -535,7 +543,19 @@ int prepare_scene(const ana_scene_desc& d, Prepared& P, std::string& err, bool t
     // Leaf references carry the first primitive in 25 bits (traverse.cuh).
     if (T >= (1u << 25)) return bad("more than 2^25 triangles");
     P.num_tris = T;
-    P.tris_on_device = tris_on_device && T > 0;
+    P.mesh_motion.clear();
+    P.motion_keys.clear();
+    const auto motion_keys_of = [&](uint32_t m) -> uint32_t {
+        return d.mesh_motion_offset ? d.mesh_motion_offset[m + 1] - d.mesh_motion_offset[m] : 0u;
+    };
+    bool anyMotion = false;
+    for (uint32_t m = 0; m < d.num_meshes; ++m) {
+        if (d.mesh_motion_offset && d.mesh_motion_offset[m + 1] < d.mesh_motion_offset[m])
+            return bad("motion key offsets not monotone");
+        if (motion_keys_of(m)) anyMotion = true;
+    }
+    if (anyMotion && !d.motion_keys) return bad("motion keys missing");
+    P.tris_on_device = tris_on_device && T > 0 && !anyMotion;  // motion meshes: host build
     P.dev_tri_nodes = 0;
     if (P.tris_on_device) {
         for (uint32_t m = 0; m < d.num_meshes; ++m)
@@ -551,6 +571,21 @@ int prepare_scene(const ana_scene_desc& d, Prepared& P, std::string& err, bool t
         if (v1i < v0i || t1 < t0) return bad("mesh offsets not monotone");
         uint32_t nv = v1i - v0i;
         bool hasN = d.mesh_has_normals && d.mesh_has_normals[m] && d.normals;
+        // motion mesh: object-space triangle data, time-expanded world bounds
+        const uint32_t nk = motion_keys_of(m);
+        const ana_motion_key* keys = nk ? d.motion_keys + d.mesh_motion_offset[m] : nullptr;
+        const uint32_t mm = uint32_t(P.mesh_motion.size());
+        if (nk) {
+            P.mesh_motion.push_back(make_uint2(uint32_t(P.motion_keys.size() / 5), nk));
+            for (uint32_t k = 0; k < nk; ++k) {
+                const float* M = keys[k].object_to_world;
+                for (int j = 0; j < 16; ++j)
+                    if (!std::isfinite(M[j])) return bad("non-finite motion key");
+                if (!std::isfinite(keys[k].time)) return bad("non-finite motion key");
+                P.motion_keys.push_back(make_float4(keys[k].time, 0.f, 0.f, 0.f));
+                for (int r = 0; r < 4; ++r) P.motion_keys.push_back(make_float4(M[4 * r], M[4 * r + 1], M[4 * r + 2], M[4 * r + 3]));
+            }
+        }
         for (uint32_t t = t0; t < t1; ++t) {
             uint32_t ia = d.indices[3 * size_t(t)], ib = d.indices[3 * size_t(t) + 1],
                      ic = d.indices[3 * size_t(t) + 2];
@@ -565,20 +600,32 @@ int prepare_scene(const ana_scene_desc& d, Prepared& P, std::string& err, bool t
                 return hasN ? safeNormalize(load3(d.normals + 3 * size_t(v0i + i))) : n;
             };
             V3 s0 = sn(ia), s1 = sn(ib), s2 = sn(ic);
-            isect[3 * size_t(t) + 0] = f4(v0, bits(t));
-            isect[3 * size_t(t) + 1] = f4(e1, 0.f);
+            isect[3 * size_t(t) + 0] = f4(v0, bits(nk ? (t | 0x80000000u) : t));
+            isect[3 * size_t(t) + 1] = f4(e1, nk ? bits(mm) : 0.f);
             isect[3 * size_t(t) + 2] = f4(e2, 0.f);
             P.tri_shade[4 * size_t(t) + 0] = f4(n, bits(m));
             P.tri_shade[4 * size_t(t) + 1] = f4(s0, bits(t - t0));
             P.tri_shade[4 * size_t(t) + 2] = f4(s1, 0.f);
             P.tri_shade[4 * size_t(t) + 3] = f4(s2, 0.f);
-            // bounds from v0, v0 + e1, v0 + e2 (BVHBackend.cpp:78-80)
+            // bounds from v0, v0 + e1, v0 + e2 (BVHBackend.cpp:78-80), for a
+            // motion mesh their world positions at every key (BVHBackend.cpp:86-95)
             Box b;
             V3 w1 = add(v0, e1), w2 = add(v0, e2);
-            float a0[3] = {v0.x, v0.y, v0.z}, a1[3] = {w1.x, w1.y, w1.z}, a2[3] = {w2.x, w2.y, w2.z};
-            b.expand(a0);
-            b.expand(a1);
-            b.expand(a2);
+            if (nk) {
+                for (uint32_t k = 0; k < nk; ++k) {
+                    const float* M = keys[k].object_to_world;
+                    const V3 q0 = xform_point(M, v0), q1 = xform_point(M, w1), q2 = xform_point(M, w2);
+                    float a0[3] = {q0.x, q0.y, q0.z}, a1[3] = {q1.x, q1.y, q1.z}, a2[3] = {q2.x, q2.y, q2.z};
+                    b.expand(a0);
+                    b.expand(a1);
+                    b.expand(a2);
+                }
+            } else {
+                float a0[3] = {v0.x, v0.y, v0.z}, a1[3] = {w1.x, w1.y, w1.z}, a2[3] = {w2.x, w2.y, w2.z};
+                b.expand(a0);
+                b.expand(a1);
+                b.expand(a2);
+            }
             for (int ax = 0; ax < 3; ++ax)
                 if (b.diag(ax) < 1e-7f) {
                     b.lo[ax] -= 1e-7f;

@@ -41,6 +41,9 @@ struct Prepared {
     // is filled in once the device build has run.
     bool tris_on_device = false;
     uint32_t dev_tri_nodes = 0;
+    // motion meshes: (first key, key count) per motion mesh, 5 float4 per key
+    std::vector<uint2> mesh_motion;
+    std::vector<float4> motion_keys;
     uint64_t bytes() const;
 };
 

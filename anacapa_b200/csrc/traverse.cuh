@@ -12,12 +12,14 @@
 #include <type_traits>
 #include "dmath.cuh"
 #include "layout.h"
+#include "motion.cuh"
 
 namespace ana {
 
 struct Ray {
     float3 o, d;
     float tmin, tmax;
+    float time;  // normalized shutter time (motion-blurred meshes)
 };
 
 // BVHBackend::makeRay4 (BVHBackend.cpp:233-247): invDir = 1/safe(d) where
@@ -127,6 +129,7 @@ struct Traversal {
     float tseg;
     float3 tang;
     float3 cd, fx, fy, cinv;  // exact direction, ray-space frame x/y, 1/d
+    float time;               // ray time: object rays of motion-blurred triangles
 };
 
 // Starts a traversal at a scene's root (kNoRoot: the scene has no triangles).
@@ -136,6 +139,8 @@ struct Traversal {
 // BVHBackend.cpp:409-444).
 __device__ __forceinline__ void trav_init(Traversal& T, const Ray& ray, uint32_t root) {
     T.r = make_tri_ray(ray);
+    T.cd = ray.d;  // read by the motion test (and reset by curve_begin)
+    T.time = ray.time;
     T.closest = ray.tmax;
     T.u = T.v = 0.f;
     T.tri = -1;
@@ -220,9 +225,25 @@ __device__ __forceinline__ void trav_interior(Traversal& T, const DevScene& S, u
     T.cur = ref[0];
 }
 
+// BVHBackend::makeObjectSpaceRay4: the world ray (origin, exact direction)
+// taken to the object space of motion mesh `mm` at the ray's time.
+__device__ __forceinline__ TriRay object_ray(const DevScene& S, uint32_t mm, const Traversal& T, float tmax) {
+    M4 o2w, w2o;
+    o2w_at(S, mm, T.time, o2w);
+    m4_inverse(o2w, w2o);
+    Ray r;
+    r.o = m4_point(w2o, T.r.o);
+    r.d = m4_vector(w2o, T.cd);
+    r.tmin = T.r.tmin;
+    r.tmax = tmax;
+    r.time = T.time;
+    return make_tri_ray(r);
+}
+
 // Tests the triangles of leaf entry `leaf`; true when an any-hit query found
-// its blocker.
-template <bool kAny, bool kCount>
+// its blocker. kMotion: triangles flagged object-space (bit 31 of the index
+// word) meet the ray in their mesh's object space at the ray's time.
+template <bool kAny, bool kCount, bool kMotion = false>
 __device__ __forceinline__ bool leaf_test(Traversal& T, const DevScene& S, uint32_t leaf, Counters* cnt) {
     const uint32_t off = leaf & 0x01FFFFFFu, c = ((leaf >> 25) & 63u) + 1u;
     for (uint32_t i = off; i < off + c; ++i) {
@@ -230,7 +251,15 @@ __device__ __forceinline__ bool leaf_test(Traversal& T, const DevScene& S, uint3
         float4 a = ldg4(tp), b = ldg4(tp + 1), e = ldg4(tp + 2);
         if (kCount) cnt->prims++;
         float t, u, v;
-        if (tri_hit(T.r, f3(a), f3(b), f3(e), kAny ? T.r.tmax : T.closest, t, u, v)) {
+        const float tmax = kAny ? T.r.tmax : T.closest;
+        bool h;
+        if (kMotion && (__float_as_uint(a.w) & 0x80000000u)) {
+            const TriRay ro = object_ray(S, __float_as_uint(b.w), T, tmax);
+            h = tri_hit(ro, f3(a), f3(b), f3(e), tmax, t, u, v);
+        } else {
+            h = tri_hit(T.r, f3(a), f3(b), f3(e), tmax, t, u, v);
+        }
+        if (h) {
             T.closest = t;
             T.u = u;
             T.v = v;
@@ -494,10 +523,10 @@ __device__ __forceinline__ void node_step(Traversal& T, const DevScene& S, uint3
     if (kCurves && T.stage) curve_interior<kCount>(T, S, stack, stackT, err, cnt);
     else trav_interior<kAny, kCount>(T, S, stack, stackT, err, cnt);
 }
-template <bool kAny, bool kCount, bool kCurves>
+template <bool kAny, bool kCount, bool kCurves, bool kMotion = false>
 __device__ __forceinline__ bool leaf_step(Traversal& T, const DevScene& S, uint32_t leaf, Counters* cnt) {
     if (kCurves && T.stage) return curve_leaf_test<kAny, kCount>(T, S, leaf, cnt);
-    return leaf_test<kAny, kCount>(T, S, leaf, cnt);
+    return leaf_test<kAny, kCount, kMotion>(T, S, leaf, cnt);
 }
 
 // A lane whose triangle traversal ended moves on to the curve BVH (unless an
@@ -526,7 +555,7 @@ __device__ __forceinline__ bool trace_again(Done& done, uint32_t i, const Traver
 // traversal of entry i (a lane-local call, see trace_again: a lane asked to
 // trace again keeps its entry). With kCurves a lane that finishes the
 // triangle BVH continues with the curve BVH in the same phases.
-template <bool kAny, bool kCount, bool kCurves, class Load, class Done>
+template <bool kAny, bool kCount, bool kCurves, bool kMotion, class Load, class Done>
 __device__ __forceinline__ void persistent_traverse(const DevScene& S, uint32_t n, uint32_t* fetch, uint32_t* err,
                                                     Counters* cnt, Load load, Done done) {
     const uint32_t lane = threadIdx.x & 31u;
@@ -572,10 +601,10 @@ __device__ __forceinline__ void persistent_traverse(const DevScene& S, uint32_t 
         // 3. leaf phase: one leaf per lane
         if (active) {
             if (parked != kEmptyChild) {
-                if (leaf_step<kAny, kCount, kCurves>(T, S, parked, cnt)) T.exhausted = true;
+                if (leaf_step<kAny, kCount, kCurves, kMotion>(T, S, parked, cnt)) T.exhausted = true;
                 parked = kEmptyChild;
             } else if (!T.exhausted && (T.cur & 0x80000000u)) {
-                if (leaf_step<kAny, kCount, kCurves>(T, S, T.cur, cnt)) T.exhausted = true;
+                if (leaf_step<kAny, kCount, kCurves, kMotion>(T, S, T.cur, cnt)) T.exhausted = true;
                 else if (!trav_pop(T, stack, stackT)) T.exhausted = true;
             }
         }

@@ -81,6 +81,8 @@ struct Flat {
     std::vector<ana_material> mats;
     std::vector<int32_t> slots;
     std::vector<ana_light> lights;
+    std::vector<uint32_t> meshMotion;  // key offsets per mesh (+1)
+    std::vector<ana_motion_key> keys;
     ana_scene_desc d{};
 };
 
@@ -154,11 +156,16 @@ bool flatten(const SceneView& scene, uint32_t width, uint32_t height, Flat& F, s
     const GeometryPool& pool = scene.accel->pool();
     F.meshVert.push_back(0);
     F.meshTri.push_back(0);
+    F.meshMotion.push_back(0);
     for (const MeshDesc& m : pool.meshes()) {
-        if (m.hasMotion()) {
-            err = "motion-blurred meshes are not supported";
-            return false;
+        for (const MotionKey& k : m.motionKeys) {  // object-space positions, keys by time
+            ana_motion_key mk;
+            mk.time = k.time;
+            for (int i = 0; i < 4; ++i)
+                for (int j = 0; j < 4; ++j) mk.object_to_world[4 * i + j] = k.objectToWorld.m[i][j];
+            F.keys.push_back(mk);
         }
+        F.meshMotion.push_back(uint32_t(F.keys.size()));
         for (const Vec3f& p : m.positions) F.pos.insert(F.pos.end(), {p.x, p.y, p.z});
         bool hasN = m.normals.size() >= m.positions.size() && !m.normals.empty();
         F.hasN.push_back(hasN ? 1 : 0);
@@ -175,10 +182,8 @@ bool flatten(const SceneView& scene, uint32_t width, uint32_t height, Flat& F, s
     F.strandWidth.push_back(0);
     if (auto* cb = dynamic_cast<const CurveBrute*>(scene.accel)) {
         for (const StrandDesc& s : cb->curvePool().strands()) {
-            if (s.hasMotion()) {
-                err = "motion-blurred strands are not supported";
-                return false;
-            }
+            // CurveBrute intersects the control points as stored, with or
+            // without motion keys (CurveBrute.cpp:332-396 read no key)
             for (const Vec3f& p : s.controlPoints) F.cps.insert(F.cps.end(), {p.x, p.y, p.z});
             F.widths.insert(F.widths.end(), s.widths.begin(), s.widths.end());
             F.strandCp.push_back(uint32_t(F.cps.size() / 3));
@@ -292,6 +297,10 @@ bool flatten(const SceneView& scene, uint32_t width, uint32_t height, Flat& F, s
     d.positions = F.pos.data();
     d.normals = F.nrm.data();
     d.indices = F.indices.data();
+    if (!F.keys.empty()) {
+        d.mesh_motion_offset = F.meshMotion.data();
+        d.motion_keys = F.keys.data();
+    }
     d.num_strands = uint32_t(F.strandSlot.size());
     d.strand_cp_offset = F.strandCp.data();
     d.control_points = F.cps.data();

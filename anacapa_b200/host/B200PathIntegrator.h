@@ -10,8 +10,8 @@
 // the camera — and uploads it; `renderFrame` renders [sampleStart,
 // sampleStart + sampleCount) samples per pixel and merges the result into the
 // Film as one full-frame TileBuffer (Film::mergeTile), returning true.
-// There is no CPU fallback: unsupported scene content (motion blur,
-// textures, a rotated dome) makes
+// There is no CPU fallback: unsupported scene content (image textures, a
+// rotated dome) makes
 // prepare/renderFrame fail with a message in lastError(); renderTile throws.
 #pragma once
 

@@ -130,6 +130,12 @@ class Scene:
     cam_basis: Optional[tuple] = None
     # SceneView::lights after the area lights, before the dome
     dir_lights: List[DirLight] = dataclasses.field(default_factory=list)
+    # Motion blur: per mesh None (static, world space) or a list of
+    # (time, 4x4 row-major objectToWorld) keys sorted by time (MeshDesc::
+    # motionKeys), the mesh's positions then in object space
+    mesh_motion: Optional[list] = None
+    # Camera::shutterOpen / shutterClose (normalized), when cam_basis is None
+    shutter: tuple = (0.0, 0.0)
 
     @property
     def num_meshes(self) -> int:
@@ -593,3 +599,66 @@ def glass(width=192, height=144, spp=16, max_depth=8, seed=5) -> Scene:
                    env_radiance=(0.15, 0.18, 0.25),
                    cam_from=(0.0, 3.2, -7.5), cam_at=(0.0, 0.6, 0.0), cam_up=(0.0, 1.0, 0.0),
                    vfov=45.0, width=width, height=height, spp=spp, max_depth=max_depth)
+
+
+def _trs(t, yaw_deg=0.0, s=1.0):
+    """Row-major objectToWorld: translate(t) * rotate_y(yaw) * scale(s)."""
+    a = np.radians(yaw_deg)
+    c, n = np.cos(a), np.sin(a)
+    M = np.array([[c * s, 0.0, n * s, t[0]], [0.0, s, 0.0, t[1]], [-n * s, 0.0, c * s, t[2]],
+                  [0.0, 0.0, 0.0, 1.0]], np.float32)
+    return M
+
+
+def motion(width=128, height=96, spp=16, max_depth=6, shutter=(0.0, 1.0), seed=9) -> Scene:
+    """Motion blur (MeshDesc::motionKeys, BVHBackend.cpp:35-50, 86-95, 356-367):
+    on the tilted ground of `sunlit`, spheres kept in object space with 2 keys
+    (a translation), 3 keys (translation with a yaw; keys at 0, 0.4, 1) and a
+    growing scale, a moving box, and static spheres, lit by an area light and a
+    constant environment; the camera's shutter samples each path's time."""
+    rng = np.random.default_rng(seed)
+    b = _Builder()
+    mg = b.material(Material(MAT_LAMBERT, albedo=(0.5, 0.5, 0.5)))
+    g, y0, y1 = 6.0, 0.0, 0.1
+    gn = np.array([0.0, 2.0 * g, -(y1 - y0)])
+    gn /= np.linalg.norm(gn)
+    b.quad([-g, y0, -g], [-g, y1, g], [g, y1, g], [g, y0, -g], gn, mg)
+    v, f = icosphere(2)
+    keys = [None]
+    movers = [
+        [(0.0, _trs((-2.0, 0.6, 0.0), 0.0, 0.5)), (1.0, _trs((-0.8, 0.6, 0.3), 0.0, 0.5))],
+        [(0.0, _trs((0.5, 0.7, 1.0), 0.0, 0.6)), (0.4, _trs((0.9, 1.1, 1.2), 40.0, 0.6)),
+         (1.0, _trs((1.6, 0.7, 1.0), 90.0, 0.6))],
+        [(0.0, _trs((1.8, 0.5, -1.2), 0.0, 0.3)), (1.0, _trs((1.8, 0.75, -1.2), 0.0, 0.55))],
+    ]
+    for mk in movers:
+        m = b.material(Material(MAT_STANDARD, base_color=tuple(map(float, rng.uniform(0.2, 0.9, 3))),
+                                roughness=float(rng.uniform(0.2, 0.7))))
+        b.mesh(v, f, m, nrm=v)
+        keys.append(mk)
+    # a box, turned and moving
+    bv = np.array([[x, y, z] for x in (-0.4, 0.4) for y in (-0.4, 0.4) for z in (-0.4, 0.4)], np.float32)
+    bf = np.array([[0, 1, 3], [0, 3, 2], [4, 6, 7], [4, 7, 5], [0, 4, 5], [0, 5, 1],
+                   [2, 3, 7], [2, 7, 6], [0, 2, 6], [0, 6, 4], [1, 5, 7], [1, 7, 3]], np.uint32)
+    mb = b.material(Material(MAT_STANDARD, base_color=(0.8, 0.7, 0.3), roughness=0.35, metalness=1.0))
+    b.mesh(bv, bf, mb)
+    keys.append([(0.0, _trs((-1.5, 0.5, -1.5), 20.0)), (1.0, _trs((-1.0, 0.5, -1.7), 50.0))])
+    for _ in range(4):
+        m = b.material(Material(MAT_STANDARD, base_color=tuple(map(float, rng.uniform(0.1, 0.9, 3))),
+                                roughness=float(rng.uniform(0.2, 0.9))))
+        r = float(rng.uniform(0.3, 0.5))
+        c = np.array([rng.uniform(-3, 3), r + 0.05, rng.uniform(1.5, 3.5)])
+        b.mesh(c + r * v, f, m, nrm=v)
+        keys.append(None)
+    le = (6.0, 5.0, 4.0)
+    ml = b.material(Material(MAT_EMISSIVE, albedo=(0.0, 0.0, 0.0), emission=le))
+    lc, lu, lv = np.array([0.5, 3.5, -0.5]), np.array([0.6, 0.0, 0.0]), np.array([0.0, 0.02, 0.5])
+    ln = np.cross(lu, lv)
+    ln /= np.linalg.norm(ln)
+    b.quad(lc - lu - lv, lc + lu - lv, lc + lu + lv, lc - lu + lv, ln, ml)
+    keys.append(None)
+    return b.scene("motion", area_lights=[AreaLight(tuple(lc), tuple(lu), tuple(lv), le)],
+                   env_radiance=(0.1, 0.12, 0.16),
+                   cam_from=(0.0, 3.5, -7.0), cam_at=(0.0, 0.6, 0.0), cam_up=(0.0, 1.0, 0.0),
+                   vfov=45.0, width=width, height=height, spp=spp, max_depth=max_depth,
+                   mesh_motion=keys, shutter=tuple(shutter))

@@ -125,6 +125,14 @@ typedef struct ana_camera {
     float basis_v[3];
 } ana_camera;
 
+/* A motion key (MotionKey, include/anacapa/accel/GeometryPool.h:16-20): a
+ * normalized shutter time and the object-to-world matrix there, row-major
+ * (m[row][col]; a point p maps to m * (p, 1) divided by its w). */
+typedef struct ana_motion_key {
+    float time;
+    float object_to_world[16];
+} ana_motion_key;
+
 /* ---- scene (GeometryPool + CurvePool + SceneView) ------------------------- */
 typedef struct ana_scene_desc {
     /* Triangle meshes (MeshDesc, include/anacapa/accel/GeometryPool.h:28-77),
@@ -173,6 +181,16 @@ typedef struct ana_scene_desc {
      * BVHBackend.h:67, CurveBrute.cpp:455). 0 = default. */
     uint32_t max_leaf_tris;
     uint32_t max_leaf_segments;
+
+    /* Motion blur (MeshDesc::motionKeys): mesh i owns the keys
+     * [mesh_motion_offset[i], mesh_motion_offset[i+1]) of motion_keys, sorted
+     * by time. A mesh without keys is static (world-space positions); a mesh
+     * with keys keeps object-space positions, bounded over all keys, and each
+     * ray meets it transformed by the keys interpolated at the ray's time and
+     * inverted (BVHBackend.cpp:35-50, 86-95, 356-367, 395-398). A ray's time
+     * is the camera's shutter sample (Camera::generateRay). NULL: all static. */
+    const uint32_t* mesh_motion_offset;
+    const ana_motion_key* motion_keys;
 } ana_scene_desc;
 
 /* ---- render ---------------------------------------------------------------- */

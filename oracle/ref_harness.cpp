@@ -173,6 +173,35 @@ int ref_add_mesh(void* sp, const float* pos, const float* nrm, const float* uv,
     return int(s->geom.addMesh(std::move(m)));
 }
 
+// A motion-blurred mesh: positions in object space and nkeys MotionKeys of
+// 17 floats each (time, objectToWorld row-major); worldToObject is the
+// inverse, as the scene loaders precompute it.
+int ref_add_mesh_motion(void* sp, const float* pos, const float* nrm, const float* uv, uint32_t nv,
+                        const uint32_t* idx, uint32_t ntri, const float* keys, uint32_t nkeys) {
+    auto* s = static_cast<RefScene*>(sp);
+    MeshDesc m;
+    m.positions.resize(nv);
+    for (uint32_t i = 0; i < nv; ++i) m.positions[i] = v3(pos + 3 * i);
+    if (nrm) {
+        m.normals.resize(nv);
+        for (uint32_t i = 0; i < nv; ++i) m.normals[i] = v3(nrm + 3 * i);
+    }
+    if (uv) {
+        m.uvs.resize(nv);
+        for (uint32_t i = 0; i < nv; ++i) m.uvs[i] = {uv[2 * i], uv[2 * i + 1]};
+    }
+    m.indices.assign(idx, idx + size_t(ntri) * 3);
+    for (uint32_t k = 0; k < nkeys; ++k) {
+        MotionKey mk;
+        mk.time = keys[17 * k];
+        for (int i = 0; i < 4; ++i)
+            for (int j = 0; j < 4; ++j) mk.objectToWorld.m[i][j] = keys[17 * k + 1 + 4 * i + j];
+        mk.worldToObject = mk.objectToWorld.inverse();
+        m.motionKeys.push_back(mk);
+    }
+    return int(s->geom.addMesh(std::move(m)));
+}
+
 int ref_add_strand(void* sp, const float* cps, uint32_t ncp, const float* widths,
                    uint32_t nw, uint32_t matSlot, const float* color) {
     auto* s = static_cast<RefScene*>(sp);
@@ -263,6 +292,13 @@ void ref_set_camera(void* sp, const float* from, const float* at, const float* u
                     float vfov, uint32_t w, uint32_t h) {
     auto* s = static_cast<RefScene*>(sp);
     s->view.camera = Camera::makePinhole(v3(from), v3(at), v3(up), vfov, w, h);
+}
+
+void ref_set_shutter(void* sp, float open, float close) {
+    auto* s = static_cast<RefScene*>(sp);
+    if (!s->view.camera) return;
+    s->view.camera->shutterOpen = open;
+    s->view.camera->shutterClose = close;
 }
 
 int ref_commit(void* sp) {

@@ -62,6 +62,8 @@ def lib(variant="record"):
     L.ref_scene_new.restype = _P
     L.ref_scene_free.argtypes = [_P]
     L.ref_add_mesh.argtypes = [_P, _F, _F, _F, C.c_uint32, _U32, C.c_uint32]
+    L.ref_add_mesh_motion.argtypes = [_P, _F, _F, _F, C.c_uint32, _U32, C.c_uint32, _F, C.c_uint32]
+    L.ref_set_shutter.argtypes = [_P, C.c_float, C.c_float]
     L.ref_add_strand.argtypes = [_P, _F, C.c_uint32, _F, C.c_uint32, C.c_uint32, _F]
     L.ref_mat_lambert.argtypes = [_P, _F]
     L.ref_mat_emissive.argtypes = [_P, _F, _F]
@@ -140,7 +142,13 @@ class RefScene:
             n = f32(scene.normals[vo[i]:vo[i + 1]]) if scene.mesh_has_normals[i] else None
             uv = f32(scene.uvs[vo[i]:vo[i + 1]]) if scene.uvs is not None else None
             idx = np.ascontiguousarray(scene.indices[to[i]:to[i + 1]], dtype=np.uint32)
-            L.ref_add_mesh(h, _fp(p), _fp(n), _fp(uv), len(p), idx.ctypes.data_as(_U32), len(idx))
+            keys = scene.mesh_motion[i] if scene.mesh_motion is not None else None
+            if keys:
+                k17 = f32([[t, *np.asarray(M, np.float32).reshape(16)] for t, M in keys])
+                L.ref_add_mesh_motion(h, _fp(p), _fp(n), _fp(uv), len(p), idx.ctypes.data_as(_U32), len(idx),
+                                      _fp(k17), len(keys))
+            else:
+                L.ref_add_mesh(h, _fp(p), _fp(n), _fp(uv), len(p), idx.ctypes.data_as(_U32), len(idx))
         co, wo_ = scene.strand_cp_offset, scene.strand_width_offset
         cps = f32(scene.control_points)
         wds = f32(scene.widths)
@@ -165,6 +173,7 @@ class RefScene:
         L.ref_set_env_radiance(h, _fp(f32(scene.env_radiance)))
         L.ref_set_camera(h, _fp(f32(scene.cam_from)), _fp(f32(scene.cam_at)),
                          _fp(f32(scene.cam_up)), scene.vfov, scene.width, scene.height)
+        L.ref_set_shutter(h, float(scene.shutter[0]), float(scene.shutter[1]))
         if commit:
             L.ref_commit(h)
 

@@ -75,6 +75,8 @@ class PoScene:
         from anacapa_b200 import scenes as S
         L = self.L = lib()
         self.scene = scene
+        if scene.mesh_motion is not None and any(k for k in scene.mesh_motion):
+            raise NotImplementedError("the restatement covers static meshes")
         h = self.h = L.po_scene_new(precision)
         for m in scene.materials:
             if m.type in (S.MAT_LAMBERT, S.MAT_EMISSIVE):

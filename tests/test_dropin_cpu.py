@@ -34,8 +34,9 @@ def dropin(lib_built, ref_built):
                                   lambda: S.throughput(96, 54, 4, 12, n_spheres=64),
                                   # the directional light is recovered by probing, an ulp
                                   # away from the description's: left out of the digest
-                                  lambda: dataclasses.replace(S.glass(96, 72, 4), dir_lights=[])],
-                         ids=["cornell", "hair", "throughput_small", "glass"])
+                                  lambda: dataclasses.replace(S.glass(96, 72, 4), dir_lights=[]),
+                                  lambda: S.motion(64, 48, 2)],
+                         ids=["cornell", "hair", "throughput_small", "glass", "motion"])
 def test_dropin_prepares_the_same_layout(dropin, make):
     sc = make()
     rs = dropin.RefScene(sc, variant="dropin")

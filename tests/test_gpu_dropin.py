@@ -24,8 +24,9 @@ def dropin(gpu, ref_built):
                                   lambda: S.hair(96, 54, 4, 10, n_strands=5000),
                                   lambda: S.throughput(96, 54, 4, 12, n_spheres=64),
                                   lambda: S.sunlit(96, 72, 8),
-                                  lambda: S.glass(96, 72, 8)],
-                         ids=["cornell", "hair", "throughput_small", "sunlit", "glass"])
+                                  lambda: S.glass(96, 72, 8),
+                                  lambda: S.motion(96, 72, 8)],
+                         ids=["cornell", "hair", "throughput_small", "sunlit", "glass", "motion"])
 def test_dropin_matches_direct_render(dropin, make):
     sc = make()
     rs = dropin.RefScene(sc, variant="dropin")
