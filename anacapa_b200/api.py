@@ -26,6 +26,7 @@ ANA_ERR_STATE = 6
 ANA_ERR_DEVICE_CHECK = 7
 ANA_RENDER_CLEAR_FILM = 1
 ANA_RENDER_COUNT_WORK = 2
+ANA_RENDER_AOVS = 8
 ANA_TRAVERSAL_DEFAULT = 0
 ANA_TRAVERSAL_PERSISTENT = 1
 ANA_TRAVERSAL_PER_RAY = 2
@@ -128,7 +129,8 @@ EXPORTS = ["ana_create", "ana_destroy", "ana_upload_scene", "ana_prepare_scene",
            "ana_batch_bytes", "ana_upload_batch", "ana_render_batch", "ana_batch_film_read",
            "ana_prepared_digest", "ana_trace_batch_noalloc", "ana_diff_counts", "ana_diff_get_params",
            "ana_forward", "ana_backward", "ana_render_tiles", "ana_render_adaptive",
-           "ana_upload_scene_device", "ana_scene_digest"]
+           "ana_upload_scene_device", "ana_scene_digest", "ana_aov_read", "ana_film_write_exr",
+           "ana_film_write_png", "ana_image_write_exr", "ana_image_write_png"]
 ANA_RENDER_GRAPH = 4
 
 _lib = None
@@ -154,6 +156,11 @@ def lib():
     L.ana_upload_scene.argtypes = [_P, C.POINTER(AnaSceneDesc)]
     L.ana_upload_scene_device.argtypes = [_P, C.POINTER(AnaSceneDesc)]
     L.ana_scene_digest.argtypes = [_P, C.POINTER(C.c_uint64)]
+    L.ana_aov_read.argtypes = [_P, _P, _P, C.c_size_t]
+    L.ana_film_write_exr.argtypes = [_P, C.c_uint32, C.c_uint32, C.c_char_p, C.c_int]
+    L.ana_film_write_png.argtypes = [_P, C.c_uint32, C.c_uint32, C.c_char_p, C.c_float]
+    L.ana_image_write_exr.argtypes = [C.c_char_p, C.c_uint32, C.c_uint32, _P, _P, _P]
+    L.ana_image_write_png.argtypes = [C.c_char_p, C.c_uint32, C.c_uint32, _P, C.c_float]
     L.ana_prepare_scene.argtypes = [C.POINTER(AnaSceneDesc), C.POINTER(_P)]
     L.ana_upload_prepared.argtypes = [_P, _P]
     L.ana_prepared_bytes.argtypes = [_P]
@@ -391,14 +398,31 @@ class Renderer:
         return int(out.value)
 
     def render(self, width, height, spp, max_depth, sample_start=0, min_depth=2, seed=0, clear=True,
-               count_work=False):
-        flags = (ANA_RENDER_CLEAR_FILM if clear else 0) | (ANA_RENDER_COUNT_WORK if count_work else 0)
+               count_work=False, aovs=False):
+        flags = ((ANA_RENDER_CLEAR_FILM if clear else 0) | (ANA_RENDER_COUNT_WORK if count_work else 0)
+                 | (ANA_RENDER_AOVS if aovs else 0))
         r = AnaRenderDesc(width, height, sample_start, spp, max_depth, min_depth, seed, flags)
         self._check(lib().ana_render(self.h, C.byref(r)))
 
-    def render_scene(self, sc: S.Scene, spp=None, clear=True, sample_start=0, seed=0, count_work=False):
+    def render_scene(self, sc: S.Scene, spp=None, clear=True, sample_start=0, seed=0, count_work=False,
+                     aovs=False):
         self.render(sc.width, sc.height, sc.spp if spp is None else spp, sc.max_depth,
-                    sample_start=sample_start, seed=seed, clear=clear, count_work=count_work)
+                    sample_start=sample_start, seed=seed, clear=clear, count_work=count_work, aovs=aovs)
+
+    def aovs(self, width, height):
+        """ana_aov_read: resolved first-hit albedo and shading normal, (H, W, 3) each."""
+        al = np.zeros((height, width, 3), np.float32)
+        nr = np.zeros((height, width, 3), np.float32)
+        self._check(lib().ana_aov_read(self.h, al.ctypes.data, nr.ctypes.data, width * height))
+        return al, nr
+
+    def write_exr(self, path, width, height, aovs=True):
+        """ana_film_write_exr (Film::writeEXR)."""
+        self._check(lib().ana_film_write_exr(self.h, width, height, str(path).encode(), 1 if aovs else 0))
+
+    def write_png(self, path, width, height, exposure=0.0):
+        """ana_film_write_png (Film::writePNG)."""
+        self._check(lib().ana_film_write_png(self.h, width, height, str(path).encode(), exposure))
 
     def render_tiles(self, width, height, max_depth, tiles, clear=False, min_depth=2, seed=0):
         """ana_render_tiles: tiles = [(x0, y0, w, h, sample_start, sample_count), ...]
@@ -546,3 +570,21 @@ class Batch:
 
 def scene_desc_tuple(sc: S.Scene, sample_start=0, seed=0):
     return (sc.width, sc.height, sc.spp, sc.max_depth, sample_start, 2, seed)
+
+
+def image_write_exr(path, rgb, albedo=None, normal=None):
+    """ana_image_write_exr: (H, W, 3) float images to a ZIP-compressed EXR."""
+    rgb = np.ascontiguousarray(rgb, np.float32)
+    h, w = rgb.shape[:2]
+    al = None if albedo is None else np.ascontiguousarray(albedo, np.float32)
+    nr = None if normal is None else np.ascontiguousarray(normal, np.float32)
+    check(lib().ana_image_write_exr(str(path).encode(), w, h, rgb.ctypes.data,
+                                    al.ctypes.data if al is not None else None,
+                                    nr.ctypes.data if nr is not None else None))
+
+
+def image_write_png(path, rgb, exposure=0.0):
+    """ana_image_write_png: (H, W, 3) linear float image to 8-bit sRGB PNG."""
+    rgb = np.ascontiguousarray(rgb, np.float32)
+    h, w = rgb.shape[:2]
+    check(lib().ana_image_write_png(str(path).encode(), w, h, rgb.ctypes.data, exposure))

@@ -25,10 +25,11 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 SOURCES = {
     "kernels.cu": ["kernels.cu", "kernels.h", "layout.h", "dmath.cuh", "sampler.cuh", "shade.cuh",
-                   "traverse.cuh"],
+                   "traverse.cuh", "motion.cuh"],
     "build.cu": ["build.cu", "build.h", "layout.h"],
     "prepare.cpp": ["prepare.cpp", "prepare.h", "layout.h"],
     "capi.cpp": ["capi.cpp", "kernels.h", "prepare.h", "build.h", "layout.h"],
+    "film_io.cpp": ["film_io.cpp"],
 }
 
 
@@ -72,7 +73,7 @@ def build(force=False, verbose=False, ptxas_info=False):
             cmd = [os.environ.get("CXX", "g++"), *flags, "-c", path, "-o", obj]
         _run(cmd, verbose)
     if rebuilt or force or not os.path.exists(LIB):
-        _run([NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lpthread"], verbose)
+        _run([NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lpthread", "-lz"], verbose)
     return LIB
 
 

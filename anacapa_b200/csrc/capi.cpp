@@ -295,6 +295,12 @@ struct ana_ctx {
     // film (all items of the last render, back to back)
     unsigned char* film = nullptr;
     size_t film_bytes = 0, film_pixels = 0;
+    // AOV film (8 floats per pixel) and per-path first-hit AOVs (6 floats)
+    unsigned char* aov_film = nullptr;
+    size_t aov_film_bytes = 0;
+    unsigned char* path_aov = nullptr;
+    size_t path_aov_bytes = 0;
+    bool aov_valid = false;  // the AOV film matches the beauty film's passes
     std::vector<size_t> item_film_offset, item_film_pixels;
     // wavefront buffers
     ana::Queues q{};
@@ -585,6 +591,16 @@ int render_items(ana_ctx* c, const std::vector<Item>& items, uint64_t totalPixel
     if (rc) return rc;
     if (c->film_pixels != totalPixels) flags |= ANA_RENDER_CLEAR_FILM;
     c->film_pixels = totalPixels;
+    const bool aovs = (flags & ANA_RENDER_AOVS) != 0 && !backward;
+    if (aovs) {
+        rc = ensure_buffer(c, &c->aov_film, &c->aov_film_bytes, totalPixels * 32, "cudaMalloc(AOV film)");
+        if (rc) return rc;
+        rc = ensure_buffer(c, &c->path_aov, &c->path_aov_bytes, size_t(cap) * 24, "cudaMalloc(path AOVs)");
+        if (rc) return rc;
+        if (!c->aov_valid && !(flags & ANA_RENDER_CLEAR_FILM))
+            return fail(c, ANA_ERR_STATE, "AOVs need a cleared film or AOVs in every pass since the last clear");
+    }
+    c->aov_valid = aovs && (c->aov_valid || (flags & ANA_RENDER_CLEAR_FILM));
     // scene records, path offsets, chunk plan
     std::vector<ana::DevSceneRec> recs(n);
     std::vector<uint32_t> pathOff(n + 1, 0);
@@ -680,6 +696,8 @@ int render_items(ana_ctx* c, const std::vector<Item>& items, uint64_t totalPixel
     p.S.num_scenes = n;
     p.q = c->q;
     p.film = c->film_px();
+    p.aov = aovs ? reinterpret_cast<float*>(c->aov_film) : nullptr;
+    p.q.aov = aovs ? reinterpret_cast<float*>(c->path_aov) : nullptr;
     p.err = c->d_err;
     p.work = c->d_work;
     ana::LaunchCfg cfg;
@@ -768,6 +786,7 @@ int render_items(ana_ctx* c, const std::vector<Item>& items, uint64_t totalPixel
     };
     auto enqueue = [&]() {
         if (clear) cudaMemsetAsync(c->film, 0, totalPixels * sizeof(ana_film_pixel), c->stream);
+        if (clear && aovs) cudaMemsetAsync(c->aov_film, 0, totalPixels * 32, c->stream);
         cudaMemsetAsync(c->d_counters, 0, ncount * 4, c->stream);
         cudaMemsetAsync(c->d_err, 0, 4, c->stream);
         if (count_work) cudaMemsetAsync(c->d_work, 0, 4 * sizeof(unsigned long long), c->stream);
@@ -801,6 +820,8 @@ int render_items(ana_ctx* c, const std::vector<Item>& items, uint64_t totalPixel
             key.insert(key.end(), bb, bb + nb);
         };
         put(&clear, sizeof(clear));
+        put(&p.aov, sizeof(p.aov));
+        put(&p.q.aov, sizeof(p.q.aov));
         put(&cfg, sizeof(cfg));
         put(&cap, sizeof(cap));
         put(&c->upload_serial, sizeof(c->upload_serial));
@@ -1015,6 +1036,8 @@ void ana_destroy(ana_ctx* c) {
     cudaFree(c->d_scene);
     cudaFree(c->d_tables);
     cudaFree(c->film);
+    cudaFree(c->aov_film);
+    cudaFree(c->path_aov);
     cudaFree(c->d_queues);
     cudaFree(c->d_counters);
     cudaFree(c->d_err);
@@ -1305,6 +1328,10 @@ int ana_film_clear(ana_ctx* c, uint32_t w, uint32_t h) {
     if (rc) return rc;
     c->film_pixels = n;
     CK(cudaMemsetAsync(c->film, 0, n * sizeof(ana_film_pixel), c->stream), "memset film");
+    rc = ensure_buffer(c, &c->aov_film, &c->aov_film_bytes, n * 32, "cudaMalloc(AOV film)");
+    if (rc) return rc;
+    CK(cudaMemsetAsync(c->aov_film, 0, n * 32, c->stream), "memset AOV film");
+    c->aov_valid = true;
     return ANA_OK;
 }
 
@@ -1329,6 +1356,74 @@ int ana_batch_film_read(ana_ctx* c, uint32_t item, ana_film_pixel* out, size_t c
                        cudaMemcpyDeviceToHost, c->stream),
        "film D2H");
     CK(cudaStreamSynchronize(c->stream), "film sync");
+    return ANA_OK;
+}
+
+int ana_aov_read(ana_ctx* c, float* albedo, float* normal, size_t count) {
+    if (!c) return ANA_ERR_INVALID_ARG;
+    if (!c->aov_valid || !c->aov_film) return fail(c, ANA_ERR_STATE, "ana_aov_read: no AOVs in the film");
+    if (count != c->film_pixels)
+        return fail(c, ANA_ERR_INVALID_ARG, "ana_aov_read: count != pixels of the last render");
+    CK(cudaSetDevice(c->device), "cudaSetDevice");
+    std::vector<float> h(count * 8);
+    CK(cudaMemcpyAsync(h.data(), c->aov_film, h.size() * 4, cudaMemcpyDeviceToHost, c->stream), "AOV D2H");
+    CK(cudaStreamSynchronize(c->stream), "AOV sync");
+    for (size_t i = 0; i < count; ++i)  // PixelAccumulator::resolve
+        for (int l = 0; l < 2; ++l) {
+            float* out = l ? normal : albedo;
+            if (!out) continue;
+            const float* a = h.data() + 8 * i + 4 * l;
+            const float w = a[3];
+            const float inv = w > 0.f ? 1.f / w : 0.f;
+            for (int k = 0; k < 3; ++k) out[3 * i + k] = w > 0.f ? a[k] * inv : 0.f;
+        }
+    return ANA_OK;
+}
+
+// The resolved beauty film (PixelAccumulator::resolve: r * (1 / weight)).
+static int resolved_film(ana_ctx* c, uint32_t w, uint32_t h, std::vector<float>& rgb) {
+    if (!c->film || size_t(w) * h != c->film_pixels)
+        return fail(c, ANA_ERR_INVALID_ARG, "film write: width * height != pixels of the last render");
+    CK(cudaSetDevice(c->device), "cudaSetDevice");
+    std::vector<ana_film_pixel> px(c->film_pixels);
+    CK(cudaMemcpyAsync(px.data(), c->film, px.size() * sizeof(ana_film_pixel), cudaMemcpyDeviceToHost, c->stream),
+       "film D2H");
+    CK(cudaStreamSynchronize(c->stream), "film sync");
+    rgb.assign(px.size() * 3, 0.f);
+    for (size_t i = 0; i < px.size(); ++i) {
+        if (!(px[i].w > 0.f)) continue;
+        const float inv = 1.f / px[i].w;
+        rgb[3 * i] = px[i].r * inv;
+        rgb[3 * i + 1] = px[i].g * inv;
+        rgb[3 * i + 2] = px[i].b * inv;
+    }
+    return ANA_OK;
+}
+
+int ana_film_write_exr(ana_ctx* c, uint32_t w, uint32_t h, const char* path, int write_aovs) {
+    if (!c || !path) return fail(c, ANA_ERR_INVALID_ARG, "ana_film_write_exr: NULL argument");
+    std::vector<float> rgb, al, nr;
+    int rc = resolved_film(c, w, h, rgb);
+    if (rc) return rc;
+    if (write_aovs) {
+        al.resize(rgb.size());
+        nr.resize(rgb.size());
+        rc = ana_aov_read(c, al.data(), nr.data(), size_t(w) * h);
+        if (rc) return rc;
+    }
+    rc = ana_image_write_exr(path, w, h, rgb.data(), write_aovs ? al.data() : nullptr,
+                             write_aovs ? nr.data() : nullptr);
+    if (rc) return fail(c, rc, std::string("ana_film_write_exr: cannot write ") + path);
+    return ANA_OK;
+}
+
+int ana_film_write_png(ana_ctx* c, uint32_t w, uint32_t h, const char* path, float exposure) {
+    if (!c || !path) return fail(c, ANA_ERR_INVALID_ARG, "ana_film_write_png: NULL argument");
+    std::vector<float> rgb;
+    int rc = resolved_film(c, w, h, rgb);
+    if (rc) return rc;
+    rc = ana_image_write_png(path, w, h, rgb.data(), exposure);
+    if (rc) return fail(c, rc, std::string("ana_film_write_png: cannot write ") + path);
     return ANA_OK;
 }
 

@@ -179,6 +179,8 @@ __global__ void __launch_bounds__(256) k_generate(const __grid_constant__ Params
         p.q.L[li] = 0.f;
         p.q.L[li + 1] = 0.f;
         p.q.L[li + 2] = 0.f;
+        if (p.aov)  // a camera ray that misses keeps black AOVs
+            for (int k = 0; k < 6; ++k) p.q.aov[6 * size_t(i) + k] = 0.f;
     }
 }
 
@@ -487,7 +489,7 @@ __global__ void __launch_bounds__(kMaxStageBlock) k_shade(const __grid_constant_
                     if (cut) {
                         if (bounce + 1u <= R.max_depth) {
                             pushExt = true;
-                            const uint32_t nm = (bounce + 1u) | (spec ? 0x100u : 0u) | (ss.dim << 16);
+                            const uint32_t nm = (bounce + 1u) | (spec ? 0x100u : 0u) | (meta & 0x200u) | (ss.dim << 16);
                             eO = pack_u(spawn_origin(si.p, si.ng, d), pid);
                             eD = pack_u(d, nm);
                             eB = pack_u(beta, sc);
@@ -499,6 +501,17 @@ __global__ void __launch_bounds__(kMaxStageBlock) k_shade(const __grid_constant_
                     } else {
                         float3 wo = -d;
                         ShadeCtx c = make_ctx(si, d);
+                        if (p.aov && !(meta & 0x200u)) {
+                            // first-hit AOVs (PathIntegrator.cpp:120-124): reflectance, si.n
+                            float* A = p.q.aov + 6 * size_t(pid - p.chunk_first_path);
+                            const float3 al = mat_reflectance(m, c);
+                            A[0] = al.x;
+                            A[1] = al.y;
+                            A[2] = al.z;
+                            A[3] = si.n.x;
+                            A[4] = si.n.y;
+                            A[5] = si.n.z;
+                        }
                         float3 Le = mat_le(m);
                         if (!is_black(Le) && (bounce == 0 || spec)) Ladd = Ladd + beta * Le;
                         if constexpr (kAdj) {
@@ -601,7 +614,7 @@ __global__ void __launch_bounds__(kMaxStageBlock) k_shade(const __grid_constant_
                             }
                             if (alive && bounce + 1u <= R.max_depth) {
                                 pushExt = true;
-                                uint32_t nm = (bounce + 1u) | (spec ? 0x100u : 0u) | (ss.dim << 16);
+                                uint32_t nm = (bounce + 1u) | (spec ? 0x100u : 0u) | 0x200u | (ss.dim << 16);
                                 eO = pack_u(org, pid);
                                 eD = pack_u(bs.wi, nm);
                                 eB = pack_u(beta, sc);
@@ -959,13 +972,38 @@ __global__ void __launch_bounds__(256) k_film(const __grid_constant__ Params p) 
             }
         }
         const float invSPP = 1.f / float(spp);
-        ana_film_pixel& f = p.film[film_index(R, sg.first_pixel + k)];
+        const size_t fi = film_index(R, sg.first_pixel + k);
+        ana_film_pixel& f = p.film[fi];
         float w = float(spp);
         f.r += (acc.x * invSPP) * w;
         f.g += (acc.y * invSPP) * w;
         f.b += (acc.z * invSPP) * w;
         f.w += w;
         f.sum_lum_sq += lsq;
+        if (p.aov) {
+            // renderTile's AOV averages over every sample of the pass
+            // (PathIntegrator.cpp:44-66), merged with weight 1 as
+            // Film::mergeTile does (Film.cpp:58-70)
+            const float* A = p.q.aov + (size_t(sg.local_path) + size_t(k) * spp) * 6;
+            float3 sa = f3(0.f, 0.f, 0.f), sn = f3(0.f, 0.f, 0.f);
+            for (uint32_t s = 0; s < spp; ++s) {
+                sa = xadd3(sa, f3(A[6 * s], A[6 * s + 1], A[6 * s + 2]));
+                sn = xadd3(sn, f3(A[6 * s + 3], A[6 * s + 4], A[6 * s + 5]));
+            }
+            const float3 al = xmul3(sa, invSPP);
+            float3 n = xmul3(sn, invSPP);
+            const float len = __fsqrt_rn(xdot(n, n));
+            if (len > 1e-6f) n = xmul3(n, xdiv(1.f, len));
+            float* F = p.aov + 8 * fi;
+            F[0] += al.x;
+            F[1] += al.y;
+            F[2] += al.z;
+            F[3] += 1.f;
+            F[4] += n.x;
+            F[5] += n.y;
+            F[6] += n.z;
+            F[7] += 1.f;
+        }
     }
 }
 

@@ -10,7 +10,8 @@ namespace ana {
 
 // Queues are structure-of-arrays of float4, indexed by queue position.
 //   extend queue: o (xyz, global path id), d (xyz, meta), beta (xyz, scene)
-//     meta bits: 0..7 bounce, 8 specular-bounce flag, 16..31 next sampler dimension
+//     meta bits: 0..7 bounce, 8 specular-bounce flag, 9 first-hit AOVs taken,
+//     16..31 next sampler dimension
 //   hit record:   (t, prim, u, v) and, for curve hits, (tangent xyz, strand v)
 //     prim: leaf-order triangle index, 0x80000000 | segment index, or ~0 (miss)
 //   shadow queue: o (xyz, path id), d (xyz, tmax), contribution (xyz, scene)
@@ -28,6 +29,7 @@ struct Queues {
     float4* mis_d;
     float4* mis_c;
     float* L;  // 3 floats per path of the chunk
+    float* aov;  // 6 floats per path of the chunk: first-hit albedo, shading normal
 };
 
 // Per-bounce device counters: [bounce][0] extend queue length, [1] shadow
@@ -82,6 +84,8 @@ struct Params {
     Queues q;
     AdjQueues a;
     ana_film_pixel* film;      // batch film (all scenes)
+    float* aov;                // AOV film, 8 floats per pixel: albedo (r, g, b, w),
+                               // normal (x, y, z, w); null: no AOVs
     uint32_t* counters;        // this chunk's counters
     uint32_t* err;             // device error word (bit 0: traversal stack overflow)
     unsigned long long* work;  // [node fetches, triangle tests, segment tests] (count mode)

@@ -926,6 +926,21 @@ __device__ __forceinline__ LightSample light_sample(const DevScene& S, const Dev
     s.delta = false;
     return s;
 }
+// IMaterial::reflectance, the first-hit albedo AOV: Lambertian.h:76-78 (an
+// emitter keeps its Lambertian albedo), StandardSurface.h:186-192,
+// MarschnerHair.h:224-232.
+__device__ __forceinline__ float3 mat_reflectance(const DevMaterial& m, const ShadeCtx& c) {
+    if (m.type == ANA_MAT_STANDARD) {
+        const float diff = (1.f - m.metal) * (1.f - m.spec * 0.5f);
+        return (m.albedo * m.base) * (diff + m.metal);
+    }
+    if (m.type == ANA_MAT_HAIR) {
+        const float3 sa = hair_sigma(m, c.color);
+        return f3(expf(-sa.x), expf(-sa.y), expf(-sa.z));
+    }
+    return m.albedo;
+}
+
 // ILight::pdf; a directional light is delta (DirectionalLight::pdf returns 0).
 __device__ __forceinline__ float light_pdf(const DevScene& S, const DevLight& L, float3 p, float3 wi) {
     if (L.type == ANA_LIGHT_DIRECTIONAL) return 0.f;

@@ -402,11 +402,14 @@ bool B200PathIntegrator::renderFrame(const SceneView& scene, uint32_t filmWidth,
     r.max_depth = m_maxDepth;
     r.min_depth = m_minDepth;
     r.seed = 0;  // HaltonSampler's default seed (RenderSession.cpp:465)
-    r.flags = ANA_RENDER_CLEAR_FILM;
+    r.flags = ANA_RENDER_CLEAR_FILM | ANA_RENDER_AOVS;
     if (ana_render(m_ctx, &r) != ANA_OK) return fail(ana_message(m_ctx));
     const size_t n = size_t(filmWidth) * filmHeight;
     std::vector<ana_film_pixel> px(n);
     if (ana_film_read(m_ctx, px.data(), n) != ANA_OK) return fail(ana_message(m_ctx));
+    // this pass's denoising AOVs (the device film was cleared: weight 1)
+    std::vector<float> albedo(3 * n), normal(3 * n);
+    if (ana_aov_read(m_ctx, albedo.data(), normal.data(), n) != ANA_OK) return fail(ana_message(m_ctx));
     // one full-frame TileBuffer, merged as the tile loop would (Film.cpp:34-73)
     TileBuffer tile(0, 0, filmWidth, filmHeight);
     for (size_t i = 0; i < n; ++i) {
@@ -415,6 +418,8 @@ bool B200PathIntegrator::renderFrame(const SceneView& scene, uint32_t filmWidth,
         tile.pixels[i].b = px[i].b;
         tile.pixels[i].weight = px[i].w;
         tile.sumLumSq[i] = px[i].sum_lum_sq;
+        tile.albedo[i] = {albedo[3 * i], albedo[3 * i + 1], albedo[3 * i + 2], 1u};
+        tile.normals[i] = {normal[3 * i], normal[3 * i + 1], normal[3 * i + 2], 1u};
     }
     film.mergeTile(tile);
     return true;

@@ -209,10 +209,16 @@ enum {
     ANA_RENDER_CLEAR_FILM = 1u << 0, /* zero the film before accumulating              */
     ANA_RENDER_COUNT_WORK = 1u << 1, /* count BVH node fetches and primitive tests of the
                                         closest-hit stage (instrumented, slower)        */
-    ANA_RENDER_GRAPH = 1u << 2       /* capture the whole chunk x bounce launch sequence
+    ANA_RENDER_GRAPH = 1u << 2,      /* capture the whole chunk x bounce launch sequence
                                         in a CUDA graph on first use and replay it while
                                         the scenes and descs are unchanged (no per-stage
                                         timing, no work counting)                         */
+    ANA_RENDER_AOVS = 1u << 3        /* denoising AOVs (PathIntegrator::renderTile,
+                                        PathIntegrator.cpp:31-66): each path's first shaded
+                                        surface gives IMaterial::reflectance and the shading
+                                        normal; per pixel their averages over the call's
+                                        samples (the normal renormalised) are added to the
+                                        AOV film with weight 1, as Film::mergeTile does   */
 };
 
 /* One device-resident film pixel: the reference's PixelAccumulator
@@ -340,6 +346,26 @@ int ana_film_clear(ana_ctx* ctx, uint32_t width, uint32_t height);
 int ana_film_read(ana_ctx* ctx, ana_film_pixel* host_out, size_t count);
 /* Device pointer of the film, for callers that keep the result on the GPU. */
 int ana_film_device_ptr(ana_ctx* ctx, void** dptr);
+
+/* The AOV film (Film::m_albedo, m_normals) resolved as PixelAccumulator::resolve
+ * does, 3 floats per pixel each (either pointer may be NULL); count = pixels of
+ * the last render, which must have accumulated AOVs (ANA_RENDER_AOVS) since the
+ * film was last cleared. */
+int ana_aov_read(ana_ctx* ctx, float* albedo_rgb, float* normal_xyz, size_t count);
+
+/* Film::writeEXR (src/film/Film.cpp:154-219): R, G, B of the resolved film and,
+ * with write_aovs, the albedo.* and normals.* layers; 32-bit float channels, ZIP
+ * compression. Film::writePNG (Film.cpp:224-272): 8-bit sRGB of the resolved
+ * film scaled by 2^exposure, written to path + ".writing.png" and renamed. The
+ * film is the last render's (width * height pixels). */
+int ana_film_write_exr(ana_ctx* ctx, uint32_t width, uint32_t height, const char* path, int write_aovs);
+int ana_film_write_png(ana_ctx* ctx, uint32_t width, uint32_t height, const char* path, float exposure);
+
+/* The same writers for host images (row 0 = top, 3 floats per pixel; albedo
+ * and normal may be NULL). No device needed. */
+int ana_image_write_exr(const char* path, uint32_t width, uint32_t height, const float* rgb,
+                        const float* albedo, const float* normal);
+int ana_image_write_png(const char* path, uint32_t width, uint32_t height, const float* rgb, float exposure);
 
 /* Batched closest-hit / occlusion queries. rays: n x 8 floats
  * (ox, oy, oz, tmin, dx, dy, dz, tmax). Replaces

@@ -392,6 +392,53 @@ double ref_render(void* sp, uint32_t W, uint32_t H, uint32_t spp, uint32_t sampl
     return std::chrono::duration<double>(t1 - t0).count();
 }
 
+// The denoising AOVs of a frame: the 64x64 tiles of ref_render, each merged
+// into plain albedo (rgbw) and normal (xyzw) accumulators with
+// Film::mergeTile's arithmetic (Film.cpp:58-70): the tile's per-pixel average
+// over its count, added with weight 1.
+void ref_render_aov(void* sp, uint32_t W, uint32_t H, uint32_t spp, uint32_t sampleStart, uint32_t maxDepth,
+                    int nthreads, float* out_albedo, float* out_normal) {
+    auto* s = static_cast<RefScene*>(sp);
+    PathIntegrator integ(maxDepth);
+    integ.prepare(s->view);
+    HaltonSampler base(spp);
+    ThreadPool pool(uint32_t(nthreads > 0 ? nthreads : 0));
+    std::vector<TileRequest> tiles;
+    const uint32_t ts = 64;
+    for (uint32_t y = 0; y < H; y += ts)
+        for (uint32_t x = 0; x < W; x += ts)
+            tiles.push_back({x, y, std::min(ts, W - x), std::min(ts, H - y), sampleStart, spp});
+    std::mutex mu;
+    pool.parallelFor(uint32_t(tiles.size()), [&](uint32_t ti) {
+        const TileRequest& t = tiles[ti];
+        auto sampler = base.clone();
+        TileBuffer tb(t.x0, t.y0, t.width, t.height);
+        integ.renderTile(s->view, t, W, H, *sampler, tb);
+        std::lock_guard<std::mutex> lk(mu);
+        for (uint32_t ty = 0; ty < t.height; ++ty)
+            for (uint32_t tx = 0; tx < t.width; ++tx) {
+                size_t fi = size_t(t.y0 + ty) * W + (t.x0 + tx);
+                size_t li = size_t(ty) * t.width + tx;
+                const auto& a = tb.albedo[li];
+                if (a.count > 0) {
+                    float inv = 1.f / static_cast<float>(a.count);
+                    out_albedo[4 * fi + 0] += a.r * inv;
+                    out_albedo[4 * fi + 1] += a.g * inv;
+                    out_albedo[4 * fi + 2] += a.b * inv;
+                    out_albedo[4 * fi + 3] += 1.f;
+                }
+                const auto& n = tb.normals[li];
+                if (n.count > 0) {
+                    float inv = 1.f / static_cast<float>(n.count);
+                    out_normal[4 * fi + 0] += n.r * inv;
+                    out_normal[4 * fi + 1] += n.g * inv;
+                    out_normal[4 * fi + 2] += n.b * inv;
+                    out_normal[4 * fi + 3] += 1.f;
+                }
+            }
+    });
+}
+
 // Radiance of single camera samples (pixel px,py, sample index s), through a
 // 1x1 tile with sampleCount 1: the tile holds exactly the sample (0 if it was
 // not finite). out: n x 3.
@@ -574,8 +621,9 @@ void ref_dist1d(const float* vals, uint32_t n, const float* us, uint32_t nu, flo
 
 namespace anacapa {
 // Film.cpp needs OpenImageIO; the check supplies Film's accumulation members
-// with the arithmetic of src/film/Film.cpp:18-90 (I/O and denoising report
-// failure).
+// with the arithmetic of src/film/Film.cpp:18-90, and its EXR / PNG writers
+// through this repository's (ana_image_write_exr / _png) with the layers
+// Film::writeEXR resolves; denoising (OIDN) reports failure.
 Film::Film(uint32_t width, uint32_t height)
     : m_width(width), m_height(height), m_pixels(width * height), m_albedo(width * height),
       m_normals(width * height) {}
@@ -600,6 +648,16 @@ void Film::mergeTile(const TileBuffer& tile) {
                 m_pixels[fi].weight.fetch_add(s.weight, std::memory_order_relaxed);
                 m_pixels[fi].sumLumSq.fetch_add(tile.sumLumSq[ti], std::memory_order_relaxed);
             }
+            const auto& a = tile.albedo[ti];
+            if (a.count > 0) {
+                float inv = 1.f / static_cast<float>(a.count);
+                m_albedo[fi].add(a.r * inv, a.g * inv, a.b * inv, 1.f);
+            }
+            const auto& n = tile.normals[ti];
+            if (n.count > 0) {
+                float inv = 1.f / static_cast<float>(n.count);
+                m_normals[fi].add(n.r * inv, n.g * inv, n.b * inv, 1.f);
+            }
         }
 }
 Spectrum Film::getPixel(uint32_t x, uint32_t y) const { return m_pixels[y * m_width + x].resolve(); }
@@ -613,8 +671,30 @@ float Film::varianceAt(uint32_t x, uint32_t y) const {
     return std::max(0.f, eLsq - meanL * meanL);
 }
 bool Film::denoise() { return false; }
-bool Film::writeEXR(const std::string&, const DenoiseOptions&) const { return false; }
-bool Film::writePNG(const std::string&, float) const { return false; }
+static void resolve_layer(const std::vector<PixelAccumulator>& acc, std::vector<float>& out) {
+    out.resize(acc.size() * 3);
+    for (size_t i = 0; i < acc.size(); ++i) {
+        const Spectrum s = acc[i].resolve();
+        out[3 * i] = s.x;
+        out[3 * i + 1] = s.y;
+        out[3 * i + 2] = s.z;
+    }
+}
+bool Film::writeEXR(const std::string& path, const DenoiseOptions& opts) const {
+    std::vector<float> rgb, al, nr;
+    resolve_layer(m_pixels, rgb);
+    if (opts.writeAOVs) {
+        resolve_layer(m_albedo, al);
+        resolve_layer(m_normals, nr);
+    }
+    return ana_image_write_exr(path.c_str(), m_width, m_height, rgb.data(), opts.writeAOVs ? al.data() : nullptr,
+                               opts.writeAOVs ? nr.data() : nullptr) == ANA_OK;
+}
+bool Film::writePNG(const std::string& path, float exposure) const {
+    std::vector<float> rgb;
+    resolve_layer(m_pixels, rgb);
+    return ana_image_write_png(path.c_str(), m_width, m_height, rgb.data(), exposure) == ANA_OK;
+}
 }  // namespace anacapa
 
 extern "C" int ref_dropin_render(void* sp, uint32_t W, uint32_t H, uint32_t spp, uint32_t maxDepth,
@@ -645,6 +725,31 @@ extern "C" int ref_dropin_render(void* sp, uint32_t W, uint32_t H, uint32_t spp,
         }
     return 0;
 }
+// The drop-in's frames written by the reference Film's writers: `passes`
+// renderFrame calls, then Film::writeEXR (with the AOV layers) and
+// Film::writePNG.
+extern "C" int ref_dropin_write(void* sp, uint32_t W, uint32_t H, uint32_t spp, uint32_t maxDepth, int passes,
+                                const char* exr, const char* png, float exposure, char* err, int errlen) {
+    auto* s = static_cast<RefScene*>(sp);
+    anacapa_b200::B200PathIntegrator integ(maxDepth);
+    if (!integ.isValid()) {
+        std::snprintf(err, size_t(errlen), "%s", integ.lastError().c_str());
+        return 1;
+    }
+    integ.prepare(s->view);
+    Film film(W, H);
+    for (int k = 0; k < passes; ++k)
+        if (!integ.renderFrame(s->view, W, H, uint32_t(k) * spp, spp, film)) {
+            std::snprintf(err, size_t(errlen), "%s", integ.lastError().c_str());
+            return 2;
+        }
+    DenoiseOptions o;
+    o.writeAOVs = true;
+    if (!film.writeEXR(exr, o)) return 3;
+    if (!film.writePNG(png, exposure)) return 4;
+    return 0;
+}
+
 // The host half of the drop-in's prepare (no device needed): the prepared
 // layout built from the reference's SceneView, for comparison with the layout
 // the C ABI builds from the same scene description. Free with

@@ -81,6 +81,8 @@ def lib(variant="record"):
     L.ref_render.argtypes = [_P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
                              C.c_int, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, _F, _F]
     L.ref_render.restype = C.c_double
+    L.ref_render_aov.argtypes = [_P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int,
+                                 _F, _F]
     L.ref_li.argtypes = [_P, C.c_uint32, C.c_uint32, C.c_uint32, _U32, C.c_uint64, _F, C.c_int]
     L.ref_dim_log.argtypes = [_P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
                               C.c_uint32, _I32, C.c_int]
@@ -103,6 +105,8 @@ def lib(variant="record"):
         L.ref_dropin_render.argtypes = [_P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int,
                                         _F, _F, C.c_char_p, C.c_int]
         L.ref_dropin_prepare.argtypes = [_P, C.c_uint32, C.c_uint32, C.c_char_p, C.c_int]
+        L.ref_dropin_write.argtypes = [_P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, C.c_char_p,
+                                       C.c_char_p, C.c_float, C.c_char_p, C.c_int]
         L.ref_dropin_prepare.restype = _P
     _LIBS[variant] = L
     return L
@@ -209,6 +213,16 @@ class RefScene:
                                  _fp(rgbw), _fp(lsq))
         return rgbw, lsq, secs
 
+    def render_aov(self, spp=None, sample_start=0, max_depth=None, nthreads=0):
+        """The frame's albedo and normal AOV accumulators, (H, W, 4) each
+        (sum of per-tile averages, weight)."""
+        s = self.scene
+        al = np.zeros((s.height, s.width, 4), np.float32)
+        nr = np.zeros((s.height, s.width, 4), np.float32)
+        self.L.ref_render_aov(self.h, s.width, s.height, s.spp if spp is None else spp, sample_start,
+                              s.max_depth if max_depth is None else max_depth, nthreads, _fp(al), _fp(nr))
+        return al, nr
+
     def dropin_render(self, spp=None, passes=1, max_depth=None):
         """Render through this repository's B200PathIntegrator driven by the
         reference's SceneView and Film (variant "dropin" only). Returns the
@@ -223,6 +237,17 @@ class RefScene:
         if rc:
             raise RuntimeError(f"drop-in render failed ({rc}): {err.value.decode()}")
         return rgb, var
+
+    def dropin_write(self, exr, png, spp=None, passes=1, exposure=0.0, max_depth=None):
+        """Render through the drop-in into a reference Film and write it with
+        Film::writeEXR (AOV layers) and Film::writePNG (variant "dropin")."""
+        s = self.scene
+        err = C.create_string_buffer(512)
+        rc = self.L.ref_dropin_write(self.h, s.width, s.height, s.spp if spp is None else spp,
+                                     s.max_depth if max_depth is None else max_depth, passes,
+                                     str(exr).encode(), str(png).encode(), exposure, err, len(err))
+        if rc:
+            raise RuntimeError(f"drop-in write failed ({rc}): {err.value.decode()}")
 
     def dropin_prepare(self, size=None):
         """The drop-in's host-side prepare of this scene (variant "dropin"
