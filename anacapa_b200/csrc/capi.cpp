@@ -462,10 +462,13 @@ int upload_blob(ana_ctx* c, const Blob& B, const ana::DeviceTris* dt = nullptr) 
     S.motion_keys = reinterpret_cast<const float4*>(b + B.o_keys);
     S.has_motion = B.has_motion ? 1 : 0;
     S.has_fibers = S.has_curves;
+    S.has_extra_shading = S.has_motion;
     {
         const auto* mats = reinterpret_cast<const ana::DevMaterial*>(B.at(B.o_mats));
-        for (size_t i = 0; i < B.n_mats; ++i)
+        for (size_t i = 0; i < B.n_mats; ++i) {
             if (mats[i].type == ANA_MAT_HAIR) S.has_fibers = 1;
+            if (mats[i].transmission > 0.001f || mats[i].opacity < 1.f) S.has_extra_shading = 1;
+        }
     }
     ana::DevEnv& E = S.env;
     E.present = B.env_meta.present ? 1 : 0;

@@ -312,7 +312,7 @@ __global__ void ANA_TRAVERSAL_BOUNDS k_extend(const __grid_constant__ Params p) 
 
 // Surface interaction of a hit (BVHBackend::fillSurfaceInteraction,
 // BVHBackend.cpp:285-317; CurveBrute intersectOneSegment, CurveBrute.cpp:209-233).
-template <bool kCurves = true>
+template <bool kCurves = true, bool kMotion = true>
 __device__ __forceinline__ SurfInt surf_int(const DevScene& S, float3 o, float3 d, float t, uint32_t prim, float u,
                                             float v, float4 h1, float time = 0.f) {
     SurfInt si;
@@ -327,7 +327,7 @@ __device__ __forceinline__ SurfInt surf_int(const DevScene& S, float3 o, float3 
         si.ng = f3(s0);
         float3 sn = safe_normalize(f3(s1) * w + f3(s2) * u + f3(s3) * v);
         si.dpdu = f3(e1);
-        if (ow & 0x80000000u) {
+        if (kMotion && (ow & 0x80000000u)) {
             // object-space triangle (fillSurfaceInteraction with worldXfm,
             // BVHBackend.cpp:290-300): objectToWorld at the ray's time
             M4 M;
@@ -423,7 +423,9 @@ __device__ __forceinline__ float sum3(float3 v) { return v.x + v.y + v.z; }
 //  - the emission gradient delta * beta of an emissive hit that counts;
 //  - the NEE and MIS gradient payloads (resolved after their rays) and the
 //    pending gradient of this vertex's continuation.
-template <bool kAdj, bool kFiber>
+// kExtra: glass, alpha masks, motion blur and AOVs compiled in (batches
+// without them take the smaller kernel).
+template <bool kAdj, bool kFiber, bool kExtra>
 __global__ void __launch_bounds__(kMaxStageBlock) k_shade(const __grid_constant__ Params p) {
     const uint32_t b = p.bounce;
     const uint32_t cur = b & 1u, nxt = cur ^ 1u;
@@ -473,8 +475,8 @@ __global__ void __launch_bounds__(kMaxStageBlock) k_shade(const __grid_constant_
                 if (bounce == 0 || spec) Ladd = beta * scene_env(S, R, d);
             } else {
                 float4 h1 = (prim & 0x80000000u) ? p.q.hit1[i] : make_float4(0, 0, 0, 0);
-                const float time = S.has_motion ? path_time(R, pid) : 0.f;
-                SurfInt si = surf_int<kFiber>(S, o, d, h0.x, prim, h0.z, h0.w, h1, time);
+                const float time = (kExtra && S.has_motion) ? path_time(R, pid) : 0.f;
+                SurfInt si = surf_int<kFiber, kExtra>(S, o, d, h0.x, prim, h0.z, h0.w, h1, time);
                 int mi = slot_material(S, R, si.slot);
                 if (mi >= 0) {
                     const DevMaterial m = S.materials[mi];
@@ -485,7 +487,7 @@ __global__ void __launch_bounds__(kMaxStageBlock) k_shade(const __grid_constant_
                     // continues the ray unshaded, one bounce later, drawing a
                     // sample dimension only for partial opacity
                     bool cut = false;
-                    if (m.opacity < 1.f) cut = m.opacity <= 0.f || ss.next() >= m.opacity;
+                    if (kExtra && m.opacity < 1.f) cut = m.opacity <= 0.f || ss.next() >= m.opacity;
                     if (cut) {
                         if (bounce + 1u <= R.max_depth) {
                             pushExt = true;
@@ -501,7 +503,7 @@ __global__ void __launch_bounds__(kMaxStageBlock) k_shade(const __grid_constant_
                     } else {
                         float3 wo = -d;
                         ShadeCtx c = make_ctx(si, d);
-                        if (p.aov && !(meta & 0x200u)) {
+                        if (kExtra && p.aov && !(meta & 0x200u)) {
                             // first-hit AOVs (PathIntegrator.cpp:120-124): reflectance, si.n
                             float* A = p.q.aov + 6 * size_t(pid - p.chunk_first_path);
                             const float3 al = mat_reflectance(m, c);
@@ -531,7 +533,7 @@ __global__ void __launch_bounds__(kMaxStageBlock) k_shade(const __grid_constant_
                             float lu0 = ss.next(), lu1 = ss.next();
                             LightSample ls = light_sample(S, L, si.p, lu0, lu1);
                             if (ls.pdf > 0.f && !is_black(ls.Li)) {
-                                BsdfEval be = mat_eval<kFiber>(m, c, wo, ls.wi);
+                                BsdfEval be = mat_eval<kFiber, kExtra>(m, c, wo, ls.wi);
                                 if (!is_black(be.f)) {
                                     float3 target = si.p + ls.wi * ls.dist;
                                     float3 dir = target - si.p;
@@ -575,7 +577,7 @@ __global__ void __launch_bounds__(kMaxStageBlock) k_shade(const __grid_constant_
                                 bu0 = ss.next();
                                 bu1 = ss.next();
                             }
-                            BsdfSample bs = deltaLight ? no_sample() : mat_sample<kFiber>(m, c, wo, bu0, bu1, uc);
+                            BsdfSample bs = deltaLight ? no_sample() : mat_sample<kFiber, kExtra>(m, c, wo, bu0, bu1, uc);
                             if (bs.valid()) {
                                 float lp = light_pdf(S, L, si.p, bs.wi);
                                 if (lp > 0.f) {
@@ -601,7 +603,7 @@ __global__ void __launch_bounds__(kMaxStageBlock) k_shade(const __grid_constant_
                         // continuation
                         float uc = ss.next();
                         float u0 = ss.next(), u1 = ss.next();
-                        BsdfSample bs = mat_sample<kFiber>(m, c, wo, u0, u1, uc);
+                        BsdfSample bs = mat_sample<kFiber, kExtra>(m, c, wo, u0, u1, uc);
                         if (bs.valid()) {
                             spec = bs.delta();
                             beta = beta * (bs.f / bs.pdf);
@@ -1100,10 +1102,12 @@ static void prime(K kernel) {
 
 void prime_kernels() {
     prime(k_generate);
-    prime(k_shade<false, false>);
-    prime(k_shade<false, true>);
-    prime(k_shade<true, false>);
-    prime(k_shade<true, true>);
+    prime(k_shade<false, false, false>);
+    prime(k_shade<false, false, true>);
+    prime(k_shade<false, true, false>);
+    prime(k_shade<false, true, true>);
+    prime(k_shade<true, false, false>);
+    prime(k_shade<true, true, false>);
     prime(k_film);
     prime(k_adj_init);
     prime(k_adj_direct);
@@ -1194,8 +1198,14 @@ void launch_extend(const Params& p, const LaunchCfg& c, cudaStream_t s, bool cou
 }
 void launch_shade(const Params& p, const LaunchCfg& c, cudaStream_t s) {
     const int g = std::min(c.grid_cap, c.stage_grid);
-    if (p.S.has_fibers) k_shade<false, true><<<g, c.block, 0, s>>>(p);
-    else k_shade<false, false><<<g, c.block, 0, s>>>(p);
+    const bool extra = p.S.has_extra_shading || p.aov;
+    if (p.S.has_fibers) {
+        if (extra) k_shade<false, true, true><<<g, c.block, 0, s>>>(p);
+        else k_shade<false, true, false><<<g, c.block, 0, s>>>(p);
+    } else {
+        if (extra) k_shade<false, false, true><<<g, c.block, 0, s>>>(p);
+        else k_shade<false, false, false><<<g, c.block, 0, s>>>(p);
+    }
 }
 template <bool kCurves, bool kPersist, bool kAdj, bool kMotion = false>
 static void sh_launch(const Params& p, const LaunchCfg& c, cudaStream_t s) {
@@ -1255,8 +1265,8 @@ void launch_adj_init(const Params& p, const LaunchCfg& c, cudaStream_t s) {
 }
 void launch_shade_adj(const Params& p, const LaunchCfg& c, cudaStream_t s) {
     const int g = std::min(c.grid_cap, c.stage_grid);
-    if (p.S.has_fibers) k_shade<true, true><<<g, c.block, 0, s>>>(p);
-    else k_shade<true, false><<<g, c.block, 0, s>>>(p);
+    if (p.S.has_fibers) k_shade<true, true, false><<<g, c.block, 0, s>>>(p);
+    else k_shade<true, false, false><<<g, c.block, 0, s>>>(p);
 }
 void launch_shadow_adj(const Params& p, const LaunchCfg& c, cudaStream_t s) { shadow_dispatch<true>(p, c, s); }
 void launch_mis_adj(const Params& p, const LaunchCfg& c, cudaStream_t s) {

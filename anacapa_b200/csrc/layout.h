@@ -160,6 +160,7 @@ struct DevScene {
     const uint2* mesh_motion;
     const float4* motion_keys;
     uint32_t has_motion;
+    uint32_t has_extra_shading;  // glass, alpha masks or motion: the shading kernel with their code
     DevEnv env;             // the (single) dome of the batch
 };
 

@@ -348,11 +348,13 @@ __device__ __forceinline__ BsdfEval glass_eval_r(const DevMaterial& m, const Sha
     return e;
 }
 
+// kGlass = false compiles the glass lobes out (batches without transmission).
+template <bool kGlass = true>
 __device__ __forceinline__ BsdfSample ss_sample(const DevMaterial& m, const ShadeCtx& c, float3 wo, float ux,
                                                 float uy, float uc) {
     float3 wol = c.to_local(wo);
     if (wol.z <= 0.f) return no_sample();
-    if (ss_glass(m)) return glass_sample(m, c, wol, ux, uy, uc);
+    if (kGlass && ss_glass(m)) return glass_sample(m, c, wol, ux, uy, uc);
     LobeWeights w;
     if (!ss_weights(m, wol.z, w)) return no_sample();
     float3 wil;
@@ -389,11 +391,12 @@ __device__ __forceinline__ BsdfSample ss_sample(const DevMaterial& m, const Shad
     return s;
 }
 
+template <bool kGlass = true>
 __device__ __forceinline__ BsdfEval ss_eval(const DevMaterial& m, const ShadeCtx& c, float3 wo, float3 wi) {
     float3 wol = c.to_local(wo), wil = c.to_local(wi);
     BsdfEval e{f3(0.f, 0.f, 0.f), 0.f};
-    if (!(wol.z * wil.z > 0.f)) return glass_eval_t(m, c, wol, wil);  // opaque: black
-    if (ss_glass(m)) return glass_eval_r(m, c, wol, wil);
+    if (!(wol.z * wil.z > 0.f)) return kGlass ? glass_eval_t(m, c, wol, wil) : e;  // opaque: black
+    if (kGlass && ss_glass(m)) return glass_eval_r(m, c, wol, wil);
     LobeWeights w;
     if (!ss_weights(m, wol.z, w)) return e;
     e.f = ss_combined(m, wol, wil, w, e.pdf);
@@ -639,13 +642,13 @@ __device__ __forceinline__ BsdfSample marschner_sample(const DevMaterial& m, con
 // ---- material dispatch (IMaterial.h:53-114) ------------------------------------
 // kHair = false compiles the hair BSDFs out, for batches without hair
 // materials (smaller shading kernels: fewer registers, fewer i-cache misses).
-template <bool kHair = true>
+template <bool kHair = true, bool kGlass = true>
 __device__ __forceinline__ BsdfSample mat_sample(const DevMaterial& m, const ShadeCtx& c, float3 wo, float ux,
                                                  float uy, float uc) {
     switch (m.type) {
         case ANA_MAT_LAMBERT:
         case ANA_MAT_EMISSIVE: return lambert_sample(m, c, wo, ux, uy);
-        case ANA_MAT_STANDARD: return ss_sample(m, c, wo, ux, uy, uc);
+        case ANA_MAT_STANDARD: return ss_sample<kGlass>(m, c, wo, ux, uy, uc);
         default:
             if constexpr (kHair)
                 return m.hair_mode == ANA_HAIR_MARSCHNER ? marschner_sample(m, c, wo, ux, uy, uc)
@@ -654,12 +657,12 @@ __device__ __forceinline__ BsdfSample mat_sample(const DevMaterial& m, const Sha
                 return no_sample();
     }
 }
-template <bool kHair = true>
+template <bool kHair = true, bool kGlass = true>
 __device__ __forceinline__ BsdfEval mat_eval(const DevMaterial& m, const ShadeCtx& c, float3 wo, float3 wi) {
     switch (m.type) {
         case ANA_MAT_LAMBERT:
         case ANA_MAT_EMISSIVE: return lambert_eval(m, c, wo, wi);
-        case ANA_MAT_STANDARD: return ss_eval(m, c, wo, wi);
+        case ANA_MAT_STANDARD: return ss_eval<kGlass>(m, c, wo, wi);
         default:
             if constexpr (kHair)
                 return m.hair_mode == ANA_HAIR_MARSCHNER ? marschner_eval(m, c, wo, wi) : kk_eval(m, c, wo, wi);
