@@ -246,6 +246,10 @@ __device__ __forceinline__ TriRay object_ray(const DevScene& S, uint32_t mm, con
 template <bool kAny, bool kCount, bool kMotion = false>
 __device__ __forceinline__ bool leaf_test(Traversal& T, const DevScene& S, uint32_t leaf, Counters* cnt) {
     const uint32_t off = leaf & 0x01FFFFFFu, c = ((leaf >> 25) & 63u) + 1u;
+    // the object ray of the leaf's last motion mesh, reused while the mesh
+    // repeats (the same value the reference recomputes per triangle)
+    uint32_t cachedMM = 0xFFFFFFFFu;
+    TriRay ro;
     for (uint32_t i = off; i < off + c; ++i) {
         const float4* tp = S.tri_isect + 3 * size_t(i);
         float4 a = ldg4(tp), b = ldg4(tp + 1), e = ldg4(tp + 2);
@@ -254,7 +258,11 @@ __device__ __forceinline__ bool leaf_test(Traversal& T, const DevScene& S, uint3
         const float tmax = kAny ? T.r.tmax : T.closest;
         bool h;
         if (kMotion && (__float_as_uint(a.w) & 0x80000000u)) {
-            const TriRay ro = object_ray(S, __float_as_uint(b.w), T, tmax);
+            const uint32_t mm = __float_as_uint(b.w);
+            if (mm != cachedMM) {
+                ro = object_ray(S, mm, T, tmax);
+                cachedMM = mm;
+            }
             h = tri_hit(ro, f3(a), f3(b), f3(e), tmax, t, u, v);
         } else {
             h = tri_hit(T.r, f3(a), f3(b), f3(e), tmax, t, u, v);

@@ -19,8 +19,11 @@ The same line carries the metric's two other parts, measured after the timed
 region: "batched" (64 Cornell variants as one graph-replayed batch render vs
 one launch sequence per scene, same samples, so equal RMSE) and "adjoint"
 (ana_backward vs ana_forward device time on the differentiable scene);
-"other_configs" times single frames of the Cornell and hair configurations
-and of a 938-sphere (about 1.2M-triangle) throughput frame.
+"other_configs" times single frames of the Cornell and hair configurations,
+of a 938-sphere (about 1.2M-triangle) throughput frame and of the glass /
+alpha-mask and motion-blur scenes; "scene_setup" compares the host build of
+the throughput scene (ana_prepare_scene) with the device build
+(ana_upload_scene_device), whose uploaded bytes must be the same.
 """
 from __future__ import annotations
 
@@ -324,7 +327,37 @@ def bench_configs(local):
     out["throughput_938_spheres"] = {"workload": f"throughput scene with 938 spheres: {thr.num_triangles:,} "
                                                  "triangles, 1920x1080x64, depth 12",
                                      **bench_frame(local, thr, chunk_paths=1 << 27)}
+    glass = S.glass(1280, 720, 16, 8)
+    out["glass_1280x720x16"] = {"workload": "glass: smooth and rough dielectric spheres and panes, "
+                                            "alpha-masked cards, directional + area light; depth 8",
+                                **bench_frame(local, glass, chunk_paths=1 << 25)}
+    mo = S.motion(1280, 720, 16, 6)
+    out["motion_1280x720x16"] = {"workload": "motion blur: object-space meshes with 2-3 motion keys, "
+                                             "shutter [0, 1]; depth 6",
+                                 **bench_frame(local, mo, chunk_paths=1 << 25)}
     return out
+
+
+def bench_scene_setup(local, scene, prep_s):
+    """Host build (ana_prepare_scene, timed by the caller) against the device
+    build (ana_upload_scene_device: triangle setup, SAH build and collapse on
+    the GPU, the rest of the scene prepared on the host), second of two calls."""
+    from anacapa_b200 import api
+    r = api.Renderer(device=local)
+    try:
+        r.upload(scene, device_build=True)
+        t0 = time.perf_counter()
+        r.upload(scene, device_build=True)
+        dev_s = time.perf_counter() - t0
+        st = r.stats()
+        digest = r.scene_digest()
+    finally:
+        r.close()
+    return {"workload": f"throughput scene, {scene.num_triangles:,} triangles",
+            "host_prepare_s": prep_s, "device_upload_s": dev_s,
+            "device_build_ms": {"setup": st.build_ms[0], "sah_levels": st.build_ms[1],
+                                "small_subtrees": st.build_ms[2], "collapse": st.build_ms[3]},
+            "sah_levels": int(st.build_levels), "speedup": prep_s / dev_s, "digest": digest}
 
 
 def bench_adjoint(local, reps=3):
@@ -364,7 +397,9 @@ def run_ours(a):
     if torch.cuda.is_available():
         torch.cuda.set_device(local)
     scene = S.throughput(a.width, a.height, a.spp, a.depth, n_spheres=a.n_spheres)
+    t_prep = time.perf_counter()
     prep = api.Prepared(scene)
+    t_prep = time.perf_counter() - t_prep
     r = api.Renderer(device=local, timing=True, traversal=a.traversal, chunk_paths=a.chunk_paths)
     r.upload(prep)
     W, H, spp = scene.width, scene.height, scene.spp
@@ -424,6 +459,9 @@ def run_ours(a):
         extra["batched"] = bench_batched(local)
         extra["adjoint"] = bench_adjoint(local)
         extra["other_configs"] = bench_configs(local)
+        setup = bench_scene_setup(local, scene, t_prep)
+        setup["same_bytes"] = setup.pop("digest") == prep.digest
+        extra["scene_setup"] = setup
     cpu = None
     if rank == 0 and ws == 1 and not a.no_cpu_baseline:
         try:
