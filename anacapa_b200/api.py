@@ -130,7 +130,7 @@ EXPORTS = ["ana_create", "ana_destroy", "ana_upload_scene", "ana_prepare_scene",
            "ana_prepared_digest", "ana_trace_batch_noalloc", "ana_diff_counts", "ana_diff_get_params",
            "ana_forward", "ana_backward", "ana_render_tiles", "ana_render_adaptive",
            "ana_upload_scene_device", "ana_scene_digest", "ana_aov_read", "ana_film_write_exr",
-           "ana_film_write_png", "ana_image_write_exr", "ana_image_write_png"]
+           "ana_film_write_png", "ana_image_write_exr", "ana_image_write_png", "ana_trace_batch_timed"]
 ANA_RENDER_GRAPH = 4
 
 _lib = None
@@ -161,6 +161,7 @@ def lib():
     L.ana_film_write_png.argtypes = [_P, C.c_uint32, C.c_uint32, C.c_char_p, C.c_float]
     L.ana_image_write_exr.argtypes = [C.c_char_p, C.c_uint32, C.c_uint32, _P, _P, _P]
     L.ana_image_write_png.argtypes = [C.c_char_p, C.c_uint32, C.c_uint32, _P, C.c_float]
+    L.ana_trace_batch_timed.argtypes = [_P, _P, _P, C.c_size_t, _P, C.c_int, C.c_int]
     L.ana_prepare_scene.argtypes = [C.POINTER(AnaSceneDesc), C.POINTER(_P)]
     L.ana_upload_prepared.argtypes = [_P, _P]
     L.ana_prepared_bytes.argtypes = [_P]
@@ -507,11 +508,18 @@ class Renderer:
         self._check(lib().ana_get_stats(self.h, C.byref(s)))
         return s
 
-    def trace(self, rays: np.ndarray, occlusion=False) -> np.ndarray:
+    def trace(self, rays: np.ndarray, occlusion=False, times=None) -> np.ndarray:
+        """ana_trace_batch (ana_trace_batch_timed with per-ray `times`)."""
         rays = np.ascontiguousarray(np.asarray(rays, np.float32).reshape(-1, 8))
         out = np.zeros(len(rays), HIT_DTYPE)
-        self._check(lib().ana_trace_batch(self.h, rays.ctypes.data, len(rays), out.ctypes.data,
-                                          1 if occlusion else 0, 0))
+        if times is None:
+            self._check(lib().ana_trace_batch(self.h, rays.ctypes.data, len(rays), out.ctypes.data,
+                                              1 if occlusion else 0, 0))
+        else:
+            tm = np.ascontiguousarray(np.asarray(times, np.float32).reshape(-1))
+            assert len(tm) == len(rays)
+            self._check(lib().ana_trace_batch_timed(self.h, rays.ctypes.data, tm.ctypes.data, len(rays),
+                                                    out.ctypes.data, 1 if occlusion else 0, 0))
         return out
 
     def trace_noalloc(self, rays: np.ndarray, occlusion=False) -> np.ndarray:

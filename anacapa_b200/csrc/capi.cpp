@@ -1437,7 +1437,9 @@ int ana_film_device_ptr(ana_ctx* c, void** dptr) {
     return ANA_OK;
 }
 
-int ana_trace_batch(ana_ctx* c, const float* rays, size_t n, ana_hit* out, int occlusion, int on_device) {
+// ana_trace_batch with optional per-ray times (host or device like the rays).
+static int trace_batch(ana_ctx* c, const float* rays, const float* times, size_t n, ana_hit* out, int occlusion,
+                       int on_device) {
     if (!c || (!rays && n) || (!out && n)) return fail(c, ANA_ERR_INVALID_ARG, "ana_trace_batch: NULL argument");
     if (!c->has_scene) return fail(c, ANA_ERR_STATE, "ana_trace_batch: no scene uploaded");
     if (n == 0) return ANA_OK;
@@ -1448,17 +1450,23 @@ int ana_trace_batch(ana_ctx* c, const float* rays, size_t n, ana_hit* out, int o
     R.tri_root = c->scenes[0].tri_root;
     R.seg_root = c->scenes[0].seg_root;
     const size_t recBytes = align_up(sizeof(R));
-    const size_t tmpBytes = recBytes + (on_device ? 0 : n * 32 + n * sizeof(ana_hit));
+    const size_t tmpBytes = recBytes + (on_device ? 0 : n * 32 + n * sizeof(ana_hit) + (times ? n * 4 : 0));
     void* tmp = nullptr;
     CK(cudaMalloc(&tmp, tmpBytes), "cudaMalloc(trace batch)");
     unsigned char* tb = static_cast<unsigned char*>(tmp);
     const float* d_rays = rays;
+    const float* d_times = times;
     ana_hit* d_out = out;
     cudaError_t e = cudaMemcpyAsync(tb, &R, sizeof(R), cudaMemcpyHostToDevice, c->stream);
     if (!on_device) {
         d_rays = reinterpret_cast<const float*>(tb + recBytes);
         d_out = reinterpret_cast<ana_hit*>(tb + recBytes + n * 32);
         if (e == cudaSuccess) e = cudaMemcpyAsync(tb + recBytes, rays, n * 32, cudaMemcpyHostToDevice, c->stream);
+        if (times) {
+            float* t = reinterpret_cast<float*>(tb + recBytes + n * 32 + n * sizeof(ana_hit));
+            d_times = t;
+            if (e == cudaSuccess) e = cudaMemcpyAsync(t, times, n * 4, cudaMemcpyHostToDevice, c->stream);
+        }
     }
     uint32_t* d_fetch = c->d_err + 32;  // fetch counter of the persistent kernel
     if (e == cudaSuccess) e = cudaMemsetAsync(c->d_err, 0, 4, c->stream);
@@ -1470,7 +1478,7 @@ int ana_trace_batch(ana_ctx* c, const float* rays, size_t n, ana_hit* out, int o
     ana::DevScene S = c->ds;
     S.scenes = reinterpret_cast<const ana::DevSceneRec*>(tb);
     S.num_scenes = 1;
-    ana::launch_trace_batch(S, 0, d_rays, n, d_out, occlusion, d_fetch, c->d_err,
+    ana::launch_trace_batch(S, 0, d_rays, d_times, n, d_out, occlusion, d_fetch, c->d_err,
                             c->opts.traversal == ANA_TRAVERSAL_PER_RAY ? 0 : 1, c->stream);
     e = cudaGetLastError();
     uint32_t herr = 0;
@@ -1482,6 +1490,15 @@ int ana_trace_batch(ana_ctx* c, const float* rays, size_t n, ana_hit* out, int o
     if (e != cudaSuccess) return cuda_fail(c, e, "trace batch");
     if (herr) return fail(c, ANA_ERR_DEVICE_CHECK, "ana_trace_batch: traversal stack overflow on the device");
     return ANA_OK;
+}
+
+int ana_trace_batch(ana_ctx* c, const float* rays, size_t n, ana_hit* out, int occlusion, int on_device) {
+    return trace_batch(c, rays, nullptr, n, out, occlusion, on_device);
+}
+
+int ana_trace_batch_timed(ana_ctx* c, const float* rays, const float* times, size_t n, ana_hit* out, int occlusion,
+                          int on_device) {
+    return trace_batch(c, rays, times, n, out, occlusion, on_device);
 }
 
 // The same query as ana_trace_batch with host buffers, staged in the fixed
@@ -1518,7 +1535,7 @@ int ana_trace_batch_noalloc(ana_ctx* c, const float* rays, size_t n, ana_hit* ou
     ana::DevScene S = c->ds;
     S.scenes = reinterpret_cast<const ana::DevSceneRec*>(base);
     S.num_scenes = 1;
-    ana::launch_trace_batch(S, 0, d_rays, n, d_out, occlusion, d_fetch, d_err,
+    ana::launch_trace_batch(S, 0, d_rays, nullptr, n, d_out, occlusion, d_fetch, d_err,
                             c->opts.traversal == ANA_TRAVERSAL_PER_RAY ? 0 : 1, c->stream);
     e = cudaGetLastError();
     uint32_t herr = 0;

@@ -1013,17 +1013,17 @@ __global__ void __launch_bounds__(256) k_film(const __grid_constant__ Params p) 
 // against one scene of the batch.
 template <bool kAny, bool kCurves, bool kPersist, bool kMotion = false>
 __global__ void ANA_TRAVERSAL_BOUNDS k_trace_batch(const __grid_constant__ DevScene S, uint32_t scene,
-                                                   const float* rays, uint32_t n, ana_hit* out, uint32_t* fetch,
-                                                   uint32_t* err) {
+                                                   const float* rays, const float* times, uint32_t n, ana_hit* out,
+                                                   uint32_t* fetch, uint32_t* err) {
     const uint32_t triRoot = S.scenes[scene].tri_root, segRoot = S.scenes[scene].seg_root;
     auto load = [&](uint32_t i, Ray& r, uint32_t& root, uint32_t& sroot) {
         const float4* rp = reinterpret_cast<const float4*>(rays + 8 * size_t(i));
         float4 a = rp[0], b = rp[1];
-        r = Ray{f3(a), f3(b), a.w, b.w};
+        r = Ray{f3(a), f3(b), a.w, b.w, times ? times[i] : 0.f};
         root = triRoot;
         sroot = kCurves ? segRoot : kNoRoot;
     };
-    // rays carry no time: Ray::time's default 0 (Types.h:259)
+    // without `times` every ray has Ray::time's default 0 (Types.h:259)
     run_traversal<kAny, false, kPersist, kCurves, kMotion>(S, n, fetch, err, nullptr, load, [&](uint32_t i, const Traversal& T) {
         ana_hit h{0, -1, -1, -1, 0.f, 0.f, 0.f, 0.f};
         if (kAny) {
@@ -1281,32 +1281,33 @@ void launch_film(const Params& p, const LaunchCfg& c, cudaStream_t s) {
     k_film<<<blocks_for(p.chunk_pixels, 256, c.grid_cap), 256, 0, s>>>(p);
 }
 template <bool kAny, bool kCurves, bool kPersist, bool kMotion = false>
-static void tb_launch(const DevScene& S, uint32_t scene, const float* rays, uint32_t n, ana_hit* out,
-                      uint32_t* fetch, uint32_t* err, int grid, cudaStream_t s) {
+static void tb_launch(const DevScene& S, uint32_t scene, const float* rays, const float* times, uint32_t n,
+                      ana_hit* out, uint32_t* fetch, uint32_t* err, int grid, cudaStream_t s) {
     auto k = k_trace_batch<kAny, kCurves, kPersist, kMotion>;
     int g = kPersist ? resident_grid(k) : grid;
-    k<<<g, kPersistBlock, 0, s>>>(S, scene, rays, n, out, fetch, err);
+    k<<<g, kPersistBlock, 0, s>>>(S, scene, rays, times, n, out, fetch, err);
 }
-void launch_trace_batch(const DevScene& S, uint32_t scene, const float* rays, size_t n, ana_hit* out, int occlusion,
+void launch_trace_batch(const DevScene& S, uint32_t scene, const float* rays, const float* times, size_t n,
+                        ana_hit* out, int occlusion,
                         uint32_t* fetch, uint32_t* err, int persistent, cudaStream_t s) {
     const bool cv = S.has_curves != 0;
     int grid = blocks_for(uint32_t(n), kPersistBlock, 1 << 20);
     uint32_t nn = uint32_t(n);
     if (S.has_motion) {
-        if (occlusion) cv ? tb_launch<true, true, true, true>(S, scene, rays, nn, out, fetch, err, grid, s)
-                          : tb_launch<true, false, true, true>(S, scene, rays, nn, out, fetch, err, grid, s);
-        else cv ? tb_launch<false, true, true, true>(S, scene, rays, nn, out, fetch, err, grid, s)
-                : tb_launch<false, false, true, true>(S, scene, rays, nn, out, fetch, err, grid, s);
+        if (occlusion) cv ? tb_launch<true, true, true, true>(S, scene, rays, times, nn, out, fetch, err, grid, s)
+                          : tb_launch<true, false, true, true>(S, scene, rays, times, nn, out, fetch, err, grid, s);
+        else cv ? tb_launch<false, true, true, true>(S, scene, rays, times, nn, out, fetch, err, grid, s)
+                : tb_launch<false, false, true, true>(S, scene, rays, times, nn, out, fetch, err, grid, s);
     } else if (occlusion) {
-        if (cv) persistent ? tb_launch<true, true, true>(S, scene, rays, nn, out, fetch, err, grid, s)
-                           : tb_launch<true, true, false>(S, scene, rays, nn, out, fetch, err, grid, s);
-        else persistent ? tb_launch<true, false, true>(S, scene, rays, nn, out, fetch, err, grid, s)
-                        : tb_launch<true, false, false>(S, scene, rays, nn, out, fetch, err, grid, s);
+        if (cv) persistent ? tb_launch<true, true, true>(S, scene, rays, times, nn, out, fetch, err, grid, s)
+                           : tb_launch<true, true, false>(S, scene, rays, times, nn, out, fetch, err, grid, s);
+        else persistent ? tb_launch<true, false, true>(S, scene, rays, times, nn, out, fetch, err, grid, s)
+                        : tb_launch<true, false, false>(S, scene, rays, times, nn, out, fetch, err, grid, s);
     } else {
-        if (cv) persistent ? tb_launch<false, true, true>(S, scene, rays, nn, out, fetch, err, grid, s)
-                           : tb_launch<false, true, false>(S, scene, rays, nn, out, fetch, err, grid, s);
-        else persistent ? tb_launch<false, false, true>(S, scene, rays, nn, out, fetch, err, grid, s)
-                        : tb_launch<false, false, false>(S, scene, rays, nn, out, fetch, err, grid, s);
+        if (cv) persistent ? tb_launch<false, true, true>(S, scene, rays, times, nn, out, fetch, err, grid, s)
+                           : tb_launch<false, true, false>(S, scene, rays, times, nn, out, fetch, err, grid, s);
+        else persistent ? tb_launch<false, false, true>(S, scene, rays, times, nn, out, fetch, err, grid, s)
+                        : tb_launch<false, false, false>(S, scene, rays, times, nn, out, fetch, err, grid, s);
     }
 }
 

@@ -126,8 +126,9 @@ void launch_shade_adj(const Params& p, const LaunchCfg& c, cudaStream_t s);
 void launch_shadow_adj(const Params& p, const LaunchCfg& c, cudaStream_t s);
 void launch_mis_adj(const Params& p, const LaunchCfg& c, cudaStream_t s);
 void launch_adj_direct(const Params& p, const LaunchCfg& c, cudaStream_t s);
-void launch_trace_batch(const DevScene& S, uint32_t scene, const float* rays, size_t n, ana_hit* out, int occlusion,
-                        uint32_t* fetch, uint32_t* err, int persistent, cudaStream_t s);
+// times: one ray time per ray (motion-blurred meshes), or null (time 0)
+void launch_trace_batch(const DevScene& S, uint32_t scene, const float* rays, const float* times, size_t n,
+                        ana_hit* out, int occlusion, uint32_t* fetch, uint32_t* err, int persistent, cudaStream_t s);
 
 // Fixed device scratch of the allocation-free trace entry point: a 256-byte
 // header (the scene record at 0, the error word at kNoAllocErrOffset and the

@@ -376,6 +376,12 @@ int ana_image_write_png(const char* path, uint32_t width, uint32_t height, const
 int ana_trace_batch(ana_ctx* ctx, const float* rays, size_t n, ana_hit* out, int occlusion_only,
                     int rays_on_device);
 
+/* ana_trace_batch with each ray's Ray::time (n floats, NULL: 0; on the device
+ * with rays_on_device): motion-blurred meshes are met at that time
+ * (BVHBackend.cpp:356-367, 420-435). */
+int ana_trace_batch_timed(ana_ctx* ctx, const float* rays, const float* times, size_t n, ana_hit* out,
+                          int occlusion_only, int rays_on_device);
+
 /* ana_trace_batch without any device allocation (no counterpart in the
  * reference). ana_trace_batch takes a temporary device buffer per call
  * (cudaMalloc / cudaFree); this variant stages the rays, the hits and its

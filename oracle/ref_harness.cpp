@@ -312,7 +312,8 @@ int ref_commit(void* sp) {
 
 // rays: n x 8 floats (ox, oy, oz, tmin, dx, dy, dz, tmax)
 // out_ids: n x 4 int32 (hit, meshID, primID, strandID); out_t: n floats
-void ref_trace(void* sp, const float* rays, uint64_t n, int32_t* out_ids, float* out_t,
+// times: one Ray::time per ray, or NULL (time 0)
+void ref_trace(void* sp, const float* rays, const float* times, uint64_t n, int32_t* out_ids, float* out_t,
                int nthreads) {
     auto* s = static_cast<RefScene*>(sp);
     ThreadPool pool(uint32_t(nthreads > 0 ? nthreads : 0));
@@ -323,6 +324,7 @@ void ref_trace(void* sp, const float* rays, uint64_t n, int32_t* out_ids, float*
         for (uint64_t i = b; i < e; ++i) {
             const float* r = rays + 8 * i;
             Ray ray{v3(r), v3(r + 4), r[3], r[7]};
+            if (times) ray.time = times[i];
             TraceResult tr = s->accel->trace(ray);
             out_ids[4 * i + 0] = tr.hit ? 1 : 0;
             out_ids[4 * i + 1] = tr.hit ? int32_t(tr.si.meshID) : -1;
@@ -333,7 +335,7 @@ void ref_trace(void* sp, const float* rays, uint64_t n, int32_t* out_ids, float*
     });
 }
 
-void ref_occluded(void* sp, const float* rays, uint64_t n, uint8_t* out, int nthreads) {
+void ref_occluded(void* sp, const float* rays, const float* times, uint64_t n, uint8_t* out, int nthreads) {
     auto* s = static_cast<RefScene*>(sp);
     ThreadPool pool(uint32_t(nthreads > 0 ? nthreads : 0));
     const uint64_t chunk = 4096;
@@ -343,6 +345,7 @@ void ref_occluded(void* sp, const float* rays, uint64_t n, uint8_t* out, int nth
         for (uint64_t i = b; i < e; ++i) {
             const float* r = rays + 8 * i;
             Ray ray{v3(r), v3(r + 4), r[3], r[7]};
+            if (times) ray.time = times[i];
             out[i] = s->accel->occluded(ray) ? 1 : 0;
         }
     });

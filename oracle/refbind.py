@@ -76,8 +76,8 @@ def lib(variant="record"):
     L.ref_set_env_radiance.argtypes = [_P, _F]
     L.ref_set_camera.argtypes = [_P, _F, _F, _F, C.c_float, C.c_uint32, C.c_uint32]
     L.ref_commit.argtypes = [_P]
-    L.ref_trace.argtypes = [_P, _F, C.c_uint64, _I32, _F, C.c_int]
-    L.ref_occluded.argtypes = [_P, _F, C.c_uint64, _U8, C.c_int]
+    L.ref_trace.argtypes = [_P, _F, _F, C.c_uint64, _I32, _F, C.c_int]
+    L.ref_occluded.argtypes = [_P, _F, _F, C.c_uint64, _U8, C.c_int]
     L.ref_render.argtypes = [_P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
                              C.c_int, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, _F, _F]
     L.ref_render.restype = C.c_double
@@ -187,18 +187,20 @@ class RefScene:
         except Exception:
             pass
 
-    def trace(self, rays, nthreads=0):
+    def trace(self, rays, nthreads=0, times=None):
         rays = f32(rays).reshape(-1, 8)
         n = len(rays)
         ids = np.zeros((n, 4), np.int32)
         t = np.zeros(n, np.float32)
-        self.L.ref_trace(self.h, _fp(rays), n, ids.ctypes.data_as(_I32), _fp(t), nthreads)
+        tm = None if times is None else f32(times)
+        self.L.ref_trace(self.h, _fp(rays), _fp(tm), n, ids.ctypes.data_as(_I32), _fp(t), nthreads)
         return ids, t
 
-    def occluded(self, rays, nthreads=0):
+    def occluded(self, rays, nthreads=0, times=None):
         rays = f32(rays).reshape(-1, 8)
         out = np.zeros(len(rays), np.uint8)
-        self.L.ref_occluded(self.h, _fp(rays), len(rays), out.ctypes.data_as(_U8), nthreads)
+        tm = None if times is None else f32(times)
+        self.L.ref_occluded(self.h, _fp(rays), _fp(tm), len(rays), out.ctypes.data_as(_U8), nthreads)
         return out.astype(bool)
 
     def render(self, spp=None, sample_start=0, max_depth=None, nthreads=0, rect=None):

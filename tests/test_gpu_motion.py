@@ -47,6 +47,33 @@ def test_hits_at_time_zero_match_reference(renderer, ref_built, occlusion):
     assert moving.sum() > 1000
 
 
+@pytest.mark.parametrize("occlusion", [False, True], ids=["closest", "any"])
+def test_hits_at_ray_times_match_reference(renderer, ref_built, occlusion):
+    """ana_trace_batch_timed: every ray at its own time in [-0.1, 1.1] (before
+    the first key, between keys, after the last): hits bit for bit."""
+    sc = S.motion(64, 48, 1)
+    rays = seeded_rays(7, 1 << 18, -2.5, 2.5)
+    rays[:, 1] = np.abs(rays[:, 1])
+    times = np.random.default_rng(8).uniform(-0.1, 1.1, len(rays)).astype(np.float32)
+    if occlusion:
+        rays[:, 7] = np.random.default_rng(9).uniform(0.05, 4.0, len(rays)).astype(np.float32)
+    renderer.upload(sc)
+    g = renderer.trace(rays, occlusion=occlusion, times=times)
+    rs = ref_built.RefScene(sc, variant="nocontract")
+    if occlusion:
+        assert np.array_equal(g["hit"] == 1, rs.occluded(rays, times=times))
+        return
+    ids, t = rs.trace(rays, times=times)
+    same = (gpu_ids(g) == ids).all(1)
+    bad = ~(same | excluded_ties(g, ids, t))
+    assert not bad.any(), (bad.sum(), gpu_ids(g)[bad][:5], ids[bad][:5])
+    hit = ids[:, 0] == 1
+    assert np.array_equal(g["t"][hit & same], t[hit & same])
+    # the times matter: at time 0 the moving meshes are hit elsewhere
+    g0 = renderer.trace(rays)
+    assert (gpu_ids(g0) != gpu_ids(g)).any(1).sum() > 100
+
+
 @pytest.mark.parametrize("shutter", [(0.0, 1.0), (0.25, 0.75)], ids=["full", "half"])
 def test_per_sample_radiance_matches_reference(renderer, ref_built, shutter):
     sc = S.motion(96, 72, 1, 6, shutter=shutter)
