@@ -70,10 +70,31 @@ def parse():
                     help="skip the batched-vs-plain and adjoint/forward measurements")
     ap.add_argument("--traversal", type=int, default=0,
                     help="0 library default, 1 persistent warps, 2 one thread per ray")
+    ap.add_argument("--scene", default="throughput", choices=["throughput", "glass", "motion", "hair"],
+                    help="the frame to time (profiling of the other scenes; the bench line's workload is "
+                         "the throughput scene)")
     return ap.parse_args()
 
 
+def make_scene(a):
+    """The timed frame: the throughput scene, or (--scene) the glass /
+    alpha-mask, motion-blur or hair scene at the same film size, spp and depth."""
+    from anacapa_b200 import scenes as S
+    if a.scene == "glass":
+        return S.glass(a.width, a.height, a.spp, a.depth)
+    if a.scene == "motion":
+        return S.motion(a.width, a.height, a.spp, a.depth)
+    if a.scene == "hair":
+        return S.hair(a.width, a.height, a.spp, a.depth)
+    return S.throughput(a.width, a.height, a.spp, a.depth, n_spheres=a.n_spheres)
+
+
 def workload_config(a, scene):
+    if a.scene != "throughput":
+        return {"workload": f"{a.scene} scene, {scene.num_triangles} triangles, {scene.num_segments} curve "
+                            f"segments; {a.width}x{a.height}, {a.spp} spp, max depth {a.depth}",
+                "paths_per_step": scene.num_paths, "triangles": scene.num_triangles,
+                "chunk_paths": min(a.chunk_paths, scene.num_paths)}
     return {
         "workload": (f"throughput scene: {a.n_spheres} icospheres (subdiv 3) + ground, "
                      f"{scene.num_triangles} triangles, GGX standard_surface, 1024x512 HDR dome; "
@@ -234,7 +255,7 @@ def run_reference(a):
     if rank != 0:
         return 0
     from anacapa_b200 import scenes as S
-    scene = S.throughput(a.width, a.height, a.spp, a.depth, n_spheres=a.n_spheres)
+    scene = make_scene(a)
     vals, desc, cores = cpu_reference_sample(scene, a.cpu_seconds, steps=a.steps, warmup=a.warmup)
     v = statistics.mean(vals)
     paths = scene.num_paths
@@ -396,7 +417,7 @@ def run_ours(a):
     from anacapa_b200 import scenes as S
     if torch.cuda.is_available():
         torch.cuda.set_device(local)
-    scene = S.throughput(a.width, a.height, a.spp, a.depth, n_spheres=a.n_spheres)
+    scene = make_scene(a)
     t_prep = time.perf_counter()
     prep = api.Prepared(scene)
     t_prep = time.perf_counter() - t_prep
@@ -438,7 +459,7 @@ def run_ours(a):
                  + (32 + 16) * work.extend_rays)
     peak, peak_kind = measured_peaks()
     achieved = (alg_bytes / ext_launches) / ((ext_ms / ext_launches) / 1e3) / 1e9 if ext_ms > 0 else None
-    tpr = extend_traffic_per_ray()
+    tpr = extend_traffic_per_ray() if a.scene == "throughput" else None  # measured on that scene
     traffic = (tpr * work.extend_rays / ext_launches) if tpr else None
     # end to end through the C ABI with host buffers
     e2e = None
