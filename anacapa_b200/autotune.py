@@ -29,7 +29,7 @@ class Config:
 
 SPACE = {
     "chunk_paths": [1 << 21, 1 << 22, 1 << 23, 1 << 24, 1 << 25, 1 << 26],
-    "block_size": [128, 256, 512],
+    "block_size": [128, 256],  # the shading kernel's blocks (at most 256 threads)
     "traversal": [api.ANA_TRAVERSAL_PERSISTENT, api.ANA_TRAVERSAL_PER_RAY],
     "max_leaf_tris": [2, 4, 8],
 }

@@ -359,6 +359,27 @@ def bench_configs(local):
     return out
 
 
+def bench_aov_film_io(r, scene, start):
+    """One frame of the timed workload with the denoising AOVs (device time
+    against the frame without them), then Film::writeEXR (beauty + albedo +
+    normals, ZIP) and Film::writePNG of it through the C ABI (wall time,
+    device-to-host read included)."""
+    W, H = scene.width, scene.height
+    r.render(W, H, scene.spp, scene.max_depth, sample_start=start, clear=True)
+    plain = r.stats().render_ms
+    r.render(W, H, scene.spp, scene.max_depth, sample_start=start, clear=True, aovs=True)
+    with_aov = r.stats().render_ms
+    with tempfile.TemporaryDirectory() as d:
+        t0 = time.perf_counter()
+        r.write_exr(os.path.join(d, "f.exr"), W, H, aovs=True)
+        t1 = time.perf_counter()
+        r.write_png(os.path.join(d, "f.png"), W, H)
+        t2 = time.perf_counter()
+        exr_mb = os.path.getsize(os.path.join(d, "f.exr")) / 1e6
+    return {"frame_ms": plain, "frame_with_aovs_ms": with_aov, "aov_overhead": with_aov / plain - 1.0,
+            "write_exr_s": t1 - t0, "exr_mb": exr_mb, "write_png_s": t2 - t1}
+
+
 def bench_scene_setup(local, scene, prep_s):
     """Host build (ana_prepare_scene, timed by the caller) against the device
     build (ana_upload_scene_device: triangle setup, SAH build and collapse on
@@ -483,6 +504,7 @@ def run_ours(a):
         setup = bench_scene_setup(local, scene, t_prep)
         setup["same_bytes"] = setup.pop("digest") == prep.digest
         extra["scene_setup"] = setup
+        extra["aov_film_io"] = bench_aov_film_io(r, scene, start)
     cpu = None
     if rank == 0 and ws == 1 and not a.no_cpu_baseline:
         try:

@@ -270,7 +270,8 @@ typedef struct ana_ctx ana_ctx;
 typedef struct ana_device_opts {
     int device;              /* CUDA ordinal                                   */
     uint32_t chunk_paths;    /* wavefront capacity in paths (0 = 2^25)         */
-    uint32_t block_size;     /* threads per block of the stage kernels (0 = default) */
+    uint32_t block_size;     /* threads per block of the shading kernel (0 = default 256;
+                                larger requests run 256-thread blocks)            */
     uint32_t timing;         /* 1: record per-stage CUDA-event times           */
     uint32_t traversal;      /* ANA_TRAVERSAL_*: schedule of the BVH traversal kernels */
 } ana_device_opts;
