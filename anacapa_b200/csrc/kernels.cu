@@ -34,7 +34,7 @@ namespace ana {
 constexpr uint32_t kMiss = 0xFFFFFFFFu;
 constexpr int kMaxBlock = 1024;
 constexpr int kPersistBlock = 256;    // traversal kernels: 8 warps per block
-constexpr int kPersistMinBlocks = 4;  // persistent schedule: 4 resident blocks/SM (<= 64 registers)
+constexpr int kPersistMinBlocks = 5;  // persistent schedule: 5 resident blocks/SM (<= 51 registers)
 // k_shade runs at most 256-thread blocks: three resident per SM (80 registers,
 // spilling to L1) for the forward kernel without fiber code measured 5 % faster
 // than two at 128 registers; the fiber and adjoint variants keep two
@@ -280,10 +280,13 @@ __device__ __forceinline__ void run_traversal(const DevScene& S, uint32_t n, uin
     }
 }
 
-// Persistent triangle kernels fit 4 blocks per SM (64 registers); with the
-// curve stage they take 2 (128 registers: the ribbon test's state).
+// Persistent triangle kernels fit 5 blocks per SM (48 registers, a few spills
+// to L1; on the throughput frame 451 ms against 467 ms at 4 blocks and 64
+// registers, and 520 ms at 6 blocks and 40); the motion variants (object-ray
+// state) keep 4 and 64 registers; with the curve stage they take 2 (128
+// registers: the ribbon test's state).
 #define ANA_TRAVERSAL_BOUNDS \
-    __launch_bounds__(kPersistBlock, kPersist ? (kCurves ? 2 : kPersistMinBlocks) : 1)
+    __launch_bounds__(kPersistBlock, kPersist ? (kCurves ? 2 : (kMotion ? 4 : kPersistMinBlocks)) : 1)
 
 __device__ __forceinline__ uint32_t scene_bits(float w) { return __float_as_uint(w); }
 
