@@ -283,10 +283,11 @@ __device__ __forceinline__ void run_traversal(const DevScene& S, uint32_t n, uin
 // Persistent triangle kernels fit 5 blocks per SM (48 registers, a few spills
 // to L1; on the throughput frame 451 ms against 467 ms at 4 blocks and 64
 // registers, and 520 ms at 6 blocks and 40); the motion variants (object-ray
-// state) keep 4 and 64 registers; with the curve stage they take 2 (128
-// registers: the ribbon test's state).
+// state) keep 4 and 64 registers; with the curve stage they take 3 (80
+// registers with spills to L1: the ribbon test's state; the hair frame
+// 1280x720x32 measured 1699 ms against 1813 ms at 2 blocks and 128).
 #define ANA_TRAVERSAL_BOUNDS \
-    __launch_bounds__(kPersistBlock, kPersist ? (kCurves ? 2 : (kMotion ? 4 : kPersistMinBlocks)) : 1)
+    __launch_bounds__(kPersistBlock, kPersist ? (kCurves ? 3 : (kMotion ? 4 : kPersistMinBlocks)) : 1)
 
 __device__ __forceinline__ uint32_t scene_bits(float w) { return __float_as_uint(w); }
 
