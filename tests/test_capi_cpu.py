@@ -119,3 +119,29 @@ def test_calls_on_null_context_are_rejected(lib_built):
     assert L.ana_film_read(None, None, 0) == api.ANA_ERR_INVALID_ARG
     st = api.AnaStats()
     assert L.ana_get_stats(None, C.byref(st)) == api.ANA_ERR_INVALID_ARG
+
+
+def test_prepare_motion_meshes(lib_built):
+    """Motion keys (MeshDesc::motionKeys): a scene with keys prepares; a
+    non-finite key is rejected; the time-expanded bounds make the layout
+    differ from the same scene with the keys removed."""
+    sc = S.motion(32, 24, 1)
+    assert _prepare_rc(sc) == api.ANA_OK
+    static = dataclasses.replace(sc, mesh_motion=None)
+    assert api.Prepared(sc).digest != api.Prepared(static).digest
+    keys = [list(k) if k else k for k in sc.mesh_motion]
+    t, M = keys[1][0]
+    M = np.array(M, np.float32)
+    M[0, 3] = np.nan
+    keys[1][0] = (t, M)
+    assert _prepare_rc(dataclasses.replace(sc, mesh_motion=keys)) == api.ANA_ERR_INVALID_ARG
+    assert "motion key" in api.last_error()
+
+
+def test_prepare_glass_and_alpha_materials(lib_built):
+    """Transmission and alpha masks prepare (glass lobes, tinted shadow rays);
+    the layout depends on the opacity of an alpha-masked material."""
+    sc = S.glass(32, 24, 1)
+    assert _prepare_rc(sc) == api.ANA_OK
+    mats = [dataclasses.replace(m, opacity=0.7) if m.alpha_mask and m.opacity > 0 else m for m in sc.materials]
+    assert api.Prepared(sc).digest != api.Prepared(dataclasses.replace(sc, materials=mats)).digest
