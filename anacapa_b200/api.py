@@ -425,20 +425,22 @@ class Renderer:
         """ana_film_write_png (Film::writePNG)."""
         self._check(lib().ana_film_write_png(self.h, width, height, str(path).encode(), exposure))
 
-    def render_tiles(self, width, height, max_depth, tiles, clear=False, min_depth=2, seed=0):
+    def render_tiles(self, width, height, max_depth, tiles, clear=False, min_depth=2, seed=0, aovs=False):
         """ana_render_tiles: tiles = [(x0, y0, w, h, sample_start, sample_count), ...]
         of one width x height frame, accumulated into the film."""
         arr = (AnaTile * max(1, len(tiles)))(*[AnaTile(*map(int, t)) for t in tiles])
         r = AnaRenderDesc(width, height, 0, 0, max_depth, min_depth, seed,
-                          ANA_RENDER_CLEAR_FILM if clear else 0)
+                          (ANA_RENDER_CLEAR_FILM if clear else 0) | (ANA_RENDER_AOVS if aovs else 0))
         self._check(lib().ana_render_tiles(self.h, C.byref(r), arr, len(tiles)))
 
-    def render_adaptive(self, width, height, spp, max_depth, tile_size=64, base_spp=0, min_depth=2, seed=0):
+    def render_adaptive(self, width, height, spp, max_depth, tile_size=64, base_spp=0, min_depth=2, seed=0,
+                        aovs=False):
         """ana_render_adaptive: the two-pass tile-adaptive schedule; returns the
         extra samples given to each tile (row-major)."""
         nt = (-(-width // tile_size)) * (-(-height // tile_size))
         extra = np.zeros(nt, np.uint32)
-        r = AnaRenderDesc(width, height, 0, spp, max_depth, min_depth, seed, ANA_RENDER_CLEAR_FILM)
+        r = AnaRenderDesc(width, height, 0, spp, max_depth, min_depth, seed,
+                          ANA_RENDER_CLEAR_FILM | (ANA_RENDER_AOVS if aovs else 0))
         self._check(lib().ana_render_adaptive(self.h, C.byref(r), tile_size, base_spp, extra.ctypes.data, nt))
         return extra
 

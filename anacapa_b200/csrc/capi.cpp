@@ -1240,7 +1240,7 @@ int ana_render_tiles(ana_ctx* c, const ana_render_desc* f, const ana_tile* tiles
         items.push_back(Item{0, W, H, t.x0, t.y0, t.width, t.height, t.sample_start, t.sample_count, f->max_depth,
                              f->min_depth, f->seed, 0});
     }
-    const uint32_t flags = f->flags & (ANA_RENDER_CLEAR_FILM | ANA_RENDER_COUNT_WORK);
+    const uint32_t flags = f->flags & (ANA_RENDER_CLEAR_FILM | ANA_RENDER_COUNT_WORK | ANA_RENDER_AOVS);
     if (items.empty()) return (flags & ANA_RENDER_CLEAR_FILM) ? ana_film_clear(c, W, H) : ANA_OK;
     const int rc = render_items(c, items, uint64_t(W) * H, flags);
     if (rc == ANA_OK) {
@@ -1268,7 +1268,7 @@ int ana_render_adaptive(ana_ctx* c, const ana_render_desc* f, uint32_t ts, uint3
     ana_render_desc b = *f;
     b.sample_start = 0;
     b.sample_count = base;
-    b.flags = ANA_RENDER_CLEAR_FILM;
+    b.flags = ANA_RENDER_CLEAR_FILM | (f->flags & ANA_RENDER_AOVS);  // renderTile's AOVs, as the tile loop merges them
     int rc = render_descs(c, &b, 1, b.flags);
     if (rc) return rc;
     std::vector<uint32_t> extraPerTile(nt, 0);
@@ -1314,7 +1314,7 @@ int ana_render_adaptive(ana_ctx* c, const ana_render_desc* f, uint32_t ts, uint3
             tiles[i].sample_count = extraPerTile[i];
         }
         ana_render_desc e = *f;
-        e.flags = 0;
+        e.flags = f->flags & ANA_RENDER_AOVS;
         rc = ana_render_tiles(c, &e, tiles.data(), nt);
         if (rc) return rc;
     }

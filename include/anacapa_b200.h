@@ -218,7 +218,9 @@ enum {
                                         surface gives IMaterial::reflectance and the shading
                                         normal; per pixel their averages over the call's
                                         samples (the normal renormalised) are added to the
-                                        AOV film with weight 1, as Film::mergeTile does   */
+                                        AOV film with weight 1, as Film::mergeTile does;
+                                        honoured by ana_render, ana_render_batch,
+                                        ana_render_tiles (per tile) and ana_render_adaptive */
 };
 
 /* One device-resident film pixel: the reference's PixelAccumulator

@@ -113,3 +113,18 @@ def test_dropin_writes_through_reference_film(gpu, ref_built, tmp_path):
     assert np.allclose(np.stack([ch["normals.R"], ch["normals.G"], ch["normals.B"]], -1), nr, rtol=1e-4,
                        atol=1e-5)
     assert (tmp_path / "d.png").exists()
+
+
+def test_tiles_carry_aovs(renderer):
+    """ana_render_tiles with ANA_RENDER_AOVS: tiles that cover the frame once
+    give every pixel the AOVs of a whole-frame pass (each tile's average,
+    weight 1, as renderTile and Film::mergeTile produce them)."""
+    sc = S.cornell(96, 80, 4)
+    renderer.upload(sc)
+    renderer.render_scene(sc, aovs=True)
+    a0, n0 = renderer.aovs(sc.width, sc.height)
+    tiles = [(x, y, min(32, sc.width - x), min(32, sc.height - y), 0, sc.spp)
+             for y in range(0, sc.height, 32) for x in range(0, sc.width, 32)]
+    renderer.render_tiles(sc.width, sc.height, sc.max_depth, tiles, clear=True, aovs=True)
+    a1, n1 = renderer.aovs(sc.width, sc.height)
+    assert np.array_equal(a0, a1) and np.array_equal(n0, n1)
