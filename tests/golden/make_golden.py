@@ -1,6 +1,7 @@
 """Generates the committed golden fixtures from the reference's own code.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py              # reference_vectors.npz
+    python tests/golden/make_golden.py --features   # feature_vectors.npz
 
 Runs here (where the reference tree was compiled into oracle/_ref by
 oracle/Makefile); the resulting .npz files travel with the repository, so the
@@ -85,5 +86,45 @@ def main():
     print("wrote", os.path.join(HERE, "reference_vectors.npz"))
 
 
+def feature_queries():
+    """The (pixel, sample) queries, rays and ray times of the feature
+    fixtures: deterministic, so tests rebuild them from the same seeds."""
+    rng = np.random.default_rng(2024)
+    q = {}
+    for name, (w, h) in {"sunlit": (96, 72), "glass": (96, 72), "motion": (96, 72)}.items():
+        q[name] = np.stack([rng.integers(0, w, 256), rng.integers(0, h, 256), rng.integers(0, 4, 256)],
+                           1).astype(np.uint32)
+    rays = seeded_rays(29, 2048, -2.5, 2.5)
+    rays[:, 1] = np.abs(rays[:, 1])
+    times = rng.uniform(-0.1, 1.1, len(rays)).astype(np.float32)
+    return q, rays, times
+
+
+def feature_scenes():
+    return {"sunlit": S.sunlit(96, 72, 1, 8, half_angle_deg=2.0), "glass": S.glass(96, 72, 1, 8),
+            "motion": S.motion(96, 72, 1, 6)}
+
+
+def features():
+    """feature_vectors.npz: per-sample radiance (PathIntegrator::Li) of the
+    directional-light, glass / alpha-mask and motion-blur scenes, and timed
+    closest hits against the motion scene (BVHBackend with Ray::time)."""
+    R.build()
+    q, rays, times = feature_queries()
+    out = {}
+    for name, sc in feature_scenes().items():
+        rs = R.RefScene(sc, variant="nocontract")
+        out[name + "_li"] = rs.li(q[name], nthreads=1)
+        if name == "motion":
+            ids, t = rs.trace(rays, nthreads=1, times=times)
+            out["motion_ids"] = ids
+            out["motion_t"] = t
+    np.savez_compressed(os.path.join(HERE, "feature_vectors.npz"), **out)
+    print("wrote", os.path.join(HERE, "feature_vectors.npz"))
+
+
 if __name__ == "__main__":
-    main()
+    if "--features" in sys.argv:
+        features()
+    else:
+        main()
