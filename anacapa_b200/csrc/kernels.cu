@@ -266,7 +266,7 @@ __device__ __forceinline__ void run_traversal(const DevScene& S, uint32_t n, uin
                             node_step<kAny, kCount, kCurves>(T, S, stack, stackT, err, cnt);
                         } else if (leaf_step<kAny, kCount, kCurves, kMotion>(T, S, T.cur, cnt)) {
                             T.exhausted = true;
-                        } else if (!trav_pop(T, stack, stackT)) {
+                        } else if (!trav_pop<kAny>(T, stack, stackT)) {
                             T.exhausted = true;
                         }
                     }
