@@ -95,6 +95,14 @@ def test_seeded_rays_match_reference(renderer, ref_built, case):
     hit = ids[:, 0] == 1
     assert np.array_equal(g["t"][hit & same], t[hit & same])
     assert hit.sum() > n // 20
+    # occlusion (any hit: children in stored order, leaves parked) over finite
+    # segments: the same answer as BVHBackend/CurveBrute::occluded, ray for ray
+    seg = rays.copy()
+    seg[:, 7] = np.random.default_rng(5).uniform(0.01, 3.0, n).astype(np.float32)
+    occ = renderer.trace(seg, occlusion=True)["hit"] == 1
+    ref_occ = rs.occluded(seg)
+    assert np.array_equal(occ, ref_occ), f"{int((occ != ref_occ).sum())} of {n} occlusion answers differ"
+    assert 0 < occ.sum() < n
     # reference flags of record (-mfma with contraction): ids equal except ties
     # and a residue where the reference's own fused multiply-adds round a
     # grazing test (a ribbon's width boundary, a triangle edge) the other way;
