@@ -23,6 +23,10 @@ namespace {
 std::mutex g_err_mu;
 std::string g_last_err;
 
+// ceil(2^64 / d), 0 for d <= 1: the kernels' div_magic gives floor(n / d) for
+// every 32-bit n from it (M*d = 2^64 + e with e < d, so n*e < 2^64).
+uint64_t magic_div(uint32_t d) { return d <= 1 ? 0 : ~0ULL / d + 1; }
+
 void set_global_err(const std::string& m) {
     std::lock_guard<std::mutex> lk(g_err_mu);
     g_last_err = m;
@@ -633,6 +637,8 @@ int render_items(ana_ctx* c, const std::vector<Item>& items, uint64_t totalPixel
         R.rect_y0 = r.y0;
         R.rect_w = r.rw;
         R.film_w = r.width;
+        R.spp_div = magic_div(r.spp);
+        R.rect_w_div = magic_div(r.rw);
         pathOff[k] = uint32_t(path);
         path += uint64_t(r.rw) * r.rh * r.spp;
     }

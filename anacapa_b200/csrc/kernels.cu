@@ -93,12 +93,19 @@ __device__ __forceinline__ uint32_t scene_of(const DevScene& S, uint32_t gid) {
     return lo;
 }
 
+// floor(n / d) from m = ceil(2^64 / d) (0 encodes d = 1): m*d = 2^64 + e with
+// e < d, so n*e < 2^64 for every 32-bit n and the high word of n*m is the
+// quotient. The scene record carries m for its spp and rectangle width.
+__device__ __forceinline__ uint32_t div_magic(uint32_t n, uint64_t m) {
+    return m ? uint32_t(__umul64hi(uint64_t(n), m)) : n;
+}
+
 __device__ __forceinline__ void path_coords(const DevSceneRec& R, uint32_t gid, uint32_t& px, uint32_t& py,
                                             uint32_t& sidx) {
     uint32_t local = gid - R.path_offset;
-    uint32_t pixel = local / R.spp;
+    uint32_t pixel = div_magic(local, R.spp_div);
     sidx = R.sample_start + (local - pixel * R.spp);
-    const uint32_t ly = pixel / R.rect_w;
+    const uint32_t ly = div_magic(pixel, R.rect_w_div);
     px = R.rect_x0 + (pixel - ly * R.rect_w);
     py = R.rect_y0 + ly;
 }
@@ -116,7 +123,7 @@ __device__ __forceinline__ float path_time(const DevSceneRec& R, uint32_t gid) {
 
 // Film index of an item's pixel (its index within the item's rectangle).
 __device__ __forceinline__ size_t film_index(const DevSceneRec& R, uint32_t pixel) {
-    const uint32_t ly = pixel / R.rect_w;
+    const uint32_t ly = div_magic(pixel, R.rect_w_div);
     return size_t(R.film_offset) + size_t(R.rect_y0 + ly) * R.film_w + R.rect_x0 + (pixel - ly * R.rect_w);
 }
 
@@ -882,7 +889,7 @@ __global__ void __launch_bounds__(256) k_adj_init(const __grid_constant__ Params
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < p.chunk_paths; i += gridDim.x * blockDim.x) {
         const uint32_t gid = p.chunk_first_path + i;
         const DevSceneRec& R = p.S.scenes[scene_of(p.S, gid)];
-        const uint32_t pixel = (gid - R.path_offset) / R.spp;
+        const uint32_t pixel = div_magic(gid - R.path_offset, R.spp_div);
         const float3 L = load3(p.a.Lp, i);
         float3 dl = f3(0.f, 0.f, 0.f);
         if (is_finite3(L)) dl = load3(p.a.d_image, film_index(R, pixel)) * (1.f / float(R.spp));

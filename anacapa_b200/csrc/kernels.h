@@ -135,7 +135,7 @@ void launch_trace_batch(const DevScene& S, uint32_t scene, const float* rays, co
 // persistent schedule's work counter 4 bytes after it), then room for
 // ANA_TRACE_NOALLOC_MAX_RAYS rays of 32 bytes, then as many 32-byte hits.
 constexpr size_t kNoAllocHeader = 256;
-constexpr size_t kNoAllocErrOffset = 192;
+constexpr size_t kNoAllocErrOffset = 240;
 constexpr size_t kNoAllocRays = kNoAllocHeader;
 constexpr size_t kNoAllocHits = kNoAllocRays + size_t(ANA_TRACE_NOALLOC_MAX_RAYS) * 32;
 constexpr size_t kNoAllocBytes = kNoAllocHits + size_t(ANA_TRACE_NOALLOC_MAX_RAYS) * sizeof(ana_hit);

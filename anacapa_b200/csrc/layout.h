@@ -133,6 +133,9 @@ struct DevSceneRec {
     // The item's pixels: a rect_w-wide rectangle at (rect_x0, rect_y0) of a
     // film_w-wide film (a TileRequest; a whole frame is the full rectangle).
     uint32_t rect_x0, rect_y0, rect_w, film_w;
+    // ceil(2^64 / spp) and ceil(2^64 / rect_w), 0 for a divisor of 1: the
+    // kernels divide path and pixel indices by multiply-high
+    uint64_t spp_div, rect_w_div;
 };
 
 struct DevScene {

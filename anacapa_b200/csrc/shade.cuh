@@ -803,7 +803,10 @@ __device__ __forceinline__ float3 env_eval(const DevEnv& E, float3 wo) {
     int c0 = int(floorf(fc)), r0 = int(floorf(fr));
     float tc = fc - float(c0), tr = fr - float(r0);
     int W = int(E.width), H = int(E.height);
-    auto wrapc = [&](int c) { return uint32_t(((c % W) + W) % W); };
+    // c0 is in [-1, W - 1] and c0 + 1 in [0, W]: one add or subtract wraps
+    // them as ((c % W) + W) % W does; the clamp only keeps a non-finite
+    // direction's index in bounds
+    auto wrapc = [&](int c) { return uint32_t(max(0, min(c < 0 ? c + W : (c >= W ? c - W : c), W - 1))); };
     auto clampr = [&](int r) { return uint32_t(max(0, min(r, H - 1))); };
     uint32_t c1 = wrapc(c0 + 1), c0u = wrapc(c0), r1u = clampr(r0 + 1), r0u = clampr(r0);
     const float* p00 = E.rgb + (size_t(r0u) * E.width + c0u) * 3;
