@@ -34,6 +34,12 @@ TRACE_NOALLOC_MAX_RAYS = 65536  # ANA_TRACE_NOALLOC_MAX_RAYS
 
 F3 = C.c_float * 3
 
+# ana_bsdf_query / ana_bsdf_result as numpy records
+BSDF_QUERY = np.dtype([("n", "<f4", 3), ("t", "<f4", 3), ("color", "<f4", 3), ("wo", "<f4", 3),
+                       ("wi", "<f4", 3), ("u", "<f4", 2), ("u_comp", "<f4"), ("is_curve", "<u4")])
+BSDF_RESULT = np.dtype([("f", "<f4", 3), ("pdf", "<f4"), ("sample_f", "<f4", 3), ("sample_pdf", "<f4"),
+                        ("sample_wi", "<f4", 3), ("sample_flags", "<u4")])
+
 
 class AnaMaterial(C.Structure):
     _fields_ = [("type", C.c_uint32), ("albedo", F3), ("emission", F3), ("base_color", F3),
@@ -130,7 +136,8 @@ EXPORTS = ["ana_create", "ana_destroy", "ana_upload_scene", "ana_prepare_scene",
            "ana_prepared_digest", "ana_trace_batch_noalloc", "ana_diff_counts", "ana_diff_get_params",
            "ana_forward", "ana_backward", "ana_render_tiles", "ana_render_adaptive",
            "ana_upload_scene_device", "ana_scene_digest", "ana_aov_read", "ana_film_write_exr",
-           "ana_film_write_png", "ana_image_write_exr", "ana_image_write_png", "ana_trace_batch_timed"]
+           "ana_film_write_png", "ana_image_write_exr", "ana_image_write_png", "ana_trace_batch_timed",
+           "ana_bsdf_batch"]
 ANA_RENDER_GRAPH = 4
 
 _lib = None
@@ -193,6 +200,7 @@ def lib():
     L.ana_diff_get_params.argtypes = [_P, C.POINTER(AnaDiffParams)]
     L.ana_forward.argtypes = [_P, C.POINTER(AnaRenderDesc), C.POINTER(AnaDiffParams), _P]
     L.ana_backward.argtypes = [_P, _P, C.POINTER(AnaDiffParams)]
+    L.ana_bsdf_batch.argtypes = [_P, C.POINTER(AnaMaterial), _P, C.c_size_t, _P]
     _lib = L
     return L
 
@@ -504,6 +512,15 @@ class Renderer:
         st = self._diff_struct(d)
         self._check(lib().ana_backward(self.h, g.ctypes.data, C.byref(st)))
         return d
+
+    def bsdf(self, material: S.Material, queries: np.ndarray) -> np.ndarray:
+        """IMaterial::evaluate and sample of `material` on the device for a
+        BSDF_QUERY record array; returns BSDF_RESULT records."""
+        q = np.ascontiguousarray(queries, BSDF_QUERY)
+        out = np.zeros(len(q), BSDF_RESULT)
+        m = material_struct(material)
+        self._check(lib().ana_bsdf_batch(self.h, C.byref(m), _ptr(q), len(q), _ptr(out)))
+        return out
 
     def stats(self) -> AnaStats:
         s = AnaStats()

@@ -11,7 +11,11 @@ Results are identical across configurations (none changes the estimator).
 """
 from __future__ import annotations
 
+import argparse
 import dataclasses
+import json
+import os
+import sys
 import time
 from typing import Dict, List, Sequence
 
@@ -28,11 +32,16 @@ class Config:
 
 
 SPACE = {
-    "chunk_paths": [1 << 21, 1 << 22, 1 << 23, 1 << 24, 1 << 25, 1 << 26],
+    "chunk_paths": [1 << k for k in range(20, 28)],  # 1M .. 128M paths in flight
     "block_size": [128, 256],  # the shading kernel's blocks (at most 256 threads)
     "traversal": [api.ANA_TRAVERSAL_PERSISTENT, api.ANA_TRAVERSAL_PER_RAY],
     "max_leaf_tris": [2, 4, 8],
 }
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+TABLES = os.path.join(os.path.dirname(HERE), "profiles")
+# the point used when no tuning table has been recorded for a workload
+DEFAULT_POINT = {"chunk": 8 << 20, "block": 256, "traversal": api.ANA_TRAVERSAL_PERSISTENT, "leaf": 2}
 
 
 class Tuner:
@@ -103,3 +112,46 @@ def tune(scenes, **kw):
     t0 = time.time()
     best = t.tune()
     return best, t.best_ms, t.table, time.time() - t0
+
+
+def table_path(workload):
+    return os.path.join(TABLES, f"autotune_{workload}.json")
+
+
+def tuned_point(workload):
+    """The best point of the recorded tuning table of a workload
+    (profiles/autotune_<workload>.json, written by this module's command
+    line), else DEFAULT_POINT."""
+    p = table_path(workload)
+    if os.path.exists(p):
+        with open(p) as f:
+            b = json.load(f)["best"]
+        return {"chunk": int(b["chunk_paths"]), "block": int(b["block_size"]), "traversal": int(b["traversal"]),
+                "leaf": int(b["max_leaf_tris"]), "source": os.path.relpath(p, os.path.dirname(TABLES))}
+    return dict(DEFAULT_POINT, source="default")
+
+
+WORKLOADS = {"batched": lambda: S.batched_variants(64, seed=0)}
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description="Tune the launch configuration of a workload and record the table.")
+    ap.add_argument("--workload", default="batched", choices=sorted(WORKLOADS))
+    ap.add_argument("--out", default=None, help="table file (default profiles/autotune_<workload>.json)")
+    ap.add_argument("--repeats", type=int, default=2)
+    a = ap.parse_args(argv)
+    scenes = WORKLOADS[a.workload]()
+    best, ms, table, secs = tune(scenes, repeats=a.repeats)
+    rec = {"workload": a.workload, "paths": sum(sc.num_paths for sc in scenes), "space": SPACE,
+           "start": dataclasses.asdict(Config()), "best": dataclasses.asdict(best), "best_ms": ms,
+           "tuning_seconds": secs, "table": table,
+           "command": f"python -m anacapa_b200.autotune --workload {a.workload} --repeats {a.repeats}"}
+    out = a.out or table_path(a.workload)
+    with open(out, "w") as f:
+        json.dump(rec, f, indent=1)
+    print(json.dumps({"best": rec["best"], "best_ms": ms, "measurements": len(table), "seconds": secs}))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1553,6 +1553,33 @@ int ana_trace_batch_noalloc(ana_ctx* c, const float* rays, size_t n, ana_hit* ou
     return ANA_OK;
 }
 
+int ana_bsdf_batch(ana_ctx* c, const ana_material* material, const ana_bsdf_query* q, size_t n,
+                   ana_bsdf_result* out) {
+    if (!c || !material || (!q && n) || (!out && n))
+        return fail(c, ANA_ERR_INVALID_ARG, "ana_bsdf_batch: NULL argument");
+    if (n >= (size_t(1) << 31)) return fail(c, ANA_ERR_INVALID_ARG, "ana_bsdf_batch: n >= 2^31");
+    ana::DevMaterial m;
+    if (const char* why = ana::make_material(*material, m))
+        return fail(c, ANA_ERR_INVALID_ARG, std::string("ana_bsdf_batch: ") + why);
+    if (n == 0) return ANA_OK;
+    CK(cudaSetDevice(c->device), "cudaSetDevice");
+    const size_t qBytes = align_up(n * sizeof(ana_bsdf_query));
+    void* tmp = nullptr;
+    CK(cudaMalloc(&tmp, qBytes + n * sizeof(ana_bsdf_result)), "cudaMalloc(bsdf query)");
+    auto* dq = static_cast<ana_bsdf_query*>(tmp);
+    auto* dr = reinterpret_cast<ana_bsdf_result*>(static_cast<unsigned char*>(tmp) + qBytes);
+    cudaError_t e = cudaMemcpyAsync(dq, q, n * sizeof(ana_bsdf_query), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) {
+        ana::launch_bsdf_query(m, dq, uint32_t(n), dr, c->stream);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, dr, n * sizeof(ana_bsdf_result), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cudaFree(tmp);
+    if (e != cudaSuccess) return cuda_fail(c, e, "ana_bsdf_batch");
+    return ANA_OK;
+}
+
 int ana_diff_counts(ana_ctx* c, uint32_t* nm, uint32_t* nl) {
     if (!c || !nm || !nl) return fail(c, ANA_ERR_INVALID_ARG, "ana_diff_counts: NULL argument");
     if (!c->has_scene) return fail(c, ANA_ERR_STATE, "ana_diff_counts: no scene uploaded");

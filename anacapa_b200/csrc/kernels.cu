@@ -1330,6 +1330,50 @@ void launch_trace_batch(const DevScene& S, uint32_t scene, const float* rays, co
 }
 
 // ---------------------------------------------------------------------------
+// BSDF queries (ana_bsdf_batch): IMaterial::evaluate and IMaterial::sample of
+// one material over a batch of shading frames, through the same device
+// functions the shade kernel calls (make_ctx, mat_eval, mat_sample).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_bsdf_query(DevMaterial m, const ana_bsdf_query* q, uint32_t n,
+                                                    ana_bsdf_result* out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const ana_bsdf_query Q = q[i];
+    SurfInt si;
+    si.p = f3(0.f, 0.f, 0.f);
+    si.n = f3(Q.n[0], Q.n[1], Q.n[2]);
+    si.ng = si.n;
+    si.dpdu = f3(Q.t[0], Q.t[1], Q.t[2]);
+    si.color = f3(Q.color[0], Q.color[1], Q.color[2]);
+    si.slot = 0;
+    si.is_curve = Q.is_curve != 0;
+    const float3 wo = f3(Q.wo[0], Q.wo[1], Q.wo[2]);
+    const ShadeCtx c = make_ctx(si, -wo);
+    const BsdfEval e = mat_eval(m, c, wo, f3(Q.wi[0], Q.wi[1], Q.wi[2]));
+    const BsdfSample b = mat_sample(m, c, wo, Q.u[0], Q.u[1], Q.u_comp);
+    ana_bsdf_result r;
+    r.f[0] = e.f.x;
+    r.f[1] = e.f.y;
+    r.f[2] = e.f.z;
+    r.pdf = e.pdf;
+    const bool ok = b.valid();
+    r.sample_f[0] = ok ? b.f.x : 0.f;
+    r.sample_f[1] = ok ? b.f.y : 0.f;
+    r.sample_f[2] = ok ? b.f.z : 0.f;
+    r.sample_pdf = ok ? b.pdf : 0.f;
+    r.sample_wi[0] = ok ? b.wi.x : 0.f;
+    r.sample_wi[1] = ok ? b.wi.y : 0.f;
+    r.sample_wi[2] = ok ? b.wi.z : 0.f;
+    r.sample_flags = ok ? b.flags : 0u;
+    out[i] = r;
+}
+
+void launch_bsdf_query(const DevMaterial& m, const ana_bsdf_query* q, uint32_t n, ana_bsdf_result* out,
+                       cudaStream_t s) {
+    k_bsdf_query<<<blocks_for(n, 128, 1 << 20), 128, 0, s>>>(m, q, n, out);
+}
+
+// ---------------------------------------------------------------------------
 // Scratch of the allocation-free trace entry point: module global memory,
 // created with the module on each device (about 4 MiB), so the entry point
 // never asks the allocator for memory. One copy per device, shared by every

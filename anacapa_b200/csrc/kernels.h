@@ -130,6 +130,10 @@ void launch_adj_direct(const Params& p, const LaunchCfg& c, cudaStream_t s);
 void launch_trace_batch(const DevScene& S, uint32_t scene, const float* rays, const float* times, size_t n,
                         ana_hit* out, int occlusion, uint32_t* fetch, uint32_t* err, int persistent, cudaStream_t s);
 
+// IMaterial::evaluate / sample of one material over n queries (ana_bsdf_batch).
+void launch_bsdf_query(const DevMaterial& m, const ana_bsdf_query* q, uint32_t n, ana_bsdf_result* out,
+                       cudaStream_t s);
+
 // Fixed device scratch of the allocation-free trace entry point: a 256-byte
 // header (the scene record at 0, the error word at kNoAllocErrOffset and the
 // persistent schedule's work counter 4 bytes after it), then room for

@@ -519,6 +519,85 @@ void derive_standard(DevMaterial& o) {
     o.is_delta = (smoothGlass || (r < 0.001f && (o.metal > 0.999f || o.spec > 0.f))) ? 1 : 0;
 }
 
+// One material in the device layout, with the derived constants each
+// reference class precomputes in its constructor (Lambertian.h:29-99,
+// StandardSurface.h:152-218, MarschnerHair.h:200-216). Returns nullptr, or
+// the reason the material is rejected.
+const char* make_material(const ana_material& m, DevMaterial& o) {
+    std::memset(&o, 0, sizeof(o));
+    o.type = m.type;
+    o.opacity = 1.f;  // IMaterial::evalOpacity's default
+    switch (m.type) {
+        case ANA_MAT_LAMBERT:
+        case ANA_MAT_EMISSIVE:  // Lambertian.h:29-99
+            o.flags = 1u | 16u;
+            o.albedo = make_float3(m.albedo[0], m.albedo[1], m.albedo[2]);
+            if (m.type == ANA_MAT_EMISSIVE)
+                o.emission = make_float3(m.emission[0], m.emission[1], m.emission[2]);
+            break;
+        case ANA_MAT_STANDARD: {  // StandardSurface.h:152-218
+            o.albedo = make_float3(m.base_color[0], m.base_color[1], m.base_color[2]);
+            o.base = m.base;
+            o.metal = m.metalness;
+            o.rough = m.roughness;
+            o.spec = m.specular;
+            o.spec_color = make_float3(m.specular_color[0], m.specular_color[1], m.specular_color[2]);
+            o.coat = m.coat;
+            o.transmission = m.transmission;
+            o.ior = m.specular_ior;
+            derive_standard(o);
+            float ca = std::max(1e-4f, m.coat_roughness * m.coat_roughness);
+            o.coat_alpha2 = ca * ca;
+            float r = (1.f - m.specular_ior) / (1.f + m.specular_ior);
+            o.f0_dielectric = r * r;
+            float rc = (1.f - 1.5f) / (1.f + 1.5f);
+            o.coat_f0 = rc * rc;
+            if (m.emission_weight > 0.f)
+                o.emission = make_float3(m.emission_color[0] * m.emission_weight,
+                                         m.emission_color[1] * m.emission_weight,
+                                         m.emission_color[2] * m.emission_weight);
+            // evalOpacity and transmittanceColor (StandardSurface.h:197-218)
+            o.opacity = m.alpha_mask ? m.opacity : 1.f;
+            if (m.alpha_mask) {
+                const float t = 1.f - m.opacity;
+                if (t > 0.f) o.tint = make_float3(t, t, t);
+            } else if (m.transmission >= 0.001f && !(m.metalness > 0.001f)) {
+                // Fresnel reflectance at normal incidence, fresnelDielectric(1, IOR)
+                const float eta = m.specular_ior;
+                const float Rs = (1.f - eta * 1.f) / (1.f + eta * 1.f);
+                const float Rp = (eta * 1.f - 1.f) / (eta * 1.f + 1.f);
+                const float Fr = 0.5f * (Rs * Rs + Rp * Rp);
+                const float k = m.transmission * (1.f - Fr);
+                o.tint = make_float3(m.base_color[0] * k, m.base_color[1] * k, m.base_color[2] * k);
+            }
+            break;
+        }
+        case ANA_MAT_HAIR: {  // MarschnerHair.h:200-216
+            o.hair_mode = m.hair_mode;
+            if (m.hair_mode > ANA_HAIR_MARSCHNER) return "unknown hair mode";
+            o.eta = m.eta;
+            o.sigma_a = make_float3(m.sigma_a[0], m.sigma_a[1], m.sigma_a[2]);
+            o.beta_m = m.beta_m;
+            float bm = std::clamp(m.beta_m, 1e-3f, 1.f);
+            float v0 = 0.726f * bm + 0.812f * bm * bm + 3.7f * std::pow(bm, 20.f);
+            o.v[0] = v0 * v0;
+            o.v[1] = o.v[0] * 0.25f;
+            o.v[2] = o.v[0] * 4.0f;
+            float bn = std::clamp(m.beta_n, 1e-3f, 1.f);
+            o.s = 0.626657069f * (0.265f * bn + 1.194f * bn * bn + 5.372f * std::pow(bn, 22.f));
+            const float kPi = 3.14159265358979323846f;
+            o.alpha_shift[0] = -m.alpha_deg * kPi / 180.f;
+            o.alpha_shift[1] = m.alpha_deg * kPi / 180.f * 0.5f;
+            o.alpha_shift[2] = -m.alpha_deg * kPi / 180.f * 1.5f;
+            o.flags = 2u | 16u | 8u;
+            break;
+        }
+        default:
+            return "unknown material type";
+    }
+    return nullptr;
+}
+
 int prepare_scene(const ana_scene_desc& d, Prepared& P, std::string& err, bool tris_on_device) {
     auto bad = [&](const char* m) {
         err = m;
@@ -728,79 +807,8 @@ int prepare_scene(const ana_scene_desc& d, Prepared& P, std::string& err, bool t
     // ---- materials -----------------------------------------------------------
     P.materials.resize(d.num_materials);
     for (uint32_t i = 0; i < d.num_materials; ++i) {
-        const ana_material& m = d.materials[i];
-        DevMaterial& o = P.materials[i];
-        std::memset(&o, 0, sizeof(o));
-        o.type = m.type;
-        o.opacity = 1.f;  // IMaterial::evalOpacity's default
-        switch (m.type) {
-            case ANA_MAT_LAMBERT:
-            case ANA_MAT_EMISSIVE:  // Lambertian.h:29-99
-                o.flags = 1u | 16u;
-                o.albedo = make_float3(m.albedo[0], m.albedo[1], m.albedo[2]);
-                if (m.type == ANA_MAT_EMISSIVE)
-                    o.emission = make_float3(m.emission[0], m.emission[1], m.emission[2]);
-                break;
-            case ANA_MAT_STANDARD: {  // StandardSurface.h:152-218
-                o.albedo = make_float3(m.base_color[0], m.base_color[1], m.base_color[2]);
-                o.base = m.base;
-                o.metal = m.metalness;
-                o.rough = m.roughness;
-                o.spec = m.specular;
-                o.spec_color = make_float3(m.specular_color[0], m.specular_color[1], m.specular_color[2]);
-                o.coat = m.coat;
-                o.transmission = m.transmission;
-                o.ior = m.specular_ior;
-                derive_standard(o);
-                float ca = std::max(1e-4f, m.coat_roughness * m.coat_roughness);
-                o.coat_alpha2 = ca * ca;
-                float r = (1.f - m.specular_ior) / (1.f + m.specular_ior);
-                o.f0_dielectric = r * r;
-                float rc = (1.f - 1.5f) / (1.f + 1.5f);
-                o.coat_f0 = rc * rc;
-                if (m.emission_weight > 0.f)
-                    o.emission = make_float3(m.emission_color[0] * m.emission_weight,
-                                             m.emission_color[1] * m.emission_weight,
-                                             m.emission_color[2] * m.emission_weight);
-                // evalOpacity and transmittanceColor (StandardSurface.h:197-218)
-                o.opacity = m.alpha_mask ? m.opacity : 1.f;
-                if (m.alpha_mask) {
-                    const float t = 1.f - m.opacity;
-                    if (t > 0.f) o.tint = make_float3(t, t, t);
-                } else if (m.transmission >= 0.001f && !(m.metalness > 0.001f)) {
-                    // Fresnel reflectance at normal incidence, fresnelDielectric(1, IOR)
-                    const float eta = m.specular_ior;
-                    const float Rs = (1.f - eta * 1.f) / (1.f + eta * 1.f);
-                    const float Rp = (eta * 1.f - 1.f) / (eta * 1.f + 1.f);
-                    const float Fr = 0.5f * (Rs * Rs + Rp * Rp);
-                    const float k = m.transmission * (1.f - Fr);
-                    o.tint = make_float3(m.base_color[0] * k, m.base_color[1] * k, m.base_color[2] * k);
-                }
-                break;
-            }
-            case ANA_MAT_HAIR: {  // MarschnerHair.h:200-216
-                o.hair_mode = m.hair_mode;
-                if (m.hair_mode > ANA_HAIR_MARSCHNER) return bad("unknown hair mode");
-                o.eta = m.eta;
-                o.sigma_a = make_float3(m.sigma_a[0], m.sigma_a[1], m.sigma_a[2]);
-                o.beta_m = m.beta_m;
-                float bm = std::clamp(m.beta_m, 1e-3f, 1.f);
-                float v0 = 0.726f * bm + 0.812f * bm * bm + 3.7f * std::pow(bm, 20.f);
-                o.v[0] = v0 * v0;
-                o.v[1] = o.v[0] * 0.25f;
-                o.v[2] = o.v[0] * 4.0f;
-                float bn = std::clamp(m.beta_n, 1e-3f, 1.f);
-                o.s = 0.626657069f * (0.265f * bn + 1.194f * bn * bn + 5.372f * std::pow(bn, 22.f));
-                const float kPi = 3.14159265358979323846f;
-                o.alpha_shift[0] = -m.alpha_deg * kPi / 180.f;
-                o.alpha_shift[1] = m.alpha_deg * kPi / 180.f * 0.5f;
-                o.alpha_shift[2] = -m.alpha_deg * kPi / 180.f * 1.5f;
-                o.flags = 2u | 16u | 8u;
-                break;
-            }
-            default:
-                return bad("unknown material type");
-        }
+        const char* why = make_material(d.materials[i], P.materials[i]);
+        if (why) return bad(why);
     }
     P.slot_material.assign(d.slot_material, d.slot_material + d.num_slots);
     P.has_emitters = false;

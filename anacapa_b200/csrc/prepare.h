@@ -53,6 +53,10 @@ struct Prepared {
 // (StandardSurface.h:152-181, 384).
 void derive_standard(DevMaterial& m);
 
+// One ana_material in the device layout with its derived constants; returns
+// nullptr, or the reason it is rejected.
+const char* make_material(const ana_material& m, DevMaterial& o);
+
 // Returns ANA_OK or an error code with a message in err. With
 // tris_on_device the triangle sections are left to the device build (the
 // mesh offsets are still validated here).

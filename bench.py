@@ -62,6 +62,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0,
                     help="target CPU work of the reference sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--config-cpu-seconds", type=float, default=5.0,
+                    help="target CPU work of each other configuration's reference sample")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--chunk-paths", type=int, default=1 << 27,
                     help="paths in flight per wavefront chunk; the default is the autotuner's best "
@@ -222,49 +224,99 @@ def extend_traffic_per_ray():
     return None
 
 
+FP64_WINDOWS = os.path.join(ROOT, "tests", "golden", "config_windows_fp64.npz")
+_fp64 = None
+
+
+def rmse_vs_fp64(name, img):
+    """RMSE of a rendered image (H, W, 3) against the FP64 converged windows
+    of its frame (tests/golden/config_windows_fp64.npz, made by the CPU
+    restatement in double precision at 4096 spp), window by window, beside the
+    reference CPU integrator's RMSE at the same spp on the same window."""
+    global _fp64
+    if _fp64 is None:
+        _fp64 = dict(np.load(FP64_WINDOWS)) if os.path.exists(FP64_WINDOWS) else {}
+    out = {"windows": [], "rmse": [], "reference_cpu_rmse": [], "fp64_spp": int(_fp64.get("conv_spp", 0))}
+    k = 0
+    while f"{name}_{k}_image" in _fp64:
+        x0, y0, x1, y1 = (int(v) for v in _fp64[f"{name}_{k}_rect"])
+        conv = _fp64[f"{name}_{k}_image"].astype(np.float64)
+        err = float(np.sqrt(np.mean((img[y0:y1, x0:x1].astype(np.float64) - conv) ** 2)))
+        out["windows"].append([x0, y0, x1, y1])
+        out["rmse"].append(err)
+        out["reference_cpu_rmse"].append(float(_fp64[f"{name}_{k}_ref_rmse"]))
+        k += 1
+    return out if k else None
+
+
 # ---------------------------------------------------------------------------
-def cpu_reference_sample(scene, target_s, steps=1, warmup=0):
+def row_bands(H, n_bands, rows):
+    """n_bands bands of `rows` rows whose centres are spread evenly over the
+    frame's height (band b centred on row (b + 1/2) H / n_bands)."""
+    out = []
+    for b in range(n_bands):
+        c = int((b + 0.5) * H / n_bands)
+        y0 = min(max(0, c - rows // 2), H - rows)
+        out.append((y0, y0 + rows))
+    return out
+
+
+def cpu_reference_sample(scene, target_s, steps=1, warmup=0, n_bands=16):
     """Time the reference's CPU PathIntegrator (oracle/_ref, flags of record)
-    through its own ThreadPool on a band of image rows at the full spp. Returns
-    (samples/s per step list, description, cores)."""
+    through its own ThreadPool on a stratified sample of the frame: n_bands
+    full-width bands of rows spread evenly over its height, all their 64x64
+    tiles in one pool dispatch, at the frame's spp and depth. The band height
+    is sized from a calibration pass (one row per band) so that one step takes
+    about target_s. Returns (samples/s per step, seconds per step, paths per
+    step, description, cores); frames small enough for target_s run whole."""
     from oracle import refbind as R
     if not R.available("record"):
         R.build()
     rs = R.RefScene(scene, variant="record")
     W, H = scene.width, scene.height
     cores = os.cpu_count() or 1
-    # calibrate on 2 rows in the middle of the frame
-    y0 = H // 2
-    _, _, secs = rs.render(rect=(0, y0, W, y0 + 2))
-    per_row = max(secs / 2.0, 1e-6)
-    rows = int(max(1, min(H - y0, target_s / per_row)))
+    n_bands = min(n_bands, H)
+    _, _, secs = rs.render_rows(row_bands(H, n_bands, 1))
+    per_row = max(secs / n_bands, 1e-6)
+    rows = int(max(1, min(H // n_bands, round(target_s / (per_row * n_bands)))))
+    bands = [(0, H)] if rows * n_bands >= H else row_bands(H, n_bands, rows)
+    nrows = sum(b - a for a, b in bands)
     for _ in range(warmup):
-        rs.render(rect=(0, y0, W, y0 + rows))
-    vals = []
+        rs.render_rows(bands)
+    vals, times = [], []
     for _ in range(steps):
-        _, _, secs = rs.render(rect=(0, y0, W, y0 + rows))
-        vals.append(W * rows * scene.spp / secs)
-    desc = (f"rows {y0}..{y0 + rows - 1} of the {W}x{H} frame at {scene.spp} spp "
-            f"({W * rows * scene.spp} paths), reference PathIntegrator via its ThreadPool, "
-            f"64x64 tiles, non-adaptive")
-    return vals, desc, cores
+        _, _, secs = rs.render_rows(bands)
+        vals.append(W * nrows * scene.spp / secs)
+        times.append(secs)
+    paths = W * nrows * scene.spp
+    if bands == [(0, H)]:
+        what = f"the whole {W}x{H} frame"
+    else:
+        what = (f"{len(bands)} bands of {rows} rows spread evenly over the {W}x{H} frame "
+                f"(rows {bands[0][0]}..{bands[0][1] - 1}, ..., {bands[-1][0]}..{bands[-1][1] - 1}; "
+                f"{nrows / H:.1%} of its pixels)")
+    desc = (f"{what} at {scene.spp} spp, depth {scene.max_depth} ({paths} paths per step), reference "
+            f"PathIntegrator via its ThreadPool, 64x64 tiles in one dispatch, non-adaptive")
+    return vals, times, paths, desc, cores
 
 
 def run_reference(a):
     ws, rank, local, pg = dist_setup(a)
     if rank != 0:
         return 0
-    from anacapa_b200 import scenes as S
     scene = make_scene(a)
-    vals, desc, cores = cpu_reference_sample(scene, a.cpu_seconds, steps=a.steps, warmup=a.warmup)
+    # each step a bounded sample, so warm-up and timed steps end within a few minutes
+    per_step = min(a.cpu_seconds, max(2.0, 150.0 / max(1, a.steps + a.warmup)))
+    vals, times, paths, desc, cores = cpu_reference_sample(scene, per_step, steps=a.steps, warmup=a.warmup)
     v = statistics.mean(vals)
-    paths = scene.num_paths
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus,
-        "steps": a.steps, "warmup": a.warmup, "ms_per_step": paths / v * 1e3,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": statistics.mean(times) * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded numpy scene generator)",
         "config": workload_config(a, scene),
+        "sample_paths_per_step": paths,
+        "frame_ms_at_this_rate": scene.num_paths / v * 1e3,
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "reference",
                          "sample": desc},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -273,28 +325,49 @@ def run_reference(a):
     return 0
 
 
+def batched_rmse(images):
+    """Per-variant RMSE of the 64 batched frames against their FP64 centre
+    windows (tests/golden/config_windows_fp64.npz, key `batched_*`)."""
+    global _fp64
+    if _fp64 is None:
+        rmse_vs_fp64("none", None)
+    if "batched_image" not in _fp64:
+        return None
+    out = []
+    for k, img in enumerate(images):
+        x0, y0, x1, y1 = (int(v) for v in _fp64["batched_rect"][k])
+        conv = _fp64["batched_image"][k].astype(np.float64)
+        out.append(float(np.sqrt(np.mean((img[y0:y1, x0:x1].astype(np.float64) - conv) ** 2))))
+    return out
+
+
 def bench_batched(local, reps=3):
     """The batched workload: 64 Cornell variants (resolutions 64^2..512^2,
     4..64 spp, depth 4..16) as one batch render replayed from a CUDA graph,
-    against the same 64 frames rendered one scene per launch sequence. Both
-    forms run the same per-variant estimator (same samples), so their images
-    and RMSE against the FP64 oracle are identical. Device time (CUDA events)
-    per form; launch configuration from the autotuner's best point (8M-path
-    chunks, 256-thread stage blocks, persistent traversal, leaves of 2)."""
+    against the same 64 frames rendered one scene per launch sequence. Device
+    time (CUDA events) per form; launch configuration from the committed
+    autotuner table (profiles/autotune_batched.json) when present. Each
+    form's per-variant RMSE against the variant's FP64 centre window is
+    measured on its own images."""
     from anacapa_b200 import api
+    from anacapa_b200 import autotune
     from anacapa_b200 import scenes as S
+    tuned = autotune.tuned_point("batched")
     scenes = S.batched_variants(64, seed=0)
-    preps = [api.Prepared(sc, max_leaf_tris=2) for sc in scenes]
+    preps = [api.Prepared(sc, max_leaf_tris=tuned["leaf"]) for sc in scenes]
     descs = [(sc.width, sc.height, sc.spp, sc.max_depth) for sc in scenes]
     paths = sum(sc.num_paths for sc in scenes)
-    r = api.Renderer(device=local, chunk_paths=8 << 20, block_size=256)
-    plain = []
+    r = api.Renderer(device=local, chunk_paths=tuned["chunk"], block_size=tuned["block"],
+                     traversal=tuned["traversal"])
+    plain, plain_img = [], []
     for it in range(reps + 1):
         ms = 0.0
         for pr, d in zip(preps, descs):
             r.upload(pr)
             r.render(*d)
             ms += r.stats().render_ms
+            if it == reps:
+                plain_img.append(r.image(d[0], d[1]))
         if it:
             plain.append(ms)
     batch = api.Batch(preps)
@@ -304,16 +377,29 @@ def bench_batched(local, reps=3):
         r.render_batch(descs, graph=True)
         if it:
             batched.append(r.stats().render_ms)
+    batch_img = []
+    for k, d in enumerate(descs):
+        f = r.batch_film(k, d[0], d[1])
+        batch_img.append(f[..., :3] / np.maximum(f[..., 3:4], 1e-30))
     r.close()
     pm, bm = statistics.median(plain), statistics.median(batched)
+    rp, rb = batched_rmse(plain_img), batched_rmse(batch_img)
+    rmse = None
+    if rp is not None:
+        rmse = {"fp64_windows": "32x32 centre window per variant, FP64 restatement at 4096 spp",
+                "plain_mean": statistics.mean(rp), "batched_mean": statistics.mean(rb),
+                "plain_max": max(rp), "batched_max": max(rb),
+                "max_abs_difference": max(abs(a - b) for a, b in zip(rp, rb)),
+                "reference_cpu_mean": float(np.mean(_fp64["batched_ref_rmse"]))}
     return {"workload": f"64 Cornell variants, {paths:,} paths", "paths": paths,
             "plain_ms": pm, "batched_graph_ms": bm,
             "plain_samples_per_s": paths / (pm / 1e3), "batched_samples_per_s": paths / (bm / 1e3),
-            "speedup": pm / bm, "equal_rmse": "identical per-variant estimator and samples"}
+            "speedup": pm / bm, "target_speedup": 20.0, "tuned_point": tuned, "rmse_vs_fp64": rmse}
 
 
-def bench_frame(local, scene, reps=3, chunk_paths=0):
-    """Device time of one frame of `scene` (median of reps after one warm-up)."""
+def bench_frame(local, scene, reps=3, chunk_paths=0, fp64_name=None):
+    """Device time of one frame of `scene` (median of reps after one warm-up),
+    and its RMSE against the FP64 windows of `fp64_name`."""
     from anacapa_b200 import api
     r = api.Renderer(device=local, chunk_paths=chunk_paths)
     r.upload(api.Prepared(scene))
@@ -323,39 +409,75 @@ def bench_frame(local, scene, reps=3, chunk_paths=0):
         if it:
             times.append(r.stats().render_ms)
     st = r.stats()
+    img = r.image(scene.width, scene.height) if fp64_name else None
     r.close()
     ms = statistics.median(times)
     rays = st.extend_rays + st.shadow_rays + st.mis_rays
-    return {"paths": scene.num_paths, "ms": ms, "samples_per_s": scene.num_paths / (ms / 1e3),
-            "rays_per_s": rays / (ms / 1e3)}
+    out = {"paths": scene.num_paths, "ms": ms, "samples_per_s": scene.num_paths / (ms / 1e3),
+           "rays_per_s": rays / (ms / 1e3)}
+    if fp64_name:
+        out["rmse_vs_fp64"] = rmse_vs_fp64(fp64_name, img)
+    return out
 
 
-def bench_configs(local):
+def config_cpu(scene, seconds, port=False):
+    """CPU baseline beside a configuration: the reference PathIntegrator on a
+    stratified row sample (cpu_reference_sample), or for a mode the reference
+    does not execute (port=True: Marschner hair) this repository's CPU
+    restatement in float on a centre band of rows, one thread per core."""
+    try:
+        if not port:
+            vals, _, _, desc, cores = cpu_reference_sample(scene, seconds)
+            return {"value": vals[0], "unit": UNIT, "cores": cores, "kind": "reference", "sample": desc}
+        from oracle import restatebind as P
+        W, H = scene.width, scene.height
+        po = P.PoScene(scene, 32)
+        t0 = time.perf_counter()
+        po.render(rect=(0, H // 2, W, H // 2 + 1))
+        per_row = max(time.perf_counter() - t0, 1e-6)
+        rows = int(max(1, min(H, seconds / per_row)))
+        y0 = max(0, H // 2 - rows // 2)
+        t0 = time.perf_counter()
+        po.render(rect=(0, y0, W, y0 + rows))
+        secs = time.perf_counter() - t0
+        return {"value": W * rows * scene.spp / secs, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                "sample": f"rows {y0}..{y0 + rows - 1} of the {W}x{H} frame at {scene.spp} spp: the CPU "
+                          "restatement (float) in Marschner mode, which the reference does not execute"}
+    except Exception as e:  # a reported baseline, never required
+        return {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port" if port else "reference",
+                "sample": f"failed: {e}"}
+
+
+def bench_configs(local, cpu_s=0.0):
     """The other single-frame configurations: Cornell 256x256x16 (depth 8),
-    hair 200k strands 1280x720x32 (depth 10), and the throughput frame with
-    938 spheres (about 1.2M triangles, the triangle count the throughput
-    configuration states; its generator gives 5.24M with 4096 spheres)."""
+    hair 200k strands 1280x720x32 (depth 10) in Kajiya-Kay mode (what the
+    reference executes) and in Marschner mode, the throughput frame with 938
+    spheres (about 1.2M triangles, the triangle count the throughput
+    configuration states; its generator gives 5.24M with 4096 spheres), and
+    the glass / alpha-mask and motion-blur scenes. With cpu_s > 0 each carries
+    a CPU baseline of about cpu_s seconds."""
     from anacapa_b200 import scenes as S
     out = {}
-    cornell = S.cornell(256, 256, 16, 8)
-    out["cornell_256x256x16"] = {"workload": "Cornell box, 36 triangles, Lambert, area light; depth 8",
-                                 **bench_frame(local, cornell)}
-    hair = S.hair(1280, 720, 32, 10)
-    out["hair_1280x720x32"] = {"workload": f"hair: 200,000 strands, {hair.num_segments:,} cubic segments, "
-                                           "Kajiya-Kay as the reference executes it, one area light; depth 10",
-                               **bench_frame(local, hair, chunk_paths=1 << 25)}
-    thr = S.throughput(n_spheres=938)
-    out["throughput_938_spheres"] = {"workload": f"throughput scene with 938 spheres: {thr.num_triangles:,} "
-                                                 "triangles, 1920x1080x64, depth 12",
-                                     **bench_frame(local, thr, chunk_paths=1 << 27)}
-    glass = S.glass(1280, 720, 16, 8)
-    out["glass_1280x720x16"] = {"workload": "glass: smooth and rough dielectric spheres and panes, "
-                                            "alpha-masked cards, directional + area light; depth 8",
-                                **bench_frame(local, glass, chunk_paths=1 << 25)}
-    mo = S.motion(1280, 720, 16, 6)
-    out["motion_1280x720x16"] = {"workload": "motion blur: object-space meshes with 2-3 motion keys, "
-                                             "shutter [0, 1]; depth 6",
-                                 **bench_frame(local, mo, chunk_paths=1 << 25)}
+    cases = [
+        ("cornell_256x256x16", "Cornell box, 36 triangles, Lambert, area light; depth 8",
+         S.cornell(256, 256, 16, 8), 0, "cornell", False),
+        ("hair_1280x720x32", None, S.hair(1280, 720, 32, 10), 1 << 25, "hair", False),
+        ("hair_marschner_1280x720x32", None, S.hair(1280, 720, 32, 10, hair_mode=1), 1 << 25, None, True),
+        ("throughput_938_spheres", None, S.throughput(n_spheres=938), 1 << 27, None, False),
+        ("glass_1280x720x16", "glass: smooth and rough dielectric spheres and panes, alpha-masked cards, "
+         "directional + area light; depth 8", S.glass(1280, 720, 16, 8), 1 << 25, None, False),
+        ("motion_1280x720x16", "motion blur: object-space meshes with 2-3 motion keys, shutter [0, 1]; depth 6",
+         S.motion(1280, 720, 16, 6), 1 << 25, None, False),
+    ]
+    for key, what, sc, chunk, fp64, port in cases:
+        if key.startswith("hair"):
+            mode = "Marschner R/TT/TRT lobes" if port else "Kajiya-Kay as the reference executes it"
+            what = f"hair: 200,000 strands, {sc.num_segments:,} cubic segments, {mode}, one area light; depth 10"
+        elif key.startswith("throughput"):
+            what = f"throughput scene with 938 spheres: {sc.num_triangles:,} triangles, 1920x1080x64, depth 12"
+        out[key] = {"workload": what, **bench_frame(local, sc, chunk_paths=chunk, fp64_name=fp64)}
+        if cpu_s > 0:
+            out[key]["cpu_baseline"] = config_cpu(sc, cpu_s, port=port)
     return out
 
 
@@ -419,16 +541,35 @@ def bench_adjoint(local, reps=3):
     for it in range(reps + 1):
         img = r.forward(W, H, spp, depth)
         f = r.stats().render_ms
-        r.backward(2.0 * (img - target) / img.size)
+        grad = r.backward(2.0 * (img - target) / img.size)
         b = r.stats().render_ms
         if it:
             fwd.append(f)
             bwd.append(b)
+    nm, nl = r.diff_counts()
     r.close()
     fm, bm = statistics.median(fwd), statistics.median(bwd)
-    return {"workload": "differentiable Cornell + icosphere 512x512x16, depth 8, L2 loss",
-            "forward_ms": fm, "backward_ms": bm, "adjoint_over_forward": bm / fm,
-            "forward_samples_per_s": W * H * spp / (fm / 1e3)}
+    out = {"workload": "differentiable Cornell + icosphere 512x512x16, depth 8, L2 loss",
+           "forward_ms": fm, "backward_ms": bm, "adjoint_over_forward": bm / fm, "target_ratio": 3.0,
+           "forward_samples_per_s": W * H * spp / (fm / 1e3),
+           "rmse_vs_fp64": rmse_vs_fp64("differentiable", img)}
+    # the gradient against the FP64 adjoint of the same frame and loss
+    # (tests/golden/adjoint_fp64_512.npz, made by tests/golden/make_adjoint_fp64.py)
+    gp = os.path.join(ROOT, "tests", "golden", "adjoint_fp64_512.npz")
+    if os.path.exists(gp):
+        ref = np.load(gp)["grad"]
+        g = np.zeros(8 * nm + 4 * nl)
+        for i in range(nm):
+            g[8 * i:8 * i + 3] = grad["albedo"][i]
+            g[8 * i + 3] = grad["roughness"][i]
+            g[8 * i + 4:8 * i + 7] = grad["emission"][i]
+        for j in range(nl):
+            g[8 * nm + 4 * j:8 * nm + 4 * j + 3] = grad["light_le"][j]
+        big = np.abs(ref) > 1e-2 * np.abs(ref).max()
+        out["grad_vs_fp64"] = {"rel_err_norm": float(np.linalg.norm(g - ref) / np.linalg.norm(ref)),
+                               "max_rel_err_large_entries": float((np.abs(g - ref)[big] / np.abs(ref)[big]).max()),
+                               "large_entries": int(big.sum()), "target": 1e-3}
+    return out
 
 
 def run_ours(a):
@@ -482,6 +623,10 @@ def run_ours(a):
     achieved = (alg_bytes / ext_launches) / ((ext_ms / ext_launches) / 1e3) / 1e9 if ext_ms > 0 else None
     tpr = extend_traffic_per_ray() if a.scene == "throughput" else None  # measured on that scene
     traffic = (tpr * work.extend_rays / ext_launches) if tpr else None
+    # the last timed frame against the FP64 windows of the configuration frame
+    rmse = None
+    if rank == 0 and a.scene == "throughput" and (W, H, spp, a.n_spheres) == (1920, 1080, 64, 4096):
+        rmse = rmse_vs_fp64("throughput", r.image(W, H))
     # end to end through the C ABI with host buffers
     e2e = None
     if not a.no_e2e:
@@ -500,7 +645,8 @@ def run_ours(a):
     if not a.no_extras:  # the metric's other two parts, outside the timed region
         extra["batched"] = bench_batched(local)
         extra["adjoint"] = bench_adjoint(local)
-        extra["other_configs"] = bench_configs(local)
+        extra["other_configs"] = bench_configs(local, cpu_s=0.0 if (a.no_cpu_baseline or ws > 1 or rank)
+                                                else a.config_cpu_seconds)
         setup = bench_scene_setup(local, scene, t_prep)
         setup["same_bytes"] = setup.pop("digest") == prep.digest
         extra["scene_setup"] = setup
@@ -508,7 +654,7 @@ def run_ours(a):
     cpu = None
     if rank == 0 and ws == 1 and not a.no_cpu_baseline:
         try:
-            vals, desc, cores = cpu_reference_sample(scene, a.cpu_seconds)
+            vals, _, _, desc, cores = cpu_reference_sample(scene, a.cpu_seconds)
             cpu = {"value": vals[0], "unit": UNIT, "cores": cores, "kind": "reference", "sample": desc}
         except Exception as e:  # the baseline is reported, never required
             cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
@@ -530,6 +676,7 @@ def run_ours(a):
                          "alg_bytes_per_launch": alg_bytes / ext_launches,
                          "launches_per_step": ext_launches},
             "gpu_launches": launches,
+            "rmse_vs_fp64": rmse,
             "e2e": e2e,
             "cpu_baseline": cpu,
             "clocks": ck,

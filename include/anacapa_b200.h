@@ -408,6 +408,40 @@ int ana_trace_batch_timed(ana_ctx* ctx, const float* rays, const float* times, s
 #define ANA_TRACE_NOALLOC_MAX_RAYS 65536
 int ana_trace_batch_noalloc(ana_ctx* ctx, const float* rays, size_t n, ana_hit* out, int occlusion_only);
 
+/* ---- BSDF queries ------------------------------------------------------------
+ * IMaterial::evaluate and IMaterial::sample (include/anacapa/shading/IMaterial.h:
+ * 53-80) of one material, run on the device for a batch of shading frames:
+ * the device code the renderer shades with, without a scene (material
+ * previews, BSDF plots, checks of the lobes). The frame is built as
+ * ShadingContext does (include/anacapa/shading/ShadingContext.h:28-50) from a
+ * surface interaction with shading and geometric normal n, fiber tangent t
+ * (is_curve != 0: hair) and per-strand colour, hit by a ray travelling along
+ * -wo. For hair materials hair_mode selects the Kajiya-Kay lobe the reference
+ * executes (MarschnerHair.h:240, 267-282) or the R/TT/TRT lobes it defines
+ * (MarschnerHair.h:242-257, 284-375). */
+typedef struct ana_bsdf_query {
+    float n[3];
+    float t[3];
+    float color[3];
+    float wo[3];
+    float wi[3];       /* direction evaluate() is asked about                     */
+    float u[2];        /* sample(): the 2-D sample and the component sample       */
+    float u_comp;
+    uint32_t is_curve;
+} ana_bsdf_query;
+
+typedef struct ana_bsdf_result {
+    float f[3];        /* evaluate(): BSDFEval::f (no cosine) and pdf             */
+    float pdf;
+    float sample_f[3]; /* sample(): BSDFSample::f (times |cos theta_i|), pdf, wi  */
+    float sample_pdf;
+    float sample_wi[3];
+    uint32_t sample_flags; /* BSDFFlags of the sample (0 when it is invalid)      */
+} ana_bsdf_result;
+
+int ana_bsdf_batch(ana_ctx* ctx, const ana_material* material, const ana_bsdf_query* queries, size_t n,
+                   ana_bsdf_result* out);
+
 /* ---- tiles and adaptive sampling ------------------------------------------ */
 /* A tile of a frame (TileRequest, include/anacapa/integrator/IIntegrator.h):
  * pixels [x0, x0 + width) x [y0, y0 + height), sample indices

@@ -136,6 +136,160 @@ StandardSurfaceMaterial::Params ssParams(const float* p) {
     return q;
 }
 
+// ---------------------------------------------------------------------------
+// The Marschner R/TT/TRT code of MarschnerHairMaterial (MarschnerHair.h:242-257
+// in evaluate, 284-375 in sample, helpers and evalLobes/evalPdf at 430-556) is
+// unreachable through the public interface: evaluate and sample return the
+// Kajiya-Kay lobe first (MarschnerHair.h:240, 267-282), and the helpers are
+// private. An explicit instantiation may name private members ([temp.spec]),
+// so the templates below hand out pointers to them without editing the
+// reference's sources; the functions called are the reference's own code.
+// ---------------------------------------------------------------------------
+template <class Tag, typename Tag::type M>
+struct Expose {
+    friend typename Tag::type member(Tag) { return M; }
+};
+struct MhLobes {
+    using type = Spectrum (MarschnerHairMaterial::*)(float, float, float, float, float, float, Spectrum) const;
+    friend type member(MhLobes);
+};
+struct MhPdf {
+    using type = float (MarschnerHairMaterial::*)(float, float, float, float, float, float, Spectrum) const;
+    friend type member(MhPdf);
+};
+struct MhSigma {
+    using type = Spectrum (MarschnerHairMaterial::*)(const ShadingContext&) const;
+    friend type member(MhSigma);
+};
+struct MhLong {
+    using type = void (*)(Vec3f, Vec3f, float&, float&);
+    friend type member(MhLong);
+};
+struct MhPhiOf {
+    using type = float (*)(Vec3f, Vec3f, Vec3f, float, float);
+    friend type member(MhPhiOf);
+};
+struct MhImpact {
+    using type = float (*)(Vec3f, Vec3f, Vec3f, float);
+    friend type member(MhImpact);
+};
+struct MhParams {
+    using type = MarschnerHairMaterial::Params MarschnerHairMaterial::*;
+    friend type member(MhParams);
+};
+struct MhVar {
+    using type = float (MarschnerHairMaterial::*)[3];
+    friend type member(MhVar);
+};
+struct MhScale {
+    using type = float MarschnerHairMaterial::*;
+    friend type member(MhScale);
+};
+struct MhAlpha {
+    using type = float (MarschnerHairMaterial::*)[3];
+    friend type member(MhAlpha);
+};
+template struct Expose<MhLobes, &MarschnerHairMaterial::evalLobes>;
+template struct Expose<MhPdf, &MarschnerHairMaterial::evalPdf>;
+template struct Expose<MhSigma, &MarschnerHairMaterial::effectiveSigmaA>;
+template struct Expose<MhLong, &MarschnerHairMaterial::hairLongitudinal>;
+template struct Expose<MhPhiOf, &MarschnerHairMaterial::hairPhi>;
+template struct Expose<MhImpact, &MarschnerHairMaterial::hairImpactParam>;
+template struct Expose<MhParams, &MarschnerHairMaterial::m_p>;
+template struct Expose<MhVar, &MarschnerHairMaterial::m_v>;
+template struct Expose<MhScale, &MarschnerHairMaterial::m_s>;
+template struct Expose<MhAlpha, &MarschnerHairMaterial::m_alpha>;
+
+// MarschnerHairMaterial::evaluate's Marschner branch (MarschnerHair.h:242-257),
+// composed of the reference's private helpers. out: f[3], pdf, pdfRev.
+void mhEvaluate(const MarschnerHairMaterial& m, const ShadingContext& ctx, Vec3f wo, Vec3f wi, float* out) {
+    float sinThetaO, cosThetaO, sinThetaI, cosThetaI;
+    member(MhLong{})(wo, ctx.t, sinThetaO, cosThetaO);
+    member(MhLong{})(wi, ctx.t, sinThetaI, cosThetaI);
+    float phi = member(MhPhiOf{})(wo, wi, ctx.t, sinThetaO, sinThetaI);
+    float h = member(MhImpact{})(wo, ctx.t, ctx.n, sinThetaO);
+    Spectrum sigA = (m.*member(MhSigma{}))(ctx);
+    Spectrum f = (m.*member(MhLobes{}))(sinThetaO, cosThetaO, sinThetaI, cosThetaI, phi, h, sigA);
+    float pd = (m.*member(MhPdf{}))(sinThetaO, cosThetaO, sinThetaI, cosThetaI, phi, h, sigA);
+    out[0] = f.x;
+    out[1] = f.y;
+    out[2] = f.z;
+    out[3] = pd;
+    out[4] = (m.*member(MhPdf{}))(sinThetaI, cosThetaI, sinThetaO, cosThetaO, -phi, h, sigA);
+}
+
+// MarschnerHairMaterial::sample's Marschner branch (MarschnerHair.h:284-375).
+// The statements between the calls are restated here in the reference's order
+// (they sit inside sample() after its early return and cannot be called);
+// every function they call is the reference's own. out: f[3], wi[3], pdf,
+// valid (0/1).
+void mhSample(const MarschnerHairMaterial& m, const ShadingContext& ctx, Vec3f wo, Vec2f u, float uComp,
+              float* out) {
+    for (int k = 0; k < 8; ++k) out[k] = 0.f;
+    const MarschnerHairMaterial::Params& P = m.*member(MhParams{});
+    const float* V = m.*member(MhVar{});
+    const float S = m.*member(MhScale{});
+    const float* A = m.*member(MhAlpha{});
+    float sinThetaO, cosThetaO;
+    member(MhLong{})(wo, ctx.t, sinThetaO, cosThetaO);
+    float h = member(MhImpact{})(wo, ctx.t, ctx.n, sinThetaO);
+    Spectrum sigA = (m.*member(MhSigma{}))(ctx);
+    auto ap = mh_Ap(cosThetaO, P.eta, h, sigA);
+    float weights[3];
+    for (int p = 0; p < 3; ++p) weights[p] = luminance(ap[p]);
+    float total = weights[0] + weights[1] + weights[2];
+    if (total < 1e-8f) return;
+    float invTotal = 1.f / total;
+    float cdf[3];
+    cdf[0] = weights[0] * invTotal;
+    cdf[1] = cdf[0] + weights[1] * invTotal;
+    cdf[2] = 1.f;
+    int lobe = 0;
+    float uRemapped = uComp;
+    if (uComp < cdf[0]) {
+        uRemapped = uComp / cdf[0];
+    } else if (uComp < cdf[1]) {
+        lobe = 1;
+        uRemapped = (uComp - cdf[0]) / (cdf[1] - cdf[0]);
+    } else {
+        lobe = 2;
+        uRemapped = (uComp - cdf[1]) / (cdf[2] - cdf[1]);
+    }
+    float thetaO = std::asin(std::clamp(sinThetaO, -1.f + 1e-5f, 1.f - 1e-5f));
+    float z = mh_sampleGaussian(u.x, u.y);
+    float thetaI = thetaO + A[lobe] + z * std::sqrt(V[lobe]);
+    thetaI = std::clamp(thetaI, -kMH_Pi * 0.5f, kMH_Pi * 0.5f);
+    float sinThetaI = std::sin(thetaI);
+    float cosThetaI = std::cos(thetaI);
+    float sin2ThetaO = 1.f - cosThetaO * cosThetaO;
+    float etaP = std::sqrt(std::max(0.f, P.eta * P.eta - sin2ThetaO)) / cosThetaO;
+    float gammaO = std::asin(std::clamp(h, -1.f + 1e-5f, 1.f - 1e-5f));
+    float sinGammaT = std::clamp(h / (etaP > 1e-5f ? etaP : 1e-5f), -1.f + 1e-5f, 1.f - 1e-5f);
+    float gammaT = std::asin(sinGammaT);
+    float phiSampled = mh_sampleTrimmedLogistic(uRemapped, S) + mh_Phi(lobe, gammaO, gammaT);
+    Vec3f woPerp = safeNormalize(wo - ctx.t * sinThetaO);
+    if (woPerp.lengthSq() < 1e-8f) {
+        Vec3f dummy;
+        buildOrthonormalBasis(ctx.t, woPerp, dummy);
+    }
+    Vec3f ctPerp = cross(ctx.t, woPerp);
+    Vec3f wi = ctx.t * sinThetaI + woPerp * (cosThetaI * std::cos(phiSampled)) +
+               ctPerp * (cosThetaI * std::sin(phiSampled));
+    wi = safeNormalize(wi);
+    float sinThetaIa, cosThetaIa;
+    member(MhLong{})(wi, ctx.t, sinThetaIa, cosThetaIa);
+    float phiActual = member(MhPhiOf{})(wo, wi, ctx.t, sinThetaO, sinThetaIa);
+    Spectrum f = (m.*member(MhLobes{}))(sinThetaO, cosThetaO, sinThetaIa, cosThetaIa, phiActual, h, sigA);
+    float pd = (m.*member(MhPdf{}))(sinThetaO, cosThetaO, sinThetaIa, cosThetaIa, phiActual, h, sigA);
+    if (pd < 1e-8f) return;
+    float cosSurf = std::abs(dot(wi, ctx.n));
+    f = f * cosSurf;
+    put3(out, f);
+    put3(out + 3, wi);
+    out[6] = pd;
+    out[7] = 1.f;
+}
+
 SurfaceInteraction makeSI(const float* s) {
     // s: p[3], n[3], ng[3], dpdu[3], color[3], isCurve
     SurfaceInteraction si;
@@ -395,6 +549,52 @@ double ref_render(void* sp, uint32_t W, uint32_t H, uint32_t spp, uint32_t sampl
     return std::chrono::duration<double>(t1 - t0).count();
 }
 
+// ref_render over several full-width row bands [rows[2k], rows[2k+1]) of the
+// frame at once: the 64x64 tiles of every band (cut as RenderSession's
+// scheduleTiles cuts a frame, clipped to the band) go to one
+// ThreadPool::parallelFor, so the pool stays busy across bands. Returns the
+// seconds of the parallelFor.
+double ref_render_rows(void* sp, uint32_t W, uint32_t H, uint32_t spp, uint32_t sampleStart, uint32_t maxDepth,
+                       int nthreads, const uint32_t* rows, uint32_t nbands, float* out_rgbw, float* out_lumsq) {
+    auto* s = static_cast<RefScene*>(sp);
+    PathIntegrator integ(maxDepth);
+    integ.prepare(s->view);
+    HaltonSampler base(spp);
+    ThreadPool pool(uint32_t(nthreads > 0 ? nthreads : 0));
+    std::vector<TileRequest> tiles;
+    const uint32_t ts = 64;
+    for (uint32_t b = 0; b < nbands; ++b) {
+        const uint32_t y0 = std::min(rows[2 * b], H), y1 = std::min(rows[2 * b + 1], H);
+        for (uint32_t y = y0; y < y1; y += ts)
+            for (uint32_t x = 0; x < W; x += ts)
+                tiles.push_back({x, y, std::min(ts, W - x), std::min(ts, y1 - y), sampleStart, spp});
+    }
+    std::mutex mu;
+    auto t0 = std::chrono::steady_clock::now();
+    pool.parallelFor(uint32_t(tiles.size()), [&](uint32_t ti) {
+        const TileRequest& t = tiles[ti];
+        auto sampler = base.clone();
+        TileBuffer tb(t.x0, t.y0, t.width, t.height);
+        integ.renderTile(s->view, t, W, H, *sampler, tb);
+        std::lock_guard<std::mutex> lk(mu);
+        for (uint32_t ty = 0; ty < t.height; ++ty)
+            for (uint32_t tx = 0; tx < t.width; ++tx) {
+                size_t fi = size_t(t.y0 + ty) * W + (t.x0 + tx);
+                size_t li = size_t(ty) * t.width + tx;
+                const auto& px = tb.pixels[li];
+                if (px.weight > 0.f) {
+                    out_rgbw[4 * fi + 0] += px.r;
+                    out_rgbw[4 * fi + 1] += px.g;
+                    out_rgbw[4 * fi + 2] += px.b;
+                    out_rgbw[4 * fi + 3] += px.weight;
+                    out_lumsq[fi] += tb.sumLumSq[li];
+                }
+            }
+    });
+    auto t1 = std::chrono::steady_clock::now();
+    return std::chrono::duration<double>(t1 - t0).count();
+}
+
 // The denoising AOVs of a frame: the 64x64 tiles of ref_render, each merged
 // into plain albedo (rgbw) and normal (xyzw) accumulators with
 // Film::mergeTile's arithmetic (Film.cpp:58-70): the tile's per-pixel average
@@ -561,6 +761,52 @@ void ref_mat_le(void* sp, int h, const float* si, const float* rayDir, const flo
 }
 
 float ref_ggx_D(float cosH, float alpha2) { return D_GGX(cosH, alpha2); }
+
+// ---- Marschner hair lobes (MarschnerHair.h) ------------------------------------
+// Evaluation and sampling through the Marschner branches (see mhEvaluate /
+// mhSample) of material handle h, which must be a MarschnerHairMaterial.
+// si: see makeSI. eval out: f[3], pdf, pdfRev; sample out: f[3], wi[3], pdf, valid.
+int ref_mh_evaluate(void* sp, int h, const float* si, const float* rayDir, const float* wo, const float* wi,
+                    float* out) {
+    auto* s = static_cast<RefScene*>(sp);
+    auto* m = dynamic_cast<const MarschnerHairMaterial*>(s->mats[size_t(h)].get());
+    if (!m) return 1;
+    ShadingContext ctx(makeSI(si), v3(rayDir));
+    mhEvaluate(*m, ctx, v3(wo), v3(wi), out);
+    return 0;
+}
+
+int ref_mh_sample(void* sp, int h, const float* si, const float* rayDir, const float* wo, const float* u2,
+                  float uc, float* out) {
+    auto* s = static_cast<RefScene*>(sp);
+    auto* m = dynamic_cast<const MarschnerHairMaterial*>(s->mats[size_t(h)].get());
+    if (!m) return 1;
+    ShadingContext ctx(makeSI(si), v3(rayDir));
+    mhSample(*m, ctx, v3(wo), Vec2f{u2[0], u2[1]}, uc, out);
+    return 0;
+}
+
+// The public lobe functions (MarschnerHair.h:88-187) over n inputs of 10
+// floats: cosI, sinI, cosR, sinR, v, x, s, u, h, cosO (eta and sigma_a shared).
+// out per input, 16 floats: mh_Mp(cosI, sinI, cosR, sinR, v),
+// mh_trimmedLogistic(x, s), mh_sampleTrimmedLogistic(u, s),
+// mh_Np(x, p, s, asin(h), 0.3 h) for p = 0..2, mh_Ap(cosO, eta, h, sigma_a)
+// (3 x rgb), mh_sampleGaussian(u, x / 2pi + 0.5).
+void ref_mh_functions(const float* in, uint32_t n, float eta, const float* sigma_a, float* out) {
+    const Spectrum sa = v3(sigma_a);
+    for (uint32_t k = 0; k < n; ++k) {
+        const float* q = in + 10 * size_t(k);
+        float* o = out + 16 * size_t(k);
+        o[0] = mh_Mp(q[0], q[1], q[2], q[3], q[4]);
+        o[1] = mh_trimmedLogistic(q[5], q[6]);
+        o[2] = mh_sampleTrimmedLogistic(q[7], q[6]);
+        const float gO = std::asin(q[8]), gT = 0.3f * q[8];
+        for (int p = 0; p < 3; ++p) o[3 + p] = mh_Np(q[5], p, q[6], gO, gT);
+        auto ap = mh_Ap(q[9], eta, q[8], sa);
+        for (int p = 0; p < 3; ++p) put3(o + 6 + 3 * p, ap[size_t(p)]);
+        o[15] = mh_sampleGaussian(q[7], q[5] * 0.15915494f + 0.5f);
+    }
+}
 
 // ---- lights ----------------------------------------------------------------
 // out: Li[3], wi[3], pdf, dist

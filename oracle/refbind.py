@@ -27,12 +27,14 @@ def _fp(a):
     return a.ctypes.data_as(_F) if a is not None else None
 
 
-def build(reference="/root/reference", quiet=True):
+def build(reference=None, quiet=True):
     """Compile the reference variants and, when the CUDA library exists, the
-    drop-in check (needs the reference tree; a no-op when the libraries are
-    already built)."""
+    drop-in check from the reference tree at `reference` (default: the
+    ANACAPA_REFERENCE environment variable). Without a tree it only reports
+    whether the libraries are already built."""
     libs = [os.path.join(REF_DIR, n) for n in ("libanacapa_ref.so", "libanacapa_ref_nocontract.so")]
-    if not os.path.isdir(reference):
+    reference = reference or os.environ.get("ANACAPA_REFERENCE")
+    if not reference or not os.path.isdir(reference):
         return all(os.path.exists(p) for p in libs)
     subprocess.run(["make", "-C", HERE, "ref", f"REF={reference}"], check=True,
                    stdout=subprocess.DEVNULL if quiet else None)
@@ -77,6 +79,9 @@ def lib(variant="record"):
     L.ref_set_camera.argtypes = [_P, _F, _F, _F, C.c_float, C.c_uint32, C.c_uint32]
     L.ref_commit.argtypes = [_P]
     L.ref_trace.argtypes = [_P, _F, _F, C.c_uint64, _I32, _F, C.c_int]
+    L.ref_render_rows.argtypes = [_P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int,
+                                  _U32, C.c_uint32, _F, _F]
+    L.ref_render_rows.restype = C.c_double
     L.ref_occluded.argtypes = [_P, _F, _F, C.c_uint64, _U8, C.c_int]
     L.ref_render.argtypes = [_P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
                              C.c_int, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, _F, _F]
@@ -91,6 +96,9 @@ def lib(variant="record"):
     L.ref_halton.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32, _F]
     L.ref_pcg.argtypes = [C.c_uint64, C.c_uint32, _U32]
     L.ref_mat_evaluate.argtypes = [_P, C.c_int, _F, _F, _F, _F, _F]
+    L.ref_mh_evaluate.argtypes = [_P, C.c_int, _F, _F, _F, _F, _F]
+    L.ref_mh_sample.argtypes = [_P, C.c_int, _F, _F, _F, _F, C.c_float, _F]
+    L.ref_mh_functions.argtypes = [_F, C.c_uint32, C.c_float, _F, _F]
     L.ref_mat_sample.argtypes = [_P, C.c_int, _F, _F, _F, _F, C.c_float, _F]
     L.ref_mat_le.argtypes = [_P, C.c_int, _F, _F, _F, _F]
     L.ref_ggx_D.argtypes = [C.c_float, C.c_float]
@@ -215,6 +223,19 @@ class RefScene:
                                  _fp(rgbw), _fp(lsq))
         return rgbw, lsq, secs
 
+    def render_rows(self, bands, spp=None, sample_start=0, max_depth=None, nthreads=0):
+        """render() over full-width row bands [(y0, y1), ...] in one thread
+        pool dispatch; returns (rgbw, lsq, seconds)."""
+        s = self.scene
+        W, H = s.width, s.height
+        rows = np.ascontiguousarray(np.asarray(bands, np.uint32).reshape(-1, 2))
+        rgbw = np.zeros((H, W, 4), np.float32)
+        lsq = np.zeros((H, W), np.float32)
+        secs = self.L.ref_render_rows(self.h, W, H, s.spp if spp is None else spp, sample_start,
+                                      s.max_depth if max_depth is None else max_depth, nthreads,
+                                      rows.ctypes.data_as(_U32), len(rows), _fp(rgbw), _fp(lsq))
+        return rgbw, lsq, secs
+
     def render_aov(self, spp=None, sample_start=0, max_depth=None, nthreads=0):
         """The frame's albedo and normal AOV accumulators, (H, W, 4) each
         (sum of per-tile averages, weight)."""
@@ -293,6 +314,90 @@ class RefScene:
         out = np.zeros((len(q), 6), np.float32)
         self.L.ref_camera_rays(self.h, s.width, s.height, q.ctypes.data_as(_U32), len(q), _fp(out))
         return out
+
+
+# ana_bsdf_query / ana_bsdf_result layouts (include/anacapa_b200.h)
+BSDF_QUERY = np.dtype([("n", "<f4", 3), ("t", "<f4", 3), ("color", "<f4", 3), ("wo", "<f4", 3),
+                       ("wi", "<f4", 3), ("u", "<f4", 2), ("u_comp", "<f4"), ("is_curve", "<u4")])
+BSDF_RESULT = np.dtype([("f", "<f4", 3), ("pdf", "<f4"), ("sample_f", "<f4", 3), ("sample_pdf", "<f4"),
+                        ("sample_wi", "<f4", 3), ("sample_flags", "<u4")])
+
+
+class RefMaterial:
+    """One of the reference's material objects, outside any scene, for BSDF
+    queries: IMaterial::evaluate / sample (the Kajiya-Kay lobe for hair, as
+    the reference executes it), or for a hair material with
+    marschner=True the Marschner branches of MarschnerHair.h (242-257,
+    284-375) through ref_mh_evaluate / ref_mh_sample."""
+
+    def __init__(self, m, variant="nocontract"):
+        from anacapa_b200 import scenes as S
+        L = self.L = lib(variant)
+        self.h = L.ref_scene_new()
+        if m.type == S.MAT_LAMBERT:
+            self.mat = L.ref_mat_lambert(self.h, _fp(f32(m.albedo)))
+        elif m.type == S.MAT_EMISSIVE:
+            self.mat = L.ref_mat_emissive(self.h, _fp(f32(m.albedo)), _fp(f32(m.emission)))
+        elif m.type == S.MAT_STANDARD:
+            self.mat = L.ref_mat_standard(self.h, _fp(m.standard_packed()))
+        elif m.type == S.MAT_HAIR:
+            self.mat = L.ref_mat_marschner(self.h, m.eta, _fp(f32(m.sigma_a)), m.beta_m, m.beta_n, m.alpha_deg)
+        else:
+            raise ValueError(m.type)
+        self.marschner = m.type == S.MAT_HAIR and m.hair_mode == 1
+
+    def __del__(self):
+        try:
+            self.L.ref_scene_free(self.h)
+        except Exception:
+            pass
+
+    def query(self, queries):
+        q = np.ascontiguousarray(queries, BSDF_QUERY)
+        out = np.zeros(len(q), BSDF_RESULT)
+        L = self.L
+        ev = np.zeros(5, np.float32)
+        sm = np.zeros(8, np.float32)
+        for k, r in enumerate(q):
+            si = np.zeros(16, np.float32)
+            si[3:6] = r["n"]
+            si[6:9] = r["n"]
+            si[9:12] = r["t"]
+            si[12:15] = r["color"]
+            si[15] = float(r["is_curve"])
+            ray_dir = f32(-r["wo"])
+            wo, wi, u = f32(r["wo"]), f32(r["wi"]), f32(r["u"])
+            if self.marschner:
+                L.ref_mh_evaluate(self.h, self.mat, _fp(si), _fp(ray_dir), _fp(wo), _fp(wi), _fp(ev))
+                L.ref_mh_sample(self.h, self.mat, _fp(si), _fp(ray_dir), _fp(wo), _fp(u), float(r["u_comp"]),
+                                _fp(sm))
+                valid = sm[7] != 0.0
+                flags = 2 | 8 | 16
+            else:
+                L.ref_mat_evaluate(self.h, self.mat, _fp(si), _fp(ray_dir), _fp(wo), _fp(wi), _fp(ev))
+                L.ref_mat_sample(self.h, self.mat, _fp(si), _fp(ray_dir), _fp(wo), _fp(u), float(r["u_comp"]),
+                                 _fp(sm))
+                valid = sm[6] > 0.0 and np.any(sm[0:3] != 0.0)
+                flags = int(sm[7])
+            o = out[k]
+            o["f"] = ev[0:3]
+            o["pdf"] = ev[3]
+            if valid:
+                o["sample_f"] = sm[0:3]
+                o["sample_wi"] = sm[3:6]
+                o["sample_pdf"] = sm[6]
+                o["sample_flags"] = flags
+        return out
+
+
+def mh_functions(inputs, eta, sigma_a, variant="nocontract"):
+    """The reference's public Marschner lobe functions (MarschnerHair.h:
+    88-187) over rows of (cosI, sinI, cosR, sinR, v, x, s, u, h, cosO); see
+    ref_mh_functions for the 16 outputs per row."""
+    x = f32(inputs).reshape(-1, 10)
+    out = np.zeros((len(x), 16), np.float32)
+    lib(variant).ref_mh_functions(_fp(x), len(x), float(eta), _fp(f32(sigma_a)), _fp(out))
+    return out
 
 
 def halton(px, py, sample_index, ndims, seed=0, variant="record"):

@@ -1740,4 +1740,29 @@ void po_adjoint(void* p, uint32_t W, uint32_t H, uint32_t spp, uint32_t s0, uint
     }
 }
 
+// The Marschner lobe functions in float over rows of (cosI, sinI, cosR, sinR,
+// v, x, s, u, h, cosO): the outputs of the reference harness's
+// ref_mh_functions, in the same order (MarschnerHair.h:88-187).
+void po_mh_functions(const float* in, uint32_t n, float eta, const float* sigma_a, float* out) {
+    const V3<float> sa(sigma_a[0], sigma_a[1], sigma_a[2]);
+    for (uint32_t k = 0; k < n; ++k) {
+        const float* q = in + 10 * size_t(k);
+        float* o = out + 16 * size_t(k);
+        o[0] = mhMp(q[0], q[1], q[2], q[3], q[4]);
+        o[1] = mhTrim(q[5], q[6]);
+        o[2] = mhSampleTrim(q[7], q[6]);
+        const float gO = std::asin(q[8]), gT = 0.3f * q[8];
+        for (int p = 0; p < 3; ++p) o[3 + p] = mhTrim(mhWrap(q[5] - mhPhi(p, gO, gT)), q[6]);
+        V3<float> ap[3];
+        mhAp(q[9], eta, q[8], sa, ap);
+        for (int p = 0; p < 3; ++p) {
+            o[6 + 3 * p] = ap[p].x;
+            o[7 + 3 * p] = ap[p].y;
+            o[8 + 3 * p] = ap[p].z;
+        }
+        const float u2 = q[5] * 0.15915494f + 0.5f;
+        o[15] = std::sqrt(-2.f * std::log(std::max(q[7], 1e-6f))) * std::cos(k2Pi<float> * u2);
+    }
+}
+
 }  // extern "C"

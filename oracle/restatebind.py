@@ -52,6 +52,7 @@ def lib():
         L.po_li.argtypes = [_P, _U32, C.c_uint64, C.c_uint32, C.c_uint64, _D, C.c_int]
         L.po_halton.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32, _F]
         L.po_pcg.argtypes = [C.c_uint64, C.c_uint32, _U32]
+        L.po_mh_functions.argtypes = [_F, C.c_uint32, C.c_float, _F, _F]
         L.po_ggx_D.argtypes = [C.c_float, C.c_float]
         L.po_ggx_D.restype = C.c_float
         L.po_num_params.argtypes = [_P]
@@ -161,6 +162,15 @@ class PoScene:
 def halton(px, py, s, n, seed=0):
     out = np.zeros(n, np.float32)
     lib().po_halton(px, py, s, seed, n, out.ctypes.data_as(_F))
+    return out
+
+
+def mh_functions(inputs, eta, sigma_a):
+    """The restatement's Marschner lobe functions in float (the layout of
+    oracle.refbind.mh_functions)."""
+    x = f32(inputs).reshape(-1, 10)
+    out = np.zeros((len(x), 16), np.float32)
+    lib().po_mh_functions(_fp(x), len(x), float(eta), _fp(f32(sigma_a)), _fp(out))
     return out
 
 

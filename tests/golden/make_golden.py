@@ -2,6 +2,7 @@
 
     python tests/golden/make_golden.py              # reference_vectors.npz
     python tests/golden/make_golden.py --features   # feature_vectors.npz
+    python tests/golden/make_golden.py --bsdf       # bsdf_vectors.npz
 
 Runs here (where the reference tree was compiled into oracle/_ref by
 oracle/Makefile); the resulting .npz files travel with the repository, so the
@@ -123,8 +124,100 @@ def features():
     print("wrote", os.path.join(HERE, "feature_vectors.npz"))
 
 
+def bsdf_materials():
+    """The materials of the BSDF fixtures: Lambert, standard_surface over
+    roughness / metalness / coat, and hair in both modes over eta, sigma_a,
+    beta_m, beta_n and the cuticle tilt."""
+    M = S.Material
+    mats = [M(S.MAT_LAMBERT, albedo=(0.7, 0.4, 0.2))]
+    for rough, metal, coat in [(0.05, 0.0, 0.0), (0.3, 0.0, 0.0), (0.6, 1.0, 0.0), (1.0, 0.0, 0.5),
+                               (0.15, 1.0, 0.3)]:
+        mats.append(M(S.MAT_STANDARD, base_color=(0.8, 0.5, 0.3), roughness=rough, metalness=metal, coat=coat))
+    for mode in (0, 1):
+        for eta, sa, bm, bn, al in [(1.55, (0.4, 0.65, 1.35), 0.3, 0.3, 2.0), (1.4, (0.05, 0.5, 2.0), 0.15, 0.6, 3.0),
+                                    (1.6, (1.5, 1.0, 0.2), 0.6, 0.2, 0.0), (1.55, (0.2, 0.2, 0.2), 0.08, 0.9, 4.0)]:
+            mats.append(M(S.MAT_HAIR, eta=eta, sigma_a=sa, beta_m=bm, beta_n=bn, alpha_deg=al, hair_mode=mode))
+    return mats
+
+
+def bsdf_queries(material, n, seed):
+    """Seeded shading frames: for hair a unit fiber tangent t and a ribbon
+    normal n perpendicular to it, wo on n's side, strand colours white (the
+    material's sigma_a) or coloured; for surfaces a normal with wo mostly
+    above it; wi anywhere on the sphere; uniform 2-D and component samples."""
+    from oracle import refbind as Rb
+    rng = np.random.default_rng(seed)
+
+    def unit(k):
+        v = rng.normal(size=(k, 3))
+        return v / np.linalg.norm(v, axis=1, keepdims=True)
+
+    q = np.zeros(n, Rb.BSDF_QUERY)
+    nrm = unit(n)
+    hair = material.type == S.MAT_HAIR
+    if hair:
+        t = unit(n)
+        nrm = nrm - t * np.sum(nrm * t, 1, keepdims=True)
+        nrm /= np.linalg.norm(nrm, axis=1, keepdims=True)
+        q["t"] = t
+        q["is_curve"] = 1
+        col = np.ones((n, 3))
+        coloured = rng.random(n) < 0.5
+        col[coloured] = rng.uniform(0.05, 0.95, (int(coloured.sum()), 3))
+        q["color"] = col
+    else:
+        q["color"] = 1.0
+    wo = unit(n)
+    flip = np.sum(wo * nrm, 1) < 0
+    if hair:
+        wo[flip] = -wo[flip]
+    else:  # one in eight below the surface
+        below = rng.random(n) < 0.125
+        wo[flip != below] = -wo[flip != below]
+    q["n"] = nrm
+    q["wo"] = wo
+    q["wi"] = unit(n)
+    q["u"] = rng.random((n, 2))
+    q["u_comp"] = rng.random(n)
+    return q
+
+
+def bsdf():
+    """bsdf_vectors.npz: IMaterial::evaluate / sample of the reference's
+    material classes on seeded shading frames (hair in Kajiya-Kay mode as the
+    reference executes it, and through the Marschner branches of
+    MarschnerHair.h for hair_mode 1), plus the public Marschner lobe functions
+    over a seeded grid. Built without FMA contraction."""
+    from oracle import refbind as Rb
+    R.build()
+    out = {}
+    for k, m in enumerate(bsdf_materials()):
+        q = bsdf_queries(m, 512, 100 + k)
+        out[f"m{k}_query"] = q
+        out[f"m{k}_result"] = Rb.RefMaterial(m, variant="nocontract").query(q)
+    rng = np.random.default_rng(77)
+    n = 4096
+    thI = rng.uniform(-np.pi / 2, np.pi / 2, n)
+    thR = rng.uniform(-np.pi / 2, np.pi / 2, n)
+    v = np.exp(rng.uniform(np.log(2e-3), np.log(1.5), n))
+    x = rng.uniform(-np.pi, np.pi, n)
+    s = rng.uniform(0.05, 1.2, n)
+    u = rng.random(n)
+    h = rng.uniform(-0.999, 0.999, n)
+    cosO = np.cos(rng.uniform(-1.5, 1.5, n))
+    grid = np.stack([np.cos(thI), np.sin(thI), np.cos(thR), np.sin(thR), v, x, s, u, h, cosO], 1).astype(np.float32)
+    out["mh_grid"] = grid
+    out["mh_eta"] = np.float32(1.55)
+    out["mh_sigma_a"] = np.array([0.4, 0.65, 1.35], np.float32)
+    out["mh_out"] = Rb.mh_functions(grid, 1.55, out["mh_sigma_a"], variant="nocontract")
+    np.savez_compressed(os.path.join(HERE, "bsdf_vectors.npz"), **out)
+    print("wrote", os.path.join(HERE, "bsdf_vectors.npz"))
+
+
 if __name__ == "__main__":
-    if "--features" in sys.argv:
+    if "--bsdf" in sys.argv:
+        bsdf()
+    elif "--features" in sys.argv:
         features()
     else:
         main()

@@ -1,0 +1,75 @@
+"""The device BSDFs (ana_bsdf_batch: the functions k_shade calls) against the
+reference's own material code on the committed fixtures
+(tests/golden/bsdf_vectors.npz): Lambert, standard_surface, and hair in
+Kajiya-Kay mode (what the reference executes) and in Marschner mode (the
+reference's R/TT/TRT branches, MarschnerHair.h:242-257 for evaluate and
+284-375 for sample).
+
+Tolerance: the device rounds differently from glibc in its transcendental
+functions (expf, logf, asinf, atan2f, sinhf, powf: a few ulps) and contracts
+multiply-adds, so values agree to about 1e-5 relative and not bit for bit.
+A query's error is the largest component error over the query's largest
+component magnitude. The bars: evaluate() within 1e-4 for 99 % of queries;
+sample() takes the same lobe and direction (wi within 1e-4) for 99 %, with f
+and pdf within 1e-3 for 98 % (a sampled direction carries the device's
+rounding into narrow lobes)."""
+import os
+
+import numpy as np
+import pytest
+
+from anacapa_b200 import api
+
+from test_golden_features import golden_module
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+@pytest.fixture(scope="module")
+def renderer(gpu):
+    r = api.Renderer()
+    yield r
+    r.close()
+
+
+def query_err(a, b):
+    a = np.asarray(a, np.float64).reshape(len(a), -1)
+    b = np.asarray(b, np.float64).reshape(len(b), -1)
+    scale = np.maximum(np.abs(b).max(1), 1e-30)
+    return np.abs(a - b).max(1) / scale
+
+
+def compare(dev, ref):
+    """Fractions of queries within the bars (see the module docstring)."""
+    ev = np.maximum(query_err(dev["f"], ref["f"]), query_err(dev["pdf"], ref["pdf"]))
+    vd, vr = dev["sample_pdf"] > 0, ref["sample_pdf"] > 0
+    both = vd & vr
+    wi = np.abs(dev["sample_wi"] - ref["sample_wi"]).max(1)
+    same = (vd == vr) & (~both | (wi <= 1e-4))
+    sv = np.maximum(query_err(dev["sample_f"][both], ref["sample_f"][both]),
+                    query_err(dev["sample_pdf"][both], ref["sample_pdf"][both]))
+    return {"eval_1e-4": float((ev <= 1e-4).mean()), "sample_same": float(same.mean()),
+            "sample_1e-3": float((sv <= 1e-3).mean()) if len(sv) else 1.0,
+            "eval_max": float(ev.max()), "valid": float(vr.mean())}
+
+
+MATS = golden_module().bsdf_materials()
+
+
+@pytest.mark.parametrize("k", range(len(MATS)),
+                         ids=[f"m{k}_{['lambert', 'emissive', 'standard', 'hair'][m.type]}"
+                              f"{'_marschner' if m.type == 3 and m.hair_mode == 1 else ''}"
+                              for k, m in enumerate(MATS)])
+def test_bsdf_against_reference(renderer, k):
+    gold = np.load(os.path.join(HERE, "golden", "bsdf_vectors.npz"))
+    dev = renderer.bsdf(MATS[k], gold[f"m{k}_query"])
+    ref = gold[f"m{k}_result"]
+    st = compare(dev, ref)
+    assert st["eval_1e-4"] >= 0.99, st
+    assert st["sample_same"] >= 0.99, st
+    assert st["sample_1e-3"] >= 0.98, st
+    # the sampled lobes' flags are the reference's where both sides sample
+    both = (dev["sample_pdf"] > 0) & (ref["sample_pdf"] > 0)
+    assert (dev["sample_flags"][both] == ref["sample_flags"][both]).mean() >= 0.99
