@@ -472,6 +472,14 @@ int upload_blob(ana_ctx* c, const Blob& B, const ana::DeviceTris* dt = nullptr) 
         for (size_t i = 0; i < B.n_mats; ++i) {
             if (mats[i].type == ANA_MAT_HAIR) S.has_fibers = 1;
             if (mats[i].transmission > 0.001f || mats[i].opacity < 1.f) S.has_extra_shading = 1;
+            if (mats[i].type == ANA_MAT_LAMBERT || mats[i].type == ANA_MAT_EMISSIVE) S.features |= ana::kFeatLambert;
+            if (mats[i].type == ANA_MAT_STANDARD) S.features |= ana::kFeatStandard;
+        }
+        const auto* lights = reinterpret_cast<const ana::DevLight*>(B.at(B.o_lights));
+        for (size_t i = 0; i < B.n_lights; ++i) {
+            if (lights[i].type == ANA_LIGHT_AREA) S.features |= ana::kFeatArea;
+            else if (lights[i].type == ANA_LIGHT_DOME) S.features |= ana::kFeatDome;
+            else S.features |= ana::kFeatDir;
         }
     }
     ana::DevEnv& E = S.env;

@@ -439,7 +439,9 @@ __device__ __forceinline__ float sum3(float3 v) { return v.x + v.y + v.z; }
 //    pending gradient of this vertex's continuation.
 // kExtra: glass, alpha masks, motion blur and AOVs compiled in (batches
 // without them take the smaller kernel).
-template <bool kAdj, bool kFiber, bool kExtra>
+// kFeat: the material and light classes compiled in (kFeat* bits); the host
+// launches a kernel whose set covers the batch's (DevScene::features).
+template <bool kAdj, bool kFiber, bool kExtra, uint32_t kFeat = kFeatAll>
 __global__ void __launch_bounds__(kShadeBlock, (!kAdj && !kFiber) ? 3 : 2) k_shade(const __grid_constant__ Params p) {
     const uint32_t b = p.bounce;
     const uint32_t cur = b & 1u, nxt = cur ^ 1u;
@@ -545,9 +547,9 @@ __global__ void __launch_bounds__(kShadeBlock, (!kAdj && !kFiber) ? 3 : 2) k_sha
                             const DevLight L = S.lights[R.light_base + lidx];
                             // light sampling
                             float lu0 = ss.next(), lu1 = ss.next();
-                            LightSample ls = light_sample(S, L, si.p, lu0, lu1);
+                            LightSample ls = light_sample<kFeat>(S, L, si.p, lu0, lu1);
                             if (ls.pdf > 0.f && !is_black(ls.Li)) {
-                                BsdfEval be = mat_eval<kFiber, kExtra>(m, c, wo, ls.wi);
+                                BsdfEval be = mat_eval<kFiber, kExtra, kFeat>(m, c, wo, ls.wi);
                                 if (!is_black(be.f)) {
                                     float3 target = si.p + ls.wi * ls.dist;
                                     float3 dir = target - si.p;
@@ -584,16 +586,16 @@ __global__ void __launch_bounds__(kShadeBlock, (!kAdj && !kFiber) ? 3 : 2) k_sha
                             // BSDF sampling toward the light: non-delta lights only,
                             // and only then are its sample dimensions drawn
                             // (estimateDirect, PathIntegrator.cpp:210)
-                            const bool deltaLight = L.type == ANA_LIGHT_DIRECTIONAL;
+                            const bool deltaLight = (kFeat & kFeatDir) != 0 && L.type == ANA_LIGHT_DIRECTIONAL;
                             float uc = 0.f, bu0 = 0.f, bu1 = 0.f;
                             if (!deltaLight) {
                                 uc = ss.next();
                                 bu0 = ss.next();
                                 bu1 = ss.next();
                             }
-                            BsdfSample bs = deltaLight ? no_sample() : mat_sample<kFiber, kExtra>(m, c, wo, bu0, bu1, uc);
+                            BsdfSample bs = deltaLight ? no_sample() : mat_sample<kFiber, kExtra, kFeat>(m, c, wo, bu0, bu1, uc);
                             if (bs.valid()) {
-                                float lp = light_pdf(S, L, si.p, bs.wi);
+                                float lp = light_pdf<kFeat>(S, L, si.p, bs.wi);
                                 if (lp > 0.f) {
                                     float w = bs.delta() ? 1.f : power_heuristic(bs.pdf, lp);
                                     float3 org = spawn_origin(si.p, si.ng, bs.wi);
@@ -617,7 +619,7 @@ __global__ void __launch_bounds__(kShadeBlock, (!kAdj && !kFiber) ? 3 : 2) k_sha
                         // continuation
                         float uc = ss.next();
                         float u0 = ss.next(), u1 = ss.next();
-                        BsdfSample bs = mat_sample<kFiber, kExtra>(m, c, wo, u0, u1, uc);
+                        BsdfSample bs = mat_sample<kFiber, kExtra, kFeat>(m, c, wo, u0, u1, uc);
                         if (bs.valid()) {
                             spec = bs.delta();
                             beta = beta * (bs.f / bs.pdf);
@@ -1120,6 +1122,9 @@ void prime_kernels() {
     prime(k_shade<false, false, true>);
     prime(k_shade<false, true, false>);
     prime(k_shade<false, true, true>);
+    prime(k_shade<false, false, false, kFeatStandard | kFeatDome>);
+    prime(k_shade<false, false, false, kFeatLambert | kFeatArea>);
+    prime(k_shade<false, true, false, kFeatLambert | kFeatArea>);
     prime(k_shade<true, false, false>);
     prime(k_shade<true, true, false>);
     prime(k_film);
@@ -1215,11 +1220,19 @@ void launch_shade(const Params& p, const LaunchCfg& c0, cudaStream_t s) {
     c.block = std::min(c.block, kShadeBlock);
     const int g = std::min(c.grid_cap, c.stage_grid);
     const bool extra = p.S.has_extra_shading || p.aov;
+    // kernels without the material / light classes a batch lacks: GGX
+    // surfaces under a dome (the throughput scene), Lambert surfaces under
+    // area lights (the Cornell boxes and the hair scene)
+    constexpr uint32_t kStdDome = kFeatStandard | kFeatDome, kLambArea = kFeatLambert | kFeatArea;
+    const uint32_t f = p.S.features;
     if (p.S.has_fibers) {
         if (extra) k_shade<false, true, true><<<g, c.block, 0, s>>>(p);
+        else if ((f & ~kLambArea) == 0) k_shade<false, true, false, kLambArea><<<g, c.block, 0, s>>>(p);
         else k_shade<false, true, false><<<g, c.block, 0, s>>>(p);
     } else {
         if (extra) k_shade<false, false, true><<<g, c.block, 0, s>>>(p);
+        else if ((f & ~kStdDome) == 0) k_shade<false, false, false, kStdDome><<<g, c.block, 0, s>>>(p);
+        else if ((f & ~kLambArea) == 0) k_shade<false, false, false, kLambArea><<<g, c.block, 0, s>>>(p);
         else k_shade<false, false, false><<<g, c.block, 0, s>>>(p);
     }
 }
@@ -1381,17 +1394,42 @@ void launch_bsdf_query(const DevMaterial& m, const ana_bsdf_query* q, uint32_t n
 // ---------------------------------------------------------------------------
 static __device__ __align__(256) unsigned char g_noalloc_trace[kNoAllocBytes];
 
+// The address is cached per device together with the context it was looked
+// up in: a device reset (cudaDeviceReset) destroys the primary context and
+// the module with it, and the next context loads the module again, possibly
+// elsewhere. The current context comes from the driver's cuCtxGetCurrent,
+// reached through cudaGetDriverEntryPoint (no link against the driver
+// library).
+static cudaError_t current_context(void** ctx) {
+    using GetCurrent = int (*)(void**);
+    static GetCurrent fn = nullptr;
+    if (!fn) {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        const cudaError_t e = cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q);
+        if (e != cudaSuccess) return e;
+        if (q != cudaDriverEntryPointSuccess || !f) return cudaErrorSymbolNotFound;
+        fn = reinterpret_cast<GetCurrent>(f);
+    }
+    return fn(ctx) == 0 ? cudaSuccess : cudaErrorDeviceUninitialized;
+}
+
 cudaError_t noalloc_trace_scratch(int device, unsigned char** base) {
     constexpr int kMaxDevices = 64;
     static std::mutex mu;
     static void* addr[kMaxDevices] = {};
+    static void* owner[kMaxDevices] = {};  // the context each address belongs to
     if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
     std::lock_guard<std::mutex> lk(mu);
-    if (!addr[device]) {
+    void* ctx = nullptr;
+    cudaError_t e = current_context(&ctx);
+    if (e != cudaSuccess) return e;
+    if (!addr[device] || owner[device] != ctx) {
         void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_trace);
+        e = cudaGetSymbolAddress(&p, g_noalloc_trace);
         if (e != cudaSuccess) return e;
         addr[device] = p;
+        owner[device] = ctx;
     }
     *base = static_cast<unsigned char*>(addr[device]);
     return cudaSuccess;

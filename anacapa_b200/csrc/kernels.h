@@ -148,7 +148,8 @@ static_assert(sizeof(ana_hit) == 32, "hit record size");
 
 // Device address of that scratch on `device`, which must be the current
 // device. The first call per device looks it up (cudaGetSymbolAddress) and
-// caches it; later calls only read the cache.
+// caches it with the current context; later calls in the same context only
+// read the cache (after a device reset the new context looks it up again).
 cudaError_t noalloc_trace_scratch(int device, unsigned char** base);
 
 }  // namespace ana

@@ -138,6 +138,16 @@ struct DevSceneRec {
     uint64_t spp_div, rect_w_div;
 };
 
+// Material and light classes present in an uploaded scene (DevScene::features).
+// Shading kernels are also compiled for subsets of them, so a batch that
+// lacks a class runs a kernel without its code.
+constexpr uint32_t kFeatLambert = 1;   // Lambertian and emissive materials
+constexpr uint32_t kFeatStandard = 2;  // standard_surface
+constexpr uint32_t kFeatArea = 4;      // area lights
+constexpr uint32_t kFeatDome = 8;      // dome lights
+constexpr uint32_t kFeatDir = 16;      // directional lights
+constexpr uint32_t kFeatAll = 31;
+
 struct DevScene {
     const Bvh4Node* tri_nodes;
     const float4* tri_isect;
@@ -164,6 +174,7 @@ struct DevScene {
     const float4* motion_keys;
     uint32_t has_motion;
     uint32_t has_extra_shading;  // glass, alpha masks or motion: the shading kernel with their code
+    uint32_t features;           // kFeat* bits of the materials and lights present
     DevEnv env;             // the (single) dome of the batch
 };
 

@@ -642,13 +642,19 @@ __device__ __forceinline__ BsdfSample marschner_sample(const DevMaterial& m, con
 // ---- material dispatch (IMaterial.h:53-114) ------------------------------------
 // kHair = false compiles the hair BSDFs out, for batches without hair
 // materials (smaller shading kernels: fewer registers, fewer i-cache misses).
-template <bool kHair = true, bool kGlass = true>
+// kFeat: the kFeat* material classes compiled in (the others return no sample
+// / a zero BSDF; the host picks a kernel whose set covers the scene's).
+template <bool kHair = true, bool kGlass = true, uint32_t kFeat = kFeatAll>
 __device__ __forceinline__ BsdfSample mat_sample(const DevMaterial& m, const ShadeCtx& c, float3 wo, float ux,
                                                  float uy, float uc) {
     switch (m.type) {
         case ANA_MAT_LAMBERT:
-        case ANA_MAT_EMISSIVE: return lambert_sample(m, c, wo, ux, uy);
-        case ANA_MAT_STANDARD: return ss_sample<kGlass>(m, c, wo, ux, uy, uc);
+        case ANA_MAT_EMISSIVE:
+            if constexpr ((kFeat & kFeatLambert) != 0) return lambert_sample(m, c, wo, ux, uy);
+            else return no_sample();
+        case ANA_MAT_STANDARD:
+            if constexpr ((kFeat & kFeatStandard) != 0) return ss_sample<kGlass>(m, c, wo, ux, uy, uc);
+            else return no_sample();
         default:
             if constexpr (kHair)
                 return m.hair_mode == ANA_HAIR_MARSCHNER ? marschner_sample(m, c, wo, ux, uy, uc)
@@ -657,12 +663,16 @@ __device__ __forceinline__ BsdfSample mat_sample(const DevMaterial& m, const Sha
                 return no_sample();
     }
 }
-template <bool kHair = true, bool kGlass = true>
+template <bool kHair = true, bool kGlass = true, uint32_t kFeat = kFeatAll>
 __device__ __forceinline__ BsdfEval mat_eval(const DevMaterial& m, const ShadeCtx& c, float3 wo, float3 wi) {
     switch (m.type) {
         case ANA_MAT_LAMBERT:
-        case ANA_MAT_EMISSIVE: return lambert_eval(m, c, wo, wi);
-        case ANA_MAT_STANDARD: return ss_eval<kGlass>(m, c, wo, wi);
+        case ANA_MAT_EMISSIVE:
+            if constexpr ((kFeat & kFeatLambert) != 0) return lambert_eval(m, c, wo, wi);
+            else return BsdfEval{f3(0.f, 0.f, 0.f), 0.f};
+        case ANA_MAT_STANDARD:
+            if constexpr ((kFeat & kFeatStandard) != 0) return ss_eval<kGlass>(m, c, wo, wi);
+            else return BsdfEval{f3(0.f, 0.f, 0.f), 0.f};
         default:
             if constexpr (kHair)
                 return m.hair_mode == ANA_HAIR_MARSCHNER ? marschner_eval(m, c, wo, wi) : kk_eval(m, c, wo, wi);
@@ -925,10 +935,23 @@ __device__ __forceinline__ LightSample dir_sample(const DevLight& L, float ux, f
     return s;
 }
 
+// kFeat: the kFeat* light classes compiled in (the others give a zero sample).
+template <uint32_t kFeat = kFeatAll>
 __device__ __forceinline__ LightSample light_sample(const DevScene& S, const DevLight& L, float3 p, float ux,
                                                     float uy) {
-    if (L.type == ANA_LIGHT_DIRECTIONAL) return dir_sample(L, ux, uy);
-    LightSample s = L.type == ANA_LIGHT_AREA ? area_sample(L, p, ux, uy) : env_sample(S.env, ux, uy);
+    if constexpr ((kFeat & kFeatDir) != 0)
+        if (L.type == ANA_LIGHT_DIRECTIONAL) return dir_sample(L, ux, uy);
+    LightSample s;
+    s.Li = f3(0.f, 0.f, 0.f);
+    s.wi = f3(0.f, 0.f, 1.f);
+    s.pdf = 0.f;
+    s.dist = 0.f;
+    if constexpr ((kFeat & kFeatArea) != 0 && (kFeat & kFeatDome) != 0)
+        s = L.type == ANA_LIGHT_AREA ? area_sample(L, p, ux, uy) : env_sample(S.env, ux, uy);
+    else if constexpr ((kFeat & kFeatArea) != 0)
+        s = area_sample(L, p, ux, uy);
+    else if constexpr ((kFeat & kFeatDome) != 0)
+        s = env_sample(S.env, ux, uy);
     s.delta = false;
     return s;
 }
@@ -948,9 +971,18 @@ __device__ __forceinline__ float3 mat_reflectance(const DevMaterial& m, const Sh
 }
 
 // ILight::pdf; a directional light is delta (DirectionalLight::pdf returns 0).
+template <uint32_t kFeat = kFeatAll>
 __device__ __forceinline__ float light_pdf(const DevScene& S, const DevLight& L, float3 p, float3 wi) {
-    if (L.type == ANA_LIGHT_DIRECTIONAL) return 0.f;
-    return L.type == ANA_LIGHT_AREA ? area_pdf(L, p, wi) : env_pdf(S.env, wi);
+    if constexpr ((kFeat & kFeatDir) != 0)
+        if (L.type == ANA_LIGHT_DIRECTIONAL) return 0.f;
+    if constexpr ((kFeat & kFeatArea) != 0 && (kFeat & kFeatDome) != 0)
+        return L.type == ANA_LIGHT_AREA ? area_pdf(L, p, wi) : env_pdf(S.env, wi);
+    else if constexpr ((kFeat & kFeatArea) != 0)
+        return area_pdf(L, p, wi);
+    else if constexpr ((kFeat & kFeatDome) != 0)
+        return env_pdf(S.env, wi);
+    else
+        return 0.f;
 }
 
 // spawnRay / spawnRayTo (Types.h:269-284)

@@ -465,7 +465,7 @@ def bench_configs(local, cpu_s=0.0):
         ("hair_marschner_1280x720x32", None, S.hair(1280, 720, 32, 10, hair_mode=1), 1 << 25, None, True),
         ("throughput_938_spheres", None, S.throughput(n_spheres=938), 1 << 27, None, False),
         ("glass_1280x720x16", "glass: smooth and rough dielectric spheres and panes, alpha-masked cards, "
-         "directional + area light; depth 8", S.glass(1280, 720, 16, 8), 1 << 25, None, False),
+         "directional + area light; depth 8", S.glass(1280, 720, 16, 8), 1 << 25, "glass", False),
         ("motion_1280x720x16", "motion blur: object-space meshes with 2-3 motion keys, shutter [0, 1]; depth 6",
          S.motion(1280, 720, 16, 6), 1 << 25, None, False),
     ]

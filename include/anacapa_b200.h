@@ -399,8 +399,10 @@ int ana_trace_batch_timed(ana_ctx* ctx, const float* rays, const float* times, s
  *   of n hits. n <= ANA_TRACE_NOALLOC_MAX_RAYS, else ANA_ERR_INVALID_ARG and
  *   nothing runs. The call returns after the hits are in `out`.
  * The first call on a device looks up the scratch address
- * (cudaGetSymbolAddress, with the context's device current) and caches it;
- * make that first call before any stream capture begins on the device. Each
+ * (cudaGetSymbolAddress, with the context's device current) and caches it
+ * for the device's current CUDA context (after a device reset the next call
+ * looks it up again); make that first call before any stream capture begins
+ * on the device. Each
  * call zeroes the error word and work counter of the scratch itself; rays
  * and hits need no clearing. The scratch is shared by every context on the
  * device: calls that overlap in time (two threads, two contexts on one

@@ -87,6 +87,10 @@ struct Mat {
     T coatAlpha2 = 0, f0 = 0, coatF0 = 0;
     uint32_t flags = 0;
     bool delta = false;
+    // glass and alpha masks (StandardSurface.h:197-218, 245-340, 410-462)
+    T transmission = 0, opacity = 1;
+    bool alphaMask = false;
+    V3<T> tint;  // transmittanceColor: black = opaque to shadow rays
     // hair
     T eta = T(1.55f), bm = T(0.3f), bn = T(0.3f), alphaDeg = 2;
     V3<T> sigma;
@@ -148,6 +152,7 @@ struct Scene {
     std::vector<Dist1D<T>> cond;
     Dist1D<T> marg;
     V3<T> envRadiance;
+    bool transmit = false;  // a material passes shadow rays (non-black transmittanceColor)
     // camera (Camera::makePinhole, IIntegrator.h:49-74)
     V3<T> camO, camLL, camH, camV;
     uint32_t W = 0, H = 0;
@@ -598,10 +603,76 @@ bool ssSampleGGX(V3<T> wo, T ux, T uy, T a2, V3<T> F0, V3<T>& wi) {  // :516-549
     return pdfRefl(wh.z, a2, dvh) > T(0) && !f.black();
 }
 
+// Dielectric glass sampling (StandardSurface.h:245-340): smooth (delta) Fresnel
+// reflection / Snell refraction, or a GGX half-vector then Fresnel reflection
+// / Walter transmission with importance transport.
+template <class T>
+BS<T> glassSample(const Mat<T>& m, const Ctx<T>& c, V3<T> wol, T ux, T uy, T uc) {
+    T eta = c.front ? m.ior : (T(1) / m.ior);
+    T cosI = wol.z;
+    BS<T> s;
+    if (m.rough < T(0.001f)) {
+        T Fr = fresnel(cosI, eta);
+        if (uc < Fr) {
+            s.wi = c.toWorld(V3<T>(-wol.x, -wol.y, wol.z));
+            s.f = m.albedo * Fr;
+            s.pdf = Fr;
+            s.flags = 4u | 16u;
+        } else {
+            T sin2T = std::max(T(0), T(1) - cosI * cosI) / (eta * eta);
+            T cosT = std::sqrt(std::max(T(0), T(1) - sin2T));
+            s.wi = c.toWorld(V3<T>(-wol.x / eta, -wol.y / eta, -cosT));
+            s.f = m.albedo * (T(1) - Fr);
+            s.pdf = T(1) - Fr;
+            s.flags = 4u | 8u;
+        }
+        return s;
+    }
+    T alpha = std::max(T(1e-4f), m.rough * m.rough);
+    T alpha2 = alpha * alpha;
+    V3<T> wh = sampleH(ux, uy, alpha2);
+    if (wh.z <= T(0)) return {};
+    T cosIH = std::max(T(0), dot(wol, wh));
+    if (cosIH <= T(0)) return {};
+    T Fr = fresnel(cosIH, eta);
+    if (uc < Fr) {
+        V3<T> wil = wh * (T(2) * cosIH) - wol;
+        if (wil.z <= T(0)) return {};
+        T D = D_GGX(wh.z, alpha2);
+        T G = G2(wol.z, wil.z, alpha2);
+        T cosO = wol.z;
+        V3<T> bsdf = V3<T>(Fr, Fr, Fr) * (D * G / (T(4) * cosO));
+        s.wi = c.toWorld(wil);
+        s.f = bsdf * m.albedo;
+        s.pdf = Fr * pdfRefl(wh.z, alpha2, cosIH);
+        s.flags = 2u | 16u;
+        return s;
+    }
+    T sin2T = std::max(T(0), T(1) - cosIH * cosIH) / (eta * eta);
+    if (sin2T >= T(1)) return {};
+    T cosTH = std::sqrt(T(1) - sin2T);
+    V3<T> wil = wol * (T(-1) / eta) + wh * (cosIH / eta - cosTH);
+    if (wil.z >= T(0)) return {};
+    T cosO = wol.z, cosIt = std::abs(wil.z);
+    T D = D_GGX(wh.z, alpha2);
+    T G = G2(cosO, cosIt, alpha2);
+    T denom = cosIH + eta * std::abs(dot(wil, wh));
+    if (denom < T(1e-6f)) return {};
+    T absCosTwh = std::abs(dot(wil, wh));
+    T pdfWh = D * wh.z;
+    T jac = eta * eta * absCosTwh / (denom * denom);
+    s.wi = c.toWorld(wil);
+    s.f = m.albedo * ((T(1) - Fr) * D * G * cosIH * absCosTwh / (cosO * denom * denom));
+    s.pdf = (T(1) - Fr) * pdfWh * jac;
+    s.flags = 2u | 8u;
+    return s;
+}
+
 template <class T>
 BS<T> ssSample(const Mat<T>& m, const Ctx<T>& c, V3<T> wo, T ux, T uy, T uc) {  // :231-405
     V3<T> wol = c.toLocal(wo);
     if (wol.z <= T(0)) return {};
+    if (m.transmission > T(0.001f) && m.metal < T(0.001f)) return glassSample(m, c, wol, ux, uy, uc);
     W4<T> w;
     if (!ssWeights(m, wol.z, w)) return {};
     T a = std::max(T(1e-4f), m.rough * m.rough), a2 = a * a;
@@ -631,10 +702,47 @@ BS<T> ssSample(const Mat<T>& m, const Ctx<T>& c, V3<T> wo, T ux, T uy, T uc) {  
 }
 
 template <class T>
-BE<T> ssEval(const Mat<T>& m, const Ctx<T>& c, V3<T> wo, V3<T> wi) {  // :410-504 (opaque)
+BE<T> ssEval(const Mat<T>& m, const Ctx<T>& c, V3<T> wo, V3<T> wi) {  // :410-504
     V3<T> wol = c.toLocal(wo), wil = c.toLocal(wi);
     BE<T> e;
-    if (!(wol.z * wil.z > T(0))) return e;
+    if (!(wol.z * wil.z > T(0))) {
+        // rough dielectric transmission (StandardSurface.h:414-442): its alpha
+        // is rough^4 without the 1e-4 clamp
+        if (m.transmission < T(0.001f) || m.rough < T(0.001f) || m.metal > T(0.001f)) return e;
+        T eta = c.front ? m.ior : (T(1) / m.ior);
+        T alpha2 = m.rough * m.rough;
+        alpha2 *= alpha2;
+        V3<T> wh = safeNormalize(wol + wil * eta);
+        if (wh.z < T(0)) wh = -wh;
+        T cosIH = std::max(T(0), dot(wol, wh));
+        T cosTH = std::abs(dot(wil, wh));
+        T Fr = fresnel(cosIH, eta);
+        T D = D_GGX(wh.z, alpha2);
+        T G = G2(wol.z, std::abs(wil.z), alpha2);
+        T denom = cosIH + eta * cosTH;
+        if (denom < T(1e-6f)) return e;
+        T bs = (T(1) - Fr) * D * G * cosIH * cosTH / (wol.z * std::abs(wil.z) * denom * denom);
+        T jac = eta * eta * cosTH / (denom * denom);
+        e.f = m.albedo * bs;
+        e.pdf = (T(1) - Fr) * D * wh.z * jac;
+        return e;
+    }
+    if (m.transmission > T(0.001f) && m.metal < T(0.001f)) {  // glass reflection (:455-473)
+        if (m.rough < T(0.001f)) return e;
+        T alpha = std::max(T(1e-4f), m.rough * m.rough);
+        T alpha2 = alpha * alpha;
+        T eta = c.front ? m.ior : (T(1) / m.ior);
+        V3<T> wh = safeNormalize(wol + wil);
+        if (wh.z < T(0)) return e;
+        T cosIH = std::max(T(0), dot(wol, wh));
+        T Fr = fresnel(cosIH, eta);
+        T D = D_GGX(wh.z, alpha2);
+        T G = G2(wol.z, wil.z, alpha2);
+        T pdf = Fr > T(0) ? Fr * pdfRefl(wh.z, alpha2, cosIH) : T(0);
+        e.f = m.albedo * (Fr * D * G / (T(4) * wol.z * wil.z));
+        e.pdf = pdf;
+        return e;
+    }
     W4<T> w;
     if (!ssWeights(m, wol.z, w)) return e;
     e.f = ssCombined(m, wol, wil, w, e.pdf);
@@ -986,7 +1094,32 @@ template <class T> const Mat<T>* matOf(const Scene<T>& S, uint32_t slot) {
     return &S.mats[size_t(S.slots[slot])];
 }
 
-// PathIntegrator::Li + estimateDirect (PathIntegrator.cpp:71-265), opaque scenes.
+// shadowTransmittance (ShadowRay.h:26-61): closest hits through at most 8
+// surfaces, multiplying their transmittanceColor; an opaque one blocks. In a
+// scene without transmissive materials this is the any-hit query.
+template <class T>
+V3<T> shadowTr(const Scene<T>& S, Ray<T> r) {
+    V3<T> Tr(1, 1, 1);
+    if (!S.transmit) return trace(S, r, true).hit ? V3<T>() : Tr;
+    for (int i = 0; i < 8; ++i) {
+        Hit<T> h = trace(S, r);
+        if (!h.hit) break;
+        SI<T> si = surface(S, r, h);
+        const Mat<T>* m = matOf(S, si.slot);
+        if (!m) return {};
+        if (m->tint.black()) return {};
+        Tr = Tr * m->tint;
+        if (Tr.black()) return {};
+        T remaining = r.tmax - h.t;
+        if (remaining <= T(1e-4f)) break;
+        r = spawnRay(si.p, si.ng, r.d);
+        r.tmax = remaining - T(1e-4f);
+    }
+    return Tr;
+}
+
+// PathIntegrator::Li + estimateDirect (PathIntegrator.cpp:71-265), static scenes
+// (opaque, glass and alpha-masked materials).
 template <class T>
 V3<T> Li(const Scene<T>& S, Ray<T> r, Halton& smp, uint32_t maxDepth, uint32_t minDepth = 2) {
     V3<T> L, beta(1, 1, 1);
@@ -1004,6 +1137,12 @@ V3<T> Li(const Scene<T>& S, Ray<T> r, Halton& smp, uint32_t maxDepth, uint32_t m
         if (!m) break;
         V3<T> wo = -r.d;
         Ctx<T> c(si, r.d);
+        // alpha test (PathIntegrator.cpp:103-118): a sample dimension only for
+        // partial opacity; a cut-out point continues the ray, one bounce later
+        if (m->opacity <= T(0) || (m->opacity < T(1) && T(smp.get1D()) >= m->opacity)) {
+            r = spawnRay(si.p, si.ng, r.d);
+            continue;
+        }
         if (!m->emission.black() && (bounce == 0 || spec)) L = L + beta * m->emission;
         if (!m->delta && nL > 0) {
             uint32_t li = std::min(uint32_t(smp.get1D() * float(nL)), nL - 1);
@@ -1017,11 +1156,12 @@ V3<T> Li(const Scene<T>& S, Ray<T> r, Halton& smp, uint32_t maxDepth, uint32_t m
                     BE<T> be = matEval(*m, c, wo, ls.wi);
                     if (!be.f.black()) {
                         Ray<T> sr = spawnRayTo(si.p, si.n, si.p + ls.wi * ls.dist);
-                        if (!trace(S, sr, true).hit) {
+                        V3<T> Tr = shadowTr(S, sr);
+                        if (!Tr.black()) {
                             T w = lt.type == 2 ? T(1) : powerH(ls.pdf, be.pdf);
                             T cosI = si.curve ? std::sqrt(std::max(T(0), T(1) - dot(ls.wi, c.t) * dot(ls.wi, c.t)))
                                               : std::abs(dot(ls.wi, si.n));
-                            Ld = Ld + be.f * ls.Li * cosI * w / ls.pdf;
+                            Ld = Ld + be.f * ls.Li * Tr * cosI * w / ls.pdf;
                         }
                     }
                 }
@@ -1036,15 +1176,39 @@ V3<T> Li(const Scene<T>& S, Ray<T> r, Halton& smp, uint32_t maxDepth, uint32_t m
                         T w = bs.delta() ? T(1) : powerH(bs.pdf, lp);
                         Ray<T> mr = spawnRay(si.p, si.ng, bs.wi);
                         mr.tmax = T(1e10f);
-                        Hit<T> mh = trace(S, mr);
+                        // the first non-transmissive surface, through at most 8
+                        // transmissive ones (PathIntegrator.cpp:220-244)
+                        V3<T> Tr(1, 1, 1);
+                        Hit<T> mh;
+                        SI<T> ms;
+                        for (int k = 0; k < 8; ++k) {
+                            mh = trace(S, mr);
+                            if (!mh.hit) break;
+                            ms = surface(S, mr, mh);
+                            const Mat<T>* tm = matOf(S, ms.slot);
+                            if (!tm) {
+                                Tr = V3<T>();
+                                break;
+                            }
+                            if (tm->tint.black()) break;
+                            Tr = Tr * tm->tint;
+                            if (Tr.black()) break;
+                            T remaining = mr.tmax - mh.t;
+                            if (remaining <= T(1e-4f)) {
+                                mh.hit = false;
+                                break;
+                            }
+                            mr = spawnRay(ms.p, ms.ng, mr.d);
+                            mr.tmax = remaining - T(1e-4f);
+                        }
                         V3<T> Lm;
                         if (!mh.hit) Lm = envLe(S, bs.wi);
                         else {
-                            SI<T> ms = surface(S, mr, mh);
                             const Mat<T>* hm = matOf(S, ms.slot);
                             if (hm) Lm = hm->emission;
                         }
-                        if (!Lm.black()) Ld = Ld + bs.f * Lm * std::abs(dot(bs.wi, si.n)) * w / bs.pdf;
+                        if (!Lm.black() && !Tr.black())
+                            Ld = Ld + bs.f * Lm * Tr * std::abs(dot(bs.wi, si.n)) * w / bs.pdf;
                     }
                 }
             }
@@ -1372,6 +1536,9 @@ void add_mesh(Scene<T>& S, uint32_t meshID, const float* pos, const float* nrm, 
 
 template <class T>
 void commit(Scene<T>& S) {
+    S.transmit = false;
+    for (int slot : S.slots)
+        if (slot >= 0 && size_t(slot) < S.mats.size() && !S.mats[size_t(slot)].tint.black()) S.transmit = true;
     build_bvh(uint32_t(S.tris.size()), [&](uint32_t i, float* b) {
         const Tri<T>& t = S.tris[i];
         V3<T> v[3] = {t.v0, t.v0 + t.e1, t.v0 + t.e2};
@@ -1557,12 +1724,24 @@ int po_add_material(void* p, int type, const float* a3, const float* e3, const f
             m.f0 = r * r;
             T rc = (T(1) - T(1.5f)) / (T(1) + T(1.5f));
             m.coatF0 = rc * rc;
+            m.transmission = T(p18[13]);
+            m.alphaMask = p18[18] != 0.f;
+            m.opacity = m.alphaMask ? T(p18[19]) : T(1);
+            if (m.alphaMask) {  // transmittanceColor (StandardSurface.h:207-218)
+                T t = T(1) - m.opacity;
+                if (t > T(0)) m.tint = V3<T>(t, t, t);
+            } else if (m.transmission >= T(0.001f) && !(m.metal > T(0.001f))) {
+                T Fr = fresnel(T(1), m.ior);
+                m.tint = m.albedo * (m.transmission * (T(1) - Fr));
+            }
             uint32_t f = 16u;
+            if (m.transmission > T(0.001f)) f |= 8u;
             if (m.rough < T(0.001f)) f |= 4u;
             else if (m.rough < T(0.3f)) f |= 2u;
             else f |= 1u;
             m.flags = f;
-            m.delta = m.rough < T(0.001f) && (m.metal > T(0.999f) || m.spec > T(0));
+            m.delta = (m.rough < T(0.001f) && m.transmission > T(0.001f) && m.metal < T(0.001f)) ||
+                      (m.rough < T(0.001f) && (m.metal > T(0.999f) || m.spec > T(0)));
         } else {  // MarschnerHair.h:200-216
             m.eta = T(hair8[0]);
             m.sigma = ld<T>(hair8 + 1);

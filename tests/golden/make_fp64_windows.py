@@ -43,6 +43,7 @@ def frames():
                        [(936, 516, 984, 564), (1500, 750, 1548, 798)]),
         "hair": (lambda: S.hair(1280, 720, 32, 10), [(500, 350, 548, 398)]),
         "differentiable": (lambda: S.differentiable(512, 512, 16, 8), [(248, 184, 376, 312)]),
+        "glass": (lambda: S.glass(1280, 720, 16, 8), [(540, 280, 588, 328)]),
     }
 
 

@@ -33,6 +33,7 @@ FRAMES = {
     "throughput": lambda: S.throughput(1920, 1080, 64, 12),
     "hair": lambda: S.hair(1280, 720, 32, 10),
     "differentiable": lambda: S.differentiable(512, 512, 16, 8),
+    "glass": lambda: S.glass(1280, 720, 16, 8),
 }
 
 

@@ -5,6 +5,8 @@ row (the second call must not see anything the first left in the scratch).
 
 The file sorts last so that it runs after every other GPU test has used the
 device; it also passes alone in a fresh process."""
+import os
+
 import numpy as np
 import pytest
 
@@ -36,15 +38,22 @@ def same_hits(a, b):
         np.testing.assert_allclose(a[f][hit], b[f][hit], rtol=1e-6, atol=0)
 
 
-@pytest.fixture(scope="module", params=["cornell", "hair"])
+@pytest.fixture(scope="module", params=["cornell", "hair", "motion"])
 def scene_renderer(gpu, request):
+    """A static mesh scene, a curve scene, and a scene with motion-blurred
+    meshes (whose traversal always takes the persistent schedule, with its work
+    counter in the scratch); rays carry time 0 in both entry points."""
     r = api.Renderer()
     if request.param == "cornell":
         r.upload(S.cornell(64, 64, 1))
         lo, hi = 0.02, 0.98
-    else:
+    elif request.param == "hair":
         r.upload(S.hair(64, 36, 1, 4, n_strands=20000))
         lo, hi = -1.5, 1.5
+    else:
+        sc = S.motion(64, 36, 1, 4)
+        r.upload(sc)
+        lo, hi = float(sc.positions.min()), float(sc.positions.max())
     yield r, lo, hi
     r.close()
 
@@ -100,3 +109,35 @@ def test_noalloc_empty_and_no_scene(gpu):
         assert len(r.trace_noalloc(np.zeros((0, 8), np.float32))) == 0
     finally:
         r.close()
+
+
+def test_noalloc_matches_the_reference_goldens(gpu):
+    """Closest hits of the committed reference rays on the Cornell scene
+    (tests/golden/reference_vectors.npz, from the reference's BVHBackend)."""
+    gold = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_vectors.npz"))
+    r = api.Renderer()
+    try:
+        r.upload(S.cornell())
+        for _ in range(2):
+            h = r.trace_noalloc(gold["cornell_rays"])
+            ids = np.stack([h["hit"], h["mesh_id"], h["prim_id"], h["strand_id"]], 1)
+            assert np.array_equal(ids, gold["cornell_ids"])
+            hit = gold["cornell_ids"][:, 0] == 1
+            assert np.array_equal(h["t"][hit], gold["cornell_t"][hit])
+    finally:
+        r.close()
+
+
+def test_noalloc_allocates_no_device_memory(scene_renderer):
+    """After a first call (the scratch address looked up, every kernel
+    loaded), further calls leave the device's free memory unchanged."""
+    torch = pytest.importorskip("torch")
+    r, lo, hi = scene_renderer
+    rays = seeded_rays(9, 20000, lo, hi)
+    r.trace_noalloc(rays)
+    torch.cuda.synchronize()
+    before = torch.cuda.mem_get_info()[0]
+    for k in range(4):
+        r.trace_noalloc(rays, occlusion=bool(k & 1))
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == before
