@@ -467,7 +467,7 @@ def bench_configs(local, cpu_s=0.0):
         ("glass_1280x720x16", "glass: smooth and rough dielectric spheres and panes, alpha-masked cards, "
          "directional + area light; depth 8", S.glass(1280, 720, 16, 8), 1 << 25, "glass", False),
         ("motion_1280x720x16", "motion blur: object-space meshes with 2-3 motion keys, shutter [0, 1]; depth 6",
-         S.motion(1280, 720, 16, 6), 1 << 25, None, False),
+         S.motion(1280, 720, 16, 6), 1 << 25, "motion", False),
     ]
     for key, what, sc, chunk, fp64, port in cases:
         if key.startswith("hair"):

@@ -51,7 +51,90 @@ template <class T>
 struct Tri {
     V3<T> v0, e1, e2, n, sn0, sn1, sn2;
     uint32_t mesh, prim;
+    bool objectSpace = false;  // a motion-blurred mesh's triangle (its keys: Scene::motion[mesh])
 };
+
+// Mat4f (include/anacapa/core/Types.h:144-229): the operations motion blur uses.
+template <class T>
+struct M4 {
+    T m[4][4] = {};
+    static M4 identity() {
+        M4 r;
+        for (int i = 0; i < 4; ++i) r.m[i][i] = T(1);
+        return r;
+    }
+    V3<T> point(V3<T> p) const {
+        T x = m[0][0] * p.x + m[0][1] * p.y + m[0][2] * p.z + m[0][3];
+        T y = m[1][0] * p.x + m[1][1] * p.y + m[1][2] * p.z + m[1][3];
+        T z = m[2][0] * p.x + m[2][1] * p.y + m[2][2] * p.z + m[2][3];
+        T w = m[3][0] * p.x + m[3][1] * p.y + m[3][2] * p.z + m[3][3];
+        return {x / w, y / w, z / w};
+    }
+    V3<T> vector(V3<T> v) const {
+        return {m[0][0] * v.x + m[0][1] * v.y + m[0][2] * v.z, m[1][0] * v.x + m[1][1] * v.y + m[1][2] * v.z,
+                m[2][0] * v.x + m[2][1] * v.y + m[2][2] * v.z};
+    }
+    V3<T> normal(V3<T> n) const {  // the transpose, as transformNormal computes it
+        return {m[0][0] * n.x + m[1][0] * n.y + m[2][0] * n.z, m[0][1] * n.x + m[1][1] * n.y + m[2][1] * n.z,
+                m[0][2] * n.x + m[1][2] * n.y + m[2][2] * n.z};
+    }
+    static M4 lerp(const M4& a, const M4& b, T t) {
+        M4 r;
+        for (int i = 0; i < 4; ++i)
+            for (int j = 0; j < 4; ++j) r.m[i][j] = a.m[i][j] * (T(1) - t) + b.m[i][j] * t;
+        return r;
+    }
+    M4 inverse() const {  // Gauss-Jordan with partial pivoting; identity when singular
+        T a[4][8];
+        for (int i = 0; i < 4; ++i) {
+            for (int j = 0; j < 4; ++j) a[i][j] = m[i][j];
+            for (int j = 0; j < 4; ++j) a[i][j + 4] = (i == j) ? T(1) : T(0);
+        }
+        for (int col = 0; col < 4; ++col) {
+            int pivot = col;
+            for (int row = col + 1; row < 4; ++row)
+                if (std::abs(a[row][col]) > std::abs(a[pivot][col])) pivot = row;
+            if (pivot != col)
+                for (int j = 0; j < 8; ++j) std::swap(a[col][j], a[pivot][j]);
+            T diag = a[col][col];
+            if (std::abs(diag) < T(1e-10f)) return identity();
+            T invDiag = T(1) / diag;
+            for (int j = 0; j < 8; ++j) a[col][j] *= invDiag;
+            for (int row = 0; row < 4; ++row) {
+                if (row == col) continue;
+                T factor = a[row][col];
+                for (int j = 0; j < 8; ++j) a[row][j] -= factor * a[col][j];
+            }
+        }
+        M4 r;
+        for (int i = 0; i < 4; ++i)
+            for (int j = 0; j < 4; ++j) r.m[i][j] = a[i][j + 4];
+        return r;
+    }
+};
+
+// A motion key (MotionKey, GeometryPool.h:16-20).
+template <class T>
+struct Key {
+    T time = 0;
+    M4<T> o2w;
+};
+
+// MeshDesc::interpolateO2W (GeometryPool.h:51-65): piecewise-linear in the keys.
+template <class T>
+M4<T> interpO2W(const std::vector<Key<T>>& k, T t) {
+    if (k.size() == 1) return k[0].o2w;
+    if (t <= k.front().time) return k.front().o2w;
+    if (t >= k.back().time) return k.back().o2w;
+    size_t lo = 0, hi = k.size() - 1;
+    while (hi - lo > 1) {
+        size_t mid = (lo + hi) / 2;
+        if (k[mid].time <= t) lo = mid;
+        else hi = mid;
+    }
+    T alpha = (t - k[lo].time) / (k[hi].time - k[lo].time);
+    return M4<T>::lerp(k[lo].o2w, k[hi].o2w, alpha);
+}
 
 template <class T>
 struct Seg {
@@ -153,6 +236,8 @@ struct Scene {
     Dist1D<T> marg;
     V3<T> envRadiance;
     bool transmit = false;  // a material passes shadow rays (non-black transmittanceColor)
+    std::vector<std::vector<Key<T>>> motion;  // per meshID: its keys (empty: static)
+    T shutterOpen = 0, shutterClose = 0;
     // camera (Camera::makePinhole, IIntegrator.h:49-74)
     V3<T> camO, camLL, camH, camV;
     uint32_t W = 0, H = 0;
@@ -344,7 +429,19 @@ Hit<T> trace(const Scene<T>& S, const Ray<T>& r, bool any = false) {
             if (nd.count) {
                 for (uint32_t i = nd.start; i < nd.start + nd.count; ++i) {
                     T t, u, v;
-                    if (tri_hit(S.tris[S.triIdx[i]], r, closest, t, u, v)) {
+                    const Tri<T>& tr = S.tris[S.triIdx[i]];
+                    bool ok;
+                    if (tr.objectSpace) {  // BVHBackend.cpp:356-367
+                        M4<T> w2o = interpO2W(S.motion[tr.mesh], r.time).inverse();
+                        Ray<T> ro;
+                        ro.o = w2o.point(r.o);
+                        ro.d = w2o.vector(r.d);
+                        ro.tmin = r.tmin;
+                        ok = tri_hit(tr, ro, closest, t, u, v);
+                    } else {
+                        ok = tri_hit(tr, r, closest, t, u, v);
+                    }
+                    if (ok) {
                         closest = t;
                         h.hit = true;
                         h.t = t;
@@ -412,11 +509,22 @@ SI<T> surface(const Scene<T>& S, const Ray<T>& r, const Hit<T>& h) {
     if (!h.curve) {  // fillSurfaceInteraction (BVHBackend.cpp:285-317)
         const Tri<T>& tr = S.tris[h.idx];
         T w = T(1) - h.u - h.v;
-        si.p = tr.v0 + tr.e1 * h.u + tr.e2 * h.v;
-        si.ng = tr.n;
-        si.n = safeNormalize(tr.sn0 * w + tr.sn1 * h.u + tr.sn2 * h.v);
+        if (tr.objectSpace) {  // the object-space triangle taken to the world at the ray's time
+            M4<T> o2w = interpO2W(S.motion[tr.mesh], r.time);
+            V3<T> pObj = tr.v0 + tr.e1 * h.u + tr.e2 * h.v;
+            V3<T> nObj = safeNormalize(cross(tr.e1, tr.e2));
+            V3<T> snObj = safeNormalize(tr.sn0 * w + tr.sn1 * h.u + tr.sn2 * h.v);
+            si.p = o2w.point(pObj);
+            si.ng = safeNormalize(o2w.normal(nObj));
+            si.n = safeNormalize(o2w.normal(snObj));
+            si.dpdu = o2w.vector(tr.e1);
+        } else {
+            si.p = tr.v0 + tr.e1 * h.u + tr.e2 * h.v;
+            si.ng = tr.n;
+            si.n = safeNormalize(tr.sn0 * w + tr.sn1 * h.u + tr.sn2 * h.v);
+            si.dpdu = tr.e1;
+        }
         if (dot(si.n, si.ng) < T(0)) si.n = -si.n;
-        si.dpdu = tr.e1;
         si.slot = tr.mesh;
         si.mesh = tr.mesh;
         si.prim = tr.prim;
@@ -1112,8 +1220,10 @@ V3<T> shadowTr(const Scene<T>& S, Ray<T> r) {
         if (Tr.black()) return {};
         T remaining = r.tmax - h.t;
         if (remaining <= T(1e-4f)) break;
+        const T time = r.time;
         r = spawnRay(si.p, si.ng, r.d);
         r.tmax = remaining - T(1e-4f);
+        r.time = time;
     }
     return Tr;
 }
@@ -1122,6 +1232,7 @@ V3<T> shadowTr(const Scene<T>& S, Ray<T> r) {
 // (opaque, glass and alpha-masked materials).
 template <class T>
 V3<T> Li(const Scene<T>& S, Ray<T> r, Halton& smp, uint32_t maxDepth, uint32_t minDepth = 2) {
+    const T time = r.time;  // every ray of the path sees the scene at the camera ray's time
     V3<T> L, beta(1, 1, 1);
     bool spec = false;
     const uint32_t nL = uint32_t(S.lights.size());
@@ -1141,6 +1252,7 @@ V3<T> Li(const Scene<T>& S, Ray<T> r, Halton& smp, uint32_t maxDepth, uint32_t m
         // partial opacity; a cut-out point continues the ray, one bounce later
         if (m->opacity <= T(0) || (m->opacity < T(1) && T(smp.get1D()) >= m->opacity)) {
             r = spawnRay(si.p, si.ng, r.d);
+            r.time = time;
             continue;
         }
         if (!m->emission.black() && (bounce == 0 || spec)) L = L + beta * m->emission;
@@ -1156,6 +1268,7 @@ V3<T> Li(const Scene<T>& S, Ray<T> r, Halton& smp, uint32_t maxDepth, uint32_t m
                     BE<T> be = matEval(*m, c, wo, ls.wi);
                     if (!be.f.black()) {
                         Ray<T> sr = spawnRayTo(si.p, si.n, si.p + ls.wi * ls.dist);
+                        sr.time = time;
                         V3<T> Tr = shadowTr(S, sr);
                         if (!Tr.black()) {
                             T w = lt.type == 2 ? T(1) : powerH(ls.pdf, be.pdf);
@@ -1176,6 +1289,7 @@ V3<T> Li(const Scene<T>& S, Ray<T> r, Halton& smp, uint32_t maxDepth, uint32_t m
                         T w = bs.delta() ? T(1) : powerH(bs.pdf, lp);
                         Ray<T> mr = spawnRay(si.p, si.ng, bs.wi);
                         mr.tmax = T(1e10f);
+                        mr.time = time;
                         // the first non-transmissive surface, through at most 8
                         // transmissive ones (PathIntegrator.cpp:220-244)
                         V3<T> Tr(1, 1, 1);
@@ -1200,6 +1314,7 @@ V3<T> Li(const Scene<T>& S, Ray<T> r, Halton& smp, uint32_t maxDepth, uint32_t m
                             }
                             mr = spawnRay(ms.p, ms.ng, mr.d);
                             mr.tmax = remaining - T(1e-4f);
+                            mr.time = time;
                         }
                         V3<T> Lm;
                         if (!mh.hit) Lm = envLe(S, bs.wi);
@@ -1221,6 +1336,7 @@ V3<T> Li(const Scene<T>& S, Ray<T> r, Halton& smp, uint32_t maxDepth, uint32_t m
         spec = bs.delta();
         beta = beta * (bs.f / bs.pdf);
         r = spawnRay(si.p, si.n, bs.wi);
+        r.time = time;
         if (bounce >= minDepth) {
             T q = T(1) - std::min(beta.maxc(), T(0.95f));
             if (T(smp.get1D()) < q) break;
@@ -1447,13 +1563,14 @@ V3<T> LiGrad(const Scene<T>& S, Ray<T> r, Halton& smp, uint32_t maxDepth, PathGr
 }
 
 // Camera::generateRay (IIntegrator.h:90-109), pinhole.
-template <class T> Ray<T> cameraRay(const Scene<T>& S, uint32_t px, uint32_t py, T jx, T jy) {
+template <class T> Ray<T> cameraRay(const Scene<T>& S, uint32_t px, uint32_t py, T jx, T jy, T timeU = 0) {
     T s = (T(px) + jx) / T(S.W);
     T t = (T(S.H - 1 - py) + jy) / T(S.H);
     V3<T> target = S.camLL + S.camH * s + S.camV * t;
     Ray<T> r;
     r.o = S.camO;
     r.d = normalize(target - S.camO);
+    r.time = S.shutterOpen + timeU * (S.shutterClose - S.shutterOpen);  // Camera::generateRay
     return r;
 }
 
@@ -1465,8 +1582,8 @@ V3<T> sampleLi(const Scene<T>& S, uint32_t px, uint32_t py, uint32_t sIdx, uint3
     T jx = T(h.get1D()), jy = T(h.get1D());
     h.get1D();
     h.get1D();
-    h.get1D();
-    return Li(S, cameraRay(S, px, py, jx, jy), h, maxDepth);
+    T tu = T(h.get1D());
+    return Li(S, cameraRay(S, px, py, jx, jy, tu), h, maxDepth);
 }
 
 // Per-row sums of the path gradients of a frame, weighted by dLoss/dL =
@@ -1534,6 +1651,25 @@ void add_mesh(Scene<T>& S, uint32_t meshID, const float* pos, const float* nrm, 
     }
 }
 
+// A motion-blurred mesh (MeshDesc with motionKeys): object-space triangles
+// and nkeys keys of 17 floats (time, objectToWorld row-major).
+template <class T>
+void add_mesh_motion(Scene<T>& S, uint32_t meshID, const float* pos, const float* nrm, uint32_t nv,
+                     const uint32_t* idx, uint32_t ntri, const float* keys, uint32_t nkeys) {
+    const size_t first = S.tris.size();
+    add_mesh(S, meshID, pos, nrm, nv, idx, ntri);
+    for (size_t i = first; i < S.tris.size(); ++i) S.tris[i].objectSpace = nkeys > 0;
+    if (S.motion.size() <= meshID) S.motion.resize(meshID + 1);
+    S.motion[meshID].clear();
+    for (uint32_t k = 0; k < nkeys; ++k) {
+        Key<T> key;
+        key.time = T(keys[17 * k]);
+        for (int i = 0; i < 4; ++i)
+            for (int j = 0; j < 4; ++j) key.o2w.m[i][j] = T(keys[17 * k + 1 + 4 * i + j]);
+        S.motion[meshID].push_back(key);
+    }
+}
+
 template <class T>
 void commit(Scene<T>& S) {
     S.transmit = false;
@@ -1542,10 +1678,28 @@ void commit(Scene<T>& S) {
     build_bvh(uint32_t(S.tris.size()), [&](uint32_t i, float* b) {
         const Tri<T>& t = S.tris[i];
         V3<T> v[3] = {t.v0, t.v0 + t.e1, t.v0 + t.e2};
-        for (int a = 0; a < 3; ++a) {
-            b[a] = float(std::min({v[0][a], v[1][a], v[2][a]}));
-            b[3 + a] = float(std::max({v[0][a], v[1][a], v[2][a]}));
+        if (!t.objectSpace) {
+            for (int a = 0; a < 3; ++a) {
+                b[a] = float(std::min({v[0][a], v[1][a], v[2][a]}));
+                b[3 + a] = float(std::max({v[0][a], v[1][a], v[2][a]}));
+            }
+            return;
         }
+        // a moving triangle: its world positions at every key bound it over
+        // the shutter (the keys' matrices are affine and lerped, so each
+        // vertex moves linearly between keys; BVHBackend.cpp:86-95)
+        for (int a = 0; a < 3; ++a) {
+            b[a] = INFINITY;
+            b[3 + a] = -INFINITY;
+        }
+        for (const Key<T>& k : S.motion[t.mesh])
+            for (const V3<T>& p : v) {
+                V3<T> w = k.o2w.point(p);
+                for (int a = 0; a < 3; ++a) {
+                    b[a] = std::min(b[a], std::nextafter(float(w[a]), -INFINITY));
+                    b[3 + a] = std::max(b[3 + a], std::nextafter(float(w[a]), INFINITY));
+                }
+            }
     }, S.triNodes, S.triIdx);
     S.segs.clear();
     S.strandColor.clear();
@@ -1678,6 +1832,26 @@ void po_add_mesh(void* p, uint32_t meshID, const float* pos, const float* nrm, u
     Handle* h = static_cast<Handle*>(p);
     if (h->precision == 64) add_mesh(h->d, meshID, pos, nrm, nv, idx, ntri);
     else add_mesh(h->f, meshID, pos, nrm, nv, idx, ntri);
+}
+
+void po_add_mesh_motion(void* p, uint32_t meshID, const float* pos, const float* nrm, uint32_t nv,
+                        const uint32_t* idx, uint32_t ntri, const float* keys, uint32_t nkeys) {
+    Handle* h = static_cast<Handle*>(p);
+    if (h->precision == 64) add_mesh_motion(h->d, meshID, pos, nrm, nv, idx, ntri, keys, nkeys);
+    else add_mesh_motion(h->f, meshID, pos, nrm, nv, idx, ntri, keys, nkeys);
+}
+
+// Camera::shutterOpen / shutterClose (normalized): each path's time is
+// shutterOpen + u * (shutterClose - shutterOpen), u its sample dimension 4.
+void po_set_shutter(void* p, float open, float close) {
+    Handle* h = static_cast<Handle*>(p);
+    auto set = [&](auto& S) {
+        using T = std::decay_t<decltype(S.env[0])>;
+        S.shutterOpen = T(open);
+        S.shutterClose = T(close);
+    };
+    if (h->precision == 64) set(h->d);
+    else set(h->f);
 }
 
 void po_add_strand(void* p, const float* cps, uint32_t ncp, const float* widths, uint32_t nw, uint32_t slot,

@@ -66,6 +66,7 @@ template <class T>
 struct Ray {
     V3<T> o, d;
     T tmin = T(1e-4f), tmax = std::numeric_limits<T>::infinity();
+    T time = 0;  // normalized shutter time (motion-blurred meshes)
 };
 
 // spawnRay / spawnRayTo (Types.h:269-284)

@@ -1,8 +1,8 @@
 """TEST INFRASTRUCTURE — ctypes binding of the CPU restatement
 (oracle/restate/pt_oracle.cpp, built by `make -C oracle restate` into
 oracle/_build/libpt_oracle.so). precision=32 reproduces the reference's float
-arithmetic; precision=64 is the FP64 oracle. It covers static scenes (opaque,
-glass and alpha-masked materials); motion-blurred meshes are rejected."""
+arithmetic; precision=64 is the FP64 oracle. It covers opaque, glass and
+alpha-masked materials and motion-blurred meshes."""
 from __future__ import annotations
 
 import ctypes as C
@@ -39,6 +39,8 @@ def lib():
         L.po_scene_free.argtypes = [_P]
         L.po_add_mesh.argtypes = [_P, C.c_uint32, _F, _F, C.c_uint32, _U32, C.c_uint32]
         L.po_add_strand.argtypes = [_P, _F, C.c_uint32, _F, C.c_uint32, C.c_uint32, _F]
+        L.po_add_mesh_motion.argtypes = [_P, C.c_uint32, _F, _F, C.c_uint32, _U32, C.c_uint32, _F, C.c_uint32]
+        L.po_set_shutter.argtypes = [_P, C.c_float, C.c_float]
         L.po_add_material.argtypes = [_P, C.c_int, _F, _F, _F, _F]
         L.po_set_slots.argtypes = [_P, _I32, C.c_uint32]
         L.po_light_area.argtypes = [_P, _F, _F, _F, _F]
@@ -77,8 +79,6 @@ class PoScene:
         from anacapa_b200 import scenes as S
         L = self.L = lib()
         self.scene = scene
-        if scene.mesh_motion is not None and any(k for k in scene.mesh_motion):
-            raise NotImplementedError("the restatement covers static meshes")
         h = self.h = L.po_scene_new(precision)
         for m in scene.materials:
             if m.type in (S.MAT_LAMBERT, S.MAT_EMISSIVE):
@@ -93,7 +93,13 @@ class PoScene:
             p = f32(scene.positions[vo[i]:vo[i + 1]])
             n = f32(scene.normals[vo[i]:vo[i + 1]]) if scene.mesh_has_normals[i] else None
             idx = np.ascontiguousarray(scene.indices[to[i]:to[i + 1]], np.uint32)
-            L.po_add_mesh(h, i, _fp(p), _fp(n), len(p), idx.ctypes.data_as(_U32), len(idx))
+            keys = scene.mesh_motion[i] if scene.mesh_motion is not None else None
+            if keys:
+                k17 = f32([[t, *np.asarray(M, np.float32).reshape(16)] for t, M in keys])
+                L.po_add_mesh_motion(h, i, _fp(p), _fp(n), len(p), idx.ctypes.data_as(_U32), len(idx),
+                                     _fp(k17), len(keys))
+            else:
+                L.po_add_mesh(h, i, _fp(p), _fp(n), len(p), idx.ctypes.data_as(_U32), len(idx))
         co, wo = scene.strand_cp_offset, scene.strand_width_offset
         cps, wds, cols = f32(scene.control_points), f32(scene.widths), f32(scene.strand_color)
         for s in range(scene.num_strands):
@@ -111,6 +117,7 @@ class PoScene:
         L.po_set_env_radiance(h, _fp(f32(scene.env_radiance)))
         L.po_set_camera(h, _fp(f32(scene.cam_from)), _fp(f32(scene.cam_at)), _fp(f32(scene.cam_up)),
                         scene.vfov, scene.width, scene.height)
+        L.po_set_shutter(h, float(scene.shutter[0]), float(scene.shutter[1]))
         L.po_commit(h)
 
     def __del__(self):

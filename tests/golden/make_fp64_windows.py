@@ -44,6 +44,7 @@ def frames():
         "hair": (lambda: S.hair(1280, 720, 32, 10), [(500, 350, 548, 398)]),
         "differentiable": (lambda: S.differentiable(512, 512, 16, 8), [(248, 184, 376, 312)]),
         "glass": (lambda: S.glass(1280, 720, 16, 8), [(540, 280, 588, 328)]),
+        "motion": (lambda: S.motion(1280, 720, 16, 6), [(520, 250, 568, 298)]),
     }
 
 

@@ -31,16 +31,14 @@ def test_feature_fixtures_reproduce_from_the_reference(ref_built):
             assert (ids[:, 0] == 1).sum() > 200
 
 
-def test_restatement_glass_and_lights_match_the_reference_fixtures(restate_built):
+def test_restatement_lights_glass_motion_match_the_reference_fixtures(restate_built):
     """The CPU restatement in float (oracle/restate) reproduces the
-    reference's per-sample radiance bit for bit on the directional-light and
-    glass / alpha-mask scenes: the FP64 windows of those frames come from the
-    same code in double."""
+    reference's per-sample radiance bit for bit on the directional-light,
+    glass / alpha-mask and motion-blur scenes: the FP64 windows of those
+    frames come from the same code in double."""
     G = golden_module()
     gold = np.load(os.path.join(HERE, "golden", "feature_vectors.npz"))
     q, _, _ = G.feature_queries()
     for name, sc in G.feature_scenes().items():
-        if name == "motion":  # the restatement covers static meshes
-            continue
         li = restate_built.PoScene(sc, 32).li(q[name], threads=1)
         assert np.array_equal(li.astype(np.float32), gold[name + "_li"]), name

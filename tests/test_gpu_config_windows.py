@@ -34,6 +34,7 @@ FRAMES = {
     "hair": lambda: S.hair(1280, 720, 32, 10),
     "differentiable": lambda: S.differentiable(512, 512, 16, 8),
     "glass": lambda: S.glass(1280, 720, 16, 8),
+    "motion": lambda: S.motion(1280, 720, 16, 6),
 }
 
 
