@@ -121,7 +121,7 @@ int build_blob(const ana::Prepared* const* list, uint32_t n, Blob& B, std::strin
     B.o_tri_nodes = take(nNodes * sizeof(ana::Bvh4Node));
     B.o_tri_isect = take(nTris * 48);
     B.o_tri_shade = take(nTris * 64);
-    B.o_seg_nodes = take(nSegNodes * sizeof(ana::BvhNode));
+    B.o_seg_nodes = take(nSegNodes * sizeof(ana::Bvh4Node));
     B.o_segs = take(nSegs * 80);
     B.o_scol = take(nStr * 12);
     B.o_mats = take(nMats * sizeof(ana::DevMaterial));
@@ -159,7 +159,7 @@ int build_blob(const ana::Prepared* const* list, uint32_t n, Blob& B, std::strin
     auto* nodes = devTris ? nullptr : reinterpret_cast<ana::Bvh4Node*>(B.at(B.o_tri_nodes));
     auto* isect = devTris ? nullptr : reinterpret_cast<float4*>(B.at(B.o_tri_isect));
     auto* shade = devTris ? nullptr : reinterpret_cast<float4*>(B.at(B.o_tri_shade));
-    auto* snodes = reinterpret_cast<ana::BvhNode*>(B.at(B.o_seg_nodes));
+    auto* snodes = reinterpret_cast<ana::Bvh4Node*>(B.at(B.o_seg_nodes));
     auto* segs = reinterpret_cast<float4*>(B.at(B.o_segs));
     auto* scol = reinterpret_cast<float*>(B.at(B.o_scol));
     auto* mats = reinterpret_cast<ana::DevMaterial*>(B.at(B.o_mats));
@@ -167,22 +167,14 @@ int build_blob(const ana::Prepared* const* list, uint32_t n, Blob& B, std::strin
     auto* lights = reinterpret_cast<ana::DevLight*>(B.at(B.o_lights));
     auto* motion = reinterpret_cast<uint2*>(B.at(B.o_motion));
     auto* keys = reinterpret_cast<float4*>(B.at(B.o_keys));
-    // 4-wide triangle nodes: interior refs shift by the scene's node base, the
-    // first-triangle field of leaf entries (bits 0..24) by its primitive base
+    // 4-wide nodes (triangles and curve segments): interior refs shift by the
+    // scene's node base, the first-primitive field of leaf entries (bits 0..24)
+    // by its primitive base
     auto fix_node4 = [](ana::Bvh4Node nd, uint32_t nodeBase, uint32_t primBase) {
         uint32_t* ref = &nd.ref.x;
         for (int k = 0; k < 4; ++k) {
             if (ref[k] == ana::kEmptyChild) continue;
             ref[k] += (ref[k] & 0x80000000u) ? primBase : nodeBase;
-        }
-        return nd;
-    };
-    // binary curve nodes: likewise, with refs and leaf counts in n3
-    auto fix_node = [](ana::BvhNode nd, uint32_t nodeBase, uint32_t primBase) {
-        float* n3 = &nd.n3.x;
-        for (int ch = 0; ch < 2; ++ch) {
-            uint32_t ref = ubits(n3[ch]), cnt = ubits(n3[2 + ch]);
-            n3[ch] = fbits(ref + (cnt ? primBase : nodeBase));
         }
         return nd;
     };
@@ -220,7 +212,7 @@ int build_blob(const ana::Prepared* const* list, uint32_t n, Blob& B, std::strin
         for (const float4& k4 : P.motion_keys) keys[iK++] = k4;
         st.seg_root = (P.num_segs && !P.seg_nodes.empty()) ? sNodeBase : ana::kNoRoot;
         if (P.num_segs) B.has_curves = true;
-        for (const ana::BvhNode& nd : P.seg_nodes) snodes[iSN++] = fix_node(nd, sNodeBase, segBase);
+        for (const ana::Bvh4Node& nd : P.seg_nodes) snodes[iSN++] = fix_node4(nd, sNodeBase, segBase);
         for (uint32_t s = 0; s < P.num_segs; ++s) {
             for (int j = 0; j < 4; ++j) segs[5 * (size_t(segBase) + s) + j] = P.segs[5 * size_t(s) + j];
             float4 r = P.segs[5 * size_t(s) + 4];
@@ -453,7 +445,7 @@ int upload_blob(ana_ctx* c, const Blob& B, const ana::DeviceTris* dt = nullptr) 
     S.tri_nodes = reinterpret_cast<const ana::Bvh4Node*>(b + B.o_tri_nodes);
     S.tri_isect = reinterpret_cast<const float4*>(b + B.o_tri_isect);
     S.tri_shade = reinterpret_cast<const float4*>(b + B.o_tri_shade);
-    S.seg_nodes = reinterpret_cast<const ana::BvhNode*>(b + B.o_seg_nodes);
+    S.seg_nodes = reinterpret_cast<const ana::Bvh4Node*>(b + B.o_seg_nodes);
     S.segs = reinterpret_cast<const float4*>(b + B.o_segs);
     S.strand_color = reinterpret_cast<const float*>(b + B.o_scol);
     S.materials = reinterpret_cast<const ana::DevMaterial*>(b + B.o_mats);

@@ -2,13 +2,13 @@
 // sm_100a kernels. Plain POD, no CUDA runtime calls.
 //
 // HBM layout (all arrays 16-byte aligned, read with 16-byte vector loads):
-//   tri_nodes   BVH2 interior nodes, 64 B each: both children's boxes live in
-//               the parent so one node fetch tests two boxes.
+//   tri_nodes   4-wide BVH nodes, 128 B each (Bvh4Node): the four children's
+//               boxes live in the parent so one node fetch tests four boxes.
 //   tri_isect   48 B per triangle in leaf order: (v0, orig index) (e1) (e2),
 //               i.e. BVHTriangle::v0/e1/e2 (src/accel/BVHBackend.h:49-59).
 //   tri_shade   64 B per triangle in mesh order: (ng, meshID) (sn0, primID)
 //               (sn1) (sn2), read once per shaded hit.
-//   seg_nodes   BVH2 nodes over cubic Bezier segments (same 64 B format).
+//   seg_nodes   4-wide BVH nodes over cubic Bezier segments (same 128 B format).
 //   segs        80 B per segment in leaf order: P0..P3 with the two half
 //               widths and the strand-parameter offset/scale, then ids.
 #pragma once
@@ -17,22 +17,7 @@
 
 namespace ana {
 
-// BVH2 node with child boxes in the parent.
-//   n0 = (c0.lo.x, c0.hi.x, c0.lo.y, c0.hi.y)
-//   n1 = (c1.lo.x, c1.hi.x, c1.lo.y, c1.hi.y)
-//   n2 = (c0.lo.z, c0.hi.z, c1.lo.z, c1.hi.z)
-//   n3 = (c0 ref, c1 ref, c0 count, c1 count) as int bits
-// A child ref with count 0 is an interior node index; count > 0 means a leaf
-// whose primitives are [ref, ref + count) in the leaf-ordered primitive array.
-// An absent child has an empty box (lo = +inf, hi = -inf).
-struct BvhNode {
-    float4 n0, n1, n2, n3;
-};
-static_assert(sizeof(BvhNode) == 64, "BvhNode must be 64 bytes");
-
-constexpr uint32_t kMaxStack = 64;   // curve traversal stack depth (reference: 64)
-
-// 4-wide triangle BVH node (128 bytes, one L2 line): the four children's
+// 4-wide BVH node (128 bytes, one L2 line): the four children's
 // boxes as structure of arrays (child k in component k) and their references
 // (an interior node index, a leaf entry: bit 31 | (count-1) << 25 | first
 // triangle, or kEmptyChild). The nodes are the reference's binary SAH tree
@@ -152,7 +137,7 @@ struct DevScene {
     const Bvh4Node* tri_nodes;
     const float4* tri_isect;
     const float4* tri_shade;
-    const BvhNode* seg_nodes;
+    const Bvh4Node* seg_nodes;  // the curve segments' 4-wide BVH
     const float4* segs;
     const float* strand_color;   // 3 per strand
     const DevMaterial* materials;

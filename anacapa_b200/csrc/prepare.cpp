@@ -79,8 +79,7 @@ struct Box {
 
 // ---------------------------------------------------------------------------
 // Binary BVH build tree (both builders produce this; flatten_bvh4 lays the
-// triangle tree out as 128-byte 4-wide nodes, flatten_bvh2 the curve tree as
-// 64-byte binary nodes).
+// triangle and the curve trees out as 128-byte 4-wide nodes).
 // ---------------------------------------------------------------------------
 struct BuildNode {
     Box box;
@@ -267,75 +266,15 @@ uint32_t curve_build(std::vector<SegWork>& w, uint32_t start, uint32_t end, uint
 }
 
 // ---------------------------------------------------------------------------
-// Flatten a build tree into 64-byte nodes, depth-first, left child first.
-// emit_leaf(start, count) appends the leaf's primitives to the leaf-ordered
-// primitive array and returns the offset of the first one.
-// ---------------------------------------------------------------------------
-template <class EmitLeaf>
-void flatten_bvh2(const NodePool& pool, uint32_t root, std::vector<BvhNode>& out, bool& rootEmpty,
-                  EmitLeaf emit_leaf) {
-    out.clear();
-    const BuildNode& R = pool.nodes[root];
-    auto put_child = [](BvhNode& n, int slot, const Box& b, uint32_t ref, uint32_t cnt) {
-        float* n0 = slot == 0 ? &n.n0.x : &n.n1.x;
-        n0[0] = b.lo[0];
-        n0[1] = b.hi[0];
-        n0[2] = b.lo[1];
-        n0[3] = b.hi[1];
-        float* n2 = &n.n2.x;
-        n2[2 * slot + 0] = b.lo[2];
-        n2[2 * slot + 1] = b.hi[2];
-        float* n3 = &n.n3.x;
-        n3[slot] = bits(ref);
-        n3[2 + slot] = bits(cnt);
-    };
-    Box empty;
-    if (R.count > 0 || R.left < 0) {
-        // Root is a leaf: one interior node holding it and an empty child.
-        rootEmpty = R.count == 0;
-        BvhNode n{};
-        uint32_t off = R.count ? emit_leaf(R.start, R.count) : 0;
-        put_child(n, 0, R.count ? R.box : empty, off, R.count);
-        put_child(n, 1, empty, 0, 0);
-        out.push_back(n);
-        return;
-    }
-    rootEmpty = false;
-    // Iterative pre-order DFS. Each interior build node gets its slot when
-    // first visited; its children's refs are patched when they are placed.
-    struct Item {
-        uint32_t bn;
-        int32_t parent;
-        int slot;
-    };
-    std::vector<Item> stack;
-    stack.push_back({root, -1, 0});
-    while (!stack.empty()) {
-        Item it = stack.back();
-        stack.pop_back();
-        const BuildNode& b = pool.nodes[it.bn];
-        if (b.count > 0) {
-            uint32_t off = emit_leaf(b.start, b.count);
-            put_child(out[size_t(it.parent)], it.slot, b.box, off, b.count);
-            continue;
-        }
-        uint32_t idx = uint32_t(out.size());
-        out.push_back(BvhNode{});
-        if (it.parent >= 0) put_child(out[size_t(it.parent)], it.slot, b.box, idx, 0);
-        // push right first so left is placed (and its leaves emitted) first
-        stack.push_back({uint32_t(b.right), int32_t(idx), 1});
-        stack.push_back({uint32_t(b.left), int32_t(idx), 0});
-    }
-}
-
-// ---------------------------------------------------------------------------
 // Collapse a binary build tree into 4-wide nodes. A node's children start as
 // its binary node's two children; the interior child of largest surface area
 // is replaced by its own two children until there are four or only leaves
 // remain. Every child box is therefore a box of the binary tree, bit for bit,
 // and a box contains its descendants' boxes, so a ray that passes a child's
 // slab test passes every skipped ancestor's: the triangles tested are those
-// the binary traversal would test. Nodes are laid out depth-first; returns the
+// the binary traversal would test (the same holds for the curve tree and
+// CurveBrute's box test, whose slab and inside tests are monotone in the
+// box). Nodes are laid out depth-first; returns the
 // worst root-to-leaf sum of (children - 1), the traversal stack bound.
 // ---------------------------------------------------------------------------
 template <class EmitLeaf>
@@ -450,7 +389,7 @@ bool finite3(const float* p) { return std::isfinite(p[0]) && std::isfinite(p[1])
 
 uint64_t Prepared::bytes() const {
     return tri_nodes.size() * sizeof(Bvh4Node) + tri_isect.size() * 16 + tri_shade.size() * 16 +
-           seg_nodes.size() * sizeof(BvhNode) + segs.size() * 16 + strand_color.size() * 4 +
+           seg_nodes.size() * sizeof(Bvh4Node) + segs.size() * 16 + strand_color.size() * 4 +
            materials.size() * sizeof(DevMaterial) + slot_material.size() * 4 +
            lights.size() * sizeof(DevLight) +
            (env.rgb.size() + env.cond_func.size() + env.cond_cdf.size() + env.cond_int.size() +
@@ -794,7 +733,7 @@ int prepare_scene(const ana_scene_desc& d, Prepared& P, std::string& err, bool t
         uint32_t root = curve_build(work, 0, uint32_t(work.size()), maxLeafS, pool, 0);
         bool empty;
         P.segs.reserve(work.size() * 5);
-        flatten_bvh2(pool, root, P.seg_nodes, empty, [&](uint32_t s, uint32_t c) {
+        const uint32_t stackBound = flatten_bvh4(pool, root, P.seg_nodes, empty, [&](uint32_t s, uint32_t c) {
             uint32_t off = uint32_t(P.segs.size() / 5);
             for (uint32_t i = s; i < s + c; ++i) {
                 size_t e = segBase[work[i].strand] + work[i].seg;
@@ -802,6 +741,7 @@ int prepare_scene(const ana_scene_desc& d, Prepared& P, std::string& err, bool t
             }
             return off;
         });
+        if (stackBound > kMaxStack4) return unsupported("curve BVH deeper than the traversal stack");
     }
 
     // ---- materials -----------------------------------------------------------

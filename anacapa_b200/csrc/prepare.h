@@ -25,7 +25,7 @@ struct Prepared {
     std::vector<float4> tri_isect;   // 3 per triangle, leaf order
     std::vector<float4> tri_shade;   // 4 per triangle, mesh order
     bool tri_root_is_empty = true;
-    std::vector<BvhNode> seg_nodes;
+    std::vector<Bvh4Node> seg_nodes;
     std::vector<float4> segs;        // 5 per segment, leaf order
     std::vector<float> strand_color;
     std::vector<DevMaterial> materials;

@@ -617,7 +617,7 @@ def run_ours(a):
     launches = int(sum(s.kernel_launches for s in stats))
     # roofline of the dominant kernel (closest-hit traversal)
     ext_launches = stats[0].extend_launches
-    alg_bytes = (128 * work.node_fetches + 64 * work.curve_node_fetches + 48 * work.tri_tests + 80 * work.seg_tests
+    alg_bytes = (128 * work.node_fetches + 128 * work.curve_node_fetches + 48 * work.tri_tests + 80 * work.seg_tests
                  + (32 + 16) * work.extend_rays)
     peak, peak_kind = measured_peaks()
     achieved = (alg_bytes / ext_launches) / ((ext_ms / ext_launches) / 1e3) / 1e9 if ext_ms > 0 else None

@@ -259,7 +259,7 @@ typedef struct ana_stats {
                                    node loads (4-wide nodes)                     */
     uint64_t tri_tests;         /*   triangle tests (48 bytes each)              */
     uint64_t seg_tests;         /*   curve segment tests (80 bytes each)         */
-    uint64_t curve_node_fetches;/*   64-byte curve BVH node loads                */
+    uint64_t curve_node_fetches;/*   128-byte curve BVH node loads (4-wide)      */
     float upload_ms;            /* wall time of the last scene upload call      */
     float build_ms[4];          /* ana_upload_scene_device phases (wall time):
                                    inputs + triangle setup, SAH levels, small
