@@ -101,8 +101,9 @@ struct Counters {
 //      warp-aggregated atomicAdd on the stage's fetch counter);
 //   2. interior phase: lanes descend interior nodes until they reach a
 //      leaf; the phase ends when every lane has a leaf to test (or nothing
-//      left), or when no lane can take another interior step, so lanes stay
-//      converged on the node-test code. Any-hit queries are speculative
+//      left), when no lane can take another interior step, or (closest hit)
+//      when at most kLeafPhaseLanes lanes still descend while others wait
+//      with a leaf, so lanes stay converged on the node-test code. Any-hit queries are speculative
 //      (Aila and Laine, "Understanding the efficiency of ray traversal on
 //      GPUs", 2009): a lane that reaches a leaf parks it and keeps descending
 //      from its next stack entry. Closest-hit queries do not speculate: a
@@ -115,6 +116,12 @@ struct Counters {
 // do not idle the warp until its slowest ray completes. Box and triangle
 // tests are the same functions as above, so results are identical.
 // ---------------------------------------------------------------------------
+// Closest-hit interior phases end once this few lanes still descend (and a
+// lane has a leaf): on the 1920x1080x64 throughput frame the extend stage took
+// 142.0 ms when the phase ran until no lane descended, 118.4 ms at 4 lanes,
+// 117.2 ms at 8 and 124.6 ms at 16, with identical hits.
+constexpr uint32_t kLeafPhaseLanes = 8;
+
 struct Traversal {
     TriRay r;
     float closest, u, v;
@@ -726,7 +733,16 @@ __device__ __forceinline__ void persistent_traverse(const DevScene& S, uint32_t 
             }
             const bool want = active && !T.exhausted && !(T.cur & 0x80000000u);
             const bool ready = !active || T.exhausted || (kAny ? parked != kEmptyChild : bool(T.cur & 0x80000000u));
-            if (!__any_sync(0xFFFFFFFFu, want) || __all_sync(0xFFFFFFFFu, ready)) break;
+            const uint32_t wantMask = __ballot_sync(0xFFFFFFFFu, want);
+            if (!wantMask || __all_sync(0xFFFFFFFFu, ready)) break;
+            // Closest hit: once at most kLeafPhaseLanes lanes still descend and
+            // another lane has a leaf, the phase ends and the leaves are tested
+            // (the descending lanes resume in the next interior phase), so few
+            // lanes do not hold the warp in the node loop. A lane with a leaf
+            // must exist, so every pass makes progress.
+            if (!kAny && __popc(wantMask) <= kLeafPhaseLanes &&
+                __any_sync(0xFFFFFFFFu, active && !T.exhausted && (T.cur & 0x80000000u)))
+                break;
             if (want) node_step<kAny, kCount, kCurves>(T, S, stack, stackT, err, cnt);
         }
         // 3. leaf phase: one leaf per lane

@@ -70,6 +70,10 @@ def parse():
                          "point for this frame (all 132,710,400 paths in one chunk, ~31 GB of queues)")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batched-vs-plain and adjoint/forward measurements")
+    ap.add_argument("--leaf-tris", type=int, default=0,
+                    help="maximum triangles per BVH leaf (0: the reference's 4)")
+    ap.add_argument("--leaf-segments", type=int, default=0,
+                    help="maximum curve segments per BVH leaf (0: the reference's 4)")
     ap.add_argument("--traversal", type=int, default=0,
                     help="0 library default, 1 persistent warps, 2 one thread per ray")
     ap.add_argument("--scene", default="throughput", choices=["throughput", "glass", "motion", "hair"],
@@ -581,7 +585,7 @@ def run_ours(a):
         torch.cuda.set_device(local)
     scene = make_scene(a)
     t_prep = time.perf_counter()
-    prep = api.Prepared(scene)
+    prep = api.Prepared(scene, max_leaf_tris=a.leaf_tris, max_leaf_segments=a.leaf_segments)
     t_prep = time.perf_counter() - t_prep
     r = api.Renderer(device=local, timing=True, traversal=a.traversal, chunk_paths=a.chunk_paths)
     r.upload(prep)
