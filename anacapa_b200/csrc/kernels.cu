@@ -37,7 +37,9 @@ constexpr int kPersistBlock = 256;    // traversal kernels: 8 warps per block
 constexpr int kPersistMinBlocks = 5;  // persistent schedule: 5 resident blocks/SM (<= 51 registers)
 // k_shade runs at most 256-thread blocks: three resident per SM (80 registers,
 // spilling to L1) for the forward kernel without fiber code measured 5 % faster
-// than two at 128 registers; the fiber and adjoint variants keep two
+// than two at 128 registers; the kernels compiled for a subset of the material
+// and light classes fit four (64 registers: throughput frame's shade stage 77.4
+// against 78.5 ms at three); the fiber and adjoint variants keep two
 constexpr int kShadeBlock = 256;
 
 // Reserves one slot per thread and queue where that thread's want flag is
@@ -442,7 +444,7 @@ __device__ __forceinline__ float sum3(float3 v) { return v.x + v.y + v.z; }
 // kFeat: the material and light classes compiled in (kFeat* bits); the host
 // launches a kernel whose set covers the batch's (DevScene::features).
 template <bool kAdj, bool kFiber, bool kExtra, uint32_t kFeat = kFeatAll>
-__global__ void __launch_bounds__(kShadeBlock, (!kAdj && !kFiber) ? 3 : 2) k_shade(const __grid_constant__ Params p) {
+__global__ void __launch_bounds__(kShadeBlock, (!kAdj && !kFiber) ? (kFeat == kFeatAll ? 3 : 4) : 2) k_shade(const __grid_constant__ Params p) {
     const uint32_t b = p.bounce;
     const uint32_t cur = b & 1u, nxt = cur ^ 1u;
     const uint32_t n = p.counters[b * kCountersPerBounce + 0];

@@ -101,9 +101,9 @@ struct Counters {
 //      warp-aggregated atomicAdd on the stage's fetch counter);
 //   2. interior phase: lanes descend interior nodes until they reach a
 //      leaf; the phase ends when every lane has a leaf to test (or nothing
-//      left), when no lane can take another interior step, or (closest hit)
-//      when at most kLeafPhaseLanes lanes still descend while others wait
-//      with a leaf, so lanes stay converged on the node-test code. Any-hit queries are speculative
+//      left), when no lane can take another interior step, or when at most
+//      kLeafPhaseLanes lanes still descend while others wait with a leaf, so
+//      lanes stay converged on the node-test code. Any-hit queries are speculative
 //      (Aila and Laine, "Understanding the efficiency of ray traversal on
 //      GPUs", 2009): a lane that reaches a leaf parks it and keeps descending
 //      from its next stack entry. Closest-hit queries do not speculate: a
@@ -116,10 +116,11 @@ struct Counters {
 // do not idle the warp until its slowest ray completes. Box and triangle
 // tests are the same functions as above, so results are identical.
 // ---------------------------------------------------------------------------
-// Closest-hit interior phases end once this few lanes still descend (and a
-// lane has a leaf): on the 1920x1080x64 throughput frame the extend stage took
-// 142.0 ms when the phase ran until no lane descended, 118.4 ms at 4 lanes,
-// 117.2 ms at 8 and 124.6 ms at 16, with identical hits.
+// Interior phases end once this few lanes still descend (and a lane has a
+// leaf): on the 1920x1080x64 throughput frame the extend stage took 142.0 ms
+// when the phase ran until no lane descended, 118.4 ms at 4 lanes, 117.2 ms at
+// 8 and 124.6 ms at 16; the any-hit shadow / MIS stages 60.3 / 86.2 ms, 56.4 /
+// 80.6 ms at 4 and 54.9 / 77.9 ms at 8; hits and occlusion answers unchanged.
 constexpr uint32_t kLeafPhaseLanes = 8;
 
 struct Traversal {
@@ -460,70 +461,44 @@ __device__ __forceinline__ bool ribbon_bounds(float3 c0, float3 c1, float3 c2, f
     return !(xadd(xmul(cx, cx), xmul(cy, cy)) > xmul(maxHalfW, maxHalfW));
 }
 
-// One node of the subdivision tree: its world-space control points, the
-// projections of its end points, its half-widths and its strand-parameter
-// interval.
-struct RibbonNode {
-    float3 P0, P1, P2, P3;
-    float3 c0, c3;
+struct SubSeg {
+    float3 P0, P1, P2, P3;  // world-space control points (further splits, tangent)
+    float3 c0, c3;          // projected end points
     float hw0, hw3, toff, tscale;
+    float zlo;              // zMin - maxHalfW: the test that depends on bestT
+    int depth;
 };
 
-// bezierSplitMid (CurveBrute.cpp:66-80) into the left (right = false) or right
-// half, with the half-width and parameter interval the reference passes down
-// (CurveBrute.cpp:152-176). Projections are left to the caller.
-__device__ __forceinline__ void ribbon_half(RibbonNode& n, bool right) {
-    const float3 Q01 = xmid(n.P0, n.P1), Q12 = xmid(n.P1, n.P2), Q23 = xmid(n.P2, n.P3);
-    const float3 R01 = xmid(Q01, Q12), R12 = xmid(Q12, Q23), M = xmid(R01, R12);
-    const float hwMid = xmul(xadd(n.hw0, n.hw3), 0.5f);
-    const float tsh = xmul(n.tscale, 0.5f);
-    if (right) {
-        n.P0 = M;
-        n.P1 = R12;
-        n.P2 = Q23;
-        n.hw0 = hwMid;
-        n.toff = xadd(n.toff, tsh);
-    } else {
-        n.P1 = Q01;
-        n.P2 = R01;
-        n.P3 = M;
-        n.hw3 = hwMid;
-    }
-    n.tscale = tsh;
-}
-
 // subdivide (CurveBrute.cpp:85-176): depth-6 de Casteljau subdivision in ray
-// space, left half first, each leaf taking the hit when it is strictly closer
-// than bestT. The recursion is run as a depth-first walk that keeps no
-// per-level copies of control points (a stack of them lived in local memory):
-// the walk holds the current node and a bit per level for a right half still
-// to visit. A split projects the five new points once (a child shares two
-// points with its parent and one with its sibling; equal world points give
-// equal projections), tests both halves and descends into the left one; a
-// surviving right half is only marked. To visit it, its control points are
-// rebuilt from the segment's four points by the same midpoint splits along
-// the current path (the same operations on the same operands as the
-// reference's recursion, so the same values), and its one bestT-dependent
-// test is repeated then (bestT only decreases, the other tests do not depend
-// on it). Every node is therefore accepted or culled, and every leaf
-// evaluated, exactly as in the recursion and in the same order.
+// space, the left half first, updating bestT on a closer hit. The reference
+// projects a node's four control points when it visits the node; a child
+// shares two of them with its parent and one with its sibling, so here a split
+// projects the five new points once (the same world points give the same
+// projections), both children are bounds-tested at once and only survivors are
+// pushed. The one test that depends on bestT (which only decreases) is
+// repeated when a child is popped, so every node is accepted or culled, and
+// every leaf evaluated, exactly as in the recursion and in the same order.
+// (A walk that kept no per-level copies, rebuilding each right half from the
+// segment's four points along the path, measured slower on the 1280x720x32
+// hair frame: extend 1024 against 842 ms, shadow 618 against 525 ms; the
+// entries stay in local memory, served by L1.)
 __device__ __forceinline__ bool ribbon_hit(const RayFrame& fr, float tmin, float3 P0, float3 P1, float3 P2,
                                            float3 P3, float hw0, float hw3, float toff, float tscale,
                                            float& bestT, float& tSeg, float3& tang) {
-    constexpr int kDepth = 6;
-    RibbonNode n{P0, P1, P2, P3, project(fr, P0), project(fr, P3), hw0, hw3, toff, tscale};
+    SubSeg st[8];
+    int sp = 0;
     {
-        const float3 c1 = project(fr, P1), c2 = project(fr, P2);
+        const float3 c0 = project(fr, P0), c1 = project(fr, P1), c2 = project(fr, P2), c3 = project(fr, P3);
         float zlo;
-        if (!ribbon_bounds(n.c0, c1, c2, n.c3, hw0, hw3, tmin, bestT, zlo)) return false;
+        if (!ribbon_bounds(c0, c1, c2, c3, hw0, hw3, tmin, bestT, zlo)) return false;
+        st[sp++] = SubSeg{P0, P1, P2, P3, c0, c3, hw0, hw3, toff, tscale, zlo, 6};
     }
-    uint32_t pending = 0;  // bit d: the right half of the level-d node on the path is still to visit
-    uint32_t path = 0;     // bit d: the path takes the right half at level d
-    int d = 0;             // level of the current node
     bool hit = false;
-    while (true) {
-        if (d == kDepth) {  // leaf (CurveBrute.cpp:119-146)
-            const float ax = n.c0.x, ay = n.c0.y, bx = n.c3.x, by = n.c3.y;
+    while (sp > 0) {
+        const SubSeg s = st[--sp];
+        if (s.zlo > bestT) continue;
+        if (s.depth == 0) {
+            const float ax = s.c0.x, ay = s.c0.y, bx = s.c3.x, by = s.c3.y;
             const float dx = xsub(bx, ax), dy = xsub(by, ay);
             const float lenSq = xadd(xmul(dx, dx), xmul(dy, dy));
             float tLine;
@@ -532,59 +507,32 @@ __device__ __forceinline__ bool ribbon_hit(const RayFrame& fr, float tmin, float
                 tLine = fmaxf(0.f, fminf(1.f, xdiv(xsub(xmul(-ax, dx), xmul(ay, dy)), lenSq)));
             const float px = xadd(ax, xmul(dx, tLine)), py = xadd(ay, xmul(dy, tLine));
             const float dist2 = xadd(xmul(px, px), xmul(py, py));
-            const float halfW = xadd(xmul(n.hw0, xsub(1.f, tLine)), xmul(n.hw3, tLine));
-            const float tRay = xadd(n.c0.z, xmul(xsub(n.c3.z, n.c0.z), tLine));
-            if (!(dist2 > xmul(halfW, halfW)) && !(tRay < tmin || tRay >= bestT)) {
-                float3 tg = bezier_tangent(n.P0, n.P1, n.P2, n.P3, tLine);
-                if (xdot(tg, tg) < 1e-12f) tg = xsub3(n.P3, n.P0);
-                const float len = __fsqrt_rn(xdot(tg, tg));
-                tg = len > 1e-8f ? xmul3(tg, xdiv(1.f, len)) : f3(0.f, 0.f, 1.f);
-                bestT = tRay;
-                tSeg = xadd(n.toff, xmul(tLine, n.tscale));
-                tang = tg;
-                hit = true;
-            }
-        } else {  // split; both halves bounds-tested, the left one entered
-            const float3 Q01 = xmid(n.P0, n.P1), Q12 = xmid(n.P1, n.P2), Q23 = xmid(n.P2, n.P3);
-            const float3 R01 = xmid(Q01, Q12), R12 = xmid(Q12, Q23), M = xmid(R01, R12);
-            const float3 cq01 = project(fr, Q01), cr01 = project(fr, R01), cm = project(fr, M),
-                         cr12 = project(fr, R12), cq23 = project(fr, Q23);
-            const float hwMid = xmul(xadd(n.hw0, n.hw3), 0.5f);
-            float zl, zr;
-            const bool okL = ribbon_bounds(n.c0, cq01, cr01, cm, n.hw0, hwMid, tmin, bestT, zl);
-            const bool okR = ribbon_bounds(cm, cr12, cq23, n.c3, hwMid, n.hw3, tmin, bestT, zr);
-            if (okR) pending |= 1u << d;
-            if (okL) {
-                n.P1 = Q01;
-                n.P2 = R01;
-                n.P3 = M;
-                n.c3 = cm;
-                n.hw3 = hwMid;
-                n.tscale = xmul(n.tscale, 0.5f);
-                path &= ~(1u << d);
-                ++d;
-                continue;
-            }
+            const float halfW = xadd(xmul(s.hw0, xsub(1.f, tLine)), xmul(s.hw3, tLine));
+            if (dist2 > xmul(halfW, halfW)) continue;
+            const float tRay = xadd(s.c0.z, xmul(xsub(s.c3.z, s.c0.z), tLine));
+            if (tRay < tmin || tRay >= bestT) continue;
+            float3 tg = bezier_tangent(s.P0, s.P1, s.P2, s.P3, tLine);
+            if (xdot(tg, tg) < 1e-12f) tg = xsub3(s.P3, s.P0);
+            const float len = __fsqrt_rn(xdot(tg, tg));
+            tg = len > 1e-8f ? xmul3(tg, xdiv(1.f, len)) : f3(0.f, 0.f, 1.f);
+            bestT = tRay;
+            tSeg = xadd(s.toff, xmul(tLine, s.tscale));
+            tang = tg;
+            hit = true;
+            continue;
         }
-        // next right half: the deepest level still marked
-        bool entered = false;
-        while (pending) {
-            const int L = 31 - __clz(pending);
-            pending &= ~(1u << L);
-            n = RibbonNode{P0, P1, P2, P3, n.c0, n.c3, hw0, hw3, toff, tscale};
-            for (int k = 0; k < L; ++k) ribbon_half(n, (path >> k) & 1u);
-            ribbon_half(n, true);
-            path |= 1u << L;
-            d = L + 1;
-            n.c0 = project(fr, n.P0);
-            n.c3 = project(fr, n.P3);
-            const float zMin = min4(n.c0.z, project(fr, n.P1).z, project(fr, n.P2).z, n.c3.z);
-            if (!(xsub(zMin, fmaxf(n.hw0, n.hw3)) > bestT)) {
-                entered = true;
-                break;
-            }
-        }
-        if (!entered) break;
+        // bezierSplitMid (CurveBrute.cpp:66-80)
+        const float3 Q01 = xmid(s.P0, s.P1), Q12 = xmid(s.P1, s.P2), Q23 = xmid(s.P2, s.P3);
+        const float3 R01 = xmid(Q01, Q12), R12 = xmid(Q12, Q23), M = xmid(R01, R12);
+        const float3 cq01 = project(fr, Q01), cr01 = project(fr, R01), cm = project(fr, M),
+                     cr12 = project(fr, R12), cq23 = project(fr, Q23);
+        const float hwMid = xmul(xadd(s.hw0, s.hw3), 0.5f);
+        const float tsh = xmul(s.tscale, 0.5f);
+        float zl, zr;
+        const bool okL = ribbon_bounds(s.c0, cq01, cr01, cm, s.hw0, hwMid, tmin, bestT, zl);
+        const bool okR = ribbon_bounds(cm, cr12, cq23, s.c3, hwMid, s.hw3, tmin, bestT, zr);
+        if (okR) st[sp++] = SubSeg{M, R12, Q23, s.P3, cm, s.c3, hwMid, s.hw3, xadd(s.toff, tsh), tsh, zr, s.depth - 1};
+        if (okL) st[sp++] = SubSeg{s.P0, Q01, R01, M, s.c0, cm, s.hw0, hwMid, s.toff, tsh, zl, s.depth - 1};
     }
     return hit;
 }
@@ -735,13 +683,14 @@ __device__ __forceinline__ void persistent_traverse(const DevScene& S, uint32_t 
             const bool ready = !active || T.exhausted || (kAny ? parked != kEmptyChild : bool(T.cur & 0x80000000u));
             const uint32_t wantMask = __ballot_sync(0xFFFFFFFFu, want);
             if (!wantMask || __all_sync(0xFFFFFFFFu, ready)) break;
-            // Closest hit: once at most kLeafPhaseLanes lanes still descend and
-            // another lane has a leaf, the phase ends and the leaves are tested
-            // (the descending lanes resume in the next interior phase), so few
-            // lanes do not hold the warp in the node loop. A lane with a leaf
-            // must exist, so every pass makes progress.
-            if (!kAny && __popc(wantMask) <= kLeafPhaseLanes &&
-                __any_sync(0xFFFFFFFFu, active && !T.exhausted && (T.cur & 0x80000000u)))
+            // Once at most kLeafPhaseLanes lanes still descend and another
+            // lane holds a leaf (any hit: a parked one), the phase ends and the
+            // leaves are tested (the descending lanes resume in the next
+            // interior phase), so few lanes do not hold the warp in the node
+            // loop. A lane with a leaf must exist, so every pass makes progress.
+            if (__popc(wantMask) <= kLeafPhaseLanes &&
+                __any_sync(0xFFFFFFFFu, active && !T.exhausted &&
+                                            (kAny ? parked != kEmptyChild : bool(T.cur & 0x80000000u))))
                 break;
             if (want) node_step<kAny, kCount, kCurves>(T, S, stack, stackT, err, cnt);
         }
