@@ -34,7 +34,6 @@ namespace ana {
 constexpr uint32_t kMiss = 0xFFFFFFFFu;
 constexpr int kMaxBlock = 1024;
 constexpr int kPersistBlock = 256;    // traversal kernels: 8 warps per block
-static_assert(kPersistBlock == 32 * kRibbonWarps, "one shared ribbon stack per warp of a traversal block");
 constexpr int kPersistMinBlocks = 5;  // persistent schedule: 5 resident blocks/SM (<= 51 registers)
 // k_shade runs at most 256-thread blocks: three resident per SM (80 registers,
 // spilling to L1) for the forward kernel without fiber code measured 5 % faster

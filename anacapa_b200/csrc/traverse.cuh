@@ -538,259 +538,6 @@ __device__ __forceinline__ bool ribbon_hit(const RayFrame& fr, float tmin, float
 }
 
 // ---------------------------------------------------------------------------
-// Warp-cooperative ribbon tests (persistent schedule). Run alone, a lane's
-// subdivision walk keeps the rest of its warp idle: on the hair frame 3.8 of
-// 32 lanes were active per instruction in the curve traversal. Here each lane
-// with a curve leaf bounds-tests its segments' roots (as subdivide does on
-// entry) and hands the surviving (ray, segment) pairs to its warp; the warp
-// then walks all their subdivision trees together from a shared stack of
-// nodes, 32 nodes per step, so every lane tests some node. A node is kept as
-// (owner lane, segment, depth, path): its control points are rebuilt from the
-// segment's four points by the midpoint splits along the path, the same
-// operations on the same operands as the recursion, hence the same values.
-//
-// Order: subdivide visits leaves depth first, left first, and accepts a leaf
-// strictly closer than the best so far. Whatever the visiting order, that
-// gives the closest accepted leaf, the first in that order among equals; here
-// every accepted leaf proposes the key (t, segment order in the leaf, path
-// read as a left-first index) to its owner with one shared-memory atomicMin,
-// so the owner gets the same leaf. Culling by the best distance so far only
-// skips nodes that cannot hold a closer leaf. The owner then evaluates the
-// winning leaf alone for its strand parameter and tangent.
-// ---------------------------------------------------------------------------
-constexpr int kRibbonWarps = 8;           // warps per block of the persistent traversal kernels
-constexpr uint32_t kRibbonStack = 288;    // shared nodes per warp (44 KB of shared memory per block)
-constexpr uint32_t kRibbonRoots = 96;     // root pairs a warp shares; later ones are walked by their lane
-// Bound: a step pops n <= 32 nodes and pushes at most 2n, and a node has at
-// most 6 ancestors, so the stack never holds more than the roots + 6 * 32.
-static_assert(kRibbonRoots + 6 * 32 <= kRibbonStack, "ribbon stack bound");
-
-struct RibbonWarp {
-    float frame[32][14];            // owner lane: o, x, y, z (ray-space frame), tmin, initial best t
-    unsigned long long best[32];    // owner lane: (t bits << 32) | (own walk << 31 | segment order << 6 | path)
-    uint32_t node[kRibbonStack][3]; // owner << 27 | segment, order << 16 | depth << 8 | path, zlo bits
-    uint32_t top;
-};
-
-// The node at `depth` levels below the segment (P, hw, toff, tscale) along
-// `path` (its first split in the highest of the depth bits, 1 = right half).
-__device__ __forceinline__ void ribbon_node(float3 (&P)[4], float& hw0, float& hw3, float& toff, float& tscale,
-                                            uint32_t depth, uint32_t path) {
-    for (int k = int(depth) - 1; k >= 0; --k) {
-        const float3 Q01 = xmid(P[0], P[1]), Q12 = xmid(P[1], P[2]), Q23 = xmid(P[2], P[3]);
-        const float3 R01 = xmid(Q01, Q12), R12 = xmid(Q12, Q23), M = xmid(R01, R12);
-        const float hwMid = xmul(xadd(hw0, hw3), 0.5f);
-        const float tsh = xmul(tscale, 0.5f);
-        if ((path >> k) & 1u) {
-            P[0] = M;
-            P[1] = R12;
-            P[2] = Q23;
-            hw0 = hwMid;
-            toff = xadd(toff, tsh);
-        } else {
-            P[1] = Q01;
-            P[2] = R01;
-            P[3] = M;
-            hw3 = hwMid;
-        }
-        tscale = tsh;
-    }
-}
-
-// The leaf test of subdivide (CurveBrute.cpp:119-146) on projected end
-// points; returns tRay, or -1 when the leaf is missed.
-__device__ __forceinline__ float ribbon_leaf(float3 c0, float3 c3, float hw0, float hw3, float tmin, float bestT,
-                                             float& tLine) {
-    const float ax = c0.x, ay = c0.y, bx = c3.x, by = c3.y;
-    const float dx = xsub(bx, ax), dy = xsub(by, ay);
-    const float lenSq = xadd(xmul(dx, dx), xmul(dy, dy));
-    if (lenSq < 1e-12f) tLine = 0.f;
-    else
-        tLine = fmaxf(0.f, fminf(1.f, xdiv(xsub(xmul(-ax, dx), xmul(ay, dy)), lenSq)));
-    const float px = xadd(ax, xmul(dx, tLine)), py = xadd(ay, xmul(dy, tLine));
-    const float dist2 = xadd(xmul(px, px), xmul(py, py));
-    const float halfW = xadd(xmul(hw0, xsub(1.f, tLine)), xmul(hw3, tLine));
-    if (dist2 > xmul(halfW, halfW)) return -1.f;
-    const float tRay = xadd(c0.z, xmul(xsub(c3.z, c0.z), tLine));
-    if (tRay < tmin || tRay >= bestT) return -1.f;
-    return tRay;
-}
-
-// Ribbon tests of the curve leaves of a warp's lanes (leaf = kEmptyChild for
-// a lane without one). Every lane of the warp must call it. A closest-hit
-// lane takes a closer ribbon hit into T; an any-hit lane returns true when it
-// found its blocker. err bit 0 is set if the shared stack would overflow
-// (the bound above rules it out).
-template <bool kAny, bool kCount>
-__device__ __forceinline__ bool coop_ribbon_leaves(Traversal& T, const DevScene& S, uint32_t leaf, uint32_t* err,
-                                                   Counters* cnt) {
-    __shared__ RibbonWarp shAll[kRibbonWarps];
-    RibbonWarp& sh = shAll[threadIdx.x >> 5];
-    const uint32_t lane = threadIdx.x & 31u;
-    const bool mine = leaf != kEmptyChild;
-    const unsigned long long init = (static_cast<unsigned long long>(__float_as_uint(T.closest)) << 32) | 0xFFFFFFFFull;
-    if (lane == 0) sh.top = 0;
-    if (mine) {
-        float* f = sh.frame[lane];
-        f[0] = T.r.o.x; f[1] = T.r.o.y; f[2] = T.r.o.z;
-        f[3] = T.fx.x;  f[4] = T.fx.y;  f[5] = T.fx.z;
-        f[6] = T.fy.x;  f[7] = T.fy.y;  f[8] = T.fy.z;
-        f[9] = T.cd.x;  f[10] = T.cd.y; f[11] = T.cd.z;
-        f[12] = T.r.tmin;
-        f[13] = T.closest;
-        sh.best[lane] = init;
-    }
-    __syncwarp();
-    // 1. roots: each lane bounds-tests its own segments (subdivide's entry test)
-    bool anyLocal = false;  // a root walked by this lane alone found a hit
-    if (mine) {
-        const RayFrame fr{T.r.o, T.fx, T.fy, T.cd};
-        const uint32_t off = leaf & 0x01FFFFFFu, c = ((leaf >> 25) & 63u) + 1u;
-        for (uint32_t j = 0; j < c; ++j) {
-            const uint32_t i = off + j;
-            const float4* sp4 = S.segs + 5 * size_t(i);
-            const float4 a = ldg4(sp4), b = ldg4(sp4 + 1), e = ldg4(sp4 + 2), g = ldg4(sp4 + 3);
-            if (kCount) cnt->segs++;
-            const float bestT = __uint_as_float(uint32_t(sh.best[lane] >> 32));
-            const float3 c0 = project(fr, f3(a)), c1 = project(fr, f3(b)), c2 = project(fr, f3(e)),
-                         c3 = project(fr, f3(g));
-            float zlo;
-            if (!ribbon_bounds(c0, c1, c2, c3, a.w, b.w, T.r.tmin, bestT, zlo)) continue;
-            const uint32_t slot = atomicAdd(&sh.top, 1u);
-            if (slot < kRibbonRoots) {
-                sh.node[slot][0] = (lane << 27) | i;
-                sh.node[slot][1] = j << 16;
-                sh.node[slot][2] = __float_as_uint(zlo);
-            } else {  // beyond the shared roots: this lane walks the segment itself
-                atomicSub(&sh.top, 1u);
-                float ts, bt = bestT;
-                float3 tg;
-                if (ribbon_hit(fr, T.r.tmin, f3(a), f3(b), f3(e), f3(g), a.w, b.w, e.w, g.w, bt, ts, tg)) {
-                    // a hit of the lane's own walk enters the shared key marked
-                    // by bit 31 (among equal distances a shared leaf wins, a
-                    // tie of the kind the hit-identity bar excludes)
-                    atomicMin(&sh.best[lane], (static_cast<unsigned long long>(__float_as_uint(bt)) << 32) |
-                                                  0x80000000ull | (j << 6));
-                    T.seg = int32_t(i);
-                    T.tseg = ts;
-                    T.tang = tg;
-                    anyLocal = true;
-                    if (kAny) break;
-                }
-            }
-        }
-    }
-    __syncwarp();
-    // 2. the warp walks the shared trees, up to 32 nodes per step
-    while (true) {
-        const uint32_t top = sh.top;
-        if (top == 0) break;
-        const uint32_t n = min(top, 32u);
-        const bool have = lane < n;
-        uint32_t w0 = 0, w1 = 0, w2 = 0;
-        if (have) {
-            w0 = sh.node[top - n + lane][0];
-            w1 = sh.node[top - n + lane][1];
-            w2 = sh.node[top - n + lane][2];
-        }
-        __syncwarp();
-        if (lane == 0) sh.top = top - n;
-        __syncwarp();
-        if (have) {
-            const uint32_t owner = w0 >> 27, seg = w0 & 0x07FFFFFFu;
-            const uint32_t order = w1 >> 16, depth = (w1 >> 8) & 0xFFu, path = w1 & 0xFFu;
-            const unsigned long long cur = sh.best[owner];
-            const float* f = sh.frame[owner];
-            const float bestT = __uint_as_float(uint32_t(cur >> 32));
-            const bool skip = (kAny && cur != ((static_cast<unsigned long long>(__float_as_uint(f[13])) << 32) |
-                                               0xFFFFFFFFull)) ||
-                              __uint_as_float(w2) > bestT;
-            if (!skip) {
-                const RayFrame fr{f3(f[0], f[1], f[2]), f3(f[3], f[4], f[5]), f3(f[6], f[7], f[8]),
-                                  f3(f[9], f[10], f[11])};
-                const float tmin = f[12];
-                const float4* sp4 = S.segs + 5 * size_t(seg);
-                const float4 a = ldg4(sp4), b = ldg4(sp4 + 1), e = ldg4(sp4 + 2), g = ldg4(sp4 + 3);
-                float3 P[4] = {f3(a), f3(b), f3(e), f3(g)};
-                float hw0 = a.w, hw3 = b.w, toff = e.w, tscale = g.w;
-                ribbon_node(P, hw0, hw3, toff, tscale, depth, path);
-                const float3 c0 = project(fr, P[0]), c3 = project(fr, P[3]);
-                if (depth == 6) {
-                    float tLine;
-                    const float tRay = ribbon_leaf(c0, c3, hw0, hw3, tmin, bestT, tLine);
-                    if (tRay >= 0.f)
-                        atomicMin(&sh.best[owner],
-                                  (static_cast<unsigned long long>(__float_as_uint(tRay)) << 32) | (order << 6) | path);
-                } else {
-                    const float3 Q01 = xmid(P[0], P[1]), Q12 = xmid(P[1], P[2]), Q23 = xmid(P[2], P[3]);
-                    const float3 R01 = xmid(Q01, Q12), R12 = xmid(Q12, Q23), M = xmid(R01, R12);
-                    const float3 cq01 = project(fr, Q01), cr01 = project(fr, R01), cm = project(fr, M),
-                                 cr12 = project(fr, R12), cq23 = project(fr, Q23);
-                    const float hwMid = xmul(xadd(hw0, hw3), 0.5f);
-                    float zl, zr;
-                    const bool okL = ribbon_bounds(c0, cq01, cr01, cm, hw0, hwMid, tmin, bestT, zl);
-                    const bool okR = ribbon_bounds(cm, cr12, cq23, c3, hwMid, hw3, tmin, bestT, zr);
-                    const uint32_t k = uint32_t(okL) + uint32_t(okR);
-                    if (k) {
-                        const uint32_t slot = atomicAdd(&sh.top, k);
-                        if (slot + k > kRibbonStack) {
-                            atomicOr(err, 1u);
-                        } else {
-                            uint32_t s = slot;
-                            const uint32_t d1 = (order << 16) | ((depth + 1u) << 8);
-                            if (okL) {
-                                sh.node[s][0] = w0;
-                                sh.node[s][1] = d1 | (path << 1);
-                                sh.node[s][2] = __float_as_uint(zl);
-                                ++s;
-                            }
-                            if (okR) {
-                                sh.node[s][0] = w0;
-                                sh.node[s][1] = d1 | (path << 1) | 1u;
-                                sh.node[s][2] = __float_as_uint(zr);
-                            }
-                        }
-                    }
-                }
-            }
-        }
-        __syncwarp();
-        if (sh.top > kRibbonStack) {  // overflow (ruled out by the bound): stop the walk
-            __syncwarp();
-            if (lane == 0) sh.top = 0;
-            __syncwarp();
-        }
-    }
-    // 3. owners take their closest leaf
-    bool found = anyLocal;
-    if (mine) {
-        const unsigned long long k = sh.best[lane];
-        if (k != init && !(k & 0x80000000ull)) {  // a shared leaf won: evaluate it for tSeg and the tangent
-            const uint32_t j = uint32_t(k >> 6) & 63u, path = uint32_t(k) & 63u;
-            const uint32_t i = (leaf & 0x01FFFFFFu) + j;
-            const float4* sp4 = S.segs + 5 * size_t(i);
-            const float4 a = ldg4(sp4), b = ldg4(sp4 + 1), e = ldg4(sp4 + 2), g = ldg4(sp4 + 3);
-            float3 P[4] = {f3(a), f3(b), f3(e), f3(g)};
-            float hw0 = a.w, hw3 = b.w, toff = e.w, tscale = g.w;
-            ribbon_node(P, hw0, hw3, toff, tscale, 6, path);
-            const RayFrame fr{T.r.o, T.fx, T.fy, T.cd};
-            float tLine;
-            ribbon_leaf(project(fr, P[0]), project(fr, P[3]), hw0, hw3, T.r.tmin, INFINITY, tLine);
-            float3 tg = bezier_tangent(P[0], P[1], P[2], P[3], tLine);
-            if (xdot(tg, tg) < 1e-12f) tg = xsub3(P[3], P[0]);
-            const float len = __fsqrt_rn(xdot(tg, tg));
-            T.tang = len > 1e-8f ? xmul3(tg, xdiv(1.f, len)) : f3(0.f, 0.f, 1.f);
-            T.tseg = xadd(toff, xmul(tLine, tscale));
-            T.seg = int32_t(i);
-            found = true;
-        }
-        if (k != init) T.closest = __uint_as_float(uint32_t(k >> 32));
-    }
-    __syncwarp();
-    return kAny && found;
-}
-
-// ---------------------------------------------------------------------------
 // Curve stage of a traversal (CurveBrute::trace's curve pass,
 // CurveBrute.cpp:398-440): after the triangle BVH, the curve BVH is traversed
 // from the triangle hit distance, keeping only strictly closer ribbon hits.
@@ -947,23 +694,14 @@ __device__ __forceinline__ void persistent_traverse(const DevScene& S, uint32_t 
                 break;
             if (want) node_step<kAny, kCount, kCurves>(T, S, stack, stackT, err, cnt);
         }
-        // 3. leaf phase: one leaf per lane; the curve leaves of the warp are
-        // tested together (coop_ribbon_leaves)
-        {
-            uint32_t leaf = kEmptyChild;
-            const bool fromParked = active && parked != kEmptyChild;
-            if (fromParked) leaf = parked;
-            else if (active && !T.exhausted && (T.cur & 0x80000000u)) leaf = T.cur;
-            const bool curveLeaf = kCurves && leaf != kEmptyChild && T.stage != 0;
-            bool blocked = false;
-            if (leaf != kEmptyChild && !curveLeaf) blocked = leaf_test<kAny, kCount, kMotion>(T, S, leaf, cnt);
-            if constexpr (kCurves) {
-                if (coop_ribbon_leaves<kAny, kCount>(T, S, curveLeaf ? leaf : kEmptyChild, err, cnt)) blocked = true;
-            }
-            if (leaf != kEmptyChild) {
-                if (blocked) T.exhausted = true;
-                else if (!fromParked && !trav_pop<kAny>(T, stack, stackT)) T.exhausted = true;
+        // 3. leaf phase: one leaf per lane
+        if (active) {
+            if (parked != kEmptyChild) {
+                if (leaf_step<kAny, kCount, kCurves, kMotion>(T, S, parked, cnt)) T.exhausted = true;
                 parked = kEmptyChild;
+            } else if (!T.exhausted && (T.cur & 0x80000000u)) {
+                if (leaf_step<kAny, kCount, kCurves, kMotion>(T, S, T.cur, cnt)) T.exhausted = true;
+                else if (!trav_pop<kAny>(T, stack, stackT)) T.exhausted = true;
             }
         }
         if (active && T.exhausted && parked == kEmptyChild) {
