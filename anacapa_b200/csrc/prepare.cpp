@@ -656,7 +656,12 @@ int prepare_scene(const ana_scene_desc& d, Prepared& P, std::string& err, bool t
         }
     }
     uint32_t maxLeafT = d.max_leaf_tris ? d.max_leaf_tris : 4;
-    uint32_t maxLeafS = d.max_leaf_segments ? d.max_leaf_segments : 4;
+    // Curve leaves default to one segment (the reference builds leaves of 4,
+    // CurveBrute.cpp:455): the 4-wide nodes then bounds-test every segment's
+    // own box before its ribbon test, which culls most root projections
+    // (1280x720x32 hair frame: 1085 ms against 1367 ms with leaves of 4). The
+    // tree is still the reference's median split, so hits are the same.
+    uint32_t maxLeafS = d.max_leaf_segments ? d.max_leaf_segments : 1;
     if (maxLeafT > 64 || maxLeafS > 64) return bad("leaf size > 64");
     P.tri_isect.clear();
     if (P.tris_on_device) {

@@ -178,7 +178,8 @@ typedef struct ana_scene_desc {
     ana_camera camera;
 
     /* BVH build: maximum triangles / curve segments per leaf (reference: 4,
-     * BVHBackend.h:67, CurveBrute.cpp:455). 0 = default. */
+     * BVHBackend.h:67, CurveBrute.cpp:455). 0 = default: 4 triangles, 1 curve
+     * segment (the same hits; each segment's box is tested in its node). */
     uint32_t max_leaf_tris;
     uint32_t max_leaf_segments;
 
