@@ -213,14 +213,15 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def extend_traffic_per_ray():
-    """DRAM bytes per closest-hit ray of the extend kernel, from the committed
-    ncu summary (profiles/extend_throughput.md), or None."""
+def extend_profile_field(name):
+    """A figure of the committed ncu summary of the extend kernel
+    (profiles/extend_throughput.md, lines `name: value`), or None:
+    dram_bytes_per_ray, lanes_active_per_instruction, l2_throughput_pct."""
     p = os.path.join(ROOT, "profiles", "extend_throughput.md")
     if not os.path.exists(p):
         return None
     for line in open(p):
-        if line.startswith("dram_bytes_per_ray:"):
+        if line.startswith(name + ":"):
             try:
                 return float(line.split(":", 1)[1].split()[0])
             except ValueError:
@@ -625,7 +626,7 @@ def run_ours(a):
                  + (32 + 16) * work.extend_rays)
     peak, peak_kind = measured_peaks()
     achieved = (alg_bytes / ext_launches) / ((ext_ms / ext_launches) / 1e3) / 1e9 if ext_ms > 0 else None
-    tpr = extend_traffic_per_ray() if a.scene == "throughput" else None  # measured on that scene
+    tpr = extend_profile_field("dram_bytes_per_ray") if a.scene == "throughput" else None  # measured on that scene
     traffic = (tpr * work.extend_rays / ext_launches) if tpr else None
     # the last timed frame against the FP64 windows of the configuration frame
     rmse = None
@@ -678,7 +679,14 @@ def run_ours(a):
                          "frac": (achieved / peak) if achieved else None,
                          "peak_kind": peak_kind, "traffic": traffic,
                          "alg_bytes_per_launch": alg_bytes / ext_launches,
-                         "launches_per_step": ext_launches},
+                         "launches_per_step": ext_launches,
+                         # the roof that binds (ncu, profiles/extend_throughput.md): issue and
+                         # the L1 data path, not HBM or L2
+                         "binding": {"limiter": "instruction issue / L1 (node and triangle gathers)",
+                                     "lanes_active_per_instruction_of_32":
+                                         extend_profile_field("lanes_active_per_instruction"),
+                                     "l2_throughput_pct_of_peak": extend_profile_field("l2_throughput_pct")}
+                         if a.scene == "throughput" else None},
             "gpu_launches": launches,
             "rmse_vs_fp64": rmse,
             "e2e": e2e,
