@@ -102,8 +102,9 @@ struct Counters {
 //   2. interior phase: lanes descend interior nodes until they reach a
 //      leaf; the phase ends when every lane has a leaf to test (or nothing
 //      left), when no lane can take another interior step, or when at most
-//      kLeafPhaseLanes lanes still descend while others wait with a leaf, so
-//      lanes stay converged on the node-test code. Any-hit queries are speculative
+//      kLeafPhaseLanes (any hit: kLeafPhaseLanesAny) lanes still descend
+//      while others wait with a leaf, so lanes stay converged on the
+//      node-test code. Any-hit queries are speculative
 //      (Aila and Laine, "Understanding the efficiency of ray traversal on
 //      GPUs", 2009): a lane that reaches a leaf parks it and keeps descending
 //      from its next stack entry. Closest-hit queries do not speculate: a
@@ -117,11 +118,15 @@ struct Counters {
 // tests are the same functions as above, so results are identical.
 // ---------------------------------------------------------------------------
 // Interior phases end once this few lanes still descend (and a lane has a
-// leaf): on the 1920x1080x64 throughput frame the extend stage took 142.0 ms
+// leaf). On the 1920x1080x64 throughput frame the extend stage took 142.0 ms
 // when the phase ran until no lane descended, 118.4 ms at 4 lanes, 117.2 ms at
-// 8 and 124.6 ms at 16; the any-hit shadow / MIS stages 60.3 / 86.2 ms, 56.4 /
-// 80.6 ms at 4 and 54.9 / 77.9 ms at 8; hits and occlusion answers unchanged.
-constexpr uint32_t kLeafPhaseLanes = 8;
+// 8 and 124.6 ms at 16; the any-hit shadow + MIS stages 146.5 ms, 137.0 at 4,
+// 132.8 at 8, 128.1 at 16, 129.8 at 24 and 191.2 at 32. Kernels with
+// motion-blurred meshes, whose leaf tests invert interpolated matrices, keep
+// the phase until no lane descends (1280x720x16 motion frame: 25.9 ms against
+// 28.6 ms at 8 / 16 lanes). Hits and occlusion answers are unchanged.
+constexpr uint32_t kLeafPhaseLanes = 8;      // closest hit
+constexpr uint32_t kLeafPhaseLanesAny = 16;  // any hit (parked leaves)
 
 struct Traversal {
     TriRay r;
@@ -683,12 +688,13 @@ __device__ __forceinline__ void persistent_traverse(const DevScene& S, uint32_t 
             const bool ready = !active || T.exhausted || (kAny ? parked != kEmptyChild : bool(T.cur & 0x80000000u));
             const uint32_t wantMask = __ballot_sync(0xFFFFFFFFu, want);
             if (!wantMask || __all_sync(0xFFFFFFFFu, ready)) break;
-            // Once at most kLeafPhaseLanes lanes still descend and another
-            // lane holds a leaf (any hit: a parked one), the phase ends and the
+            // Once at most kPhaseLanes lanes still descend and another lane
+            // holds a leaf (any hit: a parked one), the phase ends and the
             // leaves are tested (the descending lanes resume in the next
             // interior phase), so few lanes do not hold the warp in the node
             // loop. A lane with a leaf must exist, so every pass makes progress.
-            if (__popc(wantMask) <= kLeafPhaseLanes &&
+            constexpr uint32_t kPhaseLanes = kMotion ? 0u : (kAny ? kLeafPhaseLanesAny : kLeafPhaseLanes);
+            if (kPhaseLanes > 0 && __popc(wantMask) <= kPhaseLanes &&
                 __any_sync(0xFFFFFFFFu, active && !T.exhausted &&
                                             (kAny ? parked != kEmptyChild : bool(T.cur & 0x80000000u))))
                 break;
