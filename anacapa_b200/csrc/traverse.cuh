@@ -164,17 +164,59 @@ __device__ __forceinline__ void trav_init(Traversal& T, const Ray& ray, uint32_t
     T.seg = -1;
 }
 
+// Traversal stack of one thread: (entry, entry distance) pairs. The first
+// kShortStack entries live in shared memory, laid out entry-major (entry k of
+// thread t at [k][t]), so lanes at different depths hit different banks and a
+// warp's access is one wavefront; deeper entries (rare) live in local memory,
+// where lanes at different depths touch different cache lines.
+constexpr int kShortStack = 12;
+constexpr int kStackThreads = 256;  // threads per block of every traversal kernel
+struct TravStack {
+    uint32_t* sn;  // this thread's column of the shared entries
+    float* sk;     // and of their distances
+    uint32_t ln[kMaxStack4 - kShortStack];
+    float lk[kMaxStack4 - kShortStack];
+    __device__ __forceinline__ void put(int k, uint32_t v, float key) {
+        if (k < kShortStack) {
+            sn[k * kStackThreads] = v;
+            sk[k * kStackThreads] = key;
+        } else {
+            ln[k - kShortStack] = v;
+            lk[k - kShortStack] = key;
+        }
+    }
+    __device__ __forceinline__ void put_node(int k, uint32_t v) {
+        if (k < kShortStack) sn[k * kStackThreads] = v;
+        else ln[k - kShortStack] = v;
+    }
+    __device__ __forceinline__ uint32_t node(int k) const {
+        return k < kShortStack ? sn[k * kStackThreads] : ln[k - kShortStack];
+    }
+    __device__ __forceinline__ float key(int k) const {
+        return k < kShortStack ? sk[k * kStackThreads] : lk[k - kShortStack];
+    }
+};
+
+// The shared part of the stacks of a block's threads; every thread of the
+// block calls it once and keeps its TravStack.
+#define ANA_TRAV_STACK(name)                                                        \
+    __shared__ uint32_t name##_sn[kShortStack][kStackThreads];                      \
+    __shared__ float name##_sk[kShortStack][kStackThreads];                         \
+    TravStack name;                                                                 \
+    name.sn = &name##_sn[0][threadIdx.x];                                           \
+    name.sk = &name##_sk[0][threadIdx.x]
+
 template <bool kAny = false>
-__device__ __forceinline__ bool trav_pop(Traversal& T, const uint32_t* stack, const float* stackT) {
+__device__ __forceinline__ bool trav_pop(Traversal& T, const TravStack& stk) {
     if (kAny) {  // an any-hit query ends at its first hit: nothing on the stack is culled
         if (T.sp == 0) return false;
-        T.cur = stack[--T.sp];
+        T.cur = stk.node(--T.sp);
         return true;
     }
     while (T.sp > 0) {
         --T.sp;
-        if (stackT[T.sp] > T.closest) continue;
-        T.cur = stack[T.sp];
+        if (stk.key(T.sp) > T.closest) continue;
+        T.cur = stk.node(T.sp);
         return true;
     }
     return false;
@@ -211,11 +253,11 @@ __device__ __forceinline__ void cswap(float& ka, uint32_t& va, float& kb, uint32
 // steps of incoherent rays) skip the network with the same result (extend
 // stage of the throughput frame: 146.6 -> 141.9 ms). Shared by the triangle
 // and the curve BVH steps.
-__device__ __forceinline__ void enter_near_first(Traversal& T, float (&key)[4], uint32_t (&ref)[4], uint32_t* stack,
-                                                 float* stackT, uint32_t* err) {
+__device__ __forceinline__ void enter_near_first(Traversal& T, float (&key)[4], uint32_t (&ref)[4], TravStack& stk,
+                                                 uint32_t* err) {
     const int n = int(key[0] < INFINITY) + int(key[1] < INFINITY) + int(key[2] < INFINITY) + int(key[3] < INFINITY);
     if (n == 0) {
-        if (!trav_pop(T, stack, stackT)) T.exhausted = true;
+        if (!trav_pop(T, stk)) T.exhausted = true;
         return;
     }
     if (n == 1) {  // one child entered: it becomes the current node
@@ -235,8 +277,7 @@ __device__ __forceinline__ void enter_near_first(Traversal& T, float (&key)[4], 
             return;
         }
         cswap(ka, ra, kb, rb);
-        stack[T.sp] = rb;
-        stackT[T.sp] = kb;
+        stk.put(T.sp, rb, kb);
         ++T.sp;
         T.cur = ra;
         return;
@@ -255,8 +296,7 @@ __device__ __forceinline__ void enter_near_first(Traversal& T, float (&key)[4], 
 #pragma unroll
     for (int k = 3; k >= 1; --k) {
         if (k < n) {
-            stack[T.sp] = ref[k];
-            stackT[T.sp] = key[k];
+            stk.put(T.sp, ref[k], key[k]);
             ++T.sp;
         }
     }
@@ -264,7 +304,7 @@ __device__ __forceinline__ void enter_near_first(Traversal& T, float (&key)[4], 
 }
 
 template <bool kAny, bool kCount>
-__device__ __forceinline__ void trav_interior(Traversal& T, const DevScene& S, uint32_t* stack, float* stackT,
+__device__ __forceinline__ void trav_interior(Traversal& T, const DevScene& S, TravStack& stk,
                                               uint32_t* err, Counters* cnt) {
     const float4* np = reinterpret_cast<const float4*>(S.tri_nodes + T.cur);
     const float4 lx = ldg4(np), hx = ldg4(np + 1), ly = ldg4(np + 2), hy = ldg4(np + 3), lz = ldg4(np + 4),
@@ -287,7 +327,7 @@ __device__ __forceinline__ void trav_interior(Traversal& T, const DevScene& S, u
     if constexpr (kAny) {  // any hit: children entered in stored order, no distance sort
         const int n = int(key[0] < INFINITY) + int(key[1] < INFINITY) + int(key[2] < INFINITY) + int(key[3] < INFINITY);
         if (n == 0) {
-            if (!trav_pop<kAny>(T, stack, stackT)) T.exhausted = true;
+            if (!trav_pop<kAny>(T, stk)) T.exhausted = true;
             return;
         }
         if (T.sp + n - 1 > int(kMaxStack4)) {
@@ -299,14 +339,14 @@ __device__ __forceinline__ void trav_interior(Traversal& T, const DevScene& S, u
 #pragma unroll
         for (int k = 3; k >= 0; --k) {
             if (key[k] < INFINITY) {
-                if (first != kEmptyChild) stack[T.sp++] = first;
+                if (first != kEmptyChild) stk.put_node(T.sp++, first);
                 first = ref[k];
             }
         }
         T.cur = first;
         return;
     }
-    enter_near_first(T, key, ref, stack, stackT, err);
+    enter_near_first(T, key, ref, stk, err);
 }
 
 // BVHBackend::makeObjectSpaceRay4: the world ray (origin, exact direction)
@@ -364,13 +404,12 @@ __device__ __forceinline__ bool leaf_test(Traversal& T, const DevScene& S, uint3
 
 // Leaf step of the one-thread-per-ray schedule: test the current leaf, then pop.
 template <bool kAny, bool kCount>
-__device__ __forceinline__ void trav_leaf(Traversal& T, const DevScene& S, const uint32_t* stack,
-                                          const float* stackT, Counters* cnt) {
+__device__ __forceinline__ void trav_leaf(Traversal& T, const DevScene& S, const TravStack& stk, Counters* cnt) {
     if (leaf_test<kAny, kCount>(T, S, T.cur, cnt)) {
         T.exhausted = true;
         return;
     }
-    if (!trav_pop<kAny>(T, stack, stackT)) T.exhausted = true;
+    if (!trav_pop<kAny>(T, stk)) T.exhausted = true;
 }
 
 // ===========================================================================
@@ -467,12 +506,33 @@ __device__ __forceinline__ bool ribbon_bounds(float3 c0, float3 c1, float3 c2, f
 }
 
 struct SubSeg {
-    float3 P0, P1, P2, P3;  // world-space control points (further splits, tangent)
-    float3 c0, c3;          // projected end points
-    float hw0, hw3, toff, tscale;
+    float3 P0, P1, P2, P3;  // world-space control points
     float zlo;              // zMin - maxHalfW: the test that depends on bestT
-    int depth;
+    uint32_t dp;            // depth (bits 0-2, 6 = root) | path from the root (bits 3-8, 1 = right)
 };
+
+// The half-widths and strand-parameter interval of the node (depth, path)
+// below a segment's (hw0r, hw3r, toffr, tscr): the splits' own updates
+// (CurveBrute.cpp:152-176) replayed from the root.
+__device__ __forceinline__ void ribbon_params(uint32_t dp, float hw0r, float hw3r, float toffr, float tscr,
+                                              float& hw0, float& hw3, float& toff, float& tscale) {
+    const int levels = 6 - int(dp & 7u);
+    const uint32_t path = dp >> 3;
+    hw0 = hw0r;
+    hw3 = hw3r;
+    toff = toffr;
+    tscale = tscr;
+    for (int k = levels - 1; k >= 0; --k) {
+        const float hm = xmul(xadd(hw0, hw3), 0.5f), tsh = xmul(tscale, 0.5f);
+        if ((path >> k) & 1u) {
+            hw0 = hm;
+            toff = xadd(toff, tsh);
+        } else {
+            hw3 = hm;
+        }
+        tscale = tsh;
+    }
+}
 
 // subdivide (CurveBrute.cpp:85-176): depth-6 de Casteljau subdivision in ray
 // space, the left half first, updating bestT on a closer hit. The reference
@@ -483,27 +543,33 @@ struct SubSeg {
 // pushed. The one test that depends on bestT (which only decreases) is
 // repeated when a child is popped, so every node is accepted or culled, and
 // every leaf evaluated, exactly as in the recursion and in the same order.
-// (A walk that kept no per-level copies, rebuilding each right half from the
-// segment's four points along the path, measured slower on the 1280x720x32
-// hair frame: extend 1024 against 842 ms, shadow 618 against 525 ms; the
-// entries stay in local memory, served by L1.)
+// A stack entry keeps the node's four world points, that test's bound and its
+// (depth, path); the end points' projections are recomputed at a pop and the
+// half-widths and parameter interval replayed along the path with the same
+// operations (56 instead of 100 bytes per entry: hair frame's shadow stage
+// 398.6 -> 379.3 ms). (A walk that kept no points at all, rebuilding each
+// right half from the segment's four points along its path, measured slower:
+// extend 1024 against 842 ms at leaves of four.)
 __device__ __forceinline__ bool ribbon_hit(const RayFrame& fr, float tmin, float3 P0, float3 P1, float3 P2,
-                                           float3 P3, float hw0, float hw3, float toff, float tscale,
+                                           float3 P3, float hw0r, float hw3r, float toffr, float tscaler,
                                            float& bestT, float& tSeg, float3& tang) {
     SubSeg st[8];
     int sp = 0;
     {
         const float3 c0 = project(fr, P0), c1 = project(fr, P1), c2 = project(fr, P2), c3 = project(fr, P3);
         float zlo;
-        if (!ribbon_bounds(c0, c1, c2, c3, hw0, hw3, tmin, bestT, zlo)) return false;
-        st[sp++] = SubSeg{P0, P1, P2, P3, c0, c3, hw0, hw3, toff, tscale, zlo, 6};
+        if (!ribbon_bounds(c0, c1, c2, c3, hw0r, hw3r, tmin, bestT, zlo)) return false;
+        st[sp++] = SubSeg{P0, P1, P2, P3, zlo, 6u};
     }
     bool hit = false;
     while (sp > 0) {
         const SubSeg s = st[--sp];
         if (s.zlo > bestT) continue;
-        if (s.depth == 0) {
-            const float ax = s.c0.x, ay = s.c0.y, bx = s.c3.x, by = s.c3.y;
+        float hw0, hw3, toff, tscale;
+        ribbon_params(s.dp, hw0r, hw3r, toffr, tscaler, hw0, hw3, toff, tscale);
+        const float3 c0 = project(fr, s.P0), c3 = project(fr, s.P3);
+        if ((s.dp & 7u) == 0u) {
+            const float ax = c0.x, ay = c0.y, bx = c3.x, by = c3.y;
             const float dx = xsub(bx, ax), dy = xsub(by, ay);
             const float lenSq = xadd(xmul(dx, dx), xmul(dy, dy));
             float tLine;
@@ -512,32 +578,31 @@ __device__ __forceinline__ bool ribbon_hit(const RayFrame& fr, float tmin, float
                 tLine = fmaxf(0.f, fminf(1.f, xdiv(xsub(xmul(-ax, dx), xmul(ay, dy)), lenSq)));
             const float px = xadd(ax, xmul(dx, tLine)), py = xadd(ay, xmul(dy, tLine));
             const float dist2 = xadd(xmul(px, px), xmul(py, py));
-            const float halfW = xadd(xmul(s.hw0, xsub(1.f, tLine)), xmul(s.hw3, tLine));
+            const float halfW = xadd(xmul(hw0, xsub(1.f, tLine)), xmul(hw3, tLine));
             if (dist2 > xmul(halfW, halfW)) continue;
-            const float tRay = xadd(s.c0.z, xmul(xsub(s.c3.z, s.c0.z), tLine));
+            const float tRay = xadd(c0.z, xmul(xsub(c3.z, c0.z), tLine));
             if (tRay < tmin || tRay >= bestT) continue;
             float3 tg = bezier_tangent(s.P0, s.P1, s.P2, s.P3, tLine);
             if (xdot(tg, tg) < 1e-12f) tg = xsub3(s.P3, s.P0);
             const float len = __fsqrt_rn(xdot(tg, tg));
             tg = len > 1e-8f ? xmul3(tg, xdiv(1.f, len)) : f3(0.f, 0.f, 1.f);
             bestT = tRay;
-            tSeg = xadd(s.toff, xmul(tLine, s.tscale));
+            tSeg = xadd(toff, xmul(tLine, tscale));
             tang = tg;
             hit = true;
             continue;
         }
-        // bezierSplitMid (CurveBrute.cpp:66-80)
         const float3 Q01 = xmid(s.P0, s.P1), Q12 = xmid(s.P1, s.P2), Q23 = xmid(s.P2, s.P3);
         const float3 R01 = xmid(Q01, Q12), R12 = xmid(Q12, Q23), M = xmid(R01, R12);
         const float3 cq01 = project(fr, Q01), cr01 = project(fr, R01), cm = project(fr, M),
                      cr12 = project(fr, R12), cq23 = project(fr, Q23);
-        const float hwMid = xmul(xadd(s.hw0, s.hw3), 0.5f);
-        const float tsh = xmul(s.tscale, 0.5f);
+        const float hwMid = xmul(xadd(hw0, hw3), 0.5f);
         float zl, zr;
-        const bool okL = ribbon_bounds(s.c0, cq01, cr01, cm, s.hw0, hwMid, tmin, bestT, zl);
-        const bool okR = ribbon_bounds(cm, cr12, cq23, s.c3, hwMid, s.hw3, tmin, bestT, zr);
-        if (okR) st[sp++] = SubSeg{M, R12, Q23, s.P3, cm, s.c3, hwMid, s.hw3, xadd(s.toff, tsh), tsh, zr, s.depth - 1};
-        if (okL) st[sp++] = SubSeg{s.P0, Q01, R01, M, s.c0, cm, s.hw0, hwMid, s.toff, tsh, zl, s.depth - 1};
+        const bool okL = ribbon_bounds(c0, cq01, cr01, cm, hw0, hwMid, tmin, bestT, zl);
+        const bool okR = ribbon_bounds(cm, cr12, cq23, c3, hwMid, hw3, tmin, bestT, zr);
+        const uint32_t cd = (s.dp & 7u) - 1u, cp = (s.dp >> 3) << 1;
+        if (okR) st[sp++] = SubSeg{M, R12, Q23, s.P3, zr, cd | ((cp | 1u) << 3)};
+        if (okL) st[sp++] = SubSeg{s.P0, Q01, R01, M, zl, cd | (cp << 3)};
     }
     return hit;
 }
@@ -563,7 +628,7 @@ __device__ __forceinline__ void curve_begin(Traversal& T, float3 d, uint32_t seg
 // first for closest and any hit alike (on the hair frame near-first any-hit
 // steps measured faster than the stored order).
 template <bool kCount>
-__device__ __forceinline__ void curve_interior(Traversal& T, const DevScene& S, uint32_t* stack, float* stackT,
+__device__ __forceinline__ void curve_interior(Traversal& T, const DevScene& S, TravStack& stk,
                                                uint32_t* err, Counters* cnt) {
     const Ray ray{T.r.o, T.cd, T.r.tmin, T.r.tmax};
     const float4* np = reinterpret_cast<const float4*>(S.seg_nodes + T.cur);
@@ -582,7 +647,7 @@ __device__ __forceinline__ void curve_interior(Traversal& T, const DevScene& S, 
                        curve_box_hit(ray, T.cinv, l0[k], h0[k], l1[k], h1[k], l2[k], h2[k], T.closest, tn);
         key[k] = h ? tn : INFINITY;
     }
-    enter_near_first(T, key, ref, stack, stackT, err);
+    enter_near_first(T, key, ref, stk, err);
 }
 
 // Ribbon tests of one curve leaf; true when an any-hit query found its blocker.
@@ -609,10 +674,10 @@ __device__ __forceinline__ bool curve_leaf_test(Traversal& T, const DevScene& S,
 
 // Stage dispatch of the node and leaf steps.
 template <bool kAny, bool kCount, bool kCurves>
-__device__ __forceinline__ void node_step(Traversal& T, const DevScene& S, uint32_t* stack, float* stackT,
+__device__ __forceinline__ void node_step(Traversal& T, const DevScene& S, TravStack& stk,
                                           uint32_t* err, Counters* cnt) {
-    if (kCurves && T.stage) curve_interior<kCount>(T, S, stack, stackT, err, cnt);
-    else trav_interior<kAny, kCount>(T, S, stack, stackT, err, cnt);
+    if (kCurves && T.stage) curve_interior<kCount>(T, S, stk, err, cnt);
+    else trav_interior<kAny, kCount>(T, S, stk, err, cnt);
 }
 template <bool kAny, bool kCount, bool kCurves, bool kMotion = false>
 __device__ __forceinline__ bool leaf_step(Traversal& T, const DevScene& S, uint32_t leaf, Counters* cnt) {
@@ -651,8 +716,7 @@ __device__ __forceinline__ void persistent_traverse(const DevScene& S, uint32_t 
                                                     Counters* cnt, Load load, Done done) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t ltmask = (1u << lane) - 1u;
-    uint32_t stack[kMaxStack4];
-    float stackT[kMaxStack4];
+    ANA_TRAV_STACK(stk);
     Traversal T;
     bool active = false, drained = false;
     uint32_t idx = 0, parked = kEmptyChild;
@@ -682,7 +746,7 @@ __device__ __forceinline__ void persistent_traverse(const DevScene& S, uint32_t 
         while (true) {
             if (kAny && active && !T.exhausted && (T.cur & 0x80000000u) && parked == kEmptyChild) {
                 parked = T.cur;
-                if (!trav_pop<kAny>(T, stack, stackT)) T.exhausted = true;
+                if (!trav_pop<kAny>(T, stk)) T.exhausted = true;
             }
             const bool want = active && !T.exhausted && !(T.cur & 0x80000000u);
             const bool ready = !active || T.exhausted || (kAny ? parked != kEmptyChild : bool(T.cur & 0x80000000u));
@@ -698,7 +762,7 @@ __device__ __forceinline__ void persistent_traverse(const DevScene& S, uint32_t 
                 __any_sync(0xFFFFFFFFu, active && !T.exhausted &&
                                             (kAny ? parked != kEmptyChild : bool(T.cur & 0x80000000u))))
                 break;
-            if (want) node_step<kAny, kCount, kCurves>(T, S, stack, stackT, err, cnt);
+            if (want) node_step<kAny, kCount, kCurves>(T, S, stk, err, cnt);
         }
         // 3. leaf phase: one leaf per lane
         if (active) {
@@ -707,7 +771,7 @@ __device__ __forceinline__ void persistent_traverse(const DevScene& S, uint32_t 
                 parked = kEmptyChild;
             } else if (!T.exhausted && (T.cur & 0x80000000u)) {
                 if (leaf_step<kAny, kCount, kCurves, kMotion>(T, S, T.cur, cnt)) T.exhausted = true;
-                else if (!trav_pop<kAny>(T, stack, stackT)) T.exhausted = true;
+                else if (!trav_pop<kAny>(T, stk)) T.exhausted = true;
             }
         }
         if (active && T.exhausted && parked == kEmptyChild) {
