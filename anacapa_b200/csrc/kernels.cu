@@ -34,7 +34,6 @@ namespace ana {
 constexpr uint32_t kMiss = 0xFFFFFFFFu;
 constexpr int kMaxBlock = 1024;
 constexpr int kPersistBlock = 256;    // traversal kernels: 8 warps per block
-static_assert(kPersistBlock == kStackThreads, "traversal blocks hold one shared stack column per thread");
 constexpr int kPersistMinBlocks = 5;  // persistent schedule: 5 resident blocks/SM (<= 51 registers)
 // k_shade runs at most 256-thread blocks: three resident per SM (80 registers,
 // spilling to L1) for the forward kernel without fiber code measured 5 % faster
@@ -261,7 +260,8 @@ __device__ __forceinline__ void run_traversal(const DevScene& S, uint32_t n, uin
     if constexpr (kPersist) {
         persistent_traverse<kAny, kCount, kCurves, kMotion>(S, n, fetch, err, cnt, load, done);
     } else {
-        ANA_TRAV_STACK(stk);
+        uint32_t stack[kMaxStack4];
+        float stackT[kMaxStack4];
         for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
             Ray ray;
             uint32_t root, segRoot;
@@ -272,10 +272,10 @@ __device__ __forceinline__ void run_traversal(const DevScene& S, uint32_t n, uin
                 while (true) {
                     while (!T.exhausted) {
                         if (!(T.cur & 0x80000000u)) {
-                            node_step<kAny, kCount, kCurves>(T, S, stk, err, cnt);
+                            node_step<kAny, kCount, kCurves>(T, S, stack, stackT, err, cnt);
                         } else if (leaf_step<kAny, kCount, kCurves, kMotion>(T, S, T.cur, cnt)) {
                             T.exhausted = true;
-                        } else if (!trav_pop<kAny>(T, stk)) {
+                        } else if (!trav_pop<kAny>(T, stack, stackT)) {
                             T.exhausted = true;
                         }
                     }

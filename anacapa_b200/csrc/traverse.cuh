@@ -164,59 +164,17 @@ __device__ __forceinline__ void trav_init(Traversal& T, const Ray& ray, uint32_t
     T.seg = -1;
 }
 
-// Traversal stack of one thread: (entry, entry distance) pairs. The first
-// kShortStack entries live in shared memory, laid out entry-major (entry k of
-// thread t at [k][t]), so lanes at different depths hit different banks and a
-// warp's access is one wavefront; deeper entries (rare) live in local memory,
-// where lanes at different depths touch different cache lines.
-constexpr int kShortStack = 12;
-constexpr int kStackThreads = 256;  // threads per block of every traversal kernel
-struct TravStack {
-    uint32_t* sn;  // this thread's column of the shared entries
-    float* sk;     // and of their distances
-    uint32_t ln[kMaxStack4 - kShortStack];
-    float lk[kMaxStack4 - kShortStack];
-    __device__ __forceinline__ void put(int k, uint32_t v, float key) {
-        if (k < kShortStack) {
-            sn[k * kStackThreads] = v;
-            sk[k * kStackThreads] = key;
-        } else {
-            ln[k - kShortStack] = v;
-            lk[k - kShortStack] = key;
-        }
-    }
-    __device__ __forceinline__ void put_node(int k, uint32_t v) {
-        if (k < kShortStack) sn[k * kStackThreads] = v;
-        else ln[k - kShortStack] = v;
-    }
-    __device__ __forceinline__ uint32_t node(int k) const {
-        return k < kShortStack ? sn[k * kStackThreads] : ln[k - kShortStack];
-    }
-    __device__ __forceinline__ float key(int k) const {
-        return k < kShortStack ? sk[k * kStackThreads] : lk[k - kShortStack];
-    }
-};
-
-// The shared part of the stacks of a block's threads; every thread of the
-// block calls it once and keeps its TravStack.
-#define ANA_TRAV_STACK(name)                                                        \
-    __shared__ uint32_t name##_sn[kShortStack][kStackThreads];                      \
-    __shared__ float name##_sk[kShortStack][kStackThreads];                         \
-    TravStack name;                                                                 \
-    name.sn = &name##_sn[0][threadIdx.x];                                           \
-    name.sk = &name##_sk[0][threadIdx.x]
-
 template <bool kAny = false>
-__device__ __forceinline__ bool trav_pop(Traversal& T, const TravStack& stk) {
+__device__ __forceinline__ bool trav_pop(Traversal& T, const uint32_t* stack, const float* stackT) {
     if (kAny) {  // an any-hit query ends at its first hit: nothing on the stack is culled
         if (T.sp == 0) return false;
-        T.cur = stk.node(--T.sp);
+        T.cur = stack[--T.sp];
         return true;
     }
     while (T.sp > 0) {
         --T.sp;
-        if (stk.key(T.sp) > T.closest) continue;
-        T.cur = stk.node(T.sp);
+        if (stackT[T.sp] > T.closest) continue;
+        T.cur = stack[T.sp];
         return true;
     }
     return false;
@@ -253,11 +211,11 @@ __device__ __forceinline__ void cswap(float& ka, uint32_t& va, float& kb, uint32
 // steps of incoherent rays) skip the network with the same result (extend
 // stage of the throughput frame: 146.6 -> 141.9 ms). Shared by the triangle
 // and the curve BVH steps.
-__device__ __forceinline__ void enter_near_first(Traversal& T, float (&key)[4], uint32_t (&ref)[4], TravStack& stk,
-                                                 uint32_t* err) {
+__device__ __forceinline__ void enter_near_first(Traversal& T, float (&key)[4], uint32_t (&ref)[4], uint32_t* stack,
+                                                 float* stackT, uint32_t* err) {
     const int n = int(key[0] < INFINITY) + int(key[1] < INFINITY) + int(key[2] < INFINITY) + int(key[3] < INFINITY);
     if (n == 0) {
-        if (!trav_pop(T, stk)) T.exhausted = true;
+        if (!trav_pop(T, stack, stackT)) T.exhausted = true;
         return;
     }
     if (n == 1) {  // one child entered: it becomes the current node
@@ -277,7 +235,8 @@ __device__ __forceinline__ void enter_near_first(Traversal& T, float (&key)[4], 
             return;
         }
         cswap(ka, ra, kb, rb);
-        stk.put(T.sp, rb, kb);
+        stack[T.sp] = rb;
+        stackT[T.sp] = kb;
         ++T.sp;
         T.cur = ra;
         return;
@@ -296,7 +255,8 @@ __device__ __forceinline__ void enter_near_first(Traversal& T, float (&key)[4], 
 #pragma unroll
     for (int k = 3; k >= 1; --k) {
         if (k < n) {
-            stk.put(T.sp, ref[k], key[k]);
+            stack[T.sp] = ref[k];
+            stackT[T.sp] = key[k];
             ++T.sp;
         }
     }
@@ -304,7 +264,7 @@ __device__ __forceinline__ void enter_near_first(Traversal& T, float (&key)[4], 
 }
 
 template <bool kAny, bool kCount>
-__device__ __forceinline__ void trav_interior(Traversal& T, const DevScene& S, TravStack& stk,
+__device__ __forceinline__ void trav_interior(Traversal& T, const DevScene& S, uint32_t* stack, float* stackT,
                                               uint32_t* err, Counters* cnt) {
     const float4* np = reinterpret_cast<const float4*>(S.tri_nodes + T.cur);
     const float4 lx = ldg4(np), hx = ldg4(np + 1), ly = ldg4(np + 2), hy = ldg4(np + 3), lz = ldg4(np + 4),
@@ -327,7 +287,7 @@ __device__ __forceinline__ void trav_interior(Traversal& T, const DevScene& S, T
     if constexpr (kAny) {  // any hit: children entered in stored order, no distance sort
         const int n = int(key[0] < INFINITY) + int(key[1] < INFINITY) + int(key[2] < INFINITY) + int(key[3] < INFINITY);
         if (n == 0) {
-            if (!trav_pop<kAny>(T, stk)) T.exhausted = true;
+            if (!trav_pop<kAny>(T, stack, stackT)) T.exhausted = true;
             return;
         }
         if (T.sp + n - 1 > int(kMaxStack4)) {
@@ -339,14 +299,14 @@ __device__ __forceinline__ void trav_interior(Traversal& T, const DevScene& S, T
 #pragma unroll
         for (int k = 3; k >= 0; --k) {
             if (key[k] < INFINITY) {
-                if (first != kEmptyChild) stk.put_node(T.sp++, first);
+                if (first != kEmptyChild) stack[T.sp++] = first;
                 first = ref[k];
             }
         }
         T.cur = first;
         return;
     }
-    enter_near_first(T, key, ref, stk, err);
+    enter_near_first(T, key, ref, stack, stackT, err);
 }
 
 // BVHBackend::makeObjectSpaceRay4: the world ray (origin, exact direction)
@@ -404,12 +364,13 @@ __device__ __forceinline__ bool leaf_test(Traversal& T, const DevScene& S, uint3
 
 // Leaf step of the one-thread-per-ray schedule: test the current leaf, then pop.
 template <bool kAny, bool kCount>
-__device__ __forceinline__ void trav_leaf(Traversal& T, const DevScene& S, const TravStack& stk, Counters* cnt) {
+__device__ __forceinline__ void trav_leaf(Traversal& T, const DevScene& S, const uint32_t* stack,
+                                          const float* stackT, Counters* cnt) {
     if (leaf_test<kAny, kCount>(T, S, T.cur, cnt)) {
         T.exhausted = true;
         return;
     }
-    if (!trav_pop<kAny>(T, stk)) T.exhausted = true;
+    if (!trav_pop<kAny>(T, stack, stackT)) T.exhausted = true;
 }
 
 // ===========================================================================
@@ -628,7 +589,7 @@ __device__ __forceinline__ void curve_begin(Traversal& T, float3 d, uint32_t seg
 // first for closest and any hit alike (on the hair frame near-first any-hit
 // steps measured faster than the stored order).
 template <bool kCount>
-__device__ __forceinline__ void curve_interior(Traversal& T, const DevScene& S, TravStack& stk,
+__device__ __forceinline__ void curve_interior(Traversal& T, const DevScene& S, uint32_t* stack, float* stackT,
                                                uint32_t* err, Counters* cnt) {
     const Ray ray{T.r.o, T.cd, T.r.tmin, T.r.tmax};
     const float4* np = reinterpret_cast<const float4*>(S.seg_nodes + T.cur);
@@ -647,7 +608,7 @@ __device__ __forceinline__ void curve_interior(Traversal& T, const DevScene& S, 
                        curve_box_hit(ray, T.cinv, l0[k], h0[k], l1[k], h1[k], l2[k], h2[k], T.closest, tn);
         key[k] = h ? tn : INFINITY;
     }
-    enter_near_first(T, key, ref, stk, err);
+    enter_near_first(T, key, ref, stack, stackT, err);
 }
 
 // Ribbon tests of one curve leaf; true when an any-hit query found its blocker.
@@ -674,10 +635,10 @@ __device__ __forceinline__ bool curve_leaf_test(Traversal& T, const DevScene& S,
 
 // Stage dispatch of the node and leaf steps.
 template <bool kAny, bool kCount, bool kCurves>
-__device__ __forceinline__ void node_step(Traversal& T, const DevScene& S, TravStack& stk,
+__device__ __forceinline__ void node_step(Traversal& T, const DevScene& S, uint32_t* stack, float* stackT,
                                           uint32_t* err, Counters* cnt) {
-    if (kCurves && T.stage) curve_interior<kCount>(T, S, stk, err, cnt);
-    else trav_interior<kAny, kCount>(T, S, stk, err, cnt);
+    if (kCurves && T.stage) curve_interior<kCount>(T, S, stack, stackT, err, cnt);
+    else trav_interior<kAny, kCount>(T, S, stack, stackT, err, cnt);
 }
 template <bool kAny, bool kCount, bool kCurves, bool kMotion = false>
 __device__ __forceinline__ bool leaf_step(Traversal& T, const DevScene& S, uint32_t leaf, Counters* cnt) {
@@ -716,7 +677,8 @@ __device__ __forceinline__ void persistent_traverse(const DevScene& S, uint32_t 
                                                     Counters* cnt, Load load, Done done) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t ltmask = (1u << lane) - 1u;
-    ANA_TRAV_STACK(stk);
+    uint32_t stack[kMaxStack4];
+    float stackT[kMaxStack4];
     Traversal T;
     bool active = false, drained = false;
     uint32_t idx = 0, parked = kEmptyChild;
@@ -746,7 +708,7 @@ __device__ __forceinline__ void persistent_traverse(const DevScene& S, uint32_t 
         while (true) {
             if (kAny && active && !T.exhausted && (T.cur & 0x80000000u) && parked == kEmptyChild) {
                 parked = T.cur;
-                if (!trav_pop<kAny>(T, stk)) T.exhausted = true;
+                if (!trav_pop<kAny>(T, stack, stackT)) T.exhausted = true;
             }
             const bool want = active && !T.exhausted && !(T.cur & 0x80000000u);
             const bool ready = !active || T.exhausted || (kAny ? parked != kEmptyChild : bool(T.cur & 0x80000000u));
@@ -762,7 +724,7 @@ __device__ __forceinline__ void persistent_traverse(const DevScene& S, uint32_t 
                 __any_sync(0xFFFFFFFFu, active && !T.exhausted &&
                                             (kAny ? parked != kEmptyChild : bool(T.cur & 0x80000000u))))
                 break;
-            if (want) node_step<kAny, kCount, kCurves>(T, S, stk, err, cnt);
+            if (want) node_step<kAny, kCount, kCurves>(T, S, stack, stackT, err, cnt);
         }
         // 3. leaf phase: one leaf per lane
         if (active) {
@@ -771,7 +733,7 @@ __device__ __forceinline__ void persistent_traverse(const DevScene& S, uint32_t 
                 parked = kEmptyChild;
             } else if (!T.exhausted && (T.cur & 0x80000000u)) {
                 if (leaf_step<kAny, kCount, kCurves, kMotion>(T, S, T.cur, cnt)) T.exhausted = true;
-                else if (!trav_pop<kAny>(T, stk)) T.exhausted = true;
+                else if (!trav_pop<kAny>(T, stack, stackT)) T.exhausted = true;
             }
         }
         if (active && T.exhausted && parked == kEmptyChild) {
