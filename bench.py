@@ -76,6 +76,8 @@ def parse():
                     help="maximum curve segments per BVH leaf (0: the reference's 4)")
     ap.add_argument("--traversal", type=int, default=0,
                     help="0 library default, 1 persistent warps, 2 one thread per ray")
+    ap.add_argument("--hair-mode", type=int, default=0, choices=[0, 1],
+                    help="hair scene: 0 Kajiya-Kay (as the reference executes it), 1 Marschner lobes")
     ap.add_argument("--scene", default="throughput", choices=["throughput", "glass", "motion", "hair"],
                     help="the frame to time (profiling of the other scenes; the bench line's workload is "
                          "the throughput scene)")
@@ -91,7 +93,7 @@ def make_scene(a):
     if a.scene == "motion":
         return S.motion(a.width, a.height, a.spp, a.depth)
     if a.scene == "hair":
-        return S.hair(a.width, a.height, a.spp, a.depth)
+        return S.hair(a.width, a.height, a.spp, a.depth, hair_mode=a.hair_mode)
     return S.throughput(a.width, a.height, a.spp, a.depth, n_spheres=a.n_spheres)
 
 
