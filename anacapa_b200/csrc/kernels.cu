@@ -260,8 +260,7 @@ __device__ __forceinline__ void run_traversal(const DevScene& S, uint32_t n, uin
     if constexpr (kPersist) {
         persistent_traverse<kAny, kCount, kCurves, kMotion>(S, n, fetch, err, cnt, load, done);
     } else {
-        uint32_t stack[kMaxStack4];
-        float stackT[kMaxStack4];
+        uint2 stack[kMaxStack4];
         for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
             Ray ray;
             uint32_t root, segRoot;
@@ -272,10 +271,10 @@ __device__ __forceinline__ void run_traversal(const DevScene& S, uint32_t n, uin
                 while (true) {
                     while (!T.exhausted) {
                         if (!(T.cur & 0x80000000u)) {
-                            node_step<kAny, kCount, kCurves>(T, S, stack, stackT, err, cnt);
+                            node_step<kAny, kCount, kCurves>(T, S, stack, err, cnt);
                         } else if (leaf_step<kAny, kCount, kCurves, kMotion>(T, S, T.cur, cnt)) {
                             T.exhausted = true;
-                        } else if (!trav_pop<kAny>(T, stack, stackT)) {
+                        } else if (!trav_pop<kAny>(T, stack)) {
                             T.exhausted = true;
                         }
                     }

@@ -164,17 +164,22 @@ __device__ __forceinline__ void trav_init(Traversal& T, const Ray& ray, uint32_t
     T.seg = -1;
 }
 
+// Traversal stack entry (thread-local memory): x = node or leaf entry, y = the
+// entry distance's bits (closest hit; any hit writes x only). One 64-bit
+// access per push and pop instead of two 32-bit ones: the throughput frame's
+// extend stage 116.4 -> 115.7 ms, the 1920x1080x64 hair frame 4549 -> 4505 ms.
 template <bool kAny = false>
-__device__ __forceinline__ bool trav_pop(Traversal& T, const uint32_t* stack, const float* stackT) {
+__device__ __forceinline__ bool trav_pop(Traversal& T, const uint2* stack) {
     if (kAny) {  // an any-hit query ends at its first hit: nothing on the stack is culled
         if (T.sp == 0) return false;
-        T.cur = stack[--T.sp];
+        T.cur = stack[--T.sp].x;
         return true;
     }
     while (T.sp > 0) {
         --T.sp;
-        if (stackT[T.sp] > T.closest) continue;
-        T.cur = stack[T.sp];
+        const uint2 e = stack[T.sp];
+        if (__uint_as_float(e.y) > T.closest) continue;
+        T.cur = e.x;
         return true;
     }
     return false;
@@ -211,11 +216,10 @@ __device__ __forceinline__ void cswap(float& ka, uint32_t& va, float& kb, uint32
 // steps of incoherent rays) skip the network with the same result (extend
 // stage of the throughput frame: 146.6 -> 141.9 ms). Shared by the triangle
 // and the curve BVH steps.
-__device__ __forceinline__ void enter_near_first(Traversal& T, float (&key)[4], uint32_t (&ref)[4], uint32_t* stack,
-                                                 float* stackT, uint32_t* err) {
+__device__ __forceinline__ void enter_near_first(Traversal& T, float (&key)[4], uint32_t (&ref)[4], uint2* stack, uint32_t* err) {
     const int n = int(key[0] < INFINITY) + int(key[1] < INFINITY) + int(key[2] < INFINITY) + int(key[3] < INFINITY);
     if (n == 0) {
-        if (!trav_pop(T, stack, stackT)) T.exhausted = true;
+        if (!trav_pop(T, stack)) T.exhausted = true;
         return;
     }
     if (n == 1) {  // one child entered: it becomes the current node
@@ -235,8 +239,7 @@ __device__ __forceinline__ void enter_near_first(Traversal& T, float (&key)[4], 
             return;
         }
         cswap(ka, ra, kb, rb);
-        stack[T.sp] = rb;
-        stackT[T.sp] = kb;
+        stack[T.sp] = make_uint2(rb, __float_as_uint(kb));
         ++T.sp;
         T.cur = ra;
         return;
@@ -255,8 +258,7 @@ __device__ __forceinline__ void enter_near_first(Traversal& T, float (&key)[4], 
 #pragma unroll
     for (int k = 3; k >= 1; --k) {
         if (k < n) {
-            stack[T.sp] = ref[k];
-            stackT[T.sp] = key[k];
+            stack[T.sp] = make_uint2(ref[k], __float_as_uint(key[k]));
             ++T.sp;
         }
     }
@@ -264,7 +266,7 @@ __device__ __forceinline__ void enter_near_first(Traversal& T, float (&key)[4], 
 }
 
 template <bool kAny, bool kCount>
-__device__ __forceinline__ void trav_interior(Traversal& T, const DevScene& S, uint32_t* stack, float* stackT,
+__device__ __forceinline__ void trav_interior(Traversal& T, const DevScene& S, uint2* stack,
                                               uint32_t* err, Counters* cnt) {
     const float4* np = reinterpret_cast<const float4*>(S.tri_nodes + T.cur);
     const float4 lx = ldg4(np), hx = ldg4(np + 1), ly = ldg4(np + 2), hy = ldg4(np + 3), lz = ldg4(np + 4),
@@ -287,7 +289,7 @@ __device__ __forceinline__ void trav_interior(Traversal& T, const DevScene& S, u
     if constexpr (kAny) {  // any hit: children entered in stored order, no distance sort
         const int n = int(key[0] < INFINITY) + int(key[1] < INFINITY) + int(key[2] < INFINITY) + int(key[3] < INFINITY);
         if (n == 0) {
-            if (!trav_pop<kAny>(T, stack, stackT)) T.exhausted = true;
+            if (!trav_pop<kAny>(T, stack)) T.exhausted = true;
             return;
         }
         if (T.sp + n - 1 > int(kMaxStack4)) {
@@ -299,14 +301,14 @@ __device__ __forceinline__ void trav_interior(Traversal& T, const DevScene& S, u
 #pragma unroll
         for (int k = 3; k >= 0; --k) {
             if (key[k] < INFINITY) {
-                if (first != kEmptyChild) stack[T.sp++] = first;
+                if (first != kEmptyChild) stack[T.sp++].x = first;
                 first = ref[k];
             }
         }
         T.cur = first;
         return;
     }
-    enter_near_first(T, key, ref, stack, stackT, err);
+    enter_near_first(T, key, ref, stack, err);
 }
 
 // BVHBackend::makeObjectSpaceRay4: the world ray (origin, exact direction)
@@ -364,13 +366,12 @@ __device__ __forceinline__ bool leaf_test(Traversal& T, const DevScene& S, uint3
 
 // Leaf step of the one-thread-per-ray schedule: test the current leaf, then pop.
 template <bool kAny, bool kCount>
-__device__ __forceinline__ void trav_leaf(Traversal& T, const DevScene& S, const uint32_t* stack,
-                                          const float* stackT, Counters* cnt) {
+__device__ __forceinline__ void trav_leaf(Traversal& T, const DevScene& S, const uint2* stack, Counters* cnt) {
     if (leaf_test<kAny, kCount>(T, S, T.cur, cnt)) {
         T.exhausted = true;
         return;
     }
-    if (!trav_pop<kAny>(T, stack, stackT)) T.exhausted = true;
+    if (!trav_pop<kAny>(T, stack)) T.exhausted = true;
 }
 
 // ===========================================================================
@@ -589,7 +590,7 @@ __device__ __forceinline__ void curve_begin(Traversal& T, float3 d, uint32_t seg
 // first for closest and any hit alike (on the hair frame near-first any-hit
 // steps measured faster than the stored order).
 template <bool kCount>
-__device__ __forceinline__ void curve_interior(Traversal& T, const DevScene& S, uint32_t* stack, float* stackT,
+__device__ __forceinline__ void curve_interior(Traversal& T, const DevScene& S, uint2* stack,
                                                uint32_t* err, Counters* cnt) {
     const Ray ray{T.r.o, T.cd, T.r.tmin, T.r.tmax};
     const float4* np = reinterpret_cast<const float4*>(S.seg_nodes + T.cur);
@@ -608,7 +609,7 @@ __device__ __forceinline__ void curve_interior(Traversal& T, const DevScene& S, 
                        curve_box_hit(ray, T.cinv, l0[k], h0[k], l1[k], h1[k], l2[k], h2[k], T.closest, tn);
         key[k] = h ? tn : INFINITY;
     }
-    enter_near_first(T, key, ref, stack, stackT, err);
+    enter_near_first(T, key, ref, stack, err);
 }
 
 // Ribbon tests of one curve leaf; true when an any-hit query found its blocker.
@@ -635,10 +636,10 @@ __device__ __forceinline__ bool curve_leaf_test(Traversal& T, const DevScene& S,
 
 // Stage dispatch of the node and leaf steps.
 template <bool kAny, bool kCount, bool kCurves>
-__device__ __forceinline__ void node_step(Traversal& T, const DevScene& S, uint32_t* stack, float* stackT,
+__device__ __forceinline__ void node_step(Traversal& T, const DevScene& S, uint2* stack,
                                           uint32_t* err, Counters* cnt) {
-    if (kCurves && T.stage) curve_interior<kCount>(T, S, stack, stackT, err, cnt);
-    else trav_interior<kAny, kCount>(T, S, stack, stackT, err, cnt);
+    if (kCurves && T.stage) curve_interior<kCount>(T, S, stack, err, cnt);
+    else trav_interior<kAny, kCount>(T, S, stack, err, cnt);
 }
 template <bool kAny, bool kCount, bool kCurves, bool kMotion = false>
 __device__ __forceinline__ bool leaf_step(Traversal& T, const DevScene& S, uint32_t leaf, Counters* cnt) {
@@ -677,8 +678,7 @@ __device__ __forceinline__ void persistent_traverse(const DevScene& S, uint32_t 
                                                     Counters* cnt, Load load, Done done) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t ltmask = (1u << lane) - 1u;
-    uint32_t stack[kMaxStack4];
-    float stackT[kMaxStack4];
+    uint2 stack[kMaxStack4];
     Traversal T;
     bool active = false, drained = false;
     uint32_t idx = 0, parked = kEmptyChild;
@@ -708,7 +708,7 @@ __device__ __forceinline__ void persistent_traverse(const DevScene& S, uint32_t 
         while (true) {
             if (kAny && active && !T.exhausted && (T.cur & 0x80000000u) && parked == kEmptyChild) {
                 parked = T.cur;
-                if (!trav_pop<kAny>(T, stack, stackT)) T.exhausted = true;
+                if (!trav_pop<kAny>(T, stack)) T.exhausted = true;
             }
             const bool want = active && !T.exhausted && !(T.cur & 0x80000000u);
             const bool ready = !active || T.exhausted || (kAny ? parked != kEmptyChild : bool(T.cur & 0x80000000u));
@@ -724,7 +724,7 @@ __device__ __forceinline__ void persistent_traverse(const DevScene& S, uint32_t 
                 __any_sync(0xFFFFFFFFu, active && !T.exhausted &&
                                             (kAny ? parked != kEmptyChild : bool(T.cur & 0x80000000u))))
                 break;
-            if (want) node_step<kAny, kCount, kCurves>(T, S, stack, stackT, err, cnt);
+            if (want) node_step<kAny, kCount, kCurves>(T, S, stack, err, cnt);
         }
         // 3. leaf phase: one leaf per lane
         if (active) {
@@ -733,7 +733,7 @@ __device__ __forceinline__ void persistent_traverse(const DevScene& S, uint32_t 
                 parked = kEmptyChild;
             } else if (!T.exhausted && (T.cur & 0x80000000u)) {
                 if (leaf_step<kAny, kCount, kCurves, kMotion>(T, S, T.cur, cnt)) T.exhausted = true;
-                else if (!trav_pop<kAny>(T, stack, stackT)) T.exhausted = true;
+                else if (!trav_pop<kAny>(T, stack)) T.exhausted = true;
             }
         }
         if (active && T.exhausted && parked == kEmptyChild) {
