@@ -97,8 +97,9 @@ struct Counters {
 // ---------------------------------------------------------------------------
 // Persistent-warp triangle traversal. Each lane owns one ray at a time; a
 // warp loops over
-//   1. refill: lanes without a ray take the next queue entries (one
-//      warp-aggregated atomicAdd on the stage's fetch counter);
+//   1. refill: once enough lanes are without a ray (kRefill*), they take the
+//      next queue entries together (one warp-aggregated atomicAdd on the
+//      stage's fetch counter);
 //   2. interior phase: lanes descend interior nodes until they reach a
 //      leaf; the phase ends when every lane has a leaf to test (or nothing
 //      left), when no lane can take another interior step, or when at most
@@ -127,6 +128,23 @@ struct Counters {
 // 28.6 ms at 8 / 16 lanes). Hits and occlusion answers are unchanged.
 constexpr uint32_t kLeafPhaseLanes = 8;      // closest hit
 constexpr uint32_t kLeafPhaseLanesAny = 16;  // any hit (parked leaves)
+
+// Refill thresholds: idle lanes take new rays only once at least this many
+// lanes of the warp are idle (or the queue is drained and every lane is).
+// Queue entries in path order are the samples of one pixel, so lanes that
+// start together trace neighbouring rays and stay converged, where one lane
+// refilled at a time starts at the root beside lanes deep in the tree. On the
+// 1920x1080x64 throughput frame (closest hit / any hit thresholds): extend
+// 115.7 ms at 1, 114.6 at 4, 111.0 at 8, 108.8 at 12, 108.3 at 14, 107.7 at
+// 16, 108.2 at 18, 108.4 at 20, 112.4 at 24, 122.5 at 28, 140.5 at 32; shadow +
+// MIS 128.3 ms at 1, 127.3 at 8, 126.8 at 12, 127.2 at 16, 134.6 at 20. The
+// curve kernels' ribbon walks diverge anyway: the 1280x720x32 hair frame's
+// extend stage 647.5 -> 642.7 ms at 8, its shadow stage slower at 8 (376.8 ->
+// 384.0 ms), so curve any-hit refills one lane at a time.
+constexpr int kRefillLanes = 16;
+constexpr int kRefillLanesAny = 12;
+constexpr int kRefillLanesCurves = 8;
+constexpr int kRefillLanesCurvesAny = 1;
 
 struct Traversal {
     TriRay r;
@@ -686,7 +704,9 @@ __device__ __forceinline__ void persistent_traverse(const DevScene& S, uint32_t 
         // 1. refill idle lanes
         if (!drained) {
             uint32_t need = __ballot_sync(0xFFFFFFFFu, !active);
-            if (need) {
+            constexpr int kRefill = kCurves ? (kAny ? kRefillLanesCurvesAny : kRefillLanesCurves)
+                                            : (kAny ? kRefillLanesAny : kRefillLanes);
+            if (__popc(need) >= kRefill) {
                 uint32_t leader = __ffs(need) - 1u, base = 0;
                 if (lane == leader) base = atomicAdd(fetch, __popc(need));
                 base = __shfl_sync(0xFFFFFFFFu, base, leader);
