@@ -542,10 +542,12 @@ __global__ void __launch_bounds__(kShadeBlock, (!kAdj && !kFiber) ? (kFeat == kF
                                 vEmit[2] = ge.z;
                             }
                         }
+                        DevLight L;
+                        bool misPending = false;
                         if (!m.is_delta && nL > 0) {
                             float ul = ss.next();
                             uint32_t lidx = min(uint32_t(ul * float(nL)), nL - 1u);
-                            const DevLight L = S.lights[R.light_base + lidx];
+                            L = S.lights[R.light_base + lidx];
                             // light sampling
                             float lu0 = ss.next(), lu1 = ss.next();
                             LightSample ls = light_sample<kFeat>(S, L, si.p, lu0, lu1);
@@ -586,16 +588,23 @@ __global__ void __launch_bounds__(kShadeBlock, (!kAdj && !kFiber) ? (kFeat == kF
                             }
                             // BSDF sampling toward the light: non-delta lights only,
                             // and only then are its sample dimensions drawn
-                            // (estimateDirect, PathIntegrator.cpp:210)
-                            const bool deltaLight = (kFeat & kFeatDir) != 0 && L.type == ANA_LIGHT_DIRECTIONAL;
-                            float uc = 0.f, bu0 = 0.f, bu1 = 0.f;
-                            if (!deltaLight) {
-                                uc = ss.next();
-                                bu0 = ss.next();
-                                bu1 = ss.next();
-                            }
-                            BsdfSample bs = deltaLight ? no_sample() : mat_sample<kFiber, kExtra, kFeat>(m, c, wo, bu0, bu1, uc);
-                            if (bs.valid()) {
+                            // (estimateDirect, PathIntegrator.cpp:210); the sample is
+                            // taken in the loop below
+                            misPending = !((kFeat & kFeatDir) != 0 && L.type == ANA_LIGHT_DIRECTIONAL);
+                        }
+                        // BSDF samples: the one toward the light for MIS (k = 0, when
+                        // drawn), then the continuation (k = 1), each drawing (uc, u0,
+                        // u1) in that order. One copy of the sampling code in a loop
+                        // instead of two inlined ones: the throughput frame's shade
+                        // stage 76.2 -> 68.9 ms (smaller code, fewer instruction-fetch
+                        // stalls; outlining mat_sample as a call measured 89.6 ms)
+#pragma unroll 1
+                        for (int k = misPending ? 0 : 1; k < 2; ++k) {
+                            const float uc = ss.next();
+                            const float u0 = ss.next(), u1 = ss.next();
+                            BsdfSample bs = mat_sample<kFiber, kExtra, kFeat>(m, c, wo, u0, u1, uc);
+                            if (!bs.valid()) continue;
+                            if (k == 0) {
                                 float lp = light_pdf<kFeat>(S, L, si.p, bs.wi);
                                 if (lp > 0.f) {
                                     float w = bs.delta() ? 1.f : power_heuristic(bs.pdf, lp);
@@ -615,13 +624,8 @@ __global__ void __launch_bounds__(kShadeBlock, (!kAdj && !kFiber) ? (kFeat == kF
                                         mG1 = pack(db * g.dfdr, 0.f);
                                     }
                                 }
+                                continue;
                             }
-                        }
-                        // continuation
-                        float uc = ss.next();
-                        float u0 = ss.next(), u1 = ss.next();
-                        BsdfSample bs = mat_sample<kFiber, kExtra, kFeat>(m, c, wo, u0, u1, uc);
-                        if (bs.valid()) {
                             spec = bs.delta();
                             beta = beta * (bs.f / bs.pdf);
                             float3 org = spawn_origin(si.p, si.n, bs.wi);
