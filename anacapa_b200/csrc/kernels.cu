@@ -594,16 +594,19 @@ __global__ void __launch_bounds__(kShadeBlock, (!kAdj && !kFiber) ? (kFeat == kF
                         }
                         // BSDF samples: the one toward the light for MIS (k = 0, when
                         // drawn), then the continuation (k = 1), each drawing (uc, u0,
-                        // u1) in that order. One copy of the sampling code in a loop
+                        // u1) in that order. Kernels with standard_surface or hair code
+                        // run both through one copy of the sampling code in a loop
                         // instead of two inlined ones: the throughput frame's shade
                         // stage 76.2 -> 68.9 ms (smaller code, fewer instruction-fetch
-                        // stalls; outlining mat_sample as a call measured 89.6 ms)
-#pragma unroll 1
-                        for (int k = misPending ? 0 : 1; k < 2; ++k) {
+                        // stalls; outlining mat_sample as a call measured 89.6 ms).
+                        // Lambert's sampling is small, and there the loop cost more
+                        // than it saved (64 Cornell variants 72.2 -> 78.2 ms), so that
+                        // kernel inlines the step twice.
+                        auto bsdf_step = [&](int k) {
                             const float uc = ss.next();
                             const float u0 = ss.next(), u1 = ss.next();
                             BsdfSample bs = mat_sample<kFiber, kExtra, kFeat>(m, c, wo, u0, u1, uc);
-                            if (!bs.valid()) continue;
+                            if (!bs.valid()) return;
                             if (k == 0) {
                                 float lp = light_pdf<kFeat>(S, L, si.p, bs.wi);
                                 if (lp > 0.f) {
@@ -624,7 +627,7 @@ __global__ void __launch_bounds__(kShadeBlock, (!kAdj && !kFiber) ? (kFeat == kF
                                         mG1 = pack(db * g.dfdr, 0.f);
                                     }
                                 }
-                                continue;
+                                return;
                             }
                             spec = bs.delta();
                             beta = beta * (bs.f / bs.pdf);
@@ -655,6 +658,13 @@ __global__ void __launch_bounds__(kShadeBlock, (!kAdj && !kFiber) ? (kFeat == kF
                                     eG1 = pack(lr, 0.f);
                                 }
                             }
+                        };
+                        if constexpr ((kFeat & kFeatStandard) != 0 || kFiber) {
+#pragma unroll 1
+                            for (int k = misPending ? 0 : 1; k < 2; ++k) bsdf_step(k);
+                        } else {
+                            if (misPending) bsdf_step(0);
+                            bsdf_step(1);
                         }
                     }
                 }
