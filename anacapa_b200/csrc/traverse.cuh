@@ -138,13 +138,14 @@ constexpr uint32_t kLeafPhaseLanesAny = 16;  // any hit (parked leaves)
 // 115.7 ms at 1, 114.6 at 4, 111.0 at 8, 108.8 at 12, 108.3 at 14, 107.7 at
 // 16, 108.2 at 18, 108.4 at 20, 112.4 at 24, 122.5 at 28, 140.5 at 32; shadow +
 // MIS 128.3 ms at 1, 127.3 at 8, 126.8 at 12, 127.2 at 16, 134.6 at 20. The
-// curve kernels' ribbon walks diverge anyway: the 1280x720x32 hair frame's
-// extend stage 647.5 -> 642.7 ms at 8, its shadow stage slower at 8 (376.8 ->
-// 384.0 ms), so curve any-hit refills one lane at a time.
+// curve kernels' ribbon walks diverge anyway and want smaller groups: the
+// 1280x720x32 hair frame's extend stage 647.5 -> 642.7 ms at 8 (674.2 with
+// its interior phase at 4 lanes), its shadow stage 376.6 ms at 1, 371.2 at 4,
+// 384.0 at 8.
 constexpr int kRefillLanes = 16;
 constexpr int kRefillLanesAny = 12;
 constexpr int kRefillLanesCurves = 8;
-constexpr int kRefillLanesCurvesAny = 1;
+constexpr int kRefillLanesCurvesAny = 4;
 
 struct Traversal {
     TriRay r;
