@@ -692,7 +692,9 @@ __device__ __forceinline__ bool trace_again(Done& done, uint32_t i, const Traver
 // traversal of entry i (a lane-local call, see trace_again: a lane asked to
 // trace again keeps its entry). With kCurves a lane that finishes the
 // triangle BVH continues with the curve BVH in the same phases.
-template <bool kAny, bool kCount, bool kCurves, bool kMotion, class Load, class Done>
+// kPark: any-hit lanes park the first leaf they reach and keep descending
+// (speculative); false: any-hit lanes test each leaf as they reach it.
+template <bool kAny, bool kCount, bool kCurves, bool kMotion, bool kPark, class Load, class Done>
 __device__ __forceinline__ void persistent_traverse(const DevScene& S, uint32_t n, uint32_t* fetch, uint32_t* err,
                                                     Counters* cnt, Load load, Done done) {
     const uint32_t lane = threadIdx.x & 31u;
@@ -727,12 +729,12 @@ __device__ __forceinline__ void persistent_traverse(const DevScene& S, uint32_t 
         if (!__any_sync(0xFFFFFFFFu, active)) break;
         // 2. interior phase (speculative)
         while (true) {
-            if (kAny && active && !T.exhausted && (T.cur & 0x80000000u) && parked == kEmptyChild) {
+            if (kPark && active && !T.exhausted && (T.cur & 0x80000000u) && parked == kEmptyChild) {
                 parked = T.cur;
                 if (!trav_pop<kAny>(T, stack)) T.exhausted = true;
             }
             const bool want = active && !T.exhausted && !(T.cur & 0x80000000u);
-            const bool ready = !active || T.exhausted || (kAny ? parked != kEmptyChild : bool(T.cur & 0x80000000u));
+            const bool ready = !active || T.exhausted || (kPark ? parked != kEmptyChild : bool(T.cur & 0x80000000u));
             const uint32_t wantMask = __ballot_sync(0xFFFFFFFFu, want);
             if (!wantMask || __all_sync(0xFFFFFFFFu, ready)) break;
             // Once at most kPhaseLanes lanes still descend and another lane
@@ -740,10 +742,10 @@ __device__ __forceinline__ void persistent_traverse(const DevScene& S, uint32_t 
             // leaves are tested (the descending lanes resume in the next
             // interior phase), so few lanes do not hold the warp in the node
             // loop. A lane with a leaf must exist, so every pass makes progress.
-            constexpr uint32_t kPhaseLanes = kMotion ? 0u : (kAny ? kLeafPhaseLanesAny : kLeafPhaseLanes);
+            constexpr uint32_t kPhaseLanes = kMotion ? 0u : (kPark ? kLeafPhaseLanesAny : kLeafPhaseLanes);
             if (kPhaseLanes > 0 && __popc(wantMask) <= kPhaseLanes &&
                 __any_sync(0xFFFFFFFFu, active && !T.exhausted &&
-                                            (kAny ? parked != kEmptyChild : bool(T.cur & 0x80000000u))))
+                                            (kPark ? parked != kEmptyChild : bool(T.cur & 0x80000000u))))
                 break;
             if (want) node_step<kAny, kCount, kCurves>(T, S, stack, err, cnt);
         }
