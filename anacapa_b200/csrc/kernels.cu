@@ -545,6 +545,8 @@ __global__ void __launch_bounds__(kShadeBlock, (!kAdj && !kFiber) ? (kFeat == kF
                         }
                         DevLight L;
                         bool misPending = false;
+                        constexpr bool kShareSampler = (kFeat & kFeatStandard) != 0 || kFiber;
+                        constexpr int kSampleUnroll = kShareSampler ? 1 : 2;
                         if (!m.is_delta && nL > 0) {
                             float ul = ss.next();
                             uint32_t lidx = min(uint32_t(ul * float(nL)), nL - 1u);
@@ -602,12 +604,14 @@ __global__ void __launch_bounds__(kShadeBlock, (!kAdj && !kFiber) ? (kFeat == kF
                         // stalls; outlining mat_sample as a call measured 89.6 ms).
                         // Lambert's sampling is small, and there the loop cost more
                         // than it saved (64 Cornell variants 72.2 -> 78.2 ms), so that
-                        // kernel inlines the step twice.
-                        auto bsdf_step = [&](int k) {
+                        // kernel unrolls the loop into two copies.
+#pragma unroll (kSampleUnroll)
+                        for (int k = kShareSampler ? (misPending ? 0 : 1) : 0; k < 2; ++k) {
+                            if (!kShareSampler && k == 0 && !misPending) continue;
                             const float uc = ss.next();
                             const float u0 = ss.next(), u1 = ss.next();
                             BsdfSample bs = mat_sample<kFiber, kExtra, kFeat>(m, c, wo, u0, u1, uc);
-                            if (!bs.valid()) return;
+                            if (!bs.valid()) continue;
                             if (k == 0) {
                                 float lp = light_pdf<kFeat>(S, L, si.p, bs.wi);
                                 if (lp > 0.f) {
@@ -628,7 +632,7 @@ __global__ void __launch_bounds__(kShadeBlock, (!kAdj && !kFiber) ? (kFeat == kF
                                         mG1 = pack(db * g.dfdr, 0.f);
                                     }
                                 }
-                                return;
+                                continue;
                             }
                             spec = bs.delta();
                             beta = beta * (bs.f / bs.pdf);
@@ -659,13 +663,6 @@ __global__ void __launch_bounds__(kShadeBlock, (!kAdj && !kFiber) ? (kFeat == kF
                                     eG1 = pack(lr, 0.f);
                                 }
                             }
-                        };
-                        if constexpr ((kFeat & kFeatStandard) != 0 || kFiber) {
-#pragma unroll 1
-                            for (int k = misPending ? 0 : 1; k < 2; ++k) bsdf_step(k);
-                        } else {
-                            if (misPending) bsdf_step(0);
-                            bsdf_step(1);
                         }
                     }
                 }
@@ -713,10 +710,14 @@ __global__ void __launch_bounds__(kShadeBlock, (!kAdj && !kFiber) ? (kFeat == kF
 
 // NEE shadow rays: shadowTransmittance (src/integrator/ShadowRay.h:26-61) for
 // opaque scenes — any blocker in [1e-4, tmax] makes the transmittance black.
+// Triangle-only batches test each leaf as they reach it (1920x1080x64
+// throughput frame: shadow stage 53.1 ms parking leaves, 46.3 ms without; the
+// motion frame 45.8 -> 42.1 ms); with curves the lanes park leaves (the hair
+// frame's shadow stage 373.0 against 374.3 ms).
 template <bool kCurves, bool kPersist, bool kAdj, bool kMotion = false>
 __global__ void ANA_TRAVERSAL_BOUNDS k_shadow(const __grid_constant__ Params p) {
     uint32_t* cb = p.counters + p.bounce * kCountersPerBounce;
-    run_traversal<true, false, kPersist, kCurves, kMotion>(
+    run_traversal<true, false, kPersist, kCurves, kMotion, kCurves>(
         p.S, cb[1], cb + 4, p.err, nullptr,
         [&](uint32_t i, Ray& r, uint32_t& root, uint32_t& segRoot) {
             float4 o = p.q.sh_o[i], d = p.q.sh_d[i];
