@@ -121,12 +121,16 @@ struct Counters {
 // Interior phases end once this few lanes still descend (and a lane has a
 // leaf). On the 1920x1080x64 throughput frame the extend stage took 142.0 ms
 // when the phase ran until no lane descended, 118.4 ms at 4 lanes, 117.2 ms at
-// 8 and 124.6 ms at 16; the any-hit shadow + MIS stages 146.5 ms, 137.0 at 4,
-// 132.8 at 8, 128.1 at 16, 129.8 at 24 and 191.2 at 32. Kernels with
+// 8 and 124.6 ms at 16; the any-hit shadow + MIS stages, parking leaves and
+// refilling one lane at a time, 146.5 ms, 137.0 at 4, 132.8 at 8, 128.1 at 16,
+// 129.8 at 24 and 191.2 at 32. Any-hit kernels that test leaves as reached use
+// the closest-hit count (shadow + MIS 107.0 ms at 8, 111.4 at 4, 108.1 at 12,
+// 111.9 at 16); the parked count serves the kernels that still park (curve
+// shadow rays, occlusion queries of ana_trace_batch). Kernels with
 // motion-blurred meshes, whose leaf tests invert interpolated matrices, keep
 // the phase until no lane descends (1280x720x16 motion frame: 25.9 ms against
 // 28.6 ms at 8 / 16 lanes). Hits and occlusion answers are unchanged.
-constexpr uint32_t kLeafPhaseLanes = 8;      // closest hit
+constexpr uint32_t kLeafPhaseLanes = 8;      // closest hit, any hit without parking
 constexpr uint32_t kLeafPhaseLanesAny = 16;  // any hit (parked leaves)
 
 // Refill thresholds: idle lanes take new rays only once at least this many
