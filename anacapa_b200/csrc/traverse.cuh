@@ -105,13 +105,15 @@ struct Counters {
 //      left), when no lane can take another interior step, or when at most
 //      kLeafPhaseLanes (any hit: kLeafPhaseLanesAny) lanes still descend
 //      while others wait with a leaf, so lanes stay converged on the
-//      node-test code. Any-hit queries are speculative
-//      (Aila and Laine, "Understanding the efficiency of ray traversal on
-//      GPUs", 2009): a lane that reaches a leaf parks it and keeps descending
-//      from its next stack entry. Closest-hit queries do not speculate: a
-//      leaf tested early shortens the ray and culls later nodes (measured on
-//      the throughput frame: speculation cost closest hit 3 %, saved any hit
-//      8-12 %);
+//      node-test code. Any-hit queries can be speculative (kPark; Aila and
+//      Laine, "Understanding the efficiency of ray traversal on GPUs", 2009):
+//      a lane that reaches a leaf parks it and keeps descending from its next
+//      stack entry. Closest-hit queries do not speculate: a leaf tested early
+//      shortens the ray and culls later nodes (measured on the throughput
+//      frame: speculation cost closest hit 3 %, saved any hit 8-12 % with
+//      one-lane refills; with grouped refills it costs the triangle shadow
+//      and MIS kernels too, and only the curve shadow kernels and the
+//      occlusion queries of ana_trace_batch park);
 //   3. leaf phase: the parked leaf's (else the current leaf's) triangles.
 // A lane whose stack is exhausted (or, for occlusion, that found a blocker)
 // reports its ray and picks up a new one at the next refill, so finished rays
