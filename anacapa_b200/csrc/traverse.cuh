@@ -145,12 +145,12 @@ constexpr uint32_t kLeafPhaseLanesAny = 16;  // any hit (parked leaves)
 // 16, 108.2 at 18, 108.4 at 20, 112.4 at 24, 122.5 at 28, 140.5 at 32; shadow +
 // MIS 128.3 ms at 1, 127.3 at 8, 126.8 at 12, 127.2 at 16, 134.6 at 20. The
 // curve kernels' ribbon walks diverge anyway and want smaller groups: the
-// 1280x720x32 hair frame's extend stage 647.5 -> 642.7 ms at 8 (674.2 with
-// its interior phase at 4 lanes), its shadow stage 376.6 ms at 1, 371.2 at 4,
-// 384.0 at 8.
+// 1280x720x32 hair frame's extend stage 647.5 ms at 1, 634.2 at 4, 636.7 at 6,
+// 642.9 at 8, 649.3 at 10, 657.7 at 12; its shadow stage 376.6 ms at 1, 370.4
+// at 2, 369.6 at 3, 371.0 at 4, 376.4 at 6, 384.0 at 8.
 constexpr int kRefillLanes = 16;
 constexpr int kRefillLanesAny = 12;
-constexpr int kRefillLanesCurves = 8;
+constexpr int kRefillLanesCurves = 4;
 constexpr int kRefillLanesCurvesAny = 4;
 
 struct Traversal {
